@@ -1,0 +1,62 @@
+// Diagonal (local) observables: out[s] += sum_r |psi_r|^2 * diag[s][c_s(r)] for
+// every site s at once.  This is LocalTerm.get_expval in a symmetry sector
+// (edlgt/modeling/local_term.py:119-237 with exp_val_data,
+// edlgt/modeling/qmb_state.py:631-654): local terms only keep the operator
+// diagonal, so an expectation value is a weighted reduction over the basis.
+#include "internal.cuh"
+
+namespace {
+
+constexpr int kThreads = 256;
+
+__global__ void __launch_bounds__(kThreads) local_expval_k(const uint64_t* __restrict__ keys, int64_t n, int n_sites,
+                                                           edg_site_dims dims, const double* __restrict__ psi,
+                                                           int psi_complex, int64_t psi_stride,
+                                                           const double* __restrict__ diag, int dmax,
+                                                           double* __restrict__ out) {
+  __shared__ double acc[EDG_MAX_SITES];
+  for (int s = threadIdx.x; s < n_sites; s += kThreads) acc[s] = 0.0;
+  __syncthreads();
+  double loc[EDG_MAX_SITES];
+  for (int s = 0; s < n_sites; ++s) loc[s] = 0.0;
+  for (int64_t r = blockIdx.x * (int64_t)kThreads + threadIdx.x; r < n; r += (int64_t)gridDim.x * kThreads) {
+    double p2;
+    if (psi_complex) {
+      double a = psi[2 * r * psi_stride], b = psi[2 * r * psi_stride + 1];
+      p2 = a * a + b * b;
+    } else {
+      double a = psi[r * psi_stride];
+      p2 = a * a;
+    }
+    uint64_t k = keys[r];
+    for (int s = n_sites - 1; s >= 0; --s) {
+      uint64_t d = (uint64_t)dims.d[s];
+      int c = (int)(k % d);
+      k /= d;
+      loc[s] = fma(p2, diag[s * dmax + c], loc[s]);
+    }
+  }
+  for (int s = 0; s < n_sites; ++s) {
+    double v = loc[s];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(&acc[s], v);
+  }
+  __syncthreads();
+  for (int s = threadIdx.x; s < n_sites; s += kThreads) atomicAdd(out + s, acc[s]);
+}
+
+}  // namespace
+
+extern "C" int edg_local_expval(const uint64_t* keys, int64_t n, const edg_site_dims* dims, int32_t n_sites,
+                                const double* psi, int32_t psi_complex, int64_t psi_stride, const double* diag,
+                                int32_t dmax, double* out, cudaStream_t stream) {
+  EDG_REQUIRE(dims != nullptr && n >= 0 && n_sites > 0 && n_sites <= EDG_MAX_SITES && dmax > 0 && psi_stride >= 1,
+              "edg_local_expval: bad arguments");
+  cudaError_t e = cudaMemsetAsync(out, 0, sizeof(double) * n_sites, stream);
+  if (e != cudaSuccess) return edg::cuda_status(e, "edg_local_expval: reset");
+  if (n == 0) return EDG_OK;
+  local_expval_k<<<edg::grid_for(n, kThreads, 4), kThreads, 0, stream>>>(keys, n, n_sites, *dims, psi, psi_complex,
+                                                                          psi_stride, diag, dmax, out);
+  EDG_CHECK_LAUNCH("edg_local_expval");
+  return EDG_OK;
+}

@@ -1,0 +1,150 @@
+// CSR + diagonal matvec kernels: y = (A_offdiag + diag) x for nvec right-hand
+// sides stored interleaved ([row][vec]), with a shared off-diagonal matrix.
+// G threads cooperate on one row (G = 4..32, chosen from the mean row
+// length); products are accumulated in double precision.
+#pragma once
+#include "internal.cuh"
+
+namespace edg {
+
+struct cd {  // double complex accumulator
+  double re, im;
+};
+
+// Scalar storage traits: real (double/float) or complex (double2/float2).
+template <typename S>
+struct Store;
+template <>
+struct Store<double> {
+  using acc = double;
+  static constexpr bool cplx = false;
+  __device__ static double ld(const double* p, int64_t i) { return __ldg(p + i); }
+  __device__ static void st(double* p, int64_t i, double v) { p[i] = v; }
+};
+template <>
+struct Store<float> {
+  using acc = double;
+  static constexpr bool cplx = false;
+  __device__ static double ld(const float* p, int64_t i) { return (double)__ldg(p + i); }
+  __device__ static void st(float* p, int64_t i, double v) { p[i] = (float)v; }
+};
+template <>
+struct Store<double2> {
+  using acc = cd;
+  static constexpr bool cplx = true;
+  __device__ static cd ld(const double2* p, int64_t i) {
+    double2 v = __ldg(p + i);
+    return {v.x, v.y};
+  }
+  __device__ static void st(double2* p, int64_t i, cd v) { p[i] = make_double2(v.re, v.im); }
+};
+template <>
+struct Store<float2> {
+  using acc = cd;
+  static constexpr bool cplx = true;
+  __device__ static cd ld(const float2* p, int64_t i) {
+    float2 v = __ldg(p + i);
+    return {(double)v.x, (double)v.y};
+  }
+  __device__ static void st(float2* p, int64_t i, cd v) { p[i] = make_float2((float)v.re, (float)v.im); }
+};
+
+__device__ __forceinline__ void fma_acc(double& a, double v, double x) { a = fma(v, x, a); }
+__device__ __forceinline__ void fma_acc(cd& a, cd v, cd x) {
+  a.re = fma(v.re, x.re, fma(-v.im, x.im, a.re));
+  a.im = fma(v.re, x.im, fma(v.im, x.re, a.im));
+}
+__device__ __forceinline__ void zero_acc(double& a) { a = 0.0; }
+__device__ __forceinline__ void zero_acc(cd& a) { a.re = a.im = 0.0; }
+template <int G>
+__device__ __forceinline__ void group_reduce(double& a) {
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o, G);
+}
+template <int G>
+__device__ __forceinline__ void group_reduce(cd& a) {
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) {
+    a.re += __shfl_xor_sync(0xffffffffu, a.re, o, G);
+    a.im += __shfl_xor_sync(0xffffffffu, a.im, o, G);
+  }
+}
+
+// SV: matrix value/diag storage, SX: x storage, SY: y storage.
+template <typename SV, typename SX, typename SY, int NV, int G>
+__global__ void __launch_bounds__(256) spmv_k(int64_t n, const int64_t* __restrict__ rowptr,
+                                              const int32_t* __restrict__ cols, const SV* __restrict__ vals,
+                                              const SV* __restrict__ diag, const SX* __restrict__ x,
+                                              SY* __restrict__ y) {
+  using A = typename Store<SV>::acc;
+  const int lane = threadIdx.x & (G - 1);
+  const int64_t group = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / G;
+  const int64_t n_groups = ((int64_t)gridDim.x * blockDim.x) / G;
+  // every lane of a warp iterates the same number of times (shuffles need it)
+  const int64_t n_iter = (n + n_groups - 1) / n_groups;
+  for (int64_t it = 0; it < n_iter; ++it) {
+    const int64_t r = group + it * n_groups;
+    A acc[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) zero_acc(acc[v]);
+    if (r < n) {
+      const int64_t beg = __ldg(rowptr + r), end = __ldg(rowptr + r + 1);
+      for (int64_t p = beg + lane; p < end; p += G) {
+        const int64_t c = __ldg(cols + p);
+        const A a = Store<SV>::ld(vals, p);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) fma_acc(acc[v], a, Store<SX>::ld(x, c * NV + v));
+      }
+    }
+#pragma unroll
+    for (int v = 0; v < NV; ++v) group_reduce<G>(acc[v]);
+    if (r < n && lane == 0) {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        fma_acc(acc[v], Store<SV>::ld(diag, r * NV + v), Store<SX>::ld(x, r * NV + v));
+        Store<SY>::st(y, r * NV + v, acc[v]);
+      }
+    }
+  }
+}
+
+// Threads per row from the mean row length.
+inline int spmv_group(int64_t n, int64_t nnz) {
+  double avg = n > 0 ? (double)nnz / (double)n : 0.0;
+  if (avg < 6) return 4;
+  if (avg < 20) return 8;
+  if (avg < 48) return 16;
+  return 32;
+}
+
+template <typename SV, typename SX, typename SY, int NV>
+int launch_spmv_nv(int64_t n, int64_t nnz, const int64_t* rowptr, const int32_t* cols, const SV* vals,
+                   const SV* diag, const SX* x, SY* y, cudaStream_t s) {
+  const int threads = 256;
+  int g = spmv_group(n, nnz);
+  int64_t work = n * g;
+  unsigned grid = grid_for(work, threads, 8);
+  switch (g) {
+    case 4: spmv_k<SV, SX, SY, NV, 4><<<grid, threads, 0, s>>>(n, rowptr, cols, vals, diag, x, y); break;
+    case 8: spmv_k<SV, SX, SY, NV, 8><<<grid, threads, 0, s>>>(n, rowptr, cols, vals, diag, x, y); break;
+    case 16: spmv_k<SV, SX, SY, NV, 16><<<grid, threads, 0, s>>>(n, rowptr, cols, vals, diag, x, y); break;
+    default: spmv_k<SV, SX, SY, NV, 32><<<grid, threads, 0, s>>>(n, rowptr, cols, vals, diag, x, y); break;
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_status(e, "spmv");
+  return EDG_OK;
+}
+
+template <typename SV, typename SX, typename SY>
+int launch_spmv(int nvec, int64_t n, int64_t nnz, const int64_t* rowptr, const int32_t* cols, const SV* vals,
+                const SV* diag, const SX* x, SY* y, cudaStream_t s) {
+  switch (nvec) {
+    case 1: return launch_spmv_nv<SV, SX, SY, 1>(n, nnz, rowptr, cols, vals, diag, x, y, s);
+    case 2: return launch_spmv_nv<SV, SX, SY, 2>(n, nnz, rowptr, cols, vals, diag, x, y, s);
+    case 3: return launch_spmv_nv<SV, SX, SY, 3>(n, nnz, rowptr, cols, vals, diag, x, y, s);
+    case 4: return launch_spmv_nv<SV, SX, SY, 4>(n, nnz, rowptr, cols, vals, diag, x, y, s);
+    default: set_error("spmv: nvec must be 1..4, got %d", nvec); return EDG_ERR_ARG;
+  }
+}
+
+}  // namespace edg

@@ -1,0 +1,198 @@
+"""ctypes binding of libedgpu (the C ABI declared in include/edgpu.h).
+
+The library is the only compute path: loading fails loudly when the shared
+object is missing, and every call's status is turned into an exception.
+Device buffers are torch CUDA tensors passed by ``data_ptr()``.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+from ._build import LIB_PATH
+
+__all__ = ["lib", "check", "EdgError", "MAX_SITES", "MAX_OPS", "SectorTables", "LookupTable", "Assembly",
+           "LanczosProblem", "SiteDims", "EXPORTED_SYMBOLS", "ptr", "stream_handle"]
+
+MAX_SITES = 64
+MAX_OPS = 4
+
+EDG_OK = 0
+STATUS_NAMES = {
+    -1: "EDG_ERR_ARG",
+    -2: "EDG_ERR_CUDA",
+    -3: "EDG_ERR_OVERFLOW",
+    -4: "EDG_ERR_MISSING_KET",
+    -5: "EDG_ERR_NOT_CONVERGED",
+    -6: "EDG_ERR_BREAKDOWN",
+}
+
+
+class EdgError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+P = C.c_void_p
+I32 = C.c_int32
+I64 = C.c_int64
+U64 = C.c_uint64
+F64 = C.c_double
+
+
+class SectorTables(C.Structure):
+    _fields_ = [
+        ("n_sites", I32),
+        ("dmax", I32),
+        ("loc_dims", I32 * MAX_SITES),
+        ("strides", U64 * MAX_SITES),
+        ("site_allowed", P),
+        ("n_glob", I32),
+        ("glob_type", I32),
+        ("glob_val", P),
+        ("glob_target", P),
+        ("glob_rem_min", P),
+        ("glob_rem_max", P),
+        ("n_dirs", I32),
+        ("link_val", P),
+        ("link_target", P),
+        ("pair_start", P),
+        ("pair_s0", P),
+        ("pair_s1", P),
+        ("pair_dir", P),
+        ("nbody_type", I32),
+        ("nb_val", P),
+        ("nb_target", P),
+        ("nb_start", P),
+        ("nb_id", P),
+        ("nb_site_start", P),
+        ("nb_sites", P),
+    ]
+
+
+class LookupTable(C.Structure):
+    _fields_ = [
+        ("keys", P),
+        ("n", I64),
+        ("bucket_start", P),
+        ("shift", I32),
+        ("n_buckets", I64),
+    ]
+
+
+class Assembly(C.Structure):
+    _fields_ = [
+        ("n_sites", I32),
+        ("dmax", I32),
+        ("loc_dims", I32 * MAX_SITES),
+        ("strides", U64 * MAX_SITES),
+        ("sector", LookupTable),
+        ("complex_values", I32),
+        ("t_count", P),
+        ("t_ket", P),
+        ("t_amp", P),
+        ("n_terms", I32),
+        ("term_nops", P),
+        ("term_site", P),
+        ("term_table", P),
+        ("term_coef", P),
+        ("n_dterms", I32),
+        ("dterm_site", P),
+        ("dterm_diag", P),
+        ("dterm_coef", P),
+    ]
+
+
+class SiteDims(C.Structure):
+    _fields_ = [("d", I32 * MAX_SITES)]
+
+
+class LanczosProblem(C.Structure):
+    _fields_ = [
+        ("dtype", I32),
+        ("n_rows", I64),
+        ("nnz", I64),
+        ("rowptr", P),
+        ("cols", P),
+        ("vals", P),
+        ("diag", P),
+        ("nvec", I32),
+        ("k", I32),
+        ("max_iter", I32),
+        ("tol", F64),
+        ("check_every", I32),
+        ("seed", U64),
+        ("v0", P),
+    ]
+
+
+_SIGS = {
+    "edg_get_last_error": (I32, [C.c_char_p, I32]),
+    "edg_version": (I32, []),
+    "edg_scan_scratch_elems": (I64, [I64]),
+    "edg_scan_i64": (I32, [P, P, I64, P, P]),
+    "edg_sector_level_blocks": (I64, [I64]),
+    "edg_sector_level_count": (I32, [C.POINTER(SectorTables), I32, P, P, I64, P, P, P]),
+    "edg_sector_level_fill": (I32, [C.POINTER(SectorTables), I32, P, P, I64, P, P, P, P]),
+    "edg_keys_to_configs": (I32, [P, I64, I32, P, P, P]),
+    "edg_configs_to_keys": (I32, [P, I64, I32, P, P, P]),
+    "edg_lookup_build": (I32, [P, I64, I32, I64, P, P]),
+    "edg_lookup": (I32, [C.POINTER(LookupTable), P, I64, P, P]),
+    "edg_assemble_count": (I32, [C.POINTER(Assembly), P, P]),
+    "edg_assemble_fill": (I32, [C.POINTER(Assembly), P, P, P, P, P, P, P, P]),
+    "edg_assemble_compact": (I32, [I64, I32, P, P, P, P, P, P, P]),
+    "edg_spmv": (I32, [I32, I64, I64, P, P, P, P, I32, P, P, P]),
+    "edg_convert": (I32, [I32, P, I32, P, I64, P]),
+    "edg_lanczos_workspace_bytes": (I64, [C.POINTER(LanczosProblem)]),
+    "edg_lanczos": (I32, [C.POINTER(LanczosProblem), P, I64, P, P, P, P, P]),
+    "edg_tridiag_lowest": (I32, [P, P, I32, I32, P, P, P, P]),
+    "edg_local_expval": (I32, [P, I64, C.POINTER(SiteDims), I32, P, I32, I64, P, I32, P, P]),
+}
+
+EXPORTED_SYMBOLS = tuple(_SIGS)
+
+
+def _load():
+    path = Path(LIB_PATH)
+    if not path.exists():
+        raise ImportError(
+            f"libedgpu.so not found at {path}; build it with `python -m edgpu._build` "
+            "(there is no CPU fallback for the engine)"
+        )
+    handle = C.CDLL(str(path))
+    for name, (res, args) in _SIGS.items():
+        fn = getattr(handle, name)
+        fn.restype = res
+        fn.argtypes = args
+    return handle
+
+
+lib = _load()
+
+
+def last_error() -> str:
+    buf = C.create_string_buffer(512)
+    lib.edg_get_last_error(buf, 512)
+    return buf.value.decode(errors="replace")
+
+
+def check(status: int, what: str = ""):
+    if status != EDG_OK:
+        raise EdgError(status, f"{what}: {last_error()}" if what else last_error())
+    return status
+
+
+def ptr(t) -> int | None:
+    """Device pointer of a torch tensor (None for None)."""
+    if t is None:
+        return None
+    return t.data_ptr()
+
+
+def stream_handle(stream=None) -> int | None:
+    import torch
+
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return s.cuda_stream

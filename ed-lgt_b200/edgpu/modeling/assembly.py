@@ -1,0 +1,315 @@
+"""Device assembly of the sector Hamiltonian from term blocks.
+
+Host side: the term blocks are flattened into local transition tables (the
+nonzero entries, ``|op| > 1e-10``, of every site operator used, as
+``_prepare_local_transition_data`` does, edlgt/symmetries/
+sym_qmb_operations.py:32-92) plus one record per term instance.  The device
+builds the canonical matrix (duplicates summed, columns ascending) in three
+kernels: per-row entry bounds, generation + per-row merge, compaction.
+
+Real form.  The gauge models' hoppings carry factors ``-i t``; a diagonal
+unitary ``D = prod_s phi_s(c_s)`` with ``phi_s(c) = i**(w_s(c))`` (``w`` a
+per-site integer weight, typically x-coordinate times matter number) maps
+``H`` to ``D^dagger H D``, applied here factor by factor to the site
+operators.  When every transformed site table has a single common phase and
+every instance's total phase is real, the matrix is assembled real; otherwise
+the faithful complex matrix is assembled.  Eigenvalues are unchanged and
+eigenvectors map back by ``psi = D psi'``.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from .. import _lib
+from .._lib import check, lib, ptr, stream_handle
+from .terms import TermBlock
+
+__all__ = ["DeviceMatrix", "assemble_blocks", "OP_TOL"]
+
+OP_TOL = 1e-10
+
+
+class DeviceMatrix:
+    """Canonical sector matrix: off-diagonal CSR + dense diagonal, on the device.
+
+    ``vals``/``diag`` are float64 tensors (interleaved re/im when ``is_complex``).
+    ``diag_present`` marks rows whose (r, r) entry exists in the reference's
+    triplet set (a local term with ``|op_cc| >= 1e-10`` or a diagonal hit).
+    ``phase_weights`` (n_sites, dmax) integer exponents of ``i`` of the real
+    form's gauge transform, or None.
+    """
+
+    def __init__(self, n, rowptr, cols, vals, diag, diag_present, is_complex, phase_weights=None):
+        self.n = int(n)
+        self.rowptr = rowptr
+        self.cols = cols
+        self.vals = vals
+        self.diag = diag
+        self.diag_present = diag_present
+        self.is_complex = bool(is_complex)
+        self.phase_weights = phase_weights
+        self.nnz = int(cols.shape[0]) if cols is not None else 0
+
+    @property
+    def shape(self):
+        return (self.n, self.n)
+
+    def dtype_code(self):
+        return 2 if self.is_complex else 0
+
+    def to_scipy(self, include_diag=True):
+        """Host canonical CSR (pattern of the reference after summing duplicates)."""
+        from scipy.sparse import csr_matrix
+
+        rp = self.rowptr.cpu().numpy()
+        cols = self.cols.cpu().numpy()[: self.nnz].astype(np.int64)
+        v = self.vals.cpu().numpy()
+        d = self.diag.cpu().numpy()
+        if self.is_complex:
+            v = v.view(np.complex128)[: self.nnz]
+            d = d.view(np.complex128)
+        else:
+            v = v[: self.nnz]
+        rows = np.repeat(np.arange(self.n), np.diff(rp))
+        if include_diag:
+            pres = self.diag_present.cpu().numpy().astype(bool)
+            r = np.nonzero(pres)[0]
+            rows = np.concatenate([rows, r])
+            cols = np.concatenate([cols, r])
+            v = np.concatenate([v, d[r]])
+            order = np.lexsort((cols, rows))
+            rows, cols, v = rows[order], cols[order], v[order]
+        indptr = np.zeros(self.n + 1, dtype=np.int64)
+        np.add.at(indptr, rows + 1, 1)
+        indptr = np.cumsum(indptr)
+        return csr_matrix((v, cols, indptr), shape=self.shape)
+
+    def matvec(self, x: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
+        """y = H x on the device (x: float64 or complex128 tensor of length n)."""
+        if self.is_complex:
+            x = x.to(torch.complex128)
+            code = 2
+        else:
+            if x.is_complex():
+                raise TypeError("real matrix: use a real vector (or apply to real and imaginary parts)")
+            x = x.to(torch.float64)
+            code = 0
+        y = torch.empty_like(x) if out is None else out
+        check(lib.edg_spmv(code, self.n, self.nnz, ptr(self.rowptr), ptr(self.cols) if self.nnz else None,
+                           ptr(self.vals) if self.nnz else None, ptr(self.diag), 1, ptr(x), ptr(y), stream_handle()),
+              "edg_spmv")
+        return y
+
+
+def _uniform_phase(mat, tol=1e-12):
+    """Common phase e^{i theta} of all entries above OP_TOL, or None."""
+    nz = mat[np.abs(mat) > OP_TOL]
+    if nz.size == 0:
+        return 1.0 + 0.0j
+    ph = nz[np.argmax(np.abs(nz))]
+    ph = ph / abs(ph)
+    rot = nz / ph
+    if np.all(np.abs(rot.imag) <= tol * np.maximum(1.0, np.abs(rot))):
+        return ph
+    return None
+
+
+def _phase_vec(weights_row):
+    return np.power(1j, np.asarray(weights_row, dtype=np.int64) % 4)
+
+
+def assemble_blocks(sector, blocks, phase_weights=None, force_complex=False, extra_diag=None):
+    """Assemble the canonical matrix of ``sum(blocks)`` in ``sector``.
+
+    ``extra_diag``: optional constant added to every diagonal element (identity
+    terms).  Returns a :class:`DeviceMatrix`.
+    """
+    n_sites = sector.n_sites
+    loc_dims = sector.loc_dims
+    dmax = None
+    for b in blocks:
+        dmax = b.ops[0].shape[-1] if dmax is None else dmax
+    if dmax is None:
+        dmax = int(loc_dims.max())
+    dev = sector.device
+
+    # ---- off-diagonal instances: tables and records (complex, untransformed) ----
+    raw_tables = []  # list of (d x d) complex matrices
+    table_site = []
+    table_index = {}
+    terms = []  # (sites tuple, tables tuple, coef)
+    for bi, b in enumerate(blocks):
+        if b.diagonal:
+            continue
+        for dag in ([False, True] if b.add_dagger else [False]):
+            for inst in b.sites:
+                tabs = []
+                for j, s in enumerate(inst):
+                    key = (bi, j, int(s), dag)
+                    if key not in table_index:
+                        m = np.asarray(b.ops[j][int(s)], dtype=np.complex128)
+                        if dag:
+                            m = m.conj().T
+                        table_index[key] = len(raw_tables)
+                        raw_tables.append(m)
+                        table_site.append(int(s))
+                    tabs.append(table_index[key])
+                if len(set(int(s) for s in inst)) != len(inst):
+                    raise ValueError("a term instance acts twice on the same site")
+                coef = np.conj(b.strength) if dag else b.strength
+                terms.append((tuple(int(s) for s in inst), tuple(tabs), complex(coef)))
+    # diagonal terms
+    dterms = []  # (site, diag vector, coef)
+    for b in blocks:
+        if not b.diagonal:
+            continue
+        for inst in b.sites:
+            s = int(inst[0])
+            dterms.append((s, np.diagonal(np.asarray(b.ops[0][s], dtype=np.complex128)).copy(), complex(b.strength)))
+
+    # ---- real form (gauge transform + per-table phase extraction) ----
+    use_real = False
+    tables_real = None
+    coefs_real = None
+    if not force_complex:
+        tabs_t = []
+        ok = True
+        phases = []
+        for t, m in enumerate(raw_tables):
+            if phase_weights is not None:
+                phi = _phase_vec(phase_weights[table_site[t]])
+                m = np.conj(phi)[:, None] * m * phi[None, :]
+            ph = _uniform_phase(m)
+            if ph is None:
+                ok = False
+                break
+            tabs_t.append((m / ph).real)
+            phases.append(ph)
+        if ok:
+            cr = []
+            for sites, tabs, coef in terms:
+                z = coef
+                for t in tabs:
+                    z *= phases[t]
+                if abs(z.imag) > 1e-12 * max(1.0, abs(z)):
+                    ok = False
+                    break
+                cr.append(z.real)
+        if ok:
+            for _, dvec, coef in dterms:
+                if np.any(np.abs(dvec.imag) > 1e-12) or abs(coef.imag) > 1e-12:
+                    ok = False
+                    break
+        if ok:
+            use_real = True
+            tables_real = tabs_t
+            coefs_real = cr
+    is_complex = not use_real
+    nt = max(len(raw_tables), 1)
+    t_count = np.zeros((nt, dmax), dtype=np.int32)
+    t_ket = np.zeros((nt, dmax, dmax), dtype=np.uint8)
+    t_amp = np.zeros((nt, dmax, dmax, 2 if is_complex else 1), dtype=np.float64)
+    for t, m0 in enumerate(raw_tables):
+        mags = np.abs(m0)
+        m = tables_real[t] if use_real else m0
+        for bra in range(dmax):
+            kets = np.nonzero(mags[bra] > OP_TOL)[0]
+            t_count[t, bra] = len(kets)
+            t_ket[t, bra, : len(kets)] = kets
+            if is_complex:
+                t_amp[t, bra, : len(kets), 0] = m[bra, kets].real
+                t_amp[t, bra, : len(kets), 1] = m[bra, kets].imag
+            else:
+                t_amp[t, bra, : len(kets), 0] = m[bra, kets]
+    n_terms = len(terms)
+    term_nops = np.zeros(max(n_terms, 1), dtype=np.int32)
+    term_site = np.zeros((max(n_terms, 1), _lib.MAX_OPS), dtype=np.int32)
+    term_table = np.zeros((max(n_terms, 1), _lib.MAX_OPS), dtype=np.int32)
+    term_coef = np.zeros((max(n_terms, 1), 2 if is_complex else 1), dtype=np.float64)
+    for k, (sites, tabs, coef) in enumerate(terms):
+        if len(sites) > _lib.MAX_OPS:
+            raise ValueError(f"at most {_lib.MAX_OPS} operator factors per term instance")
+        term_nops[k] = len(sites)
+        term_site[k, : len(sites)] = sites
+        term_table[k, : len(tabs)] = tabs
+        if is_complex:
+            term_coef[k] = (coef.real, coef.imag)
+        else:
+            term_coef[k, 0] = coefs_real[k]
+    n_d = len(dterms)
+    dterm_site = np.zeros(max(n_d, 1), dtype=np.int32)
+    dterm_diag = np.zeros((max(n_d, 1), dmax, 2 if is_complex else 1), dtype=np.float64)
+    dterm_coef = np.zeros((max(n_d, 1), 2 if is_complex else 1), dtype=np.float64)
+    for k, (s, dvec, coef) in enumerate(dterms):
+        dterm_site[k] = s
+        if is_complex:
+            dterm_diag[k, : len(dvec), 0] = dvec.real
+            dterm_diag[k, : len(dvec), 1] = dvec.imag
+            dterm_coef[k] = (coef.real, coef.imag)
+        else:
+            dterm_diag[k, : len(dvec), 0] = dvec.real
+            dterm_coef[k, 0] = coef.real
+
+    def up(a):
+        return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+
+    keep = [up(t_count), up(t_ket), up(t_amp), up(term_nops), up(term_site), up(term_table), up(term_coef),
+            up(dterm_site), up(dterm_diag), up(dterm_coef)]
+    a = _lib.Assembly()
+    a.n_sites = n_sites
+    a.dmax = dmax
+    for s in range(n_sites):
+        a.loc_dims[s] = int(loc_dims[s])
+        a.strides[s] = int(sector.strides[s])
+    a.sector = sector.lookup_table()
+    a.complex_values = 1 if is_complex else 0
+    a.t_count, a.t_ket, a.t_amp = ptr(keep[0]), ptr(keep[1]), ptr(keep[2])
+    a.n_terms = n_terms
+    a.term_nops, a.term_site, a.term_table, a.term_coef = ptr(keep[3]), ptr(keep[4]), ptr(keep[5]), ptr(keep[6])
+    a.n_dterms = n_d
+    a.dterm_site, a.dterm_diag, a.dterm_coef = ptr(keep[7]), ptr(keep[8]), ptr(keep[9])
+
+    import ctypes
+
+    st = stream_handle()
+    n = len(sector)
+    w = 2 if is_complex else 1
+    bound = torch.empty(max(n, 1), dtype=torch.int64, device=dev)
+    check(lib.edg_assemble_count(ctypes.byref(a), ptr(bound), st), "edg_assemble_count")
+    offsets = torch.empty(n + 1, dtype=torch.int64, device=dev)
+    scratch = torch.empty(lib.edg_scan_scratch_elems(n), dtype=torch.int64, device=dev)
+    check(lib.edg_scan_i64(ptr(bound), ptr(offsets), n, ptr(scratch), st), "edg_scan_i64")
+    total = int(offsets[n].item())
+    tmp_cols = torch.empty(max(total, 1), dtype=torch.int32, device=dev)
+    tmp_vals = torch.empty(max(total, 1) * w, dtype=torch.float64, device=dev)
+    row_nnz = torch.empty(max(n, 1), dtype=torch.int64, device=dev)
+    diag = torch.empty(max(n, 1) * w, dtype=torch.float64, device=dev)
+    present = torch.empty(max(n, 1), dtype=torch.uint8, device=dev)
+    err = torch.zeros(1, dtype=torch.int32, device=dev)
+    check(lib.edg_assemble_fill(ctypes.byref(a), ptr(offsets), ptr(tmp_cols), ptr(tmp_vals), ptr(row_nnz),
+                                ptr(diag), ptr(present), ptr(err), st), "edg_assemble_fill")
+    rowptr = torch.empty(n + 1, dtype=torch.int64, device=dev)
+    check(lib.edg_scan_i64(ptr(row_nnz), ptr(rowptr), n, ptr(scratch), st), "edg_scan_i64")
+    nnz = int(rowptr[n].item())
+    e = int(err.item())
+    if e != 0:
+        raise _lib.EdgError(e, "an operator maps a sector configuration outside the sector")
+    cols = torch.empty(max(nnz, 1), dtype=torch.int32, device=dev)
+    vals = torch.empty(max(nnz, 1) * w, dtype=torch.float64, device=dev)
+    check(lib.edg_assemble_compact(n, 1 if is_complex else 0, ptr(offsets), ptr(tmp_cols), ptr(tmp_vals),
+                                   ptr(rowptr), ptr(cols), ptr(vals), st), "edg_assemble_compact")
+    del tmp_cols, tmp_vals
+    diag = diag[: n * w]
+    if extra_diag is not None and extra_diag != 0:
+        if is_complex:
+            diag.view(-1, 2)[:, 0] += float(np.real(extra_diag))
+            diag.view(-1, 2)[:, 1] += float(np.imag(extra_diag))
+        else:
+            diag += float(np.real(extra_diag))
+        present.fill_(1)
+    mat = DeviceMatrix(n, rowptr, cols[:nnz], vals[: nnz * w], diag, present[:n], is_complex,
+                       phase_weights if (use_real and phase_weights is not None) else None)
+    mat._keep = keep
+    return mat

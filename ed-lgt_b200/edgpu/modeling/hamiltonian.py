@@ -1,0 +1,187 @@
+"""``QMB_hamiltonian`` backed by the device engine.
+
+Same surface as edlgt/modeling/qmb_hamiltonian.py:24-426: ``add_term``,
+``build(format)``, ``diagonalize(n_eigs, format, loc_dims)``,
+``time_evolution(initial_state, time_line, loc_dims)`` and the attributes
+``shape``, ``Ham_type``, ``Nenergies`` (energy densities, ascending),
+``Npsi`` (list of :class:`QMB_state`), ``GSenergy``, ``GSpsi``, ``psi_time``.
+Terms are :class:`TermBlock` objects (or scipy/dense matrices that are
+diagonal, e.g. identity shifts); the matrix lives on the device.
+"""
+
+from __future__ import annotations
+
+import logging
+
+import numpy as np
+import torch
+
+from .assembly import assemble_blocks
+from .terms import TermBlock
+
+logger = logging.getLogger(__name__)
+
+__all__ = ["QMB_hamiltonian", "QMB_state"]
+
+
+class QMB_state:
+    """A state vector in the sector basis (host copy made on first access)."""
+
+    def __init__(self, psi, lvals=None, loc_dims=None):
+        self._psi_dev = psi if isinstance(psi, torch.Tensor) else None
+        self._psi = None if isinstance(psi, torch.Tensor) else np.asarray(psi)
+        self.lvals = lvals
+        self.loc_dims = loc_dims
+
+    @property
+    def psi(self) -> np.ndarray:
+        if self._psi is None:
+            self._psi = self._psi_dev.detach().cpu().numpy()
+        return self._psi
+
+    def device(self, dev=None) -> torch.Tensor:
+        if self._psi_dev is None:
+            self._psi_dev = torch.from_numpy(np.ascontiguousarray(self._psi)).to(dev or "cuda")
+        return self._psi_dev
+
+    def get_norm(self):
+        return float(np.sqrt(np.real(np.vdot(self.psi, self.psi))))
+
+
+class QMB_hamiltonian:
+    def __init__(self, lvals, size, sector=None, phase_weights=None):
+        self.lvals = list(lvals)
+        self.shape = (int(size), int(size))
+        self.sector = sector
+        self.phase_weights = phase_weights
+        self.blocks: list[TermBlock] = []
+        self.extra_diag = 0.0
+        self.mat = None
+        self.Ham_type = None
+
+    # ------------------------------------------------------------------ terms
+    def add_term(self, term):
+        if isinstance(term, TermBlock):
+            self.blocks.append(term)
+            self.mat = None
+            return
+        from scipy.sparse import issparse
+
+        m = term
+        if issparse(m) or isinstance(m, np.ndarray):
+            mm = m.tocoo() if issparse(m) else None
+            if mm is not None:
+                off = mm.row != mm.col
+                if np.any(np.abs(mm.data[off]) > 0):
+                    raise TypeError("only diagonal matrix terms are accepted besides term blocks")
+                d = np.zeros(self.shape[0], dtype=complex)
+                np.add.at(d, mm.row[~off], mm.data[~off])
+            else:
+                if np.any(m - np.diag(np.diagonal(m))):
+                    raise TypeError("only diagonal matrix terms are accepted besides term blocks")
+                d = np.diagonal(m)
+            if not np.allclose(d, d[0]):
+                raise TypeError("only constant diagonal (identity) matrix terms are accepted")
+            self.extra_diag += complex(d[0])
+            self.mat = None
+            return
+        raise TypeError("Unsupported term type: expected a TermBlock or a diagonal matrix")
+
+    # ------------------------------------------------------------------ build
+    def build(self, format="gpu", force_complex=False):
+        if self.sector is None:
+            raise ValueError("the device Hamiltonian needs a symmetry sector")
+        if format not in ("gpu", "sparse", "linear"):
+            raise ValueError(f"format must be 'gpu' (or the aliases 'sparse'/'linear'), got {format}")
+        ed = self.extra_diag
+        self.mat = assemble_blocks(self.sector, self.blocks, phase_weights=self.phase_weights,
+                                   force_complex=force_complex, extra_diag=ed if ed != 0 else None)
+        self.Ham_type = "gpu"
+        logger.info(f"SPARSITY: {(self.mat.nnz + self.shape[0]) / self.shape[0] ** 2:.3e}")
+
+    def to_scipy(self):
+        if self.mat is None:
+            self.build()
+        return self.mat.to_scipy()
+
+    # -------------------------------------------------------------- phases
+    def _row_phase(self):
+        """i**e(row) of the real form's gauge transform (None if not used)."""
+        w = self.mat.phase_weights if self.mat is not None else None
+        if w is None:
+            return None
+        cfg = torch.from_numpy(self.sector.configs.astype(np.int64)).to(self.sector.device)
+        wt = torch.from_numpy(np.asarray(w, dtype=np.int64)).to(self.sector.device)
+        e = wt[torch.arange(cfg.shape[1], device=cfg.device)[None, :], cfg].sum(dim=1) % 4
+        table = torch.tensor([1, 1j, -1, -1j], dtype=torch.complex128, device=cfg.device)
+        return table[e]
+
+    def to_original_basis(self, psi: torch.Tensor) -> torch.Tensor:
+        """Map a real-form vector back to the reference (complex) basis."""
+        ph = self._row_phase()
+        if ph is None:
+            return psi
+        return ph * psi.to(torch.complex128)
+
+    def from_original_basis(self, psi: torch.Tensor) -> torch.Tensor:
+        ph = self._row_phase()
+        if ph is None:
+            return psi
+        return torch.conj(ph) * psi.to(torch.complex128)
+
+    # -------------------------------------------------------- diagonalize
+    def diagonalize(self, n_eigs, format="gpu", loc_dims=None, print_results=False, tol=1e-12, precision="fp64",
+                    max_iter=None):
+        from ..solvers import lanczos, lanczos_mixed
+
+        if self.mat is None:
+            self.build(format)
+        n = self.shape[0]
+        if isinstance(n_eigs, str) and n_eigs == "full":
+            k = n
+        elif isinstance(n_eigs, int):
+            if n_eigs > n:
+                raise ValueError(f"n_eigs must be < H.shape[0]={n}, got {n_eigs}")
+            k = n_eigs
+        else:
+            raise ValueError(f"n_eigs must be int or 'full', not {n_eigs}.")
+        self.loc_dims = loc_dims
+        self.n_eigs = k
+        if k > 16:
+            raise NotImplementedError("the device Lanczos returns at most 16 eigenpairs")
+        if max_iter is None:
+            max_iter = min(n, 600)
+        if precision == "mixed":
+            r64, _ = lanczos_mixed(self.mat, k=k, tol=tol, max_iter=max_iter)
+            evals = r64.evals[0][:1]
+            vecs = r64.evecs[:, :, 0].T
+            if k > 1:
+                raise NotImplementedError("mixed precision refines the ground state only")
+        else:
+            evals, vecs, _ = lanczos(self.mat, k=k, tol=tol, max_iter=max_iter)
+        n_sites = int(np.prod(self.lvals))
+        if print_results:
+            for e in evals:
+                logger.info(f"{e:.10f}  {e / n_sites:.10f}")
+        self.Nenergies = np.asarray(evals) / n_sites
+        self.Npsi = [QMB_state(self.to_original_basis(vecs[:, i]), self.lvals, loc_dims) for i in range(k)]
+        self.GSenergy = self.Nenergies[0]
+        self.GSpsi = self.Npsi[0]
+
+    # ------------------------------------------------------- time evolution
+    def time_evolution(self, initial_state, time_line, loc_dims=None, m_krylov=30, precision="c128",
+                       observables=None):
+        from ..dynamics import krylov_evolve
+
+        if self.mat is None:
+            self.build()
+        self.loc_dims = loc_dims
+        psi0 = initial_state if isinstance(initial_state, torch.Tensor) else torch.from_numpy(
+            np.asarray(initial_state, dtype=np.complex128)).to(self.sector.device)
+        psi0 = self.from_original_basis(psi0)
+        states = krylov_evolve(self.mat, psi0, np.asarray(time_line, dtype=float), m=m_krylov, precision=precision,
+                               keep_states=observables is None, observables=observables)
+        if observables is None:
+            self.psi_time = [QMB_state(self.to_original_basis(s), self.lvals, loc_dims) for s in states]
+        else:
+            self.obs_time = states

@@ -1,0 +1,163 @@
+"""U(1) quantum-link model (QED) on the device engine.
+
+Mirrors edlgt/models/QED_model.py: constructor and sector specification
+(:23-201: N = n_sites/2 for matter, link constraints E_p - E_m = 0, surface
+flux constraints for pure PBC theories), couplings ``QED_Hamiltonian_couplings``
+(:719-776) and the truncated Hamiltonian (``build_truncated_Hamiltonian``
+:235-394: electric energy, plaquettes, theta term, staggered mass, hopping).
+"""
+
+from __future__ import annotations
+
+import logging
+
+import numpy as np
+
+from ..lattice import origin_surfaces, staggered_mask
+from ..modeling import LocalTerm, PlaquetteTerm, TwoBodyTerm
+from ..operators import qed_dressed_site_operators, qed_gauge_invariant_states
+from .quantum_model import QuantumModel
+
+logger = logging.getLogger(__name__)
+
+__all__ = ["QED_Model"]
+
+
+class QED_Model(QuantumModel):
+    def __init__(self, spin, pure_theory, bg_list=None, plaq_basis=False, link_symmetries=True, get_only_bulk=False,
+                 charge=0, **kwargs):
+        super().__init__(**kwargs)
+        if isinstance(spin, str):
+            raise NotImplementedError("the integrated-gauge QED model is not part of the device engine yet")
+        if plaq_basis:
+            raise NotImplementedError("the plaquette basis is not part of the device engine yet")
+        if bg_list is not None:
+            bg = np.asarray(bg_list, dtype=float)
+            if bg.shape != (self.n_sites,):
+                raise ValueError(f"len(bg_list) must match n_sites = {self.n_sites}: got {bg.shape}")
+            self.bg_list = bg.tolist()
+        else:
+            self.bg_list = None
+        self.spin = spin
+        self.pure_theory = pure_theory
+        self.plaq_basis = plaq_basis
+        self.link_symmetries = link_symmetries
+        self.staggered_basis = not pure_theory
+        self.background = 0
+        if self.bg_list is not None:
+            self.background = int(max(np.abs(self.bg_list)))
+            if self.background == 0:
+                self.bg_list = None
+        self.gauge_basis, self.gauge_states = qed_gauge_invariant_states(
+            spin, pure_theory, lattice_dim=self.dim, background=self.background, get_only_bulk=get_only_bulk)
+        ops = qed_dressed_site_operators(spin, pure_theory, self.dim, background=self.background)
+        self.project_operators(ops, self.bg_list)
+        # global symmetry
+        if pure_theory:
+            global_ops, global_sectors = None, None
+        else:
+            # total charge Q = N - n_sites/2 (nonzero Q needs static charges summing to -Q)
+            global_ops, global_sectors = [self.ops["N"]], [int(self.n_sites / 2) + int(charge)]
+        # link symmetries
+        if link_symmetries:
+            link_ops = [[self.ops[f"E_p{d}"], -self.ops[f"E_m{d}"]] for d in self.directions]
+            link_sectors = [0 for _ in self.directions]
+        else:
+            link_ops, link_sectors = None, None
+        # electric-flux n-body constraints (pure theory, PBC, D > 1)
+        nbody_ops = nbody_sectors = nbody_sites = None
+        nbody_type = None
+        if pure_theory and not any(self.has_obc) and self.dim > 1:
+            surfaces = origin_surfaces(self.lvals)
+            face = {"x": "y", "y": "x"} if self.dim == 2 else {"x": "yz", "y": "xz", "z": "xy"}
+            nbody_sectors = np.zeros(self.dim)
+            nbody_ops, nbody_sites = [], []
+            for d in self.directions:
+                nbody_sites.append(np.array(surfaces[face[d]], dtype=np.int64))
+                nbody_ops.append(self.ops[f"E_p{d}"])
+            nbody_type = "U"
+        self.get_abelian_symmetry_sector(global_ops=global_ops, global_sectors=global_sectors, link_ops=link_ops,
+                                         link_sectors=link_sectors, nbody_ops=nbody_ops, nbody_sectors=nbody_sectors,
+                                         nbody_sites_list=nbody_sites, nbody_sym_type=nbody_type)
+        if not pure_theory:
+            self.phase_weights = self._matter_phase_weights(self.ops["N"])
+        self.default_params()
+
+    def _bg_values(self, states):
+        return np.asarray(states, dtype=float)[:, 0]
+
+    def QED_Hamiltonian_couplings(self, g, m=None, theta=0.0, magnetic_basis=False):
+        if magnetic_basis:
+            self.coeffs = {"g": g, "E": -g, "B": -0.5 / g}
+            return
+        E, B = g / 2, -1 / (2 * g)
+        coeffs = {"g": g, "E": E, "B": B, "theta": -theta * g}
+        if not self.pure_theory and m is not None:
+            t = 1 / 2
+            coeffs |= {
+                "t": -complex(0, t),
+                "tx_even": -complex(0, t),
+                "tx_odd": -complex(0, t),
+                "ty_even": -t,
+                "ty_odd": t,
+                "tz_even": -complex(0, t),
+                "tz_odd": complex(0, t),
+                "m": m,
+                "m_odd": -m,
+                "m_even": m,
+            }
+        self.coeffs = coeffs
+
+    def build_Hamiltonian(self, g, m=None, theta=0.0, dtype_mode="auto"):
+        return self.build_truncated_Hamiltonian(g, m, theta, dtype_mode)
+
+    def hamiltonian_blocks(self, g, m=None, theta=0.0):
+        """Term blocks of the truncated Hamiltonian (reference term order)."""
+        self.QED_Hamiltonian_couplings(g, m, theta)
+        c = self.coeffs
+        dp = self.def_params
+        blocks = [LocalTerm(self.ops["E2"], "E2", **dp).get_Hamiltonian(strength=c["E"])]
+        planes = []
+        if self.dim > 1:
+            planes.append((["x", "y"], ["C_px,py", "C_py,mx", "C_my,px", "C_mx,my"]))
+        if self.dim == 3:
+            planes.append((["x", "z"], ["C_px,pz", "C_pz,mx", "C_mz,px", "C_mx,mz"]))
+            planes.append((["y", "z"], ["C_py,pz", "C_pz,my", "C_mz,py", "C_my,mz"]))
+        for axes, names in planes:
+            term = PlaquetteTerm(axes, [self.ops[o] for o in names], names, **dp)
+            blocks.append(term.get_Hamiltonian(strength=c["B"], add_dagger=True))
+        if self.dim == 2 and abs(c["theta"]) > 10e-10:
+            names = ["C_px,py", "C_py,mx", "C_my,px", "C_mx,my"]
+            term = PlaquetteTerm(["x", "y"], [self.ops[o] for o in names], names, **dp)
+            blocks.append(term.get_Hamiltonian(strength=c["theta"], add_dagger=True))
+        if self.dim == 3 and abs(c["theta"]) > 10e-10:
+            for axes, names in (
+                (["x", "y"], ["EzC_px,py", "C_py,mx", "C_my,px", "C_mx,my"]),
+                (["x", "z"], ["EyC_px,pz", "C_pz,mx", "C_mz,px", "C_mx,mz"]),
+                (["y", "z"], ["ExC_py,pz", "C_pz,my", "C_mz,py", "C_my,mz"]),
+            ):
+                term = PlaquetteTerm(axes, [self.ops[o] for o in names], names, **dp)
+                blocks.append(term.get_Hamiltonian(strength=c["theta"], add_dagger=True))
+        if not self.pure_theory:
+            for lab in ("even", "odd"):
+                term = LocalTerm(self.ops["N"], "N", **dp)
+                blocks.append(term.get_Hamiltonian(c[f"m_{lab}"], staggered_mask(self.lvals, lab)))
+            for d in self.directions:
+                for lab in ("even", "odd"):
+                    names = [f"Q_p{d}_dag", f"Q_m{d}"]
+                    term = TwoBodyTerm(d, [self.ops[o] for o in names], names, **dp)
+                    blocks.append(term.get_Hamiltonian(strength=c[f"t{d}_{lab}"], add_dagger=True,
+                                                       mask=staggered_mask(self.lvals, lab)))
+        if not self.link_symmetries:
+            blocks.append(LocalTerm(self.ops["E2"], "E2", **dp).get_Hamiltonian(strength=100))
+            for d in self.directions:
+                names = [f"E_p{d}", f"E_m{d}"]
+                term = TwoBodyTerm(d, [self.ops[o] for o in names], names, **dp)
+                blocks.append(term.get_Hamiltonian(strength=-100))
+        return blocks
+
+    def build_truncated_Hamiltonian(self, g, m=None, theta=0.0, dtype_mode="auto"):
+        self.default_params()
+        for b in self.hamiltonian_blocks(g, m, theta):
+            self.H.add_term(b)
+        self.H.build(self.ham_format, force_complex=(dtype_mode == "complex"))

@@ -1,0 +1,286 @@
+"""``QuantumModel``: operator projection, device sector, Hamiltonian container,
+diagonalisation, dynamics and observables.
+
+Mirrors edlgt/models/quantum_model.py (``project_operators`` :400-502,
+``get_abelian_symmetry_sector`` :504-604, ``default_params`` :171-211,
+``diagonalize_Hamiltonian`` :606-611, ``time_evolution_Hamiltonian``
+:613-615, ``get_qmb_state_from_configs`` :826-862, ``get_observables`` /
+``measure_observables`` / ``link_avg`` / ``stag_avg`` :1158-1333).  The
+sector lives on the device as sorted keys; ``sector_configs`` is the
+reference's uint16 table, decoded on demand.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import logging
+from math import prod
+
+import numpy as np
+import torch
+
+from .. import _lib
+from .._lib import check, lib, ptr, stream_handle
+from ..lattice import lattice_labels, link_site_pairs, neighbor_sites, staggered_mask, zig_zag
+from ..modeling import LocalTerm, PlaquetteTerm, QMB_hamiltonian, QMB_state, TwoBodyTerm
+from ..modeling.assembly import assemble_blocks
+from ..operators.common import project
+from ..symmetries import SectorSpec, enumerate_sector, get_symmetry_sector_generators
+
+logger = logging.getLogger(__name__)
+
+__all__ = ["QuantumModel"]
+
+
+class QuantumModel:
+    def __init__(self, lvals, has_obc, ham_format="gpu", basis_projector=None, device=None):
+        self.lvals = list(lvals)
+        self.dim = len(self.lvals)
+        self.directions = "xyz"[: self.dim]
+        self.n_sites = prod(self.lvals)
+        self.has_obc = list(has_obc)
+        self.ham_format = ham_format
+        self.basis_projector = basis_projector
+        self.device = torch.device(device) if device is not None else torch.device("cuda")
+        self.sector = None
+        self.gauge_basis = None
+        self.gauge_states = None
+        self.staggered_basis = False
+        self.momentum_basis = None
+        self.phase_weights = None
+        self.res = {}
+        self.H = None
+
+    # ------------------------------------------------------------- sector
+    @property
+    def sector_configs(self):
+        return None if self.sector is None else self.sector.configs
+
+    @property
+    def sector_dim(self):
+        return None if self.sector is None else len(self.sector)
+
+    # ------------------------------------------------------- projection
+    def project_operators(self, ops_dict, bg_sector_list=None, bg_label_col=None):
+        """Project local operators onto each site's gauge-invariant basis.
+
+        ``self.ops[name]`` becomes a ``(n_sites, dmax, dmax)`` complex array,
+        zero-padded beyond each site's local dimension.
+        """
+        if self.gauge_basis is not None:
+            labels = lattice_labels(self.lvals, self.has_obc, self.staggered_basis)
+            loc_dims = np.array([self.gauge_basis[l].shape[1] for l in labels], dtype=np.int64)
+            self.lattice_labels = np.array(labels, dtype=object)
+        else:
+            d = next(iter(ops_dict.values())).shape[0]
+            loc_dims = np.full(self.n_sites, d, dtype=np.int64)
+            self.lattice_labels = None
+        if self.basis_projector is not None:
+            loc_dims = np.full(self.n_sites, self.basis_projector.shape[1], dtype=np.int64)
+            bg_sector_list = None
+        self.loc_dims = loc_dims.copy()
+        cols_per_site = None
+        self.gauge_states_per_site = []
+        if bg_sector_list is not None and self.gauge_basis is not None:
+            if len(bg_sector_list) != self.n_sites:
+                raise ValueError("bg_sector_list must have length n_sites")
+            cols_per_site = []
+            for ii in range(self.n_sites):
+                lab = self.lattice_labels[ii]
+                col = self._bg_values(self.gauge_states[lab])
+                cols = np.flatnonzero(np.isclose(col, float(bg_sector_list[ii]), rtol=0.0, atol=1e-12))
+                if cols.size == 0:
+                    raise ValueError(f"No GI states at site {ii} label={lab} with bg {bg_sector_list[ii]}")
+                cols_per_site.append(cols)
+                self.loc_dims[ii] = cols.size
+                self.gauge_states_per_site.append(self.gauge_states[lab][cols])
+        elif self.gauge_basis is not None:
+            for ii in range(self.n_sites):
+                self.gauge_states_per_site.append(self.gauge_states[self.lattice_labels[ii]])
+        dmax = int(np.max(self.loc_dims))
+        self.ops = {}
+        cache = {}
+        for name, op in ops_dict.items():
+            arr = np.zeros((self.n_sites, dmax, dmax), dtype=np.complex128)
+            for jj in range(self.n_sites):
+                d = int(self.loc_dims[jj])
+                if self.gauge_basis is not None:
+                    lab = self.lattice_labels[jj]
+                    cols = None if cols_per_site is None else tuple(cols_per_site[jj])
+                    key = (name, lab, cols)
+                    if key not in cache:
+                        basis = self.gauge_basis[lab]
+                        if cols is not None:
+                            basis = basis[:, list(cols)]
+                        cache[key] = project(basis, op)
+                    eff = cache[key]
+                else:
+                    eff = op.toarray() if hasattr(op, "toarray") else np.asarray(op)
+                if self.basis_projector is not None:
+                    eff = project(self.basis_projector, eff)
+                arr[jj, :d, :d] = eff
+            self.ops[name] = arr
+
+    def _bg_values(self, states):
+        """Background charge of each local basis state (first label column)."""
+        return np.asarray(states, dtype=float)[:, 0]
+
+    # ---------------------------------------------------------- symmetries
+    def get_abelian_symmetry_sector(self, global_ops=None, global_sectors=None, global_sym_type="U", link_ops=None,
+                                    link_sectors=None, nbody_ops=None, nbody_sectors=None, nbody_sites_list=None,
+                                    nbody_sym_type=None, string_ops=None, string_sectors=None):
+        g_diags = get_symmetry_sector_generators(global_ops, "global") if global_ops is not None else None
+        l_diags = get_symmetry_sector_generators(link_ops, "link") if link_ops is not None else None
+        pairs = link_site_pairs(self.lvals, self.has_obc) if link_ops is not None else None
+        n_diags = get_symmetry_sector_generators(nbody_ops, "nbody") if nbody_ops is not None else None
+        s_diags = get_symmetry_sector_generators(string_ops, "global") if string_ops is not None else None
+        if g_diags is None and l_diags is None and n_diags is None:
+            logger.info("NO SYMMETRY DETECTED: no sector_configs")
+            self.sector = None
+            return
+        nb_type = nbody_sym_type if nbody_sym_type is not None else "U"
+        # plain description of the constraints (also what the CPU oracle consumes)
+        self.sector_inputs = dict(loc_dims=self.loc_dims, glob_diags=g_diags, glob_sectors=global_sectors,
+                                  glob_type=global_sym_type, link_diags=l_diags, link_sectors=link_sectors,
+                                  pair_list=pairs, string_diags=s_diags, string_sectors=string_sectors,
+                                  nbody_diags=n_diags, nbody_sectors=nbody_sectors, nbody_sites=nbody_sites_list,
+                                  nbody_type=nb_type)
+        self.sector_spec = SectorSpec(self.loc_dims, g_diags, global_sectors, global_sym_type, l_diags, link_sectors,
+                                      pairs, s_diags, string_sectors, n_diags, nbody_sectors, nbody_sites_list, nb_type)
+        if self.device.type != "cuda":
+            # description only: every compute call needs the device engine
+            self.sector = None
+            return
+        self.sector = enumerate_sector(self.sector_spec, self.device)
+        logger.info(f"SEC DIM: {len(self.sector)}")
+
+    def default_params(self):
+        self.def_params = {
+            "lvals": self.lvals,
+            "has_obc": self.has_obc,
+            "loc_dims": self.loc_dims,
+            "staggered_basis": self.staggered_basis,
+            "gauge_basis": self.gauge_basis,
+            "sector_configs": None,
+            "momentum_basis": self.momentum_basis,
+        }
+        if self.sector is not None:
+            self.H = QMB_hamiltonian(self.lvals, len(self.sector), sector=self.sector,
+                                     phase_weights=self.phase_weights)
+        else:
+            self.H = None
+
+    def _matter_phase_weights(self, number_op):
+        """Per-site exponents x_s * n(c) of the real form's gauge transform."""
+        n = np.rint(np.real(np.array([np.diagonal(number_op[s]) for s in range(self.n_sites)]))).astype(np.int64)
+        xs = np.array([zig_zag(self.lvals, s)[0] for s in range(self.n_sites)], dtype=np.int64)
+        return (xs[:, None] * n) % 4
+
+    # ---------------------------------------------------------- solve
+    def diagonalize_Hamiltonian(self, n_eigs, format="gpu", print_results=False, precision="fp64", tol=1e-12):
+        self.H.diagonalize(n_eigs, format, self.loc_dims, print_results, tol=tol, precision=precision)
+        self.n_eigs = self.H.n_eigs
+        self.res["energy"] = self.H.Nenergies
+
+    def time_evolution_Hamiltonian(self, initial_state, time_line, **kwargs):
+        self.H.time_evolution(initial_state, time_line, self.loc_dims, **kwargs)
+
+    def get_qmb_state_from_configs(self, configs):
+        idx = self.sector.index_of(np.asarray(configs).reshape(len(configs), -1))
+        if np.any(idx < 0):
+            raise ValueError("config not compatible with the symmetry sector")
+        state = np.zeros(len(self.sector), dtype=np.complex128)
+        state[idx] = complex(1 / np.sqrt(len(configs)), 0)
+        return state
+
+    # ------------------------------------------------------- observables
+    def local_expval(self, op, psi) -> np.ndarray:
+        """<psi| op_s |psi> for every site (diagonal of op, as LocalTerm)."""
+        diag = np.real(np.array([np.diagonal(op[s]) for s in range(self.n_sites)])).astype(np.float64)
+        dmax = diag.shape[1]
+        dd = torch.from_numpy(np.ascontiguousarray(diag)).to(self.device)
+        if isinstance(psi, QMB_state):
+            psi = psi.device(self.device)
+        elif not isinstance(psi, torch.Tensor):
+            psi = torch.from_numpy(np.asarray(psi)).to(self.device)
+        if psi.is_complex():
+            p = torch.view_as_real(psi.to(torch.complex128).contiguous())
+            cpx = 1
+        else:
+            p = psi.to(torch.float64).contiguous()
+            cpx = 0
+        out = torch.empty(self.n_sites, dtype=torch.float64, device=self.device)
+        dims = _lib.SiteDims()
+        for s in range(self.n_sites):
+            dims.d[s] = int(self.loc_dims[s])
+        check(lib.edg_local_expval(ptr(self.sector.keys), len(self.sector), ctypes.byref(dims), self.n_sites, ptr(p),
+                                   cpx, 1, ptr(dd), dmax, ptr(out), stream_handle()), "edg_local_expval")
+        return out.cpu().numpy()
+
+    def get_observables(self, local_obs=(), twobody_obs=(), plaquette_obs=(), nbody_obs=(), nbody_dist=(),
+                        twobody_axes=None):
+        self.local_obs = list(local_obs)
+        self.twobody_obs = list(twobody_obs)
+        self.plaquette_obs = [list(x) for x in plaquette_obs]
+        self.obs_list = {}
+        self._plaq_mats = {}
+        for names in self.plaquette_obs:
+            axes = [names[-1][3], names[-1][6]]
+            term = PlaquetteTerm(axes, [self.ops[o] for o in names], names, **self.def_params)
+            self.obs_list["_".join(names)] = term
+        if twobody_obs:
+            raise NotImplementedError("two-body correlators are not part of the device engine yet")
+
+    def _state(self, index, dynamics):
+        return self.H.Npsi[index] if not dynamics else self.H.psi_time[index]
+
+    def measure_observables(self, index, dynamics=False):
+        st = self._state(index, dynamics)
+        for obs in self.local_obs:
+            self.res[obs] = self.local_expval(self.ops[obs], st)
+        for names in self.plaquette_obs:
+            key = "_".join(names)
+            self.res[key] = self.plaquette_avg(names, st)
+
+    def plaquette_avg(self, names, st, component="real"):
+        """Average over plaquettes of <Re P> (PlaquetteTerm.get_expval)."""
+        key = "_".join(names)
+        psi = st.device(self.device) if isinstance(st, QMB_state) else st  # reference basis
+        if key not in self._plaq_mats:
+            term = self.obs_list[key]
+            mats = []
+            from ..lattice import plaquette_sites
+
+            for ii in range(self.n_sites):
+                sl = plaquette_sites(zig_zag(self.lvals, ii), self.lvals, term.axes, self.has_obc)
+                if sl is None:
+                    continue
+                blk = term.get_Hamiltonian(1.0, add_dagger=False)
+                blk.sites = np.array([sl])
+                mats.append(assemble_blocks(self.sector, [blk], phase_weights=self.phase_weights, force_complex=True))
+            self._plaq_mats[key] = mats
+        vals = []
+        psi_c = psi.to(torch.complex128)
+        for m in self._plaq_mats[key]:
+            y = m.matvec(psi_c)
+            z = torch.vdot(psi_c, y).item()
+            vals.append(z.real if component == "real" else z.imag)
+        return float(np.mean(vals))
+
+    def link_avg(self, obs_name):
+        avg, cnt = 0.0, 0
+        for ii in range(self.n_sites):
+            coords = zig_zag(self.lvals, ii)
+            for d in self.directions:
+                if neighbor_sites(coords, self.lvals, d, self.has_obc) is not None:
+                    avg += self.res[f"{obs_name}_p{d}"][ii]
+                    cnt += 1
+        return avg / cnt
+
+    def stag_avg(self, obs_name, staggered_avg=None):
+        values = np.asarray(self.res[obs_name])
+        if staggered_avg is None:
+            return float(np.mean(values))
+        mask2d = staggered_mask(self.lvals, staggered_avg)
+        mask1d = np.array([mask2d[zig_zag(self.lvals, s)] for s in range(self.n_sites)])
+        return float(np.mean(values[mask1d]))

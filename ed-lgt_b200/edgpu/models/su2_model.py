@@ -1,0 +1,131 @@
+"""SU(2) Yang-Mills (+ staggered matter) with hard-core gluons, j_max = 1/2.
+
+Mirrors edlgt/models/SU2_model.py: constructor and sector (:31-171: total
+fermion number ``sectors``, link Casimir constraints T2_p - T2_m = 0, Z2 flux
+parities for pure PBC theories, optional static charges ``bg_list``),
+couplings ``SU2_Hamiltonian_couplings`` (:555-624) and
+``build_base_Hamiltonian`` (:200-355).
+"""
+
+from __future__ import annotations
+
+import logging
+
+import numpy as np
+
+from ..lattice import origin_surfaces, staggered_mask
+from ..modeling import LocalTerm, PlaquetteTerm, TwoBodyTerm
+from ..operators import su2_dressed_site_operators, su2_gauge_invariant_states
+from .quantum_model import QuantumModel
+
+logger = logging.getLogger(__name__)
+
+__all__ = ["SU2_Model"]
+
+
+class SU2_Model(QuantumModel):
+    def __init__(self, spin, pure_theory, bg_list=None, sectors=None, use_generic_model=False, **kwargs):
+        super().__init__(**kwargs)
+        if use_generic_model or spin >= 1:
+            raise NotImplementedError("only the hard-core-gluon (j_max = 1/2) SU(2) model runs on the device engine")
+        self.spin = spin
+        self.pure_theory = pure_theory
+        self.background = max(bg_list) if bg_list is not None else 0
+        self.bg_list = bg_list if self.background != 0 else None
+        self.gauge_basis, self.gauge_states = su2_gauge_invariant_states(spin, pure_theory, lattice_dim=self.dim,
+                                                                         background=self.background)
+        ops = su2_dressed_site_operators(spin, pure_theory, lattice_dim=self.dim, background=self.background)
+        self.project_operators(ops, bg_sector_list=self.bg_list)
+        if pure_theory:
+            global_ops, global_sectors = None, None
+            self.zero_density = None
+        else:
+            global_ops, global_sectors = [self.ops["N_tot"]], sectors
+            self.zero_density = sectors[0] == self.n_sites
+        link_ops = [[self.ops[f"T2_p{d}"], -self.ops[f"T2_m{d}"]] for d in self.directions]
+        link_sectors = [0 for _ in self.directions]
+        nbody_ops = nbody_sectors = nbody_sites = None
+        nbody_type = None
+        if pure_theory and not any(self.has_obc) and self.dim > 1:
+            surfaces = origin_surfaces(self.lvals)
+            face = {"x": "y", "y": "x"} if self.dim == 2 else {"x": "yz", "y": "xz", "z": "xy"}
+            nbody_sectors = list(np.ones(self.dim))
+            nbody_ops, nbody_sites = [], []
+            for d in self.directions:
+                nbody_sites.append(np.array(surfaces[face[d]], dtype=np.int64))
+                nbody_ops.append(self.ops[f"P_p{d}"])
+            nbody_type = "Z"
+        self.get_abelian_symmetry_sector(global_ops=global_ops, global_sectors=global_sectors, link_ops=link_ops,
+                                         link_sectors=link_sectors, nbody_ops=nbody_ops, nbody_sectors=nbody_sectors,
+                                         nbody_sites_list=nbody_sites, nbody_sym_type=nbody_type)
+        if self.sector is not None and len(self.sector) == 0:
+            raise ValueError("No configurations found for the given symmetry sectors")
+        if not pure_theory:
+            self.phase_weights = self._matter_phase_weights(self.ops["N_tot"])
+        self.default_params()
+
+    def _bg_values(self, states):
+        # first label of a local state is twice the background spin
+        return np.asarray(states, dtype=float)[:, 0] / 2.0
+
+    def SU2_Hamiltonian_couplings(self, g, m=None, theta=0.0):
+        if self.dim == 1:
+            E, B = 8 * g / 3, 0
+        else:
+            E, B = g / 2, -1 / (2 * g)
+        self.coeffs = {"g": g, "E": E, "B": B, "theta": -theta * g}
+        if not self.pure_theory and m is not None:
+            t = 2 * np.sqrt(2)
+            self.coeffs |= {
+                "tx_even": -complex(0, t),
+                "tx_odd": -complex(0, t),
+                "ty_even": -t,
+                "ty_odd": t,
+                "tz_even": -t,
+                "tz_odd": t,
+                "m": m,
+                "m_odd": -m,
+                "m_even": m,
+            }
+
+    def build_Hamiltonian(self, g, m=None, theta=0.0, lambda_noise=0.0, dtype_mode="auto"):
+        self.build_base_Hamiltonian(g, m, theta, lambda_noise, dtype_mode)
+
+    def hamiltonian_blocks(self, g, m=None, theta=0.0, lambda_noise=0.0):
+        self.SU2_Hamiltonian_couplings(g, m, theta)
+        c = self.coeffs
+        dp = self.def_params
+        blocks = [LocalTerm(self.ops["E_square"], "E_square", **dp).get_Hamiltonian(strength=c["E"])]
+        planes = []
+        if self.dim > 1:
+            planes.append((["x", "y"], ["C_px,py", "C_py,mx", "C_my,px", "C_mx,my"]))
+        if self.dim == 3:
+            planes.append((["x", "z"], ["C_px,pz", "C_pz,mx", "C_mz,px", "C_mx,mz"]))
+            planes.append((["y", "z"], ["C_py,pz", "C_pz,my", "C_mz,py", "C_my,mz"]))
+        for axes, names in planes:
+            term = PlaquetteTerm(axes, [self.ops[o] for o in names], names, **dp)
+            blocks.append(term.get_Hamiltonian(strength=c["B"], add_dagger=True))
+        if not self.pure_theory:
+            for lab in ("even", "odd"):
+                term = LocalTerm(self.ops["N-1"], "N-1", **dp)
+                blocks.append(term.get_Hamiltonian(c[f"m_{lab}"], staggered_mask(self.lvals, lab)))
+            for d in self.directions:
+                for lab in ("even", "odd"):
+                    names = [f"Qp{d}_dag", f"Qm{d}"]
+                    term = TwoBodyTerm(d, [self.ops[o] for o in names], names, **dp)
+                    blocks.append(term.get_Hamiltonian(strength=c[f"t{d}_{lab}"], add_dagger=True,
+                                                       mask=staggered_mask(self.lvals, lab)))
+        if self.dim == 3 and abs(c["theta"]) > 10e-10:
+            raise NotImplementedError("the 3D theta term is not part of the device engine yet")
+        noise = [self.background > 0, lambda_noise > 0] + [not obc for obc in self.has_obc]
+        if all(noise):
+            names = ["Vpx_dag", "Vmx"]
+            term = TwoBodyTerm("x", [self.ops[o] for o in names], names, **dp)
+            blocks.append(term.get_Hamiltonian(strength=-lambda_noise, add_dagger=True))
+        return blocks
+
+    def build_base_Hamiltonian(self, g, m=None, theta=0.0, lambda_noise=0.0, dtype_mode="auto"):
+        self.default_params()
+        for b in self.hamiltonian_blocks(g, m, theta, lambda_noise):
+            self.H.add_term(b)
+        self.H.build(self.ham_format, force_complex=(dtype_mode == "complex"))

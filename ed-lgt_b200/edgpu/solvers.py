@@ -1,0 +1,115 @@
+"""Ground-state solvers on the device.
+
+* :func:`lanczos` -- the drop-in for ``scipy.sparse.linalg.eigsh(H, k,
+  which="SA")`` (called at edlgt/modeling/qmb_hamiltonian.py:313): Lanczos with
+  full reorthogonalisation, f64 vectors, f64 recurrence and device tridiagonal
+  eigen-solve.
+* :func:`lanczos_mixed` -- f32 Krylov vectors and matvec (f64 accumulation,
+  f64 inner products / recurrence / reorthogonalisation / tridiagonal solve),
+  then a short f64 Lanczos restarted from the f32 Ritz vector refines the
+  pair ("residual-correction" refinement).  Works on up to four problems that
+  share the off-diagonal matrix and differ in the diagonal (coupling sweeps),
+  in one batched matvec.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import check, lib, ptr, stream_handle
+
+__all__ = ["LanczosResult", "lanczos", "lanczos_mixed", "stack_diagonals"]
+
+
+class LanczosResult:
+    def __init__(self, evals, evecs, iters, resid):
+        self.evals = evals      # (nvec, k) float64 numpy
+        self.evecs = evecs      # device tensor (k, n, nvec) or None
+        self.iters = iters      # (nvec,) int
+        self.resid = resid      # (nvec, k)
+
+
+def _problem(dtype, n, nnz, rowptr, cols, vals, diag, nvec, k, max_iter, tol, check_every, seed, v0):
+    p = _lib.LanczosProblem()
+    p.dtype = dtype
+    p.n_rows = n
+    p.nnz = nnz
+    p.rowptr = ptr(rowptr)
+    p.cols = ptr(cols) if nnz else None
+    p.vals = ptr(vals) if nnz else None
+    p.diag = ptr(diag)
+    p.nvec = nvec
+    p.k = k
+    p.max_iter = max_iter
+    p.tol = tol
+    p.check_every = check_every
+    p.seed = seed
+    p.v0 = ptr(v0) if v0 is not None else None
+    return p
+
+
+def run_lanczos(dtype, n, nnz, rowptr, cols, vals, diag, nvec=1, k=1, max_iter=300, tol=1e-12, check_every=5,
+                seed=1234, v0=None, want_vectors=True, allow_unconverged=False, workspace=None):
+    """Low-level call of ``edg_lanczos``; ``diag`` is ``[n][nvec]`` in the dtype."""
+    max_iter = int(min(max_iter, n))
+    p = _problem(dtype, n, nnz, rowptr, cols, vals, diag, nvec, k, max_iter, tol, check_every, seed, v0)
+    wb = lib.edg_lanczos_workspace_bytes(ctypes.byref(p))
+    if wb < 0:
+        raise _lib.EdgError(-1, _lib.last_error())
+    dev = rowptr.device
+    ws = workspace if (workspace is not None and workspace.numel() >= wb) else torch.empty(wb, dtype=torch.uint8, device=dev)
+    tdt = torch.float64 if dtype == 0 else torch.float32
+    evecs = torch.empty((k, n, nvec), dtype=tdt, device=dev) if want_vectors else None
+    evals = np.zeros(nvec * k)
+    iters = np.zeros(nvec, dtype=np.int32)
+    resid = np.zeros(nvec * k)
+    st = lib.edg_lanczos(ctypes.byref(p), ptr(ws), wb, evals.ctypes.data, ptr(evecs) if want_vectors else None,
+                         iters.ctypes.data, resid.ctypes.data, stream_handle())
+    if st == -5 and allow_unconverged:
+        pass
+    else:
+        check(st, "edg_lanczos")
+    return LanczosResult(evals.reshape(nvec, k), evecs, iters, resid.reshape(nvec, k))
+
+
+def lanczos(mat, k=1, tol=1e-12, max_iter=400, check_every=5, seed=1234, v0=None):
+    """f64 Lanczos on a real DeviceMatrix; returns (evals[k], evecs (n, k) device)."""
+    if mat.is_complex:
+        raise NotImplementedError("complex Hermitian Lanczos: assemble the real form of the model")
+    r = run_lanczos(0, mat.n, mat.nnz, mat.rowptr, mat.cols, mat.vals, mat.diag, nvec=1, k=k, max_iter=max_iter,
+                    tol=tol, check_every=check_every, seed=seed, v0=v0)
+    return r.evals[0], r.evecs[:, :, 0].T.contiguous(), r
+
+
+def stack_diagonals(diags, dtype):
+    """[n] diagonals of several problems -> interleaved [n][nvec] tensor."""
+    return torch.stack([d.to(dtype) for d in diags], dim=1).contiguous()
+
+
+def lanczos_mixed(mat, diags=None, k=1, tol32=1e-6, tol=1e-12, max_iter=400, refine_iter=8, check_every=5,
+                  seed=1234):
+    """Mixed-precision (f32 Krylov, f64 recurrence) Lanczos + f64 refinement.
+
+    ``diags``: list of f64 device diagonals (one per problem, <= 4) sharing the
+    off-diagonal part of ``mat``; default ``[mat.diag]``.  Returns the refined
+    f64 eigenvalues (nvec, k), the f64 Ritz vectors and diagnostics.
+    """
+    if mat.is_complex:
+        raise NotImplementedError("mixed Lanczos needs the real form")
+    diags = [mat.diag] if diags is None else list(diags)
+    nvec = len(diags)
+    vals32 = mat.vals.to(torch.float32)
+    diag32 = stack_diagonals(diags, torch.float32)
+    r32 = run_lanczos(1, mat.n, mat.nnz, mat.rowptr, mat.cols, vals32, diag32, nvec=nvec, k=k, max_iter=max_iter,
+                      tol=tol32, check_every=check_every, seed=seed)
+    diag64 = stack_diagonals(diags, torch.float64)
+    # f64 refinement: short Lanczos restarted from the f32 Ritz vector (ground state)
+    v0 = r32.evecs[0].to(torch.float64).contiguous()
+    r64 = run_lanczos(0, mat.n, mat.nnz, mat.rowptr, mat.cols, mat.vals, diag64, nvec=nvec, k=1,
+                      max_iter=refine_iter, tol=tol, check_every=refine_iter, seed=seed, v0=v0,
+                      allow_unconverged=True)
+    return r64, r32

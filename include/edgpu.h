@@ -1,0 +1,300 @@
+/*
+ * edgpu.h -- C ABI of libedgpu, the sm_100a exact-diagonalization engine for
+ * lattice gauge theories (sector enumeration, config->index lookup, sector
+ * Hamiltonian assembly, matvec, Lanczos and Krylov time evolution).
+ *
+ * Conventions for every entry point:
+ *   - all array arguments are DEVICE pointers owned by the caller (typically
+ *     torch tensors passed as data_ptr()); the library never allocates,
+ *     frees or retains them;
+ *   - sizes are int64_t; configurations are packed into uint64 keys
+ *     key = sum_s c_s * stride_s with the last site the fastest digit, so that
+ *     ascending keys == lexicographic configuration order;
+ *   - work is enqueued on the given stream and is asynchronous unless the
+ *     comment says the call synchronizes;
+ *   - the return value is EDG_OK (0) or a negative status; the message of the
+ *     last failure on the calling thread is returned by edg_get_last_error.
+ *
+ * Each entry point cites the ed-lgt (edlgt 0.2.3) function it replaces.
+ */
+#ifndef EDGPU_H
+#define EDGPU_H
+
+#include <stdint.h>
+#include <cuda_runtime.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EDG_OK 0
+#define EDG_ERR_ARG -1          /* invalid argument / unsupported shape        */
+#define EDG_ERR_CUDA -2         /* CUDA runtime error                          */
+#define EDG_ERR_OVERFLOW -3     /* a count or key does not fit its type       */
+#define EDG_ERR_MISSING_KET -4  /* an operator maps a sector state outside it */
+#define EDG_ERR_NOT_CONVERGED -5
+#define EDG_ERR_BREAKDOWN -6    /* Krylov space exhausted before convergence  */
+
+#define EDG_MAX_OPS 4           /* max operator factors of one term instance  */
+#define EDG_MAX_SITES 64        /* max lattice sites of one configuration     */
+
+/* ------------------------------------------------------------------------ */
+/* Library                                                                  */
+/* ------------------------------------------------------------------------ */
+
+/* Copies the last failure message of the calling thread into buf. */
+int edg_get_last_error(char* buf, int len);
+/* ABI version (major * 100 + minor). */
+int edg_version(void);
+
+/* ------------------------------------------------------------------------ */
+/* Exclusive prefix sum of int64 counts (the two-pass count/scan/fill idiom  */
+/* of edlgt/symmetries/sym_qmb_operations.py:139-164, with int64 offsets).   */
+/* ------------------------------------------------------------------------ */
+
+/* Scratch elements (int64) edg_scan_i64 needs for n inputs. */
+int64_t edg_scan_scratch_elems(int64_t n);
+/* out[i] = sum_{k<i} in[i] for i in [0, n]; out has n+1 entries (out[n] is the
+ * total). in and out may alias. */
+int edg_scan_i64(const int64_t* in, int64_t* out, int64_t n, int64_t* scratch,
+                 cudaStream_t stream);
+
+/* ------------------------------------------------------------------------ */
+/* Sector enumeration                                                        */
+/* Replaces iterative_sitebased_sym_sector_configs,                          */
+/* iterative_sitebased_sym_sector_configs1, iterative_link_sector_configs,    */
+/* iterative_link_sector_configs_plus (edlgt/symmetries/symmetry_sector.py:   */
+/* 785-967, 970-1164, 1237-1326, 1329-1469) and global_abelian_sector          */
+/* (edlgt/symmetries/global_abelian_sym.py:147-244).                          */
+/* Generator diagonals are passed as integers (the dyadic values times a     */
+/* power of two), which makes every accept/reject decision exact.            */
+/* ------------------------------------------------------------------------ */
+
+typedef struct {
+  int32_t n_sites;
+  int32_t dmax;                   /* padded local dimension                  */
+  int32_t loc_dims[EDG_MAX_SITES];   /* by value: local dimension per site   */
+  uint64_t strides[EDG_MAX_SITES];   /* by value: key stride per site        */
+  const uint8_t* site_allowed;    /* [n_sites][dmax] 1 = state allowed       */
+  /* global symmetries: U(1) sums or Z2 parities (type 0 / 1)                */
+  int32_t n_glob;                 /* <= 4                                    */
+  int32_t glob_type;
+  const int32_t* glob_val;        /* [n_glob][n_sites][dmax] (Z2: 0/1 bits)  */
+  const int32_t* glob_target;     /* [n_glob]                                */
+  const int32_t* glob_rem_min;    /* [n_glob][n_sites+1] reachable minimum   */
+  const int32_t* glob_rem_max;    /* [n_glob][n_sites+1] reachable maximum   */
+  /* link constraints val0[dir][site0][c0] + val1[dir][site1][c1] == target  */
+  int32_t n_dirs;
+  const int32_t* link_val;        /* [n_dirs][2][n_sites][dmax]              */
+  const int32_t* link_target;     /* [n_dirs]                                */
+  const int32_t* pair_start;      /* [n_sites+1] pairs grouped by activation */
+  const int32_t* pair_s0;         /* [n_pairs]                               */
+  const int32_t* pair_s1;         /* [n_pairs]                               */
+  const int32_t* pair_dir;        /* [n_pairs]                               */
+  /* n-body constraints: sum (type 0) or parity (type 1) over a site set     */
+  int32_t nbody_type;
+  const int32_t* nb_val;          /* [n_nb][n_sites][dmax]                   */
+  const int32_t* nb_target;       /* [n_nb]                                  */
+  const int32_t* nb_start;        /* [n_sites+1] constraints by activation   */
+  const int32_t* nb_id;           /* [n_act] constraint id                   */
+  const int32_t* nb_site_start;   /* [n_nb+1] site list offsets              */
+  const int32_t* nb_sites;        /* flattened site lists                    */
+} edg_sector_tables;
+
+/* Number of per-block counters (int64) the level kernels need for n
+ * candidate prefixes; scratch for edg_sector_level_count must hold this many
+ * elements plus edg_scan_scratch_elems of it. */
+int64_t edg_sector_level_blocks(int64_t n_candidates);
+
+/* Level `depth` of the prefix expansion: every parent prefix (depth-1 sites,
+ * n_prev of them; n_prev = 1 with an empty parent at depth 0) is extended by
+ * each state of site `depth`; survivors keep the parent order and the state
+ * order, so the final level is sorted.  Count writes, into block_offsets
+ * (edg_sector_level_blocks(n_prev*d)+1 entries), the exclusive per-block
+ * offsets and, at block_offsets[n_blocks], the number of survivors. */
+int edg_sector_level_count(const edg_sector_tables* t, int32_t depth,
+                           const uint64_t* prev_keys, const int32_t* prev_sums,
+                           int64_t n_prev, int64_t* block_offsets,
+                           int64_t* scratch, cudaStream_t stream);
+/* Writes the survivors counted by edg_sector_level_count. */
+int edg_sector_level_fill(const edg_sector_tables* t, int32_t depth,
+                          const uint64_t* prev_keys, const int32_t* prev_sums,
+                          int64_t n_prev, const int64_t* block_offsets,
+                          uint64_t* next_keys, int32_t* next_sums,
+                          cudaStream_t stream);
+
+/* keys -> uint16 configurations [n][n_sites] (index_to_config over a sector,
+ * edlgt/symmetries/generate_configs.py:30-54). */
+int edg_keys_to_configs(const uint64_t* keys, int64_t n, int32_t n_sites,
+                        const int32_t* loc_dims, uint16_t* configs,
+                        cudaStream_t stream);
+/* uint16 configurations -> keys (encode_all_configs,
+ * edlgt/tools/magic.py:111-140). */
+int edg_configs_to_keys(const uint16_t* configs, int64_t n, int32_t n_sites,
+                        const uint64_t* strides, uint64_t* keys,
+                        cudaStream_t stream);
+
+/* ------------------------------------------------------------------------ */
+/* config -> index lookup                                                    */
+/* Replaces config_to_index_binarysearch (edlgt/symmetries/                   */
+/* generate_configs.py:145-173): index of the key in the sorted sector, or   */
+/* -1 when absent.  A bucket table over the top key bits narrows each search.*/
+/* ------------------------------------------------------------------------ */
+
+typedef struct {
+  const uint64_t* keys;         /* [n] sorted ascending, unique              */
+  int64_t n;
+  const int64_t* bucket_start;  /* [n_buckets+1]                             */
+  int32_t shift;                /* bucket = key >> shift                     */
+  int64_t n_buckets;
+} edg_lookup_table;
+
+/* Fills bucket_start (n_buckets+1 entries) for keys < n_buckets << shift. */
+int edg_lookup_build(const uint64_t* keys, int64_t n, int32_t shift,
+                     int64_t n_buckets, int64_t* bucket_start,
+                     cudaStream_t stream);
+int edg_lookup(const edg_lookup_table* table, const uint64_t* queries,
+               int64_t m, int64_t* index_out, cudaStream_t stream);
+
+/* ------------------------------------------------------------------------ */
+/* Sector Hamiltonian assembly                                               */
+/* Replaces nbody_term / nbody_data / nbody_data_2sites / nbody_data_4sites /  */
+/* localbody_data_par (edlgt/symmetries/sym_qmb_operations.py:32-602), the     */
+/* term site loops (edlgt/modeling/{local,twobody,plaquette}_term.py) and the */
+/* triplet -> matrix build (edlgt/modeling/qmb_hamiltonian.py:173-225,          */
+/* 667-702).  Output is the canonical matrix: off-diagonal entries as CSR      */
+/* with duplicate (row, col) summed and columns ascending, and the diagonal as */
+/* a dense vector with a presence flag per row.                               */
+/* ------------------------------------------------------------------------ */
+
+typedef struct {
+  int32_t n_sites;
+  int32_t dmax;
+  int32_t loc_dims[EDG_MAX_SITES];   /* by value                              */
+  uint64_t strides[EDG_MAX_SITES];   /* by value                              */
+  edg_lookup_table sector;        /* sorted sector keys = matrix rows        */
+  int32_t complex_values;         /* 0: real double, 1: interleaved complex  */
+  /* local transition tables (nonzero entries of one site operator)         */
+  const int32_t* t_count;         /* [n_tables][dmax]                        */
+  const uint8_t* t_ket;           /* [n_tables][dmax][dmax]                  */
+  const double* t_amp;            /* [n_tables][dmax][dmax](x2 if complex)   */
+  /* off-diagonal term instances: product of n_ops site operators           */
+  int32_t n_terms;
+  const int32_t* term_nops;       /* [n_terms] in 1..EDG_MAX_OPS             */
+  const int32_t* term_site;       /* [n_terms][EDG_MAX_OPS]                  */
+  const int32_t* term_table;      /* [n_terms][EDG_MAX_OPS]                  */
+  const double* term_coef;        /* [n_terms] (x2 if complex)               */
+  /* diagonal terms: coef * op[c_site][c_site] (only the diagonal is used)   */
+  int32_t n_dterms;
+  const int32_t* dterm_site;      /* [n_dterms]                              */
+  const double* dterm_diag;       /* [n_dterms][dmax] (x2 if complex)        */
+  const double* dterm_coef;       /* [n_dterms] (x2 if complex)              */
+} edg_assembly;
+
+/* Per-row upper bound of off-diagonal entries (before merging duplicates). */
+int edg_assemble_count(const edg_assembly* a, int64_t* row_bound,
+                       cudaStream_t stream);
+/* Generates the entries of each row into its [offsets[r], offsets[r+1])
+ * window of tmp_cols/tmp_vals, merges duplicate columns, and writes the
+ * merged count to row_nnz; the diagonal goes to diag/diag_present.
+ * error_flag (one int32, zero-initialised by the caller) receives
+ * EDG_ERR_MISSING_KET when a ket is outside the sector. */
+int edg_assemble_fill(const edg_assembly* a, const int64_t* offsets,
+                      int32_t* tmp_cols, double* tmp_vals, int64_t* row_nnz,
+                      double* diag, uint8_t* diag_present, int32_t* error_flag,
+                      cudaStream_t stream);
+/* Copies the merged windows into the final CSR (rowptr from a scan of
+ * row_nnz). */
+int edg_assemble_compact(int64_t n_rows, int32_t complex_values,
+                         const int64_t* offsets, const int32_t* tmp_cols,
+                         const double* tmp_vals, const int64_t* rowptr,
+                         int32_t* cols, double* vals, cudaStream_t stream);
+
+/* ------------------------------------------------------------------------ */
+/* Matvec y = (A_offdiag + diag) x                                           */
+/* Replaces csr_spmv / csr_matmat (edlgt/modeling/qmb_hamiltonian.py:705-764)*/
+/* and the SciPy CSC matvec behind eigsh / expm_multiply.                    */
+/* dtype: 0 = f64, 1 = f32, 2 = complex128, 3 = complex64 (values, diag and */
+/* vectors share the dtype; accumulation is in double precision).           */
+/* Batched form: nvec right-hand sides stored interleaved x[row][vec],      */
+/* sharing the off-diagonal matrix, with a per-vector diagonal diag[row][vec].*/
+/* ------------------------------------------------------------------------ */
+
+int edg_spmv(int32_t dtype, int64_t n_rows, int64_t nnz,
+             const int64_t* rowptr, const int32_t* cols, const void* vals,
+             const void* diag, int32_t nvec, const void* x, void* y,
+             cudaStream_t stream);
+
+/* Casts between f64 <-> f32 (or c128 <-> c64) arrays of n scalars. */
+int edg_convert(int32_t dtype_in, const void* in, int32_t dtype_out, void* out,
+                int64_t n_scalars, cudaStream_t stream);
+
+/* ------------------------------------------------------------------------ */
+/* Lanczos ground states                                                     */
+/* Replaces scipy.sparse.linalg.eigsh(H, k, which="SA") as called from       */
+/* QMB_hamiltonian.diagonalize (edlgt/modeling/qmb_hamiltonian.py:260-332).  */
+/* Lanczos with full (classical Gram-Schmidt, twice) reorthogonalisation on  */
+/* nvec independent problems that share the off-diagonal matrix, vectors in  */
+/* f64 or f32 (dtype 0/1) and every inner product, recurrence coefficient    */
+/* and the tridiagonal eigensolve in f64 on the device.  Stops when the k   */
+/* lowest Ritz values of every problem have residual                         */
+/* |beta_{j+1} s_j| <= tol * max(1, |theta|), or after max_iter steps.       */
+/* ------------------------------------------------------------------------ */
+
+typedef struct {
+  int32_t dtype;          /* 0 f64, 1 f32 (real symmetric matrices)          */
+  int64_t n_rows;
+  int64_t nnz;
+  const int64_t* rowptr;
+  const int32_t* cols;
+  const void* vals;
+  const void* diag;       /* [n_rows][nvec]                                 */
+  int32_t nvec;           /* independent problems, <= 4                     */
+  int32_t k;              /* eigenpairs wanted per problem                  */
+  int32_t max_iter;       /* Krylov dimension limit                         */
+  double tol;
+  int32_t check_every;    /* steps between convergence checks               */
+  uint64_t seed;          /* start vector: uniform(-1,1) from this seed     */
+  const void* v0;         /* optional start vectors [n_rows][nvec] or NULL  */
+} edg_lanczos_problem;
+
+/* Bytes of device workspace edg_lanczos needs. */
+int64_t edg_lanczos_workspace_bytes(const edg_lanczos_problem* p);
+/* Runs to convergence (synchronizes every check_every steps).  Outputs:
+ * evals [nvec][k] (f64), evecs [k][n_rows][nvec] in the problem dtype (may be
+ * NULL), iters_out [nvec] steps used, resid_out [nvec][k] residual bounds. */
+int edg_lanczos(const edg_lanczos_problem* p, void* workspace,
+                int64_t workspace_bytes, double* evals, void* evecs,
+                int32_t* iters_out, double* resid_out, cudaStream_t stream);
+
+/* Tridiagonal eigen-solve on the device (multisection + inverse iteration)
+ * of T = tridiag(beta[1..m-1], alpha[0..m-1], beta[1..m-1]): the k <= 16
+ * lowest eigenvalues and eigenvectors S [k][m] (f64; evecs may be NULL).
+ * work holds 6*m doubles. */
+int edg_tridiag_lowest(const double* alpha, const double* beta, int32_t m,
+                       int32_t k, double* evals, double* evecs, double* work,
+                       cudaStream_t stream);
+
+/* ------------------------------------------------------------------------ */
+/* Local (diagonal) observables                                              */
+/* Replaces LocalTerm.get_expval in a symmetry sector (edlgt/modeling/       */
+/* local_term.py:119-237, exp_val_data edlgt/modeling/qmb_state.py:631-654): */
+/* out[s] = sum_r |psi_r|^2 diag[s][c_s(r)] for all sites at once.           */
+/* ------------------------------------------------------------------------ */
+
+typedef struct {
+  int32_t d[EDG_MAX_SITES];   /* local dimension per site (by value)        */
+} edg_site_dims;
+
+/* psi: f64 (psi_complex = 0) or interleaved complex128 (1), element r at
+ * psi[r * psi_stride]; diag: [n_sites][dmax] f64; out: [n_sites] f64. */
+int edg_local_expval(const uint64_t* keys, int64_t n, const edg_site_dims* dims,
+                     int32_t n_sites, const double* psi, int32_t psi_complex,
+                     int64_t psi_stride, const double* diag, int32_t dmax,
+                     double* out, cudaStream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EDGPU_H */

@@ -1,0 +1,47 @@
+"""Model cases of the golden fixtures (same parameters as make_golden.py)."""
+
+QED_CASES = {
+    "qed1d_L4_obc": (dict(spin=1, pure_theory=False, lvals=[4], has_obc=[True]), 1.0, 1.0),
+    "qed1d_L4_pbc": (dict(spin=1, pure_theory=False, lvals=[4], has_obc=[False]), 1.0, 1.0),
+    "qed1d_L8_obc": (dict(spin=1, pure_theory=False, lvals=[8], has_obc=[True]), 1.0, 1.0),
+    "qed2d_3x2_bg": (dict(spin=1, pure_theory=False, lvals=[3, 2], has_obc=[True, True],
+                          bg_list=[-1, 0, 0, 0, 0, 1]), 1.0, 1.0),
+    "qed2d_3x2_q0": (dict(spin=1, pure_theory=False, lvals=[3, 2], has_obc=[True, True]), 0.7, 0.4),
+    "qed2d_2x2_pure_pbc": (dict(spin=1, pure_theory=True, lvals=[2, 2], has_obc=[False, False]), 1.3, None),
+    "qed2d_3x2_pure_obc": (dict(spin=1, pure_theory=True, lvals=[3, 2], has_obc=[True, True]), 0.8, None),
+}
+QED_CHARGE = {-2: [1, 0, 0, 0, 0, 1], -1: [1, 0, 0, 0, 0, 0], 1: [-1, 0, 0, 0, 0, 0], 2: [-1, 0, 0, 0, 0, -1]}
+for _q, _bg in QED_CHARGE.items():
+    QED_CASES[f"qed2d_3x2_Q{_q:+d}"] = (dict(spin=1, pure_theory=False, lvals=[3, 2], has_obc=[True, True],
+                                             bg_list=_bg, charge=_q), 1.0, 1.0)
+
+SU2_CASES = {
+    "su2_1d_L6_pbc": (dict(spin=0.5, pure_theory=False, lvals=[6], has_obc=[False], sectors=[6]), 1.0, 5.0),
+    "su2_1d_L8_obc": (dict(spin=0.5, pure_theory=False, lvals=[8], has_obc=[True], sectors=[8]), 1.0, 0.5),
+    "su2_1d_L10_obc": (dict(spin=0.5, pure_theory=False, lvals=[10], has_obc=[True], sectors=[10]), 1.0, 0.5),
+    "su2_1d_L10_pbc": (dict(spin=0.5, pure_theory=False, lvals=[10], has_obc=[False], sectors=[10]), 2.0, 0.5),
+    "su2_1d_L8_obc_bg": (dict(spin=0.5, pure_theory=False, lvals=[8], has_obc=[True], sectors=[8],
+                              bg_list=[0, 0, 0.5, 0, 0, 0.5, 0, 0]), 1.0, 1.0),
+    "su2_2d_2x2_pure_pbc": (dict(spin=0.5, pure_theory=True, lvals=[2, 2], has_obc=[False, False]), 1.0, None),
+    "su2_2d_2x2_obc": (dict(spin=0.5, pure_theory=False, lvals=[2, 2], has_obc=[True, True], sectors=[4]), 1.0, 1.0),
+}
+
+ALL_CASES = {**QED_CASES, **SU2_CASES}
+
+BIG_CASES = {
+    "su2_1d_L12_obc": dict(spin=0.5, pure_theory=False, lvals=[12], has_obc=[True], sectors=[12]),
+    "su2_1d_L14_obc": dict(spin=0.5, pure_theory=False, lvals=[14], has_obc=[True], sectors=[14]),
+    "su2_1d_L14_pbc": dict(spin=0.5, pure_theory=False, lvals=[14], has_obc=[False], sectors=[14]),
+    "su2_1d_L16_obc_pair": dict(spin=0.5, pure_theory=False, lvals=[16], has_obc=[True], sectors=[16],
+                                bg_list=[0] * 5 + [0.5] + [0] * 4 + [0.5] + [0] * 5),
+}
+
+
+def build(name, device="cpu", big=False):
+    from edgpu.models import QED_Model, SU2_Model
+
+    if big:
+        return SU2_Model(**BIG_CASES[name], device=device)
+    kw, g, m = ALL_CASES[name]
+    cls = QED_Model if name.startswith("qed") else SU2_Model
+    return cls(**kw, device=device), g, m

@@ -1,0 +1,46 @@
+import os
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+for p in (os.path.join(ROOT, "ed-lgt_b200"), ROOT):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200) and libedgpu.so")
+
+
+@pytest.fixture(scope="session")
+def golden_small():
+    import numpy as np
+
+    return np.load(os.path.join(GOLDEN, "small_cases.npz"))
+
+
+@pytest.fixture(scope="session")
+def golden_pins():
+    import numpy as np
+
+    return np.load(os.path.join(GOLDEN, "validation_pins.npz"))
+
+
+@pytest.fixture(scope="session")
+def golden_big():
+    import numpy as np
+
+    path = os.path.join(GOLDEN, "big_cases.npz")
+    if not os.path.exists(path):
+        pytest.skip("big_cases.npz not generated")
+    return np.load(path)
+
+
+@pytest.fixture(scope="session")
+def golden_dyn():
+    import numpy as np
+
+    return np.load(os.path.join(GOLDEN, "dynamics_cases.npz"))

@@ -1,0 +1,296 @@
+"""Generate golden fixtures by running ed-lgt (the reference) itself.
+
+Run in a container that has the reference checkout (EDLGT_PATH, default
+/root/reference) and numba/scipy/sympy:
+
+    python tests/golden/make_golden.py [group ...]
+
+Groups: sectors, matrices, spectra, dynamics, big.  Output: .npz files next to
+this script.  Nothing here is imported by the library or by the GPU tests;
+the tests only read the .npz files.
+
+Digests.  A sector is stored as its sorted uint64 keys (key = sum_s c_s *
+stride_s, last site fastest) or, when large, as (dimension, sha256 of the key
+bytes).  A matrix is the reference's triplets summed into canonical CSR
+(scipy sum_duplicates), stored whole when small or as (nnz, sha256 of the
+(row, col) pattern, weighted value sums) when large.
+"""
+
+from __future__ import annotations
+
+import hashlib
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+import _refshim  # noqa: E402,F401
+
+import logging  # noqa: E402
+
+logging.disable(logging.INFO)
+
+from scipy.sparse import coo_matrix  # noqa: E402
+
+import edlgt.models.SU2_model as _su2mod  # noqa: E402
+from edlgt.models import QED_Model, SU2_Model  # noqa: E402
+
+# the reference's SU(2) static-charge path formats floats with ':d' in a log
+# helper; silence that helper so the path can run.
+_su2mod.format_loc_dims = lambda *a, **k: None
+
+
+def keys_of(configs, loc_dims):
+    loc_dims = np.asarray(loc_dims, dtype=np.uint64)
+    strides = np.ones(len(loc_dims), dtype=np.uint64)
+    for k in range(len(loc_dims) - 2, -1, -1):
+        strides[k] = strides[k + 1] * loc_dims[k + 1]
+    return (np.asarray(configs, dtype=np.uint64) * strides[None, :]).sum(axis=1, dtype=np.uint64)
+
+
+def sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def canonical(model):
+    H = model.H
+    H._materialize_triplets()
+    n = H.shape[0]
+    m = coo_matrix((H.value_list, (H.row_list.astype(np.int64), H.col_list.astype(np.int64))), shape=(n, n)).tocsr()
+    m.sum_duplicates()
+    m.sort_indices()
+    return m
+
+
+def value_weights(rows, cols):
+    return 1.0 / (1.0 + ((rows * 7919 + cols * 104729) % 1009))
+
+
+def matrix_record(m, prefix, store_full):
+    rows = np.repeat(np.arange(m.shape[0], dtype=np.int64), np.diff(m.indptr))
+    cols = m.indices.astype(np.int64)
+    vals = np.asarray(m.data, dtype=np.complex128)
+    out = {
+        f"{prefix}nnz": np.int64(len(vals)),
+        f"{prefix}pattern_sha": np.array(sha(np.stack([rows, cols]))),
+        f"{prefix}wsum": np.complex128(np.sum(vals * value_weights(rows, cols))),
+        f"{prefix}abssum": np.float64(np.sum(np.abs(vals))),
+    }
+    if store_full:
+        out |= {f"{prefix}indptr": m.indptr.astype(np.int64), f"{prefix}indices": cols.astype(np.int32),
+                f"{prefix}data": vals}
+    return out
+
+
+def sector_record(model, prefix, store_full):
+    cfg = model.sector_configs
+    keys = keys_of(cfg, model.loc_dims)
+    out = {f"{prefix}dim": np.int64(len(keys)), f"{prefix}keys_sha": np.array(sha(keys)),
+           f"{prefix}loc_dims": np.asarray(model.loc_dims, dtype=np.int64)}
+    if store_full:
+        out[f"{prefix}keys"] = keys
+    return out
+
+
+# ---------------------------------------------------------------------------
+QED_CASES = {
+    # name: (kwargs, g, m)
+    "qed1d_L4_obc": (dict(spin=1, pure_theory=False, lvals=[4], has_obc=[True]), 1.0, 1.0),
+    "qed1d_L4_pbc": (dict(spin=1, pure_theory=False, lvals=[4], has_obc=[False]), 1.0, 1.0),
+    "qed1d_L8_obc": (dict(spin=1, pure_theory=False, lvals=[8], has_obc=[True]), 1.0, 1.0),
+    "qed2d_3x2_bg": (dict(spin=1, pure_theory=False, lvals=[3, 2], has_obc=[True, True],
+                          bg_list=[-1, 0, 0, 0, 0, 1]), 1.0, 1.0),
+    "qed2d_3x2_q0": (dict(spin=1, pure_theory=False, lvals=[3, 2], has_obc=[True, True]), 0.7, 0.4),
+    "qed2d_2x2_pure_pbc": (dict(spin=1, pure_theory=True, lvals=[2, 2], has_obc=[False, False]), 1.3, None),
+    "qed2d_3x2_pure_obc": (dict(spin=1, pure_theory=True, lvals=[3, 2], has_obc=[True, True]), 0.8, None),
+}
+# charge sectors of the 3x2 lattice: static charges summing to -Q, N = 3 + Q
+QED_CHARGE = {-2: [1, 0, 0, 0, 0, 1], -1: [1, 0, 0, 0, 0, 0], 1: [-1, 0, 0, 0, 0, 0], 2: [-1, 0, 0, 0, 0, -1]}
+
+SU2_CASES = {
+    "su2_1d_L6_pbc": (dict(spin=0.5, pure_theory=False, lvals=[6], has_obc=[False], sectors=[6]), 1.0, 5.0),
+    "su2_1d_L8_obc": (dict(spin=0.5, pure_theory=False, lvals=[8], has_obc=[True], sectors=[8]), 1.0, 0.5),
+    "su2_1d_L10_obc": (dict(spin=0.5, pure_theory=False, lvals=[10], has_obc=[True], sectors=[10]), 1.0, 0.5),
+    "su2_1d_L10_pbc": (dict(spin=0.5, pure_theory=False, lvals=[10], has_obc=[False], sectors=[10]), 2.0, 0.5),
+    "su2_1d_L8_obc_bg": (dict(spin=0.5, pure_theory=False, lvals=[8], has_obc=[True], sectors=[8],
+                              bg_list=[0, 0, 0.5, 0, 0, 0.5, 0, 0]), 1.0, 1.0),
+    "su2_2d_2x2_pure_pbc": (dict(spin=0.5, pure_theory=True, lvals=[2, 2], has_obc=[False, False]), 1.0, None),
+    "su2_2d_2x2_obc": (dict(spin=0.5, pure_theory=False, lvals=[2, 2], has_obc=[True, True], sectors=[4]), 1.0, 1.0),
+}
+
+
+def qed_model(kwargs):
+    return QED_Model(**kwargs)
+
+
+def su2_model(kwargs):
+    m = SU2_Model(**kwargs)
+    m.default_params()
+    return m
+
+
+def qed_charge_model(q):
+    m = QED_Model(spin=1, pure_theory=False, lvals=[3, 2], has_obc=[True, True], bg_list=QED_CHARGE[q])
+    link_ops = [[m.ops[f"E_p{d}"], -m.ops[f"E_m{d}"]] for d in m.directions]
+    m.get_abelian_symmetry_sector(global_ops=[m.ops["N"]], global_sectors=[3 + q], link_ops=link_ops,
+                                  link_sectors=[0, 0])
+    m.default_params()
+    return m
+
+
+def gen_small(store_spectra=True):
+    out = {}
+    t0 = time.time()
+    for name, (kw, g, mass) in QED_CASES.items():
+        model = qed_model(kw)
+        out |= sector_record(model, f"{name}/", True)
+        model.build_Hamiltonian(g, mass)
+        out |= matrix_record(canonical(model), f"{name}/H_", True)
+        out[f"{name}/g"] = np.float64(g)
+        out[f"{name}/m"] = np.float64(np.nan if mass is None else mass)
+        if store_spectra:
+            k = 2 if len(model.sector_configs) > 3 else 1
+            model.diagonalize_Hamiltonian(k, "sparse")
+            out[f"{name}/energies"] = np.asarray(model.H.Nenergies)
+        print(name, len(model.sector_configs), f"{time.time() - t0:.1f}s", flush=True)
+    for q, bg in QED_CHARGE.items():
+        name = f"qed2d_3x2_Q{q:+d}"
+        model = qed_charge_model(q)
+        out |= sector_record(model, f"{name}/", True)
+        model.build_Hamiltonian(1.0, 1.0)
+        out |= matrix_record(canonical(model), f"{name}/H_", True)
+        model.diagonalize_Hamiltonian(1, "sparse")
+        out[f"{name}/energies"] = np.asarray(model.H.Nenergies)
+        print(name, len(model.sector_configs), flush=True)
+    for name, (kw, g, mass) in SU2_CASES.items():
+        model = su2_model(kw)
+        out |= sector_record(model, f"{name}/", True)
+        model.build_Hamiltonian(g, mass)
+        out |= matrix_record(canonical(model), f"{name}/H_", True)
+        out[f"{name}/g"] = np.float64(g)
+        out[f"{name}/m"] = np.float64(np.nan if mass is None else mass)
+        model.diagonalize_Hamiltonian(1, "sparse")
+        out[f"{name}/energies"] = np.asarray(model.H.Nenergies)
+        print(name, len(model.sector_configs), f"{time.time() - t0:.1f}s", flush=True)
+    np.savez_compressed(os.path.join(HERE, "small_cases.npz"), **out)
+
+
+def gen_validation_pins():
+    """Known answers of the reference's own validation suite, re-run here."""
+    from edlgt.workflows.qed import run_QED_spectrum
+    from edlgt.workflows.su2 import run_SU2_spectrum
+
+    out = {}
+    par = {"model": {"lvals": [4], "has_obc": [True], "spin": 1, "pure_theory": False, "ham_format": "sparse",
+                     "bg_list": None}, "hamiltonian": {"n_eigs": 1}, "observables": {"measure_obs": True},
+           "g": 1.0, "m": 1.0}
+    r = run_QED_spectrum(par)
+    out |= {"qed1d_L4_obc/energy": r["energy"][0], "qed1d_L4_obc/E2": r["E2"][0], "qed1d_L4_obc/N": r["N"][0]}
+    par["model"]["has_obc"] = [False]
+    r = run_QED_spectrum(par)
+    out |= {"qed1d_L4_pbc/energy": r["energy"][0], "qed1d_L4_pbc/E2": r["E2"][0], "qed1d_L4_pbc/N": r["N"][0]}
+    par = {"model": {"lvals": [3, 2], "has_obc": [True, True], "spin": 1, "pure_theory": False,
+                     "ham_format": "sparse", "bg_list": [-1, 0, 0, 0, 0, 1]}, "hamiltonian": {"n_eigs": 1},
+           "observables": {"measure_obs": True}, "g": 1, "m": 1}
+    r = run_QED_spectrum(par)
+    out |= {"qed2d_3x2_bg/energy": r["energy"][0], "qed2d_3x2_bg/E2": r["E2"][0], "qed2d_3x2_bg/N": r["N"][0],
+            "qed2d_3x2_bg/plaq": r["C_px,py_C_py,mx_C_my,px_C_mx,my"][0]}
+    par = {"model": {"lvals": [6], "sectors": [6], "has_obc": [False], "spin": 0.5, "pure_theory": False,
+                     "ham_format": "sparse"}, "hamiltonian": {"n_eigs": 1}, "observables": {"measure_obs": True},
+           "g": 1, "m": 5}
+    r = run_SU2_spectrum(par)
+    for k in ("energy", "E2", "N_tot", "N_single", "N_pair", "N_zero"):
+        out[f"su2_1d_L6_pbc/{k}"] = r[k][0]
+    np.savez(os.path.join(HERE, "validation_pins.npz"), **{k: np.float64(v) for k, v in out.items()})
+    print(out)
+
+
+def gen_big():
+    """Sector digests and matrix digests at the benchmark sizes."""
+    out = {}
+    for name, kw, g, mass, with_matrix in (
+        ("su2_1d_L12_obc", dict(spin=0.5, pure_theory=False, lvals=[12], has_obc=[True], sectors=[12]), 1.0, 0.5,
+         True),
+        ("su2_1d_L14_obc", dict(spin=0.5, pure_theory=False, lvals=[14], has_obc=[True], sectors=[14]), 1.0, 0.5,
+         True),
+        ("su2_1d_L14_pbc", dict(spin=0.5, pure_theory=False, lvals=[14], has_obc=[False], sectors=[14]), 1.0, 0.5,
+         False),
+        ("su2_1d_L16_obc_pair", dict(spin=0.5, pure_theory=False, lvals=[16], has_obc=[True], sectors=[16],
+                                     bg_list=[0] * 5 + [0.5] + [0] * 4 + [0.5] + [0] * 5), 1.0, 1.0, False),
+    ):
+        t0 = time.time()
+        model = su2_model(kw)
+        out |= sector_record(model, f"{name}/", len(model.sector_configs) <= 100_000)
+        if with_matrix:
+            model.build_Hamiltonian(g, mass)
+            out |= matrix_record(canonical(model), f"{name}/H_", False)
+            out[f"{name}/triplets"] = np.int64(len(model.H.row_list))
+            t1 = time.time()
+            model.diagonalize_Hamiltonian(1, "sparse")
+            out[f"{name}/energies"] = np.asarray(model.H.Nenergies)
+            out[f"{name}/eigsh_seconds"] = np.float64(time.time() - t1)
+        print(name, len(model.sector_configs), f"{time.time() - t0:.1f}s", flush=True)
+    # the coupling sweep of the L=14 OBC benchmark: g^2 in {0.5, 1, 2}, m = 0.5
+    model = su2_model(dict(spin=0.5, pure_theory=False, lvals=[14], has_obc=[True], sectors=[14]))
+    for g in (0.5, 1.0, 2.0):
+        model.default_params()
+        model.build_Hamiltonian(g, 0.5)
+        model.diagonalize_Hamiltonian(1, "sparse")
+        out[f"su2_1d_L14_obc/sweep_g{g}"] = np.asarray(model.H.Nenergies)
+        print("sweep", g, model.H.Nenergies, flush=True)
+    np.savez_compressed(os.path.join(HERE, "big_cases.npz"), **out)
+
+
+def gen_dynamics():
+    """Quench observables from the reference's expm_multiply path."""
+    out = {}
+    # SU(2) L=6 PBC, bare vacuum, g=1, m=5, t in [0, 0.5] step 0.01 (the
+    # reference's own golden-dynamics case), and L=10 OBC string state.
+    for name, kw, g, mass, state, tline in (
+        ("su2_1d_L6_pbc_V", dict(spin=0.5, pure_theory=False, lvals=[6], has_obc=[False], sectors=[6]), 1.0, 5.0,
+         "V", np.arange(0.0, 0.5 + 0.01, 0.01)),
+        ("su2_1d_L10_obc_pair", dict(spin=0.5, pure_theory=False, lvals=[10], has_obc=[True], sectors=[10],
+                                     bg_list=[0, 0, 0, 0.5, 0, 0, 0.5, 0, 0, 0]), 1.0, 1.0, None,
+         np.arange(0.0, 2.0 + 0.05, 0.05)),
+    ):
+        model = su2_model(kw)
+        model.build_Hamiltonian(g, mass)
+        if state is not None:
+            config = model.overlap_QMB_state(state)
+        else:
+            # a string product state: the first sector configuration with the
+            # most sites in the local state 0 of each site (deterministic)
+            cfg = model.sector_configs
+            config = cfg[np.argmax((cfg == 0).sum(axis=1))]
+        psi0 = model.get_qmb_state_from_configs([config])
+        model.time_evolution_Hamiltonian(psi0, tline)
+        T2 = np.zeros((len(tline), model.n_sites))
+        NP = np.zeros((len(tline), model.n_sites))
+        from edlgt.modeling import LocalTerm
+
+        lt = LocalTerm(model.ops["T2_px"], "T2_px", **model.def_params)
+        lp = LocalTerm(model.ops["N_pair"], "N_pair", **model.def_params)
+        for k in range(len(tline)):
+            lt.get_expval(model.H.psi_time[k], print_values=False)
+            lp.get_expval(model.H.psi_time[k], print_values=False)
+            T2[k] = lt.obs
+            NP[k] = lp.obs
+        out |= {f"{name}/time": tline, f"{name}/config": np.asarray(config, dtype=np.int64), f"{name}/T2_px": T2,
+                f"{name}/N_pair": NP, f"{name}/g": np.float64(g), f"{name}/m": np.float64(mass)}
+        print(name, len(model.sector_configs), flush=True)
+    np.savez_compressed(os.path.join(HERE, "dynamics_cases.npz"), **out)
+
+
+if __name__ == "__main__":
+    groups = sys.argv[1:] or ["small", "pins", "dynamics", "big"]
+    if "small" in groups:
+        gen_small()
+    if "pins" in groups:
+        gen_validation_pins()
+    if "dynamics" in groups:
+        gen_dynamics()
+    if "big" in groups:
+        gen_big()

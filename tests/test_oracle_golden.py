@@ -1,0 +1,88 @@
+"""The CPU oracle (restatement of the reference) pinned against fixtures
+produced by the reference itself; the operator factories and term lists of
+the package feed both, so these tests also pin the host model layer."""
+
+import numpy as np
+import pytest
+
+from cases import ALL_CASES, build
+from oracle import edlgt_oracle as O
+
+
+@pytest.mark.parametrize("name", sorted(ALL_CASES))
+def test_sector_matches_reference(name, golden_small):
+    model, g, m = build(name)
+    cfg = O.sector_configs(**model.sector_inputs)
+    keys = O.keys_of(cfg, model.loc_dims)
+    assert np.array_equal(model.loc_dims, golden_small[f"{name}/loc_dims"])
+    assert np.array_equal(keys, golden_small[f"{name}/keys"])
+
+
+@pytest.mark.parametrize("name", sorted(ALL_CASES))
+def test_matrix_and_energies_match_reference(name, golden_small):
+    model, g, m = build(name)
+    cfg = O.sector_configs(**model.sector_inputs)
+    H = O.assemble(model.hamiltonian_blocks(g, m), cfg, model.loc_dims)
+    assert np.array_equal(H.indptr, golden_small[f"{name}/H_indptr"])
+    assert np.array_equal(H.indices, golden_small[f"{name}/H_indices"])
+    ref = golden_small[f"{name}/H_data"]
+    assert np.max(np.abs(H.data - ref)) <= 1e-13 * max(1.0, np.max(np.abs(ref)))
+    e_ref = golden_small[f"{name}/energies"]
+    w, _ = O.lowest_eigs(H, len(e_ref))
+    assert np.allclose(w / model.n_sites, e_ref, atol=1e-10, rtol=0)
+
+
+def test_validation_pins(golden_pins):
+    """Energies and observables pinned by the reference's validation suite."""
+    # QED 1D L=4 OBC/PBC (validation/qed/test_qed_1d_matter.py)
+    for name in ("qed1d_L4_obc", "qed1d_L4_pbc"):
+        model, g, m = build(name)
+        cfg = O.sector_configs(**model.sector_inputs)
+        H = O.assemble(model.hamiltonian_blocks(g, m), cfg, model.loc_dims)
+        w, v = O.lowest_eigs(H, 1)
+        assert abs(w[0] / 4 - golden_pins[f"{name}/energy"]) < 1e-10
+        e2 = O.local_expval(v[:, 0], model.ops["E2_px"], cfg)
+        n_ev = O.local_expval(v[:, 0], model.ops["N"], cfg)
+        nz = O.local_expval(v[:, 0], model.ops["N_zero"], cfg)
+        links = [s for s in range(4) if (s < 3 or not model.has_obc[0])]
+        assert abs(np.mean(e2[links]) - golden_pins[f"{name}/E2"]) < 1e-10
+        n_val = 0.5 * np.mean(n_ev[0::2]) + 0.5 * np.mean(nz[1::2])
+        assert abs(n_val - golden_pins[f"{name}/N"]) < 1e-10
+    # SU(2) L=6 PBC (validation/su2/test_su2_spectrum.py)
+    model, g, m = build("su2_1d_L6_pbc")
+    cfg = O.sector_configs(**model.sector_inputs)
+    H = O.assemble(model.hamiltonian_blocks(g, m), cfg, model.loc_dims)
+    w, v = O.lowest_eigs(H, 1)
+    assert abs(w[0] / 6 - golden_pins["su2_1d_L6_pbc/energy"]) < 1e-10
+    # staggered densities as edlgt/workflows/su2.py:211-218 combines them
+    ev = {k: O.local_expval(v[:, 0], model.ops[k], cfg) for k in ("N_single", "N_pair", "N_zero", "T2_px")}
+    single = np.mean(ev["N_single"])
+    pair = 0.5 * np.mean(ev["N_pair"][0::2]) + 0.5 * np.mean(ev["N_zero"][1::2])
+    zero = 0.5 * np.mean(ev["N_zero"][0::2]) + 0.5 * np.mean(ev["N_pair"][1::2])
+    got = {"N_single": single, "N_pair": pair, "N_zero": zero, "N_tot": single + 2 * pair,
+           "E2": np.mean(ev["T2_px"])}
+    for k, val in got.items():
+        assert abs(val - golden_pins[f"su2_1d_L6_pbc/{k}"]) < 1e-10, k
+
+
+def test_charge_sector_dimensions(golden_small):
+    dims = {q: int(golden_small[f"qed2d_3x2_Q{q:+d}/dim"]) for q in (-2, -1, 1, 2)}
+    dims[0] = int(golden_small["qed2d_3x2_q0/dim"])
+    assert dims == {-2: 26, -1: 52, 0: 90, 1: 67, 2: 26}
+
+
+def test_dynamics_oracle(golden_dyn):
+    """expm_multiply restatement reproduces the reference's quench observables."""
+    for name, key in (("su2_1d_L6_pbc", "su2_1d_L6_pbc_V"),):
+        model, _, _ = build(name)
+        g = float(golden_dyn[f"{key}/g"])
+        m = float(golden_dyn[f"{key}/m"])
+        cfg = O.sector_configs(**model.sector_inputs)
+        H = O.assemble(model.hamiltonian_blocks(g, m), cfg, model.loc_dims)
+        idx = O.config_to_index(golden_dyn[f"{key}/config"][None, :], cfg, model.loc_dims)[0]
+        psi0 = np.zeros(H.shape[0], complex)
+        psi0[idx] = 1
+        t = golden_dyn[f"{key}/time"]
+        psi_t = O.evolve(H, psi0, t)
+        T2 = np.array([O.local_expval(p, model.ops["T2_px"], cfg) for p in psi_t])
+        assert np.max(np.abs(T2 - golden_dyn[f"{key}/T2_px"])) < 1e-9
