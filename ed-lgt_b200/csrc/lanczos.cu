@@ -119,17 +119,98 @@ __global__ void __launch_bounds__(kThreads) dots_k(const T* __restrict__ V, int6
   }
 }
 
-// h[i][v] = sum_b partial[b][i][v]; alpha accumulates h[j].
+// h[i][v] = sum_b partial[b][i][v] (one CTA per Krylov index i, fixed summation
+// order); alpha accumulates h[j].
 template <int NV>
-__global__ void reduce_h_k(const double* __restrict__ partial, int nblocks, int ld_i, int j, double* __restrict__ h,
-                           double* __restrict__ alpha_j /* [NV] or null */) {
-  int idx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= (j + 1) * NV) return;
-  int i = idx / NV, v = idx % NV;
-  double a = 0.0;
-  for (int b = 0; b < nblocks; ++b) a += partial[((int64_t)b * ld_i + i) * NV + v];
-  h[idx] = a;
-  if (alpha_j && i == j) alpha_j[v] += a;
+__global__ void __launch_bounds__(kThreads) reduce_h_k(const double* __restrict__ partial, int nblocks, int ld_i,
+                                                       int j, double* __restrict__ h, double* __restrict__ alpha_j) {
+  __shared__ double red[(kThreads / 32) * NV];
+  const int i = blockIdx.x;
+  double a[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) a[v] = 0.0;
+  for (int b = threadIdx.x; b < nblocks; b += kThreads)
+#pragma unroll
+    for (int v = 0; v < NV; ++v) a[v] += partial[((int64_t)b * ld_i + i) * NV + v];
+  block_sum<NV>(a, red);
+  if (threadIdx.x < NV) {
+    h[i * NV + threadIdx.x] = a[threadIdx.x];
+    if (alpha_j && i == j) alpha_j[threadIdx.x] += a[threadIdx.x];
+  }
+}
+
+// Pass 1 update fused with pass 2 inner products:
+//   w[r] -= sum_i V[i][r] h[i] ;  partial[b][i] = sum_{r in block b} V[i][r] w[r]
+// Each CTA owns a contiguous row chunk; the Krylov entries of a row tile are
+// read once for the update and then again (from L1) for the new dots.
+template <typename T, int NV>
+__global__ void __launch_bounds__(kThreads) update_dots_k(const T* __restrict__ V, int64_t n, int j,
+                                                          const double* __restrict__ h, double* __restrict__ w,
+                                                          double* __restrict__ partial, int ld_i, int64_t stride_i) {
+  extern __shared__ double hs[];  // [(j+1)][NV]
+  __shared__ double red[(kThreads / 32) * kItile * NV];
+  __shared__ double out[kItile * NV];
+  for (int t = threadIdx.x; t < (j + 1) * NV; t += kThreads) hs[t] = h[t];
+  __syncthreads();
+  const int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
+  const int64_t r0 = blockIdx.x * chunk;
+  const int64_t r1 = min(n, r0 + chunk);
+  // update all rows of the chunk first (each thread its own rows)
+  for (int64_t r = r0 + threadIdx.x; r < r1; r += kThreads) {
+    double s[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) s[v] = 0.0;
+    for (int i = 0; i <= j; ++i) {
+      const T* Vi = V + (int64_t)i * stride_i + r * NV;
+#pragma unroll
+      for (int v = 0; v < NV; ++v) s[v] = fma(ldv(Vi, v), hs[i * NV + v], s[v]);
+    }
+#pragma unroll
+    for (int v = 0; v < NV; ++v) w[r * NV + v] -= s[v];
+  }
+  // the same thread re-reads the rows it updated: no barrier needed for w
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int i0 = 0; i0 <= j; i0 += kItile) {
+    double acc[kItile][NV];
+#pragma unroll
+    for (int t = 0; t < kItile; ++t)
+#pragma unroll
+      for (int v = 0; v < NV; ++v) acc[t][v] = 0.0;
+    for (int64_t r = r0 + threadIdx.x; r < r1; r += kThreads) {
+      double wr[NV];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) wr[v] = w[r * NV + v];
+#pragma unroll
+      for (int t = 0; t < kItile; ++t) {
+        if (i0 + t <= j) {
+          const T* Vi = V + (int64_t)(i0 + t) * stride_i + r * NV;
+#pragma unroll
+          for (int v = 0; v < NV; ++v) acc[t][v] = fma(ldv(Vi, v), wr[v], acc[t][v]);
+        }
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < kItile; ++t)
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        double a = acc[t][v];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+        if (lane == 0) red[(warp * kItile + t) * NV + v] = a;
+      }
+    __syncthreads();
+    if (threadIdx.x < kItile * NV) {
+      double a = 0.0;
+      for (int wi = 0; wi < kThreads / 32; ++wi) a += red[wi * kItile * NV + threadIdx.x];
+      out[threadIdx.x] = a;
+    }
+    __syncthreads();
+    if (threadIdx.x < kItile * NV) {
+      int t = threadIdx.x / NV, v = threadIdx.x % NV;
+      if (i0 + t <= j) partial[((int64_t)blockIdx.x * ld_i + (i0 + t)) * NV + v] = out[threadIdx.x];
+    }
+    __syncthreads();
+  }
 }
 
 // w[r][v] -= sum_i V[i][r][v] h[i][v]; block partial of |w|^2 per vector.
@@ -178,14 +259,19 @@ __global__ void __launch_bounds__(kThreads) norm_k(const double* __restrict__ w,
   if (threadIdx.x < NV) norm_partial[blockIdx.x * NV + threadIdx.x] = nrm[threadIdx.x];
 }
 
-// beta[v] = sqrt(sum_b norm_partial[b][v])
+// beta[v] = sqrt(sum_b norm_partial[b][v]) (one CTA, fixed order)
 template <int NV>
-__global__ void beta_k(const double* __restrict__ norm_partial, int nblocks, double* __restrict__ beta) {
-  int v = threadIdx.x;
-  if (v >= NV) return;
-  double a = 0.0;
-  for (int b = 0; b < nblocks; ++b) a += norm_partial[b * NV + v];
-  beta[v] = sqrt(a);
+__global__ void __launch_bounds__(kThreads) beta_k(const double* __restrict__ norm_partial, int nblocks,
+                                                   double* __restrict__ beta) {
+  __shared__ double red[(kThreads / 32) * NV];
+  double a[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) a[v] = 0.0;
+  for (int b = threadIdx.x; b < nblocks; b += kThreads)
+#pragma unroll
+    for (int v = 0; v < NV; ++v) a[v] += norm_partial[b * NV + v];
+  block_sum<NV>(a, red);
+  if (threadIdx.x < NV) beta[threadIdx.x] = sqrt(a[threadIdx.x]);
 }
 
 // V[j+1] = w / beta (beta = 0 leaves a zero vector: invariant subspace)
@@ -447,14 +533,16 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
   cudaError_t e;
   start_k<T><<<g_vec, 256, 0, s>>>(n * NV, p->seed, (const T*)p->v0, w);
   norm_k<NV><<<L.nblk_upd, kThreads, 0, s>>>(w, n, normp);
-  beta_k<NV><<<1, 32, 0, s>>>(normp, L.nblk_upd, h);
+  beta_k<NV><<<1, kThreads, 0, s>>>(normp, L.nblk_upd, h);
   scale_store_k<T, NV><<<g_vec, 256, 0, s>>>(w, n, h, V);
   zero_k<NV><<<(NV * ld_b + 255) / 256, 256, 0, s>>>(beta, NV * ld_b);
   zero_k<NV><<<(NV * ld_a + 255) / 256, 256, 0, s>>>(alpha, NV * ld_a);
   if ((e = cudaGetLastError()) != cudaSuccess) return edg::cuda_status(e, "edg_lanczos: start");
   const size_t upd_smem = (size_t)(L.m_max + 1) * NV * sizeof(double);
-  if (upd_smem > 48 * 1024) {
+  if (upd_smem > 40 * 1024) {
     e = cudaFuncSetAttribute(update_k<T, NV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)upd_smem);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(update_dots_k<T, NV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)upd_smem + 8192);
     if (e != cudaSuccess) return edg::cuda_status(e, "edg_lanczos: smem attribute");
   }
   std::vector<double> hb((size_t)NV * ld_b), ha((size_t)NV * ld_a), hev((size_t)NV * kMaxK),
@@ -475,21 +563,49 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
   };
   int status = EDG_OK;
   int j = 0;
+  // optional phase timing with CUDA events on the launch stream
+  const bool timing = p->stats != nullptr;
+  std::vector<cudaEvent_t> ev;
+  int ev_done = 0;  // steps whose events were already accumulated
+  double t_spmv = 0.0, t_reorth = 0.0, t_check = 0.0;
+  int64_t launches = 7;  // start-vector kernels
+  auto event_at = [&](int idx) -> cudaEvent_t {
+    while ((int)ev.size() <= idx) {
+      cudaEvent_t e2;
+      cudaEventCreate(&e2);
+      ev.push_back(e2);
+    }
+    return ev[idx];
+  };
+  auto accumulate = [&](int upto) {
+    for (; ev_done < upto; ++ev_done) {
+      float a = 0.f, b = 0.f;
+      cudaEventElapsedTime(&a, ev[3 * ev_done], ev[3 * ev_done + 1]);
+      cudaEventElapsedTime(&b, ev[3 * ev_done + 1], ev[3 * ev_done + 2]);
+      t_spmv += a;
+      t_reorth += b;
+    }
+  };
   for (; j < L.m_max; ++j) {
     const T* vj = V + (int64_t)j * stride_i;
+    if (timing) cudaEventRecord(event_at(3 * j), s);
     int st = edg::launch_spmv<T, T, double>(NV, n, p->nnz, p->rowptr, p->cols, (const T*)p->vals, (const T*)p->diag,
                                             vj, w, s);
     if (st) return st;
+    if (timing) cudaEventRecord(event_at(3 * j + 1), s);
+    launches += 10;
     zero_k<NV><<<1, 32, 0, s>>>(alpha_cur, NV);
-    for (int pass = 0; pass < 2; ++pass) {
-      dots_k<T, NV><<<L.nblk_dot, kThreads, 0, s>>>(V, n, j, w, partial, ld_a, stride_i);
-      reduce_h_k<NV><<<((j + 1) * NV + 127) / 128, 128, 0, s>>>(partial, L.nblk_dot, ld_a, j, h, alpha_cur);
-      update_k<T, NV><<<L.nblk_upd, kThreads, upd_smem, s>>>(V, n, j, h, w, normp, stride_i);
-    }
+    // classical Gram-Schmidt twice: dots | update+dots | update (3 reads of V)
+    dots_k<T, NV><<<L.nblk_dot, kThreads, 0, s>>>(V, n, j, w, partial, ld_a, stride_i);
+    reduce_h_k<NV><<<j + 1, kThreads, 0, s>>>(partial, L.nblk_dot, ld_a, j, h, alpha_cur);
+    update_dots_k<T, NV><<<L.nblk_dot, kThreads, upd_smem, s>>>(V, n, j, h, w, partial, ld_a, stride_i);
+    reduce_h_k<NV><<<j + 1, kThreads, 0, s>>>(partial, L.nblk_dot, ld_a, j, h, alpha_cur);
+    update_k<T, NV><<<L.nblk_upd, kThreads, upd_smem, s>>>(V, n, j, h, w, normp, stride_i);
     scatter_coef_k<NV><<<1, 32, 0, s>>>(alpha_cur, alpha, ld_a, j);
-    beta_k<NV><<<1, 32, 0, s>>>(normp, L.nblk_upd, h);  // h[0..NV) = beta_{j+1}
+    beta_k<NV><<<1, kThreads, 0, s>>>(normp, L.nblk_upd, h);  // h[0..NV) = beta_{j+1}
     scatter_coef_k<NV><<<1, 32, 0, s>>>(h, beta, ld_b, j + 1);
     scale_store_k<T, NV><<<g_vec, 256, 0, s>>>(w, n, h, V + (int64_t)(j + 1) * stride_i);
+    if (timing) cudaEventRecord(event_at(3 * j + 2), s);
     if ((e = cudaGetLastError()) != cudaSuccess) return edg::cuda_status(e, "edg_lanczos: step");
     const int m = j + 1;
     const bool check = (m % p->check_every == 0) || m == L.m_max || (int64_t)m == n;
@@ -499,6 +615,14 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
     if (e == cudaSuccess) e = cudaMemcpyAsync(ha.data(), alpha, sizeof(double) * NV * ld_a, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return edg::cuda_status(e, "edg_lanczos: coefficients");
+    if (timing) accumulate(m);
+    cudaEvent_t c0 = nullptr, c1 = nullptr;
+    if (timing) {
+      c0 = event_at(3 * L.m_max + 0);
+      c1 = event_at(3 * L.m_max + 1);
+      cudaEventRecord(c0, s);
+    }
+    launches += 1 + NV;
     std::vector<bool> exact(NV, false);
     for (int v = 0; v < NV; ++v) {
       if (m_conv[v]) { m_use[v] = m_conv[v]; continue; }
@@ -513,8 +637,14 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
     if ((st = tridiag_all(m_use))) return st;
     e = cudaMemcpyAsync(hev.data(), tri_eval, sizeof(double) * NV * kMaxK, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(hs.data(), tri_vec, sizeof(double) * NV * kMaxK * ld_s, cudaMemcpyDeviceToHost, s);
+    if (timing && e == cudaSuccess) e = cudaEventRecord(c1, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return edg::cuda_status(e, "edg_lanczos: ritz values");
+    if (timing) {
+      float a = 0.f;
+      cudaEventElapsedTime(&a, c0, c1);
+      t_check += a;
+    }
     bool all = true;
     for (int v = 0; v < NV; ++v) {
       if (m_conv[v]) continue;
@@ -554,13 +684,24 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
     for (int q = 0; q < k; ++q) {
       ritz_k<T, NV><<<g_vec, 256, 0, s>>>(V, n, m_all, tri_vec, kMaxK, q, ld_s, stride_i, w);
       norm_k<NV><<<L.nblk_upd, kThreads, 0, s>>>(w, n, normp);
-      beta_k<NV><<<1, 32, 0, s>>>(normp, L.nblk_upd, h);
+      beta_k<NV><<<1, kThreads, 0, s>>>(normp, L.nblk_upd, h);
       scale_store_k<T, NV><<<g_vec, 256, 0, s>>>(w, n, h, (T*)evecs + (int64_t)q * stride_i);
     }
     if ((e = cudaGetLastError()) != cudaSuccess) return edg::cuda_status(e, "edg_lanczos: ritz vectors");
   }
   e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return edg::cuda_status(e, "edg_lanczos: finish");
+  if (timing) {
+    accumulate(j);
+    launches += 1 + NV + (evecs ? 4 * k : 0);
+    p->stats[0] = t_spmv;
+    p->stats[1] = (double)ev_done;
+    p->stats[2] = t_reorth;
+    p->stats[3] = (double)launches;
+    p->stats[4] = (double)j;
+    p->stats[5] = t_check;
+    for (auto& x : ev) cudaEventDestroy(x);
+  }
   if (status == EDG_ERR_NOT_CONVERGED) edg::set_error("edg_lanczos: not converged in %d steps", L.m_max);
   return status;
 }

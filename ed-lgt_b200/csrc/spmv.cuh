@@ -122,8 +122,9 @@ int launch_spmv_nv(int64_t n, int64_t nnz, const int64_t* rowptr, const int32_t*
                    const SV* diag, const SX* x, SY* y, cudaStream_t s) {
   const int threads = 256;
   int g = spmv_group(n, nnz);
-  int64_t work = n * g;
-  unsigned grid = grid_for(work, threads, 8);
+  // one row per thread group: enough resident groups to hide the gather latency
+  int64_t blocks = ceil_div(n * g, threads);
+  unsigned grid = (unsigned)(blocks < (int64_t)kSmCount * 256 ? blocks : (int64_t)kSmCount * 256);
   switch (g) {
     case 4: spmv_k<SV, SX, SY, NV, 4><<<grid, threads, 0, s>>>(n, rowptr, cols, vals, diag, x, y); break;
     case 8: spmv_k<SV, SX, SY, NV, 8><<<grid, threads, 0, s>>>(n, rowptr, cols, vals, diag, x, y); break;

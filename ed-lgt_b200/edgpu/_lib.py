@@ -125,6 +125,7 @@ class LanczosProblem(C.Structure):
         ("check_every", I32),
         ("seed", U64),
         ("v0", P),
+        ("stats", P),
     ]
 
 

@@ -33,7 +33,7 @@ class LanczosResult:
         self.resid = resid      # (nvec, k)
 
 
-def _problem(dtype, n, nnz, rowptr, cols, vals, diag, nvec, k, max_iter, tol, check_every, seed, v0):
+def _problem(dtype, n, nnz, rowptr, cols, vals, diag, nvec, k, max_iter, tol, check_every, seed, v0, stats=None):
     p = _lib.LanczosProblem()
     p.dtype = dtype
     p.n_rows = n
@@ -49,14 +49,19 @@ def _problem(dtype, n, nnz, rowptr, cols, vals, diag, nvec, k, max_iter, tol, ch
     p.check_every = check_every
     p.seed = seed
     p.v0 = ptr(v0) if v0 is not None else None
+    p.stats = stats.ctypes.data if stats is not None else None
     return p
 
 
 def run_lanczos(dtype, n, nnz, rowptr, cols, vals, diag, nvec=1, k=1, max_iter=300, tol=1e-12, check_every=5,
-                seed=1234, v0=None, want_vectors=True, allow_unconverged=False, workspace=None):
-    """Low-level call of ``edg_lanczos``; ``diag`` is ``[n][nvec]`` in the dtype."""
+                seed=1234, v0=None, want_vectors=True, allow_unconverged=False, workspace=None, stats=None):
+    """Low-level call of ``edg_lanczos``; ``diag`` is ``[n][nvec]`` in the dtype.
+
+    ``stats``: optional float64 numpy array of 6 entries filled with the
+    phase timings of the run (see edg_lanczos_problem.stats).
+    """
     max_iter = int(min(max_iter, n))
-    p = _problem(dtype, n, nnz, rowptr, cols, vals, diag, nvec, k, max_iter, tol, check_every, seed, v0)
+    p = _problem(dtype, n, nnz, rowptr, cols, vals, diag, nvec, k, max_iter, tol, check_every, seed, v0, stats)
     wb = lib.edg_lanczos_workspace_bytes(ctypes.byref(p))
     if wb < 0:
         raise _lib.EdgError(-1, _lib.last_error())
@@ -91,7 +96,7 @@ def stack_diagonals(diags, dtype):
 
 
 def lanczos_mixed(mat, diags=None, k=1, tol32=1e-6, tol=1e-12, max_iter=400, refine_iter=8, check_every=5,
-                  seed=1234):
+                  seed=1234, stats32=None, stats64=None, vals32=None, diag32=None, diag64=None):
     """Mixed-precision (f32 Krylov, f64 recurrence) Lanczos + f64 refinement.
 
     ``diags``: list of f64 device diagonals (one per problem, <= 4) sharing the
@@ -102,14 +107,18 @@ def lanczos_mixed(mat, diags=None, k=1, tol32=1e-6, tol=1e-12, max_iter=400, ref
         raise NotImplementedError("mixed Lanczos needs the real form")
     diags = [mat.diag] if diags is None else list(diags)
     nvec = len(diags)
-    vals32 = mat.vals.to(torch.float32)
-    diag32 = stack_diagonals(diags, torch.float32)
+    if vals32 is None:
+        vals32 = mat.vals.to(torch.float32)
+    if diag32 is None:
+        diag32 = stack_diagonals(diags, torch.float32)
+    if diag64 is None:
+        diag64 = stack_diagonals(diags, torch.float64)
     r32 = run_lanczos(1, mat.n, mat.nnz, mat.rowptr, mat.cols, vals32, diag32, nvec=nvec, k=k, max_iter=max_iter,
-                      tol=tol32, check_every=check_every, seed=seed)
-    diag64 = stack_diagonals(diags, torch.float64)
+                      tol=tol32, check_every=check_every, seed=seed, stats=stats32)
     # f64 refinement: short Lanczos restarted from the f32 Ritz vector (ground state)
-    v0 = r32.evecs[0].to(torch.float64).contiguous()
+    v0 = torch.empty((mat.n, nvec), dtype=torch.float64, device=diag64.device)
+    check(lib.edg_convert(1, ptr(r32.evecs), 0, ptr(v0), mat.n * nvec, stream_handle()), "edg_convert")
     r64 = run_lanczos(0, mat.n, mat.nnz, mat.rowptr, mat.cols, mat.vals, diag64, nvec=nvec, k=1,
                       max_iter=refine_iter, tol=tol, check_every=refine_iter, seed=seed, v0=v0,
-                      allow_unconverged=True)
+                      allow_unconverged=True, stats=stats64)
     return r64, r32

@@ -256,6 +256,10 @@ typedef struct {
   int32_t check_every;    /* steps between convergence checks               */
   uint64_t seed;          /* start vector: uniform(-1,1) from this seed     */
   const void* v0;         /* optional start vectors [n_rows][nvec] or NULL  */
+  double* stats;          /* optional HOST array of 6 doubles, or NULL:     */
+                          /* [0] matvec ms, [1] matvec launches, [2] reorth */
+                          /* ms, [3] kernel launches, [4] Lanczos steps,    */
+                          /* [5] check ms (CUDA events on the stream)       */
 } edg_lanczos_problem;
 
 /* Bytes of device workspace edg_lanczos needs. */
