@@ -9,25 +9,35 @@ namespace {
 
 constexpr int kThreads = 256;
 
+template <int PT>
+__device__ __forceinline__ double prob(const void* psi, int64_t r, int64_t stride) {
+  if (PT == 0) {
+    double a = ((const double*)psi)[r * stride];
+    return a * a;
+  } else if (PT == 1) {
+    double a = ((const float*)psi)[r * stride];
+    return a * a;
+  } else if (PT == 2) {
+    double2 a = ((const double2*)psi)[r * stride];
+    return a.x * a.x + a.y * a.y;
+  } else {
+    float2 a = ((const float2*)psi)[r * stride];
+    return (double)a.x * a.x + (double)a.y * a.y;
+  }
+}
+
+template <int PT>
 __global__ void __launch_bounds__(kThreads) local_expval_k(const uint64_t* __restrict__ keys, int64_t n, int n_sites,
-                                                           edg_site_dims dims, const double* __restrict__ psi,
-                                                           int psi_complex, int64_t psi_stride,
-                                                           const double* __restrict__ diag, int dmax,
-                                                           double* __restrict__ out) {
+                                                           edg_site_dims dims, const void* __restrict__ psi,
+                                                           int64_t psi_stride, const double* __restrict__ diag,
+                                                           int dmax, double* __restrict__ out) {
   __shared__ double acc[EDG_MAX_SITES];
   for (int s = threadIdx.x; s < n_sites; s += kThreads) acc[s] = 0.0;
   __syncthreads();
   double loc[EDG_MAX_SITES];
   for (int s = 0; s < n_sites; ++s) loc[s] = 0.0;
   for (int64_t r = blockIdx.x * (int64_t)kThreads + threadIdx.x; r < n; r += (int64_t)gridDim.x * kThreads) {
-    double p2;
-    if (psi_complex) {
-      double a = psi[2 * r * psi_stride], b = psi[2 * r * psi_stride + 1];
-      p2 = a * a + b * b;
-    } else {
-      double a = psi[r * psi_stride];
-      p2 = a * a;
-    }
+    const double p2 = prob<PT>(psi, r, psi_stride);
     uint64_t k = keys[r];
     for (int s = n_sites - 1; s >= 0; --s) {
       uint64_t d = (uint64_t)dims.d[s];
@@ -48,15 +58,21 @@ __global__ void __launch_bounds__(kThreads) local_expval_k(const uint64_t* __res
 }  // namespace
 
 extern "C" int edg_local_expval(const uint64_t* keys, int64_t n, const edg_site_dims* dims, int32_t n_sites,
-                                const double* psi, int32_t psi_complex, int64_t psi_stride, const double* diag,
+                                const void* psi, int32_t psi_dtype, int64_t psi_stride, const double* diag,
                                 int32_t dmax, double* out, cudaStream_t stream) {
   EDG_REQUIRE(dims != nullptr && n >= 0 && n_sites > 0 && n_sites <= EDG_MAX_SITES && dmax > 0 && psi_stride >= 1,
               "edg_local_expval: bad arguments");
+  EDG_REQUIRE(psi_dtype >= 0 && psi_dtype <= 3, "edg_local_expval: psi_dtype must be 0..3");
   cudaError_t e = cudaMemsetAsync(out, 0, sizeof(double) * n_sites, stream);
   if (e != cudaSuccess) return edg::cuda_status(e, "edg_local_expval: reset");
   if (n == 0) return EDG_OK;
-  local_expval_k<<<edg::grid_for(n, kThreads, 4), kThreads, 0, stream>>>(keys, n, n_sites, *dims, psi, psi_complex,
-                                                                          psi_stride, diag, dmax, out);
+  const unsigned g = edg::grid_for(n, kThreads, 4);
+  switch (psi_dtype) {
+    case 0: local_expval_k<0><<<g, kThreads, 0, stream>>>(keys, n, n_sites, *dims, psi, psi_stride, diag, dmax, out); break;
+    case 1: local_expval_k<1><<<g, kThreads, 0, stream>>>(keys, n, n_sites, *dims, psi, psi_stride, diag, dmax, out); break;
+    case 2: local_expval_k<2><<<g, kThreads, 0, stream>>>(keys, n, n_sites, *dims, psi, psi_stride, diag, dmax, out); break;
+    default: local_expval_k<3><<<g, kThreads, 0, stream>>>(keys, n, n_sites, *dims, psi, psi_stride, diag, dmax, out); break;
+  }
   EDG_CHECK_LAUNCH("edg_local_expval");
   return EDG_OK;
 }

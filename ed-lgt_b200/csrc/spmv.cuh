@@ -50,6 +50,11 @@ struct Store<float2> {
 };
 
 __device__ __forceinline__ void fma_acc(double& a, double v, double x) { a = fma(v, x, a); }
+// real matrix entry times complex vector entry
+__device__ __forceinline__ void fma_acc(cd& a, double v, cd x) {
+  a.re = fma(v, x.re, a.re);
+  a.im = fma(v, x.im, a.im);
+}
 __device__ __forceinline__ void fma_acc(cd& a, cd v, cd x) {
   a.re = fma(v.re, x.re, fma(-v.im, x.im, a.re));
   a.im = fma(v.re, x.im, fma(v.im, x.re, a.im));
@@ -70,13 +75,27 @@ __device__ __forceinline__ void group_reduce(cd& a) {
   }
 }
 
-// SV: matrix value/diag storage, SX: x storage, SY: y storage.
+// SV: matrix value/diag storage, SX: x storage, SY: y storage.  The
+// accumulator is complex when either the matrix or the vector is.
+template <typename SV, typename SX>
+struct AccOf {
+  using type = typename Store<SX>::acc;
+};
+template <>
+struct AccOf<double2, double> {
+  using type = cd;
+};
+template <>
+struct AccOf<float2, float> {
+  using type = cd;
+};
+
 template <typename SV, typename SX, typename SY, int NV, int G>
 __global__ void __launch_bounds__(256) spmv_k(int64_t n, const int64_t* __restrict__ rowptr,
                                               const int32_t* __restrict__ cols, const SV* __restrict__ vals,
                                               const SV* __restrict__ diag, const SX* __restrict__ x,
                                               SY* __restrict__ y) {
-  using A = typename Store<SV>::acc;
+  using A = typename AccOf<SV, SX>::type;
   const int lane = threadIdx.x & (G - 1);
   const int64_t group = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / G;
   const int64_t n_groups = ((int64_t)gridDim.x * blockDim.x) / G;
@@ -91,7 +110,7 @@ __global__ void __launch_bounds__(256) spmv_k(int64_t n, const int64_t* __restri
       const int64_t beg = __ldg(rowptr + r), end = __ldg(rowptr + r + 1);
       for (int64_t p = beg + lane; p < end; p += G) {
         const int64_t c = __ldg(cols + p);
-        const A a = Store<SV>::ld(vals, p);
+        const auto a = Store<SV>::ld(vals, p);
 #pragma unroll
         for (int v = 0; v < NV; ++v) fma_acc(acc[v], a, Store<SX>::ld(x, c * NV + v));
       }

@@ -13,7 +13,7 @@ from pathlib import Path
 from ._build import LIB_PATH
 
 __all__ = ["lib", "check", "EdgError", "MAX_SITES", "MAX_OPS", "SectorTables", "LookupTable", "Assembly",
-           "LanczosProblem", "SiteDims", "EXPORTED_SYMBOLS", "ptr", "stream_handle"]
+           "LanczosProblem", "SiteDims", "KrylovProblem", "EXPORTED_SYMBOLS", "ptr", "stream_handle"]
 
 MAX_SITES = 64
 MAX_OPS = 4
@@ -129,6 +129,21 @@ class LanczosProblem(C.Structure):
     ]
 
 
+class KrylovProblem(C.Structure):
+    _fields_ = [
+        ("vec_dtype", I32),
+        ("mat_dtype", I32),
+        ("n_rows", I64),
+        ("nnz", I64),
+        ("rowptr", P),
+        ("cols", P),
+        ("vals", P),
+        ("diag", P),
+        ("m", I32),
+        ("reorth_passes", I32),
+    ]
+
+
 _SIGS = {
     "edg_get_last_error": (I32, [C.c_char_p, I32]),
     "edg_version": (I32, []),
@@ -150,6 +165,8 @@ _SIGS = {
     "edg_lanczos": (I32, [C.POINTER(LanczosProblem), P, I64, P, P, P, P, P]),
     "edg_tridiag_lowest": (I32, [P, P, I32, I32, P, P, P, P]),
     "edg_local_expval": (I32, [P, I64, C.POINTER(SiteDims), I32, P, I32, I64, P, I32, P, P]),
+    "edg_krylov_workspace_bytes": (I64, [C.POINTER(KrylovProblem)]),
+    "edg_krylov_step": (I32, [C.POINTER(KrylovProblem), P, F64, P, I64, P, P]),
 }
 
 EXPORTED_SYMBOLS = tuple(_SIGS)

@@ -170,7 +170,7 @@ class QMB_hamiltonian:
 
     # ------------------------------------------------------- time evolution
     def time_evolution(self, initial_state, time_line, loc_dims=None, m_krylov=30, precision="c128",
-                       observables=None):
+                       observables=None, reorth_passes=1):
         from ..dynamics import krylov_evolve
 
         if self.mat is None:
@@ -179,8 +179,11 @@ class QMB_hamiltonian:
         psi0 = initial_state if isinstance(initial_state, torch.Tensor) else torch.from_numpy(
             np.asarray(initial_state, dtype=np.complex128)).to(self.sector.device)
         psi0 = self.from_original_basis(psi0)
+        obs = None
+        if observables is not None:
+            obs = {name: (self.sector, op) for name, op in observables.items()}
         states = krylov_evolve(self.mat, psi0, np.asarray(time_line, dtype=float), m=m_krylov, precision=precision,
-                               keep_states=observables is None, observables=observables)
+                               keep_states=observables is None, observables=obs, reorth_passes=reorth_passes)
         if observables is None:
             self.psi_time = [QMB_state(self.to_original_basis(s), self.lvals, loc_dims) for s in states]
         else:

@@ -32,6 +32,31 @@ logger = logging.getLogger(__name__)
 __all__ = ["QuantumModel"]
 
 
+_DIAG_CACHE = {}
+
+
+def site_expval_device(sector, op, psi, out=None):
+    """Device vector of <psi| op_s |psi> over sites (op diagonal only)."""
+    key = (id(op), sector.device)
+    if key not in _DIAG_CACHE:
+        diag = np.real(np.array([np.diagonal(op[s]) for s in range(op.shape[0])])).astype(np.float64)
+        _DIAG_CACHE[key] = (op, torch.from_numpy(np.ascontiguousarray(diag)).to(sector.device))
+    dd = _DIAG_CACHE[key][1]
+    codes = {torch.float64: 0, torch.float32: 1, torch.complex128: 2, torch.complex64: 3}
+    if psi.dtype not in codes:
+        psi = psi.to(torch.complex128)
+    p = psi.contiguous()
+    n_sites = sector.n_sites
+    if out is None:
+        out = torch.empty(n_sites, dtype=torch.float64, device=sector.device)
+    dims = _lib.SiteDims()
+    for s in range(n_sites):
+        dims.d[s] = int(sector.loc_dims[s])
+    check(lib.edg_local_expval(ptr(sector.keys), len(sector), ctypes.byref(dims), n_sites, ptr(p), codes[p.dtype], 1,
+                               ptr(dd), dd.shape[1], ptr(out), stream_handle()), "edg_local_expval")
+    return out
+
+
 class QuantumModel:
     def __init__(self, lvals, has_obc, ham_format="gpu", basis_projector=None, device=None):
         self.lvals = list(lvals)
@@ -196,26 +221,11 @@ class QuantumModel:
     # ------------------------------------------------------- observables
     def local_expval(self, op, psi) -> np.ndarray:
         """<psi| op_s |psi> for every site (diagonal of op, as LocalTerm)."""
-        diag = np.real(np.array([np.diagonal(op[s]) for s in range(self.n_sites)])).astype(np.float64)
-        dmax = diag.shape[1]
-        dd = torch.from_numpy(np.ascontiguousarray(diag)).to(self.device)
         if isinstance(psi, QMB_state):
             psi = psi.device(self.device)
         elif not isinstance(psi, torch.Tensor):
             psi = torch.from_numpy(np.asarray(psi)).to(self.device)
-        if psi.is_complex():
-            p = torch.view_as_real(psi.to(torch.complex128).contiguous())
-            cpx = 1
-        else:
-            p = psi.to(torch.float64).contiguous()
-            cpx = 0
-        out = torch.empty(self.n_sites, dtype=torch.float64, device=self.device)
-        dims = _lib.SiteDims()
-        for s in range(self.n_sites):
-            dims.d[s] = int(self.loc_dims[s])
-        check(lib.edg_local_expval(ptr(self.sector.keys), len(self.sector), ctypes.byref(dims), self.n_sites, ptr(p),
-                                   cpx, 1, ptr(dd), dmax, ptr(out), stream_handle()), "edg_local_expval")
-        return out.cpu().numpy()
+        return site_expval_device(self.sector, op, psi).cpu().numpy()
 
     def get_observables(self, local_obs=(), twobody_obs=(), plaquette_obs=(), nbody_obs=(), nbody_dist=(),
                         twobody_axes=None):

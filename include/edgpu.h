@@ -280,6 +280,36 @@ int edg_tridiag_lowest(const double* alpha, const double* beta, int32_t m,
                        cudaStream_t stream);
 
 /* ------------------------------------------------------------------------ */
+/* Krylov time evolution psi <- exp(-i H dt) psi                             */
+/* Replaces scipy.sparse.linalg.expm_multiply(-iH, psi0, ...) as called from */
+/* QMB_hamiltonian.time_evolution (edlgt/modeling/qmb_hamiltonian.py:        */
+/* 334-426).  Krylov vectors complex128 or complex64, Lanczos recurrence and  */
+/* the small exponential in f64; no host synchronisation inside a step       */
+/* unless err_out is given.                                                  */
+/* ------------------------------------------------------------------------ */
+
+typedef struct {
+  int32_t vec_dtype;      /* 2 complex128, 3 complex64 (psi and the basis) */
+  int32_t mat_dtype;      /* 0 f64, 1 f32 (real form), 2 c128, 3 c64; same  */
+                          /* precision as the vectors                       */
+  int64_t n_rows;
+  int64_t nnz;
+  const int64_t* rowptr;
+  const int32_t* cols;
+  const void* vals;
+  const void* diag;       /* [n_rows]                                       */
+  int32_t m;              /* Krylov dimension, <= 64                        */
+  int32_t reorth_passes;  /* 0 local recurrence, 1 or 2 full Gram-Schmidt   */
+} edg_krylov_problem;
+
+int64_t edg_krylov_workspace_bytes(const edg_krylov_problem* p);
+/* One step of length dt in place on psi [n_rows] (complex, vec_dtype).
+ * err_out (host, may be NULL): a posteriori error estimate of the step. */
+int edg_krylov_step(const edg_krylov_problem* p, void* psi, double dt,
+                    void* workspace, int64_t workspace_bytes, double* err_out,
+                    cudaStream_t stream);
+
+/* ------------------------------------------------------------------------ */
 /* Local (diagonal) observables                                              */
 /* Replaces LocalTerm.get_expval in a symmetry sector (edlgt/modeling/       */
 /* local_term.py:119-237, exp_val_data edlgt/modeling/qmb_state.py:631-654): */
@@ -290,10 +320,10 @@ typedef struct {
   int32_t d[EDG_MAX_SITES];   /* local dimension per site (by value)        */
 } edg_site_dims;
 
-/* psi: f64 (psi_complex = 0) or interleaved complex128 (1), element r at
+/* psi: dtype 0 f64, 1 f32, 2 complex128, 3 complex64, element r at
  * psi[r * psi_stride]; diag: [n_sites][dmax] f64; out: [n_sites] f64. */
 int edg_local_expval(const uint64_t* keys, int64_t n, const edg_site_dims* dims,
-                     int32_t n_sites, const double* psi, int32_t psi_complex,
+                     int32_t n_sites, const void* psi, int32_t psi_dtype,
                      int64_t psi_stride, const double* diag, int32_t dmax,
                      double* out, cudaStream_t stream);
 
