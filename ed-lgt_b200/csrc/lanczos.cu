@@ -14,6 +14,7 @@
 #include "spmv.cuh"
 
 #include <cmath>
+#include <mutex>
 #include <vector>
 
 namespace {
@@ -757,5 +758,61 @@ extern "C" int edg_tridiag_lowest(const double* alpha, const double* beta, int32
   EDG_REQUIRE(alpha && beta && evals && work, "edg_tridiag_lowest: null pointer");
   tridiag_k<<<1, kThreads, 0, stream>>>(alpha, m, beta, m, m, k, evals, evecs, m, work, 6 * m);
   EDG_CHECK_LAUNCH("edg_tridiag_lowest");
+  return EDG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of edg_tridiag_lowest.
+//
+// For callers that cannot call cudaMalloc (for example code running inside a
+// host callback, a memory-capped plugin host, or a language runtime without a
+// device allocator): the 6*m doubles of scratch live in a file-scope device
+// array of fixed size, so the call allocates nothing.  Every GPU that loads
+// the library holds this array (6 * 4096 doubles = 192 KiB) until exit.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int kNoAllocMaxM = 4096;
+static __device__ __align__(256) double g_tridiag_scratch[6 * kNoAllocMaxM];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_scratch_mu;
+double* g_scratch_ptr[kMaxDevices] = {nullptr};
+
+// Device address of g_tridiag_scratch on the current device.  The host-side
+// symbol is only a stand-in for the device array: it must not be passed to a
+// kernel, so the address is looked up once per device with that device current.
+int scratch_address(double** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return edg::cuda_status(e, "edg_tridiag_lowest_noalloc: current device");
+  EDG_REQUIRE(dev >= 0 && dev < kMaxDevices, "edg_tridiag_lowest_noalloc: device index %d out of range", dev);
+  std::lock_guard<std::mutex> lock(g_scratch_mu);
+  if (g_scratch_ptr[dev] == nullptr) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_tridiag_scratch);
+    if (e != cudaSuccess) return edg::cuda_status(e, "edg_tridiag_lowest_noalloc: cudaGetSymbolAddress");
+    g_scratch_ptr[dev] = (double*)p;
+  }
+  *out = g_scratch_ptr[dev];
+  return EDG_OK;
+}
+
+}  // namespace
+
+extern "C" int edg_tridiag_lowest_noalloc(const double* alpha, const double* beta, int32_t m, int32_t k,
+                                          double* evals, double* evecs, cudaStream_t stream) {
+  EDG_REQUIRE(m >= 1 && k >= 1 && k <= m && k <= kMaxK, "edg_tridiag_lowest_noalloc: need 1 <= k <= min(m, %d)",
+              kMaxK);
+  EDG_REQUIRE(m <= kNoAllocMaxM, "edg_tridiag_lowest_noalloc: m = %d exceeds the static scratch limit of %d", m,
+              kNoAllocMaxM);
+  EDG_REQUIRE(alpha && beta && evals, "edg_tridiag_lowest_noalloc: null pointer");
+  double* work = nullptr;
+  int st = scratch_address(&work);
+  if (st) return st;
+  // tridiag_k writes every scratch element before reading it, so the array
+  // needs no clearing between calls.
+  tridiag_k<<<1, kThreads, 0, stream>>>(alpha, m, beta, m, m, k, evals, evecs, m, work, 6 * m);
+  EDG_CHECK_LAUNCH("edg_tridiag_lowest_noalloc");
   return EDG_OK;
 }

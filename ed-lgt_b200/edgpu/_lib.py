@@ -164,6 +164,7 @@ _SIGS = {
     "edg_lanczos_workspace_bytes": (I64, [C.POINTER(LanczosProblem)]),
     "edg_lanczos": (I32, [C.POINTER(LanczosProblem), P, I64, P, P, P, P, P]),
     "edg_tridiag_lowest": (I32, [P, P, I32, I32, P, P, P, P]),
+    "edg_tridiag_lowest_noalloc": (I32, [P, P, I32, I32, P, P, P]),
     "edg_local_expval": (I32, [P, I64, C.POINTER(SiteDims), I32, P, I32, I64, P, I32, P, P]),
     "edg_krylov_workspace_bytes": (I64, [C.POINTER(KrylovProblem)]),
     "edg_krylov_step": (I32, [C.POINTER(KrylovProblem), P, F64, P, I64, P, P]),

@@ -279,6 +279,20 @@ int edg_tridiag_lowest(const double* alpha, const double* beta, int32_t m,
                        int32_t k, double* evals, double* evecs, double* work,
                        cudaStream_t stream);
 
+/* Same as edg_tridiag_lowest, for callers that cannot allocate device memory
+ * (code running where cudaMalloc is unavailable or forbidden, e.g. inside a
+ * host callback or a memory-capped plugin host).  No counterpart in the
+ * reference.  The 6*m doubles of scratch come from a static device array
+ * compiled into the library, so m is limited to 4096 (larger m returns
+ * EDG_ERR_ARG) and the call allocates nothing.  The first call on a device
+ * looks up the array's device address (with that device current); make that
+ * first call before any stream capture.  All calls share the one array:
+ * calls that overlap on the GPU race, so serialise them (one stream, or
+ * events).  Inputs and outputs are caller-owned device pointers. */
+int edg_tridiag_lowest_noalloc(const double* alpha, const double* beta,
+                               int32_t m, int32_t k, double* evals,
+                               double* evecs, cudaStream_t stream);
+
 /* ------------------------------------------------------------------------ */
 /* Krylov time evolution psi <- exp(-i H dt) psi                             */
 /* Replaces scipy.sparse.linalg.expm_multiply(-iH, psi0, ...) as called from */
