@@ -320,7 +320,7 @@ int run_step(const edg_krylov_problem* p, T* psi, double dt, char* ws, double* e
   for (int j = 0; j < m; ++j) {
     const T* vj = V + (int64_t)j * n;
     int st = edg::launch_spmv<SV, T, double2>(1, n, p->nnz, p->rowptr, p->cols, (const SV*)p->vals,
-                                              (const SV*)p->diag, vj, w, s);
+                                              (const SV*)p->diag, vj, w, s, 0, p->spmv_group);
     if (st) return st;
     // reorth_passes = 0: local recurrence (against v_{j-1}, v_j only);
     // 1 or 2: classical Gram-Schmidt over the whole basis, once or twice

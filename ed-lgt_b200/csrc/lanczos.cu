@@ -12,6 +12,7 @@
 // computed on the device (multisection + inverse iteration) and the residual
 // bound |beta_{j+1} s_{j}| is compared with tol * max(1, |theta|).
 #include "spmv.cuh"
+#include "tridiag.cuh"
 
 #include <cmath>
 #include <mutex>
@@ -19,6 +20,7 @@
 
 namespace {
 
+using edg::tridiag_body;
 constexpr int kThreads = 256;
 constexpr int kItile = 8;  // Krylov vectors per reduction tile
 constexpr int kMaxK = 16;
@@ -33,20 +35,41 @@ __device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
 template <typename T>
 __device__ __forceinline__ double ldv(const T* p, int64_t i) { return (double)p[i]; }
 
-// w = uniform(-1, 1) or w = v0
-template <typename T>
-__global__ void start_k(int64_t len, uint64_t seed, const T* __restrict__ v0, double* __restrict__ w) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < len; i += (int64_t)gridDim.x * blockDim.x) {
-    if (v0) {
-      w[i] = (double)v0[i];
-    } else {
-      uint64_t r = splitmix64(seed ^ splitmix64((uint64_t)i));
-      w[i] = ((double)(r >> 11) * (1.0 / 9007199254740992.0)) * 2.0 - 1.0;
+// Four consecutive Krylov entries (16-byte aligned: planes are padded to 4 rows).
+__device__ __forceinline__ void ld4(const float* p, double* out) {
+  float4 v = *reinterpret_cast<const float4*>(p);
+  out[0] = v.x; out[1] = v.y; out[2] = v.z; out[3] = v.w;
+}
+__device__ __forceinline__ void ld4(const double* p, double* out) {
+  double2 a = *reinterpret_cast<const double2*>(p);
+  double2 b = *reinterpret_cast<const double2*>(p + 2);
+  out[0] = a.x; out[1] = a.y; out[2] = b.x; out[3] = b.y;
+}
+__device__ __forceinline__ void st4(double* p, const double* v) {
+  *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
+  *reinterpret_cast<double2*>(p + 2) = make_double2(v[2], v[3]);
+}
+
+// w (planar [NV][n_pad]) = uniform(-1, 1) or the interleaved start vectors v0
+template <typename T, int NV>
+__global__ void start_k(int64_t n, int64_t n_pad, uint64_t seed, const T* __restrict__ v0, double* __restrict__ w) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n_pad * NV; i += (int64_t)gridDim.x * blockDim.x) {
+    const int v = (int)(i / n_pad);
+    const int64_t r = i - v * n_pad;
+    double x = 0.0;
+    if (r < n) {
+      if (v0) {
+        x = (double)v0[r * NV + v];
+      } else {
+        uint64_t z = splitmix64(seed ^ splitmix64((uint64_t)(r * NV + v)));
+        x = ((double)(z >> 11) * (1.0 / 9007199254740992.0)) * 2.0 - 1.0;
+      }
     }
+    w[i] = x;
   }
 }
 
-// Block-reduces NV doubles per thread; thread 0 gets the totals in out[].
+// Block-reduces NV doubles per thread; threads < NV get the totals in vals[tid].
 template <int NV>
 __device__ __forceinline__ void block_sum(double* vals, double* smem /*[kThreads/32][NV]*/) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -61,67 +84,63 @@ __device__ __forceinline__ void block_sum(double* vals, double* smem /*[kThreads
   if (threadIdx.x < NV) {
     double a = 0.0;
     for (int wi = 0; wi < kThreads / 32; ++wi) a += smem[wi * NV + threadIdx.x];
-    vals[threadIdx.x] = a;  // only meaningful in threads < NV
+    vals[threadIdx.x] = a;
   }
   __syncthreads();
 }
 
-// partial[b][i][v] = sum over the rows of block b of V[i][r][v] * w[r][v], i <= j.
+// partial[bx][i][v] = sum over the rows of chunk bx of V[i][v][r] w[v][r], for
+// the Krylov tile i in [blockIdx.y*kItile, ...] (i <= j).  Rows are read in
+// quads (16-byte loads); blockIdx.x strides over row chunks.
 template <typename T, int NV>
-__global__ void __launch_bounds__(kThreads) dots_k(const T* __restrict__ V, int64_t n, int j,
+__global__ void __launch_bounds__(kThreads, 4) dots_k(const T* __restrict__ V, int64_t n_pad, int j,
                                                    const double* __restrict__ w, double* __restrict__ partial,
-                                                   int ld_i, int64_t stride_i /* entries per Krylov vector */) {
-  __shared__ double red[(kThreads / 32) * kItile * NV];
-  __shared__ double out[kItile * NV];
-  const int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
-  const int64_t r0 = blockIdx.x * chunk;
-  const int64_t r1 = min(n, r0 + chunk);
+                                                   int ld_i, int64_t stride_i) {
+  __shared__ double red[(kThreads / 32) * kItile];
+  const int i0 = blockIdx.y * kItile;
+  const int nt = min(kItile, j + 1 - i0);
+  const int64_t nq = n_pad / 4;
+  const int64_t cq = (nq + gridDim.x - 1) / gridDim.x;
+  const int64_t q0 = blockIdx.x * cq, q1 = min(nq, q0 + cq);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int i0 = 0; i0 <= j; i0 += kItile) {
-    double acc[kItile][NV];
+#pragma unroll 1
+  for (int v = 0; v < NV; ++v) {
+    double acc[kItile];
 #pragma unroll
-    for (int t = 0; t < kItile; ++t)
-#pragma unroll
-      for (int v = 0; v < NV; ++v) acc[t][v] = 0.0;
-    for (int64_t r = r0 + threadIdx.x; r < r1; r += kThreads) {
-      double wr[NV];
-#pragma unroll
-      for (int v = 0; v < NV; ++v) wr[v] = w[r * NV + v];
+    for (int t = 0; t < kItile; ++t) acc[t] = 0.0;
+    const double* wv = w + (int64_t)v * n_pad;
+    const T* Vv = V + (int64_t)i0 * stride_i + (int64_t)v * n_pad;
+    for (int64_t q = q0 + threadIdx.x; q < q1; q += kThreads) {
+      double w4[4];
+      ld4(wv + 4 * q, w4);
 #pragma unroll
       for (int t = 0; t < kItile; ++t) {
-        if (i0 + t <= j) {
-          const T* Vi = V + (int64_t)(i0 + t) * stride_i + r * NV;
-#pragma unroll
-          for (int v = 0; v < NV; ++v) acc[t][v] = fma(ldv(Vi, v), wr[v], acc[t][v]);
+        if (t < nt) {
+          double x4[4];
+          ld4(Vv + (int64_t)t * stride_i + 4 * q, x4);
+          acc[t] = fma(x4[0], w4[0], fma(x4[1], w4[1], fma(x4[2], w4[2], fma(x4[3], w4[3], acc[t]))));
         }
       }
     }
 #pragma unroll
-    for (int t = 0; t < kItile; ++t)
+    for (int t = 0; t < kItile; ++t) {
+      double a = acc[t];
 #pragma unroll
-      for (int v = 0; v < NV; ++v) {
-        double a = acc[t][v];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
-        if (lane == 0) red[(warp * kItile + t) * NV + v] = a;
-      }
-    __syncthreads();
-    if (threadIdx.x < kItile * NV) {
-      double a = 0.0;
-      for (int wi = 0; wi < kThreads / 32; ++wi) a += red[wi * kItile * NV + threadIdx.x];
-      out[threadIdx.x] = a;
+      for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+      if (lane == 0) red[warp * kItile + t] = a;
     }
     __syncthreads();
-    if (threadIdx.x < kItile * NV) {
-      int t = threadIdx.x / NV, v = threadIdx.x % NV;
-      if (i0 + t <= j) partial[((int64_t)blockIdx.x * ld_i + (i0 + t)) * NV + v] = out[threadIdx.x];
+    if (threadIdx.x < nt) {
+      double a = 0.0;
+      for (int wi = 0; wi < kThreads / 32; ++wi) a += red[wi * kItile + threadIdx.x];
+      partial[((int64_t)blockIdx.x * ld_i + i0 + threadIdx.x) * NV + v] = a;
     }
     __syncthreads();
   }
 }
 
-// h[i][v] = sum_b partial[b][i][v] (one CTA per Krylov index i, fixed summation
-// order); alpha accumulates h[j].
+// h[i][v] = sum_b partial[b][i][v] (one CTA per Krylov index i, fixed order);
+// alpha accumulates h[j].
 template <int NV>
 __global__ void __launch_bounds__(kThreads) reduce_h_k(const double* __restrict__ partial, int nblocks, int ld_i,
                                                        int j, double* __restrict__ h, double* __restrict__ alpha_j) {
@@ -140,85 +159,12 @@ __global__ void __launch_bounds__(kThreads) reduce_h_k(const double* __restrict_
   }
 }
 
-// Pass 1 update fused with pass 2 inner products:
-//   w[r] -= sum_i V[i][r] h[i] ;  partial[b][i] = sum_{r in block b} V[i][r] w[r]
-// Each CTA owns a contiguous row chunk; the Krylov entries of a row tile are
-// read once for the update and then again (from L1) for the new dots.
+// w[v][r] -= sum_{i<=j} V[i][v][r] h[i][v] over row quads; block partials of
+// |w_v|^2 (padding rows are zero in V and w and stay zero).
 template <typename T, int NV>
-__global__ void __launch_bounds__(kThreads) update_dots_k(const T* __restrict__ V, int64_t n, int j,
-                                                          const double* __restrict__ h, double* __restrict__ w,
-                                                          double* __restrict__ partial, int ld_i, int64_t stride_i) {
-  extern __shared__ double hs[];  // [(j+1)][NV]
-  __shared__ double red[(kThreads / 32) * kItile * NV];
-  __shared__ double out[kItile * NV];
-  for (int t = threadIdx.x; t < (j + 1) * NV; t += kThreads) hs[t] = h[t];
-  __syncthreads();
-  const int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
-  const int64_t r0 = blockIdx.x * chunk;
-  const int64_t r1 = min(n, r0 + chunk);
-  // update all rows of the chunk first (each thread its own rows)
-  for (int64_t r = r0 + threadIdx.x; r < r1; r += kThreads) {
-    double s[NV];
-#pragma unroll
-    for (int v = 0; v < NV; ++v) s[v] = 0.0;
-    for (int i = 0; i <= j; ++i) {
-      const T* Vi = V + (int64_t)i * stride_i + r * NV;
-#pragma unroll
-      for (int v = 0; v < NV; ++v) s[v] = fma(ldv(Vi, v), hs[i * NV + v], s[v]);
-    }
-#pragma unroll
-    for (int v = 0; v < NV; ++v) w[r * NV + v] -= s[v];
-  }
-  // the same thread re-reads the rows it updated: no barrier needed for w
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int i0 = 0; i0 <= j; i0 += kItile) {
-    double acc[kItile][NV];
-#pragma unroll
-    for (int t = 0; t < kItile; ++t)
-#pragma unroll
-      for (int v = 0; v < NV; ++v) acc[t][v] = 0.0;
-    for (int64_t r = r0 + threadIdx.x; r < r1; r += kThreads) {
-      double wr[NV];
-#pragma unroll
-      for (int v = 0; v < NV; ++v) wr[v] = w[r * NV + v];
-#pragma unroll
-      for (int t = 0; t < kItile; ++t) {
-        if (i0 + t <= j) {
-          const T* Vi = V + (int64_t)(i0 + t) * stride_i + r * NV;
-#pragma unroll
-          for (int v = 0; v < NV; ++v) acc[t][v] = fma(ldv(Vi, v), wr[v], acc[t][v]);
-        }
-      }
-    }
-#pragma unroll
-    for (int t = 0; t < kItile; ++t)
-#pragma unroll
-      for (int v = 0; v < NV; ++v) {
-        double a = acc[t][v];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
-        if (lane == 0) red[(warp * kItile + t) * NV + v] = a;
-      }
-    __syncthreads();
-    if (threadIdx.x < kItile * NV) {
-      double a = 0.0;
-      for (int wi = 0; wi < kThreads / 32; ++wi) a += red[wi * kItile * NV + threadIdx.x];
-      out[threadIdx.x] = a;
-    }
-    __syncthreads();
-    if (threadIdx.x < kItile * NV) {
-      int t = threadIdx.x / NV, v = threadIdx.x % NV;
-      if (i0 + t <= j) partial[((int64_t)blockIdx.x * ld_i + (i0 + t)) * NV + v] = out[threadIdx.x];
-    }
-    __syncthreads();
-  }
-}
-
-// w[r][v] -= sum_i V[i][r][v] h[i][v]; block partial of |w|^2 per vector.
-template <typename T, int NV>
-__global__ void __launch_bounds__(kThreads) update_k(const T* __restrict__ V, int64_t n, int j, const double* __restrict__ h,
-                                                     double* __restrict__ w, double* __restrict__ norm_partial,
-                                                     int64_t stride_i) {
+__global__ void __launch_bounds__(kThreads) update_k(const T* __restrict__ V, int64_t n_pad, int j,
+                                                     const double* __restrict__ h, double* __restrict__ w,
+                                                     double* __restrict__ norm_partial, int64_t stride_i) {
   extern __shared__ double hs[];  // [(j+1)][NV]
   __shared__ double red[(kThreads / 32) * NV];
   for (int t = threadIdx.x; t < (j + 1) * NV; t += kThreads) hs[t] = h[t];
@@ -226,36 +172,60 @@ __global__ void __launch_bounds__(kThreads) update_k(const T* __restrict__ V, in
   double nrm[NV];
 #pragma unroll
   for (int v = 0; v < NV; ++v) nrm[v] = 0.0;
-  for (int64_t r = blockIdx.x * (int64_t)kThreads + threadIdx.x; r < n; r += (int64_t)gridDim.x * kThreads) {
-    double s[NV];
+  const int64_t nq = n_pad / 4;
+  for (int64_t g = blockIdx.x * (int64_t)kThreads + threadIdx.x; g < nq * NV; g += (int64_t)gridDim.x * kThreads) {
+    const int v = (int)(g / nq);
+    const int64_t q = g - v * nq;
+    const T* Vp = V + (int64_t)v * n_pad + 4 * q;
+    double s[4] = {0.0, 0.0, 0.0, 0.0};
+    int i = 0;
+    for (; i + 1 <= j; i += 2) {
+      double a4[4], b4[4];
+      ld4(Vp + (int64_t)i * stride_i, a4);
+      ld4(Vp + (int64_t)(i + 1) * stride_i, b4);
+      const double ha = hs[i * NV + v], hb = hs[(i + 1) * NV + v];
 #pragma unroll
-    for (int v = 0; v < NV; ++v) s[v] = 0.0;
-    for (int i = 0; i <= j; ++i) {
-      const T* Vi = V + (int64_t)i * stride_i + r * NV;
-#pragma unroll
-      for (int v = 0; v < NV; ++v) s[v] = fma(ldv(Vi, v), hs[i * NV + v], s[v]);
+      for (int k = 0; k < 4; ++k) s[k] = fma(a4[k], ha, fma(b4[k], hb, s[k]));
     }
+    for (; i <= j; ++i) {
+      double a4[4];
+      ld4(Vp + (int64_t)i * stride_i, a4);
+      const double ha = hs[i * NV + v];
 #pragma unroll
-    for (int v = 0; v < NV; ++v) {
-      double x = w[r * NV + v] - s[v];
-      w[r * NV + v] = x;
-      nrm[v] = fma(x, x, nrm[v]);
+      for (int k = 0; k < 4; ++k) s[k] = fma(a4[k], ha, s[k]);
     }
+    double* wp = w + (int64_t)v * n_pad + 4 * q;
+    double w4[4];
+    ld4(wp, w4);
+    double sq = 0.0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      w4[k] -= s[k];
+      sq = fma(w4[k], w4[k], sq);
+    }
+    st4(wp, w4);
+#pragma unroll
+    for (int vv = 0; vv < NV; ++vv)
+      if (vv == v) nrm[vv] += sq;
   }
   block_sum<NV>(nrm, red);
   if (threadIdx.x < NV) norm_partial[blockIdx.x * NV + threadIdx.x] = nrm[threadIdx.x];
 }
 
-// |w|^2 block partials (start vector)
+// |w_v|^2 block partials (planar w)
 template <int NV>
-__global__ void __launch_bounds__(kThreads) norm_k(const double* __restrict__ w, int64_t n, double* __restrict__ norm_partial) {
+__global__ void __launch_bounds__(kThreads) norm_k(const double* __restrict__ w, int64_t n_pad,
+                                                   double* __restrict__ norm_partial) {
   __shared__ double red[(kThreads / 32) * NV];
   double nrm[NV];
 #pragma unroll
   for (int v = 0; v < NV; ++v) nrm[v] = 0.0;
-  for (int64_t r = blockIdx.x * (int64_t)kThreads + threadIdx.x; r < n; r += (int64_t)gridDim.x * kThreads)
+  for (int64_t r = blockIdx.x * (int64_t)kThreads + threadIdx.x; r < n_pad; r += (int64_t)gridDim.x * kThreads)
 #pragma unroll
-    for (int v = 0; v < NV; ++v) nrm[v] = fma(w[r * NV + v], w[r * NV + v], nrm[v]);
+    for (int v = 0; v < NV; ++v) {
+      const double x = w[(int64_t)v * n_pad + r];
+      nrm[v] = fma(x, x, nrm[v]);
+    }
   block_sum<NV>(nrm, red);
   if (threadIdx.x < NV) norm_partial[blockIdx.x * NV + threadIdx.x] = nrm[threadIdx.x];
 }
@@ -275,193 +245,47 @@ __global__ void __launch_bounds__(kThreads) beta_k(const double* __restrict__ no
   if (threadIdx.x < NV) beta[threadIdx.x] = sqrt(a[threadIdx.x]);
 }
 
-// V[j+1] = w / beta (beta = 0 leaves a zero vector: invariant subspace)
+// v = w / beta (beta = 0 leaves a zero vector: invariant subspace), written to
+// the planar Krylov slot (may be null) and to the interleaved matvec input X
+// (may be null).
 template <typename T, int NV>
-__global__ void scale_store_k(const double* __restrict__ w, int64_t n, const double* __restrict__ beta,
-                              T* __restrict__ out) {
+__global__ void scale_store_k(const double* __restrict__ w, int64_t n, int64_t n_pad, const double* __restrict__ beta,
+                              T* __restrict__ plane, T* __restrict__ X) {
   double inv[NV];
 #pragma unroll
   for (int v = 0; v < NV; ++v) inv[v] = beta[v] > 0.0 ? 1.0 / beta[v] : 0.0;
-  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x)
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n_pad; r += (int64_t)gridDim.x * blockDim.x) {
 #pragma unroll
-    for (int v = 0; v < NV; ++v) out[r * NV + v] = (T)(w[r * NV + v] * inv[v]);
+    for (int v = 0; v < NV; ++v) {
+      const T x = (T)(w[(int64_t)v * n_pad + r] * inv[v]);
+      if (plane) plane[(int64_t)v * n_pad + r] = x;
+      if (X && r < n) X[r * NV + v] = x;
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------
 // Tridiagonal eigen-solve (one CTA per problem)
 // ---------------------------------------------------------------------------
-__device__ int sturm_count(const double* a, const double* b2, int m, double x, double pivmin) {
-  int cnt = 0;
-  double q = a[0] - x;
-  if (fabs(q) < pivmin) q = -pivmin;
-  cnt += q < 0.0;
-  for (int i = 1; i < m; ++i) {
-    q = a[i] - x - b2[i] / q;
-    if (fabs(q) < pivmin) q = -pivmin;
-    cnt += q < 0.0;
-  }
-  return cnt;
-}
-
-// alpha: [m] ; beta: [m] with beta[i] coupling i-1 and i (beta[0] unused);
-// stride between problems given by lda (alpha) / ldb (beta) in doubles.
 __global__ void __launch_bounds__(kThreads) tridiag_k(const double* __restrict__ alpha, int lda,
                                                       const double* __restrict__ beta, int ldb, int m, int k,
                                                       double* __restrict__ evals, double* __restrict__ evecs,
                                                       int ldv, double* __restrict__ work, int ldw) {
   const int prob = blockIdx.x;
-  const double* a = alpha + (int64_t)prob * lda;
-  const double* bb = beta + (int64_t)prob * ldb;
-  double* wk = work + (int64_t)prob * ldw;  // [m] b^2, then scratch for inverse iteration
-  double* b2 = wk;
-  __shared__ double lo_s, hi_s, xs[kThreads + 1];
-  __shared__ int cnt_s[kThreads + 1];
-  __shared__ double gl_s, gu_s, pivmin_s;
-  for (int i = threadIdx.x; i < m; i += kThreads) b2[i] = i == 0 ? 0.0 : bb[i] * bb[i];
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double gl = 1e300, gu = -1e300, bmax = 0.0;
-    for (int i = 0; i < m; ++i) {
-      double off = (i > 0 ? fabs(bb[i]) : 0.0) + (i + 1 < m ? fabs(bb[i + 1]) : 0.0);
-      gl = fmin(gl, a[i] - off);
-      gu = fmax(gu, a[i] + off);
-      if (i > 0) bmax = fmax(bmax, b2[i]);
-    }
-    double span = fmax(fabs(gl), fabs(gu));
-    gl_s = gl - 2.0 * span * 1e-15 - 1e-300;
-    gu_s = gu + 2.0 * span * 1e-15 + 1e-300;
-    pivmin_s = fmax(1e-290, 2.2e-308 * fmax(1.0, bmax));
-  }
-  __syncthreads();
-  for (int e = 0; e < k && e < m; ++e) {
-    if (threadIdx.x == 0) {
-      lo_s = gl_s;
-      hi_s = gu_s;
-    }
-    __syncthreads();
-    for (int round = 0; round < 12; ++round) {
-      double lo = lo_s, hi = hi_s;
-      if (!(hi - lo > 2.2e-16 * fmax(fabs(lo), fabs(hi)) + 1e-300)) break;
-      // kThreads interior points; count(x) = #eigenvalues < x
-      double x = lo + (hi - lo) * (double)(threadIdx.x + 1) / (double)(kThreads + 1);
-      xs[threadIdx.x] = x;
-      cnt_s[threadIdx.x] = sturm_count(a, b2, m, x, pivmin_s);
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        // first point with count >= e+1 bounds eigenvalue e from above
-        double nlo = lo, nhi = hi;
-        for (int t = 0; t < kThreads; ++t) {
-          if (cnt_s[t] >= e + 1) {
-            nhi = xs[t];
-            break;
-          }
-          nlo = xs[t];
-        }
-        lo_s = nlo;
-        hi_s = nhi;
-      }
-      __syncthreads();
-    }
-    if (threadIdx.x == 0) evals[(int64_t)prob * k + e] = 0.5 * (lo_s + hi_s);
-    __syncthreads();
-  }
-  // inverse iteration for eigenvectors (thread 0; m is small)
-  if (threadIdx.x == 0 && evecs != nullptr) {
-    double* dl = wk + m;      // LU factors of tridiagonal T - theta
-    double* dd = wk + 2 * m;
-    double* du = wk + 3 * m;
-    double* du2 = wk + 4 * m;
-    int* piv = (int*)(wk + 5 * m);
-    for (int e = 0; e < k && e < m; ++e) {
-      double theta = evals[(int64_t)prob * k + e];
-      double* s = evecs + ((int64_t)prob * k + e) * ldv;
-      double scale = 0.0;
-      for (int i = 0; i < m; ++i) scale = fmax(scale, fabs(a[i]) + (i > 0 ? fabs(bb[i]) : 0.0));
-      double eps_shift = 2.2e-16 * fmax(scale, 1e-300);
-      // factor (T - theta I) with partial pivoting (dgttrf)
-      for (int i = 0; i < m; ++i) {
-        dd[i] = a[i] - theta;
-        if (i + 1 < m) {
-          dl[i] = bb[i + 1];
-          du[i] = bb[i + 1];
-        }
-        du2[i] = 0.0;
-      }
-      for (int i = 0; i < m - 1; ++i) {
-        if (fabs(dd[i]) >= fabs(dl[i])) {
-          piv[i] = i;
-          if (dd[i] == 0.0) dd[i] = eps_shift;
-          double f = dl[i] / dd[i];
-          dl[i] = f;
-          dd[i + 1] -= f * du[i];
-          if (i + 1 < m - 1) du2[i] = 0.0;
-        } else {
-          piv[i] = i + 1;
-          double f = dd[i] / dl[i];
-          dd[i] = dl[i];
-          dl[i] = f;
-          double tmp = du[i];
-          du[i] = dd[i + 1];
-          dd[i + 1] = tmp - f * dd[i + 1];
-          if (i + 1 < m - 1) {
-            du2[i] = du[i + 1];
-            du[i + 1] = -f * du[i + 1];
-          }
-        }
-      }
-      if (dd[m - 1] == 0.0) dd[m - 1] = eps_shift;
-      for (int i = 0; i < m; ++i) s[i] = 1.0 / sqrt((double)m) * (1.0 + 0.01 * (double)((i * 7 + e * 3) % 5));
-      for (int it = 0; it < 3; ++it) {
-        // solve L U x = P s
-        for (int i = 0; i < m - 1; ++i) {
-          if (piv[i] == i) {
-            s[i + 1] -= dl[i] * s[i];
-          } else {
-            double t = s[i];
-            s[i] = s[i + 1];
-            s[i + 1] = t - dl[i] * s[i];
-          }
-        }
-        s[m - 1] /= dd[m - 1];
-        if (m > 1) s[m - 2] = (s[m - 2] - du[m - 2] * s[m - 1]) / dd[m - 2];
-        for (int i = m - 3; i >= 0; --i) s[i] = (s[i] - du[i] * s[i + 1] - du2[i] * s[i + 2]) / dd[i];
-        // orthogonalise against earlier eigenvectors (near-degenerate pairs)
-        for (int f = 0; f < e; ++f) {
-          const double* sf = evecs + ((int64_t)prob * k + f) * ldv;
-          double p = 0.0;
-          for (int i = 0; i < m; ++i) p += sf[i] * s[i];
-          for (int i = 0; i < m; ++i) s[i] -= p * sf[i];
-        }
-        double nn = 0.0;
-        for (int i = 0; i < m; ++i) nn += s[i] * s[i];
-        nn = 1.0 / sqrt(nn);
-        for (int i = 0; i < m; ++i) s[i] *= nn;
-      }
-      // sign convention: largest component positive
-      int imax = 0;
-      for (int i = 1; i < m; ++i)
-        if (fabs(s[i]) > fabs(s[imax])) imax = i;
-      if (s[imax] < 0.0)
-        for (int i = 0; i < m; ++i) s[i] = -s[i];
-    }
-  }
+  tridiag_body(alpha + (int64_t)prob * lda, beta + (int64_t)prob * ldb, m, k, evals + (int64_t)prob * k,
+               evecs ? evecs + (int64_t)prob * k * ldv : nullptr, ldv, work + (int64_t)prob * ldw);
 }
 
-// x[r][v] (for eigenpair e) = sum_i V[i][r][v] S[v][e][i]
+// w (planar) = sum_{i<m} V[i][v][r] S[v][e][i]
 template <typename T, int NV>
-__global__ void ritz_k(const T* __restrict__ V, int64_t n, int m, const double* __restrict__ S, int k, int e,
-                       int lds, int64_t stride_i, double* __restrict__ x) {
-  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
-    double acc[NV];
-#pragma unroll
-    for (int v = 0; v < NV; ++v) acc[v] = 0.0;
-    for (int i = 0; i < m; ++i) {
-      const T* Vi = V + (int64_t)i * stride_i + r * NV;
-#pragma unroll
-      for (int v = 0; v < NV; ++v) acc[v] = fma(ldv(Vi, v), S[((int64_t)v * k + e) * lds + i], acc[v]);
-    }
-#pragma unroll
-    for (int v = 0; v < NV; ++v) x[r * NV + v] = acc[v];
+__global__ void ritz_k(const T* __restrict__ V, int64_t n_pad, int m, const double* __restrict__ S, int ldk, int e,
+                       int lds, int64_t stride_i, double* __restrict__ w) {
+  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < n_pad * NV; g += (int64_t)gridDim.x * blockDim.x) {
+    const int v = (int)(g / n_pad);
+    const double* s = S + ((int64_t)v * ldk + e) * lds;
+    double acc = 0.0;
+    for (int i = 0; i < m; ++i) acc = fma(ldv(V, (int64_t)i * stride_i + g), s[i], acc);
+    w[g] = acc;
   }
 }
 
@@ -469,8 +293,9 @@ __global__ void ritz_k(const T* __restrict__ V, int64_t n, int m, const double* 
 // Workspace layout
 // ---------------------------------------------------------------------------
 struct Layout {
-  int64_t V, w, h, partial, normp, alpha, beta, tri_eval, tri_vec, tri_work, total;
+  int64_t V, X, w, h, partial, normp, alpha, beta, tri_eval, tri_vec, tri_work, total;
   int nblk_dot, nblk_upd, m_max, ld_h;
+  int64_t n_pad;
 };
 
 inline int64_t align256(int64_t x) { return (x + 255) & ~int64_t(255); }
@@ -479,13 +304,15 @@ Layout make_layout(const edg_lanczos_problem* p) {
   Layout L{};
   const int64_t n = p->n_rows, nv = p->nvec;
   const int esz = p->dtype == 0 ? 8 : 4;
+  L.n_pad = (n + 3) & ~int64_t(3);
   L.m_max = p->max_iter;
   L.ld_h = L.m_max + 1;
-  L.nblk_dot = edg::kSmCount * 4;
+  L.nblk_dot = edg::kSmCount * 8;  // upper bound of the row-chunk grid of dots_k
   L.nblk_upd = edg::kSmCount * 8;
   int64_t off = 0;
-  L.V = off; off = align256(off + (int64_t)(L.m_max + 1) * n * nv * esz);
-  L.w = off; off = align256(off + n * nv * 8);
+  L.V = off; off = align256(off + (int64_t)(L.m_max + 1) * L.n_pad * nv * esz);
+  L.X = off; off = align256(off + n * nv * esz);
+  L.w = off; off = align256(off + L.n_pad * nv * 8);
   L.h = off; off = align256(off + (int64_t)(L.m_max + 1) * nv * 8);
   L.partial = off; off = align256(off + (int64_t)L.nblk_dot * (L.m_max + 1) * nv * 8);
   L.normp = off; off = align256(off + (int64_t)L.nblk_upd * nv * 8);
@@ -511,13 +338,36 @@ __global__ void zero_k(double* p, int n) {
   if (t < n) p[t] = 0.0;
 }
 
+// per-problem Krylov dimension of a batched tridiagonal solve
+struct Dims4 {
+  int m[4];
+  int k[4];
+};
+
+__global__ void __launch_bounds__(kThreads) tridiag_batch_k(const double* __restrict__ alpha, int lda,
+                                                            const double* __restrict__ beta, int ldb, Dims4 dims,
+                                                            double* __restrict__ evals, int ld_eval,
+                                                            double* __restrict__ evecs, int ldk, int lds,
+                                                            double* __restrict__ work, int ldw);
+
+__global__ void __launch_bounds__(kThreads) tridiag_batch_k(const double* __restrict__ alpha, int lda,
+                                                            const double* __restrict__ beta, int ldb, Dims4 dims,
+                                                            double* __restrict__ evals, int ld_eval,
+                                                            double* __restrict__ evecs, int ldk, int lds,
+                                                            double* __restrict__ work, int ldw) {
+  const int prob = blockIdx.x;
+  tridiag_body(alpha + (int64_t)prob * lda, beta + (int64_t)prob * ldb, dims.m[prob], dims.k[prob],
+               evals + (int64_t)prob * ld_eval, evecs + (int64_t)prob * ldk * lds, lds, work + (int64_t)prob * ldw);
+}
+
 template <typename T, int NV>
 int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* evecs, int32_t* iters_out,
                 double* resid_out, cudaStream_t s) {
   const Layout L = make_layout(p);
-  const int64_t n = p->n_rows;
+  const int64_t n = p->n_rows, n_pad = L.n_pad;
   const int k = p->k;
   T* V = (T*)(ws + L.V);
+  T* X = (T*)(ws + L.X);
   double* w = (double*)(ws + L.w);
   double* h = (double*)(ws + L.h);
   double* partial = (double*)(ws + L.partial);
@@ -528,22 +378,22 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
   double* tri_vec = (double*)(ws + L.tri_vec);  // [NV][kMaxK][m_max+1]
   double* tri_work = (double*)(ws + L.tri_work);
   const int ld_a = L.m_max + 1, ld_b = L.m_max + 2, ld_s = L.m_max + 1;
-  const int64_t stride_i = n * NV;
+  const int64_t stride_i = n_pad * NV;  // entries per Krylov vector (all problems)
   double* alpha_cur = h + (int64_t)L.m_max * NV;  // last NV slots of h (h[i] only used for i < m_max)
-  const unsigned g_vec = edg::grid_for(n * NV, 256);
+  const unsigned g_vec = edg::grid_for(n_pad, 256);
   cudaError_t e;
-  start_k<T><<<g_vec, 256, 0, s>>>(n * NV, p->seed, (const T*)p->v0, w);
-  norm_k<NV><<<L.nblk_upd, kThreads, 0, s>>>(w, n, normp);
+  // padding rows (r >= n) of w are zero from start_k on, so every Krylov plane
+  // written from w has zero padding and no reset of V is needed
+  start_k<T, NV><<<edg::grid_for(n_pad * NV, 256), 256, 0, s>>>(n, n_pad, p->seed, (const T*)p->v0, w);
+  norm_k<NV><<<L.nblk_upd, kThreads, 0, s>>>(w, n_pad, normp);
   beta_k<NV><<<1, kThreads, 0, s>>>(normp, L.nblk_upd, h);
-  scale_store_k<T, NV><<<g_vec, 256, 0, s>>>(w, n, h, V);
+  scale_store_k<T, NV><<<g_vec, 256, 0, s>>>(w, n, n_pad, h, V, X);
   zero_k<NV><<<(NV * ld_b + 255) / 256, 256, 0, s>>>(beta, NV * ld_b);
   zero_k<NV><<<(NV * ld_a + 255) / 256, 256, 0, s>>>(alpha, NV * ld_a);
   if ((e = cudaGetLastError()) != cudaSuccess) return edg::cuda_status(e, "edg_lanczos: start");
   const size_t upd_smem = (size_t)(L.m_max + 1) * NV * sizeof(double);
   if (upd_smem > 40 * 1024) {
     e = cudaFuncSetAttribute(update_k<T, NV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)upd_smem);
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(update_dots_k<T, NV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)upd_smem + 8192);
     if (e != cudaSuccess) return edg::cuda_status(e, "edg_lanczos: smem attribute");
   }
   std::vector<double> hb((size_t)NV * ld_b), ha((size_t)NV * ld_a), hev((size_t)NV * kMaxK),
@@ -552,24 +402,23 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
   auto tridiag_all = [&](const std::vector<int>& mv) -> int {
     cudaError_t err = cudaMemsetAsync(tri_vec, 0, sizeof(double) * NV * kMaxK * ld_s, s);
     if (err != cudaSuccess) return edg::cuda_status(err, "edg_lanczos: tridiag reset");
+    Dims4 d{};
     for (int v = 0; v < NV; ++v) {
-      int kk = k < mv[v] ? k : mv[v];
-      tridiag_k<<<1, kThreads, 0, s>>>(alpha + (int64_t)v * ld_a, ld_a, beta + (int64_t)v * ld_b, ld_b, mv[v], kk,
-                                       tri_eval + v * kMaxK, tri_vec + (int64_t)v * kMaxK * ld_s, ld_s,
-                                       tri_work + (int64_t)v * 6 * ld_s, 6 * ld_s);
+      d.m[v] = mv[v];
+      d.k[v] = k < mv[v] ? k : mv[v];
     }
+    tridiag_batch_k<<<NV, kThreads, 0, s>>>(alpha, ld_a, beta, ld_b, d, tri_eval, kMaxK, tri_vec, kMaxK, ld_s,
+                                            tri_work, 6 * ld_s);
     err = cudaGetLastError();
     if (err != cudaSuccess) return edg::cuda_status(err, "edg_lanczos: tridiag");
     return EDG_OK;
   };
-  int status = EDG_OK;
-  int j = 0;
   // optional phase timing with CUDA events on the launch stream
   const bool timing = p->stats != nullptr;
   std::vector<cudaEvent_t> ev;
-  int ev_done = 0;  // steps whose events were already accumulated
+  int ev_done = 0;
   double t_spmv = 0.0, t_reorth = 0.0, t_check = 0.0;
-  int64_t launches = 7;  // start-vector kernels
+  int64_t launches = 8;
   auto event_at = [&](int idx) -> cudaEvent_t {
     while ((int)ev.size() <= idx) {
       cudaEvent_t e2;
@@ -587,29 +436,42 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
       t_reorth += b;
     }
   };
+  const int first_check = p->check_every > 8 ? p->check_every : 8;
+  // Residuals of the last two checks give a per-step contraction estimate;
+  // the next check is scheduled where the slowest problem should be near tol
+  // (never later than 4 * check_every, never earlier than check_every).
+  int next_check = first_check;
+  double prev_worst = -1.0;
+  int prev_m = 0;
+  int status = EDG_OK;
+  int j = 0;
   for (; j < L.m_max; ++j) {
-    const T* vj = V + (int64_t)j * stride_i;
     if (timing) cudaEventRecord(event_at(3 * j), s);
     int st = edg::launch_spmv<T, T, double>(NV, n, p->nnz, p->rowptr, p->cols, (const T*)p->vals, (const T*)p->diag,
-                                            vj, w, s);
+                                            X, w, s, n_pad, p->spmv_group);
     if (st) return st;
     if (timing) cudaEventRecord(event_at(3 * j + 1), s);
-    launches += 10;
+    launches += 11;
     zero_k<NV><<<1, 32, 0, s>>>(alpha_cur, NV);
-    // classical Gram-Schmidt twice: dots | update+dots | update (3 reads of V)
-    dots_k<T, NV><<<L.nblk_dot, kThreads, 0, s>>>(V, n, j, w, partial, ld_a, stride_i);
-    reduce_h_k<NV><<<j + 1, kThreads, 0, s>>>(partial, L.nblk_dot, ld_a, j, h, alpha_cur);
-    update_dots_k<T, NV><<<L.nblk_dot, kThreads, upd_smem, s>>>(V, n, j, h, w, partial, ld_a, stride_i);
-    reduce_h_k<NV><<<j + 1, kThreads, 0, s>>>(partial, L.nblk_dot, ld_a, j, h, alpha_cur);
-    update_k<T, NV><<<L.nblk_upd, kThreads, upd_smem, s>>>(V, n, j, h, w, normp, stride_i);
+    // classical Gram-Schmidt twice against V[0..j]; the row-chunk grid shrinks
+    // as the Krylov tiles grow so that about 8 CTAs per SM are in flight
+    const int tiles = (j + kItile) / kItile;
+    int nx = L.nblk_dot / tiles;
+    if (nx < edg::kSmCount) nx = edg::kSmCount;
+    const dim3 gd(nx, tiles);
+    for (int pass = 0; pass < 2; ++pass) {
+      dots_k<T, NV><<<gd, kThreads, 0, s>>>(V, n_pad, j, w, partial, ld_a, stride_i);
+      reduce_h_k<NV><<<j + 1, kThreads, 0, s>>>(partial, nx, ld_a, j, h, alpha_cur);
+      update_k<T, NV><<<L.nblk_upd, kThreads, upd_smem, s>>>(V, n_pad, j, h, w, normp, stride_i);
+    }
     scatter_coef_k<NV><<<1, 32, 0, s>>>(alpha_cur, alpha, ld_a, j);
     beta_k<NV><<<1, kThreads, 0, s>>>(normp, L.nblk_upd, h);  // h[0..NV) = beta_{j+1}
     scatter_coef_k<NV><<<1, 32, 0, s>>>(h, beta, ld_b, j + 1);
-    scale_store_k<T, NV><<<g_vec, 256, 0, s>>>(w, n, h, V + (int64_t)(j + 1) * stride_i);
+    scale_store_k<T, NV><<<g_vec, 256, 0, s>>>(w, n, n_pad, h, V + (int64_t)(j + 1) * stride_i, X);
     if (timing) cudaEventRecord(event_at(3 * j + 2), s);
     if ((e = cudaGetLastError()) != cudaSuccess) return edg::cuda_status(e, "edg_lanczos: step");
     const int m = j + 1;
-    const bool check = (m % p->check_every == 0) || m == L.m_max || (int64_t)m == n;
+    const bool check = m >= next_check || m == L.m_max || (int64_t)m == n;
     if (!check) continue;
     // recurrence coefficients to the host (a few KB) to detect invariant subspaces
     e = cudaMemcpyAsync(hb.data(), beta, sizeof(double) * NV * ld_b, cudaMemcpyDeviceToHost, s);
@@ -623,7 +485,7 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
       c1 = event_at(3 * L.m_max + 1);
       cudaEventRecord(c0, s);
     }
-    launches += 1 + NV;
+    launches += 2;
     std::vector<bool> exact(NV, false);
     for (int v = 0; v < NV; ++v) {
       if (m_conv[v]) { m_use[v] = m_conv[v]; continue; }
@@ -663,6 +525,25 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
     }
     if (all) { ++j; break; }
     if (m == L.m_max) { status = EDG_ERR_NOT_CONVERGED; ++j; break; }
+    // schedule the next check from the worst relative residual
+    double worst = 0.0;
+    for (int v = 0; v < NV; ++v) {
+      if (m_conv[v]) continue;
+      for (int q = 0; q < k; ++q) {
+        const double theta = hev[v * kMaxK + q];
+        worst = fmax(worst, res[v * k + q] / fmax(1.0, fabs(theta)));
+      }
+    }
+    int step = p->check_every;
+    if (prev_worst > 0.0 && worst > 0.0 && worst < prev_worst && m > prev_m) {
+      const double rate = log(worst / prev_worst) / (double)(m - prev_m);  // < 0
+      const double need = log(p->tol / worst) / rate;                      // steps to reach tol
+      int predicted = (int)floor(need * 0.8);
+      if (predicted > step) step = predicted < 4 * p->check_every ? predicted : 4 * p->check_every;
+    }
+    prev_worst = worst;
+    prev_m = m;
+    next_check = m + step;
   }
   for (int v = 0; v < NV; ++v) m_use[v] = m_conv[v] ? m_conv[v] : (j < 1 ? 1 : j);
   int st = tridiag_all(m_use);
@@ -683,10 +564,11 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
   if (evecs) {
     // S rows beyond each problem's m are zero, so one pass over m_all vectors serves all problems
     for (int q = 0; q < k; ++q) {
-      ritz_k<T, NV><<<g_vec, 256, 0, s>>>(V, n, m_all, tri_vec, kMaxK, q, ld_s, stride_i, w);
-      norm_k<NV><<<L.nblk_upd, kThreads, 0, s>>>(w, n, normp);
+      ritz_k<T, NV><<<edg::grid_for(n_pad * NV, 256), 256, 0, s>>>(V, n_pad, m_all, tri_vec, kMaxK, q, ld_s,
+                                                                   stride_i, w);
+      norm_k<NV><<<L.nblk_upd, kThreads, 0, s>>>(w, n_pad, normp);
       beta_k<NV><<<1, kThreads, 0, s>>>(normp, L.nblk_upd, h);
-      scale_store_k<T, NV><<<g_vec, 256, 0, s>>>(w, n, h, (T*)evecs + (int64_t)q * stride_i);
+      scale_store_k<T, NV><<<g_vec, 256, 0, s>>>(w, n, n_pad, h, (T*)nullptr, (T*)evecs + (int64_t)q * n * NV);
     }
     if ((e = cudaGetLastError()) != cudaSuccess) return edg::cuda_status(e, "edg_lanczos: ritz vectors");
   }
@@ -694,7 +576,7 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
   if (e != cudaSuccess) return edg::cuda_status(e, "edg_lanczos: finish");
   if (timing) {
     accumulate(j);
-    launches += 1 + NV + (evecs ? 4 * k : 0);
+    launches += 2 + (evecs ? 4 * k : 0);
     p->stats[0] = t_spmv;
     p->stats[1] = (double)ev_done;
     p->stats[2] = t_reorth;

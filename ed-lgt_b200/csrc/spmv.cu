@@ -14,23 +14,29 @@ __global__ void convert_k(const A* __restrict__ in, B* __restrict__ out, int64_t
 extern "C" int edg_spmv(int32_t dtype, int64_t n_rows, int64_t nnz, const int64_t* rowptr, const int32_t* cols,
                         const void* vals, const void* diag, int32_t nvec, const void* x, void* y,
                         cudaStream_t stream) {
+  return edg_spmv_group(dtype, n_rows, nnz, rowptr, cols, vals, diag, nvec, x, y, 0, stream);
+}
+
+extern "C" int edg_spmv_group(int32_t dtype, int64_t n_rows, int64_t nnz, const int64_t* rowptr,
+                              const int32_t* cols, const void* vals, const void* diag, int32_t nvec, const void* x,
+                              void* y, int32_t group, cudaStream_t stream) {
   EDG_REQUIRE(n_rows >= 0 && nnz >= 0, "edg_spmv: negative size");
   EDG_REQUIRE(rowptr && diag && x && y && (nnz == 0 || (cols && vals)), "edg_spmv: null pointer");
   if (n_rows == 0) return EDG_OK;
   switch (dtype) {
     case 0:
       return edg::launch_spmv<double, double, double>(nvec, n_rows, nnz, rowptr, cols, (const double*)vals,
-                                                      (const double*)diag, (const double*)x, (double*)y, stream);
+                                                      (const double*)diag, (const double*)x, (double*)y, stream, 0, group);
     case 1:
       return edg::launch_spmv<float, float, float>(nvec, n_rows, nnz, rowptr, cols, (const float*)vals,
-                                                   (const float*)diag, (const float*)x, (float*)y, stream);
+                                                   (const float*)diag, (const float*)x, (float*)y, stream, 0, group);
     case 2:
       return edg::launch_spmv<double2, double2, double2>(nvec, n_rows, nnz, rowptr, cols, (const double2*)vals,
                                                          (const double2*)diag, (const double2*)x, (double2*)y,
-                                                         stream);
+                                                         stream, 0, group);
     case 3:
       return edg::launch_spmv<float2, float2, float2>(nvec, n_rows, nnz, rowptr, cols, (const float2*)vals,
-                                                      (const float2*)diag, (const float2*)x, (float2*)y, stream);
+                                                      (const float2*)diag, (const float2*)x, (float2*)y, stream, 0, group);
     default:
       edg::set_error("edg_spmv: unknown dtype %d", dtype);
       return EDG_ERR_ARG;

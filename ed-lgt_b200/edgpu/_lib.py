@@ -13,7 +13,7 @@ from pathlib import Path
 from ._build import LIB_PATH
 
 __all__ = ["lib", "check", "EdgError", "MAX_SITES", "MAX_OPS", "SectorTables", "LookupTable", "Assembly",
-           "LanczosProblem", "SiteDims", "KrylovProblem", "EXPORTED_SYMBOLS", "ptr", "stream_handle"]
+           "LanczosProblem", "SiteDims", "KrylovProblem", "SmallBatch", "EXPORTED_SYMBOLS", "ptr", "stream_handle"]
 
 MAX_SITES = 64
 MAX_OPS = 4
@@ -125,6 +125,7 @@ class LanczosProblem(C.Structure):
         ("check_every", I32),
         ("seed", U64),
         ("v0", P),
+        ("spmv_group", I32),
         ("stats", P),
     ]
 
@@ -141,6 +142,31 @@ class KrylovProblem(C.Structure):
         ("diag", P),
         ("m", I32),
         ("reorth_passes", I32),
+        ("spmv_group", I32),
+    ]
+
+
+class SmallBatch(C.Structure):
+    _fields_ = [
+        ("n_inst", I32),
+        ("max_dim", I32),
+        ("dims", P),
+        ("row_off", P),
+        ("rowptr_off", P),
+        ("rowptr", P),
+        ("cols", P),
+        ("vals", P),
+        ("diag", P),
+        ("work", P),
+        ("work_off", P),
+        ("k", I32),
+        ("max_iter", I32),
+        ("check_every", I32),
+        ("tol", F64),
+        ("seed", U64),
+        ("evals", P),
+        ("evecs", P),
+        ("iters", P),
     ]
 
 
@@ -161,11 +187,14 @@ _SIGS = {
     "edg_assemble_compact": (I32, [I64, I32, P, P, P, P, P, P, P]),
     "edg_spmv": (I32, [I32, I64, I64, P, P, P, P, I32, P, P, P]),
     "edg_convert": (I32, [I32, P, I32, P, I64, P]),
+    "edg_spmv_group": (I32, [I32, I64, I64, P, P, P, P, I32, P, P, I32, P]),
     "edg_lanczos_workspace_bytes": (I64, [C.POINTER(LanczosProblem)]),
     "edg_lanczos": (I32, [C.POINTER(LanczosProblem), P, I64, P, P, P, P, P]),
     "edg_tridiag_lowest": (I32, [P, P, I32, I32, P, P, P, P]),
     "edg_tridiag_lowest_noalloc": (I32, [P, P, I32, I32, P, P, P]),
     "edg_local_expval": (I32, [P, I64, C.POINTER(SiteDims), I32, P, I32, I64, P, I32, P, P]),
+    "edg_small_batch_work_elems": (I64, [I64, I32, I32]),
+    "edg_lanczos_small_batched": (I32, [C.POINTER(SmallBatch), P, P]),
     "edg_krylov_workspace_bytes": (I64, [C.POINTER(KrylovProblem)]),
     "edg_krylov_step": (I32, [C.POINTER(KrylovProblem), P, F64, P, I64, P, P]),
 }

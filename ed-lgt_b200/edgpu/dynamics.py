@@ -26,7 +26,7 @@ __all__ = ["KrylovEvolver", "krylov_evolve"]
 class KrylovEvolver:
     """Holds the device copies and the workspace of one Hamiltonian."""
 
-    def __init__(self, mat, m=30, precision="c128", reorth_passes=1):
+    def __init__(self, mat, m=30, precision="c128", reorth_passes=1, spmv_group=None):
         if precision not in ("c128", "c64"):
             raise ValueError("precision must be 'c128' or 'c64'")
         self.mat = mat
@@ -55,6 +55,14 @@ class KrylovEvolver:
         p.diag = ptr(diag)
         p.m = self.m
         p.reorth_passes = reorth_passes
+        if spmv_group is None:
+            # a complex vector is two real right-hand sides for a real matrix:
+            # tune on that shape (real forms only)
+            from .solvers import tune_spmv_group
+
+            spmv_group = 0 if mat.is_complex else tune_spmv_group(
+                mat, 2, 0 if precision == "c128" else 1, vals=mat.vals if precision == "c128" else vals)
+        p.spmv_group = int(spmv_group)
         self.p = p
         wb = lib.edg_krylov_workspace_bytes(ctypes.byref(p))
         if wb < 0:

@@ -10,6 +10,7 @@ signs, Gauss law with staggered matter charge ``n - (site odd)``) reproduce
 
 from __future__ import annotations
 
+from functools import lru_cache
 from itertools import product
 
 import numpy as np
@@ -61,6 +62,11 @@ def _rishon_chain(dim: int, placements: dict) -> list[str]:
 
 def qed_dressed_site_operators(spin, pure_theory, lattice_dim, U="ladder", fermionic=True, background=0) -> dict:
     """Dressed-site operator dictionary (scipy CSR, full local space)."""
+    return dict(_qed_ops_cached(spin, pure_theory, lattice_dim, U, fermionic, background))
+
+
+@lru_cache(maxsize=32)
+def _qed_ops_cached(spin, pure_theory, lattice_dim, U, fermionic, background):
     if lattice_dim not in (1, 2, 3):
         raise ValueError("lattice_dim must be 1, 2 or 3")
     D = lattice_dim
@@ -129,6 +135,12 @@ def qed_dressed_site_operators(spin, pure_theory, lattice_dim, U="ladder", fermi
 
 
 def qed_gauge_invariant_states(spin, pure_theory, lattice_dim, background=0, get_only_bulk=False):
+    basis, states = _qed_states_cached(spin, pure_theory, lattice_dim, background, get_only_bulk)
+    return dict(basis), dict(states)
+
+
+@lru_cache(maxsize=32)
+def _qed_states_cached(spin, pure_theory, lattice_dim, background, get_only_bulk):
     """Gauss-law-satisfying local states and their selection bases.
 
     Returns ``(gauge_basis, gauge_states)`` keyed by ``site``/``even``/``odd``

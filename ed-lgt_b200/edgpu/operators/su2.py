@@ -19,6 +19,7 @@ from __future__ import annotations
 
 from decimal import Decimal, getcontext
 from fractions import Fraction
+from functools import lru_cache
 from itertools import product
 from math import factorial
 
@@ -125,6 +126,12 @@ def _cg_float(sign, sq):
 
 
 def su2_gauge_invariant_states(spin, pure_theory, lattice_dim, background=0):
+    basis, states = _su2_states_cached(float(spin), pure_theory, lattice_dim, float(background))
+    return dict(basis), dict(states)
+
+
+@lru_cache(maxsize=32)
+def _su2_states_cached(spin, pure_theory, lattice_dim, background=0):
     """Singlet bases of a dressed site (``spin`` = 1/2 rishon truncation).
 
     Returns ``(gauge_basis, gauge_states)`` keyed by ``site`` and
@@ -248,6 +255,11 @@ def su2_generators(jmax, matter=False):
 
 def su2_dressed_site_operators(spin, pure_theory, lattice_dim, background=0) -> dict:
     """Dressed-site operators for j_max = 1/2 (full local space, scipy CSR)."""
+    return dict(_su2_ops_cached(float(spin), pure_theory, lattice_dim, float(background)))
+
+
+@lru_cache(maxsize=32)
+def _su2_ops_cached(spin, pure_theory, lattice_dim, background=0):
     if abs(spin - 0.5) > 1e-12:
         raise ValueError("the hard-core-gluon SU(2) operators exist only for spin = 1/2")
     D = lattice_dim

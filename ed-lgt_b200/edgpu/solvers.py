@@ -22,7 +22,50 @@ import torch
 from . import _lib
 from ._lib import check, lib, ptr, stream_handle
 
-__all__ = ["LanczosResult", "lanczos", "lanczos_mixed", "stack_diagonals"]
+__all__ = ["LanczosResult", "lanczos", "lanczos_mixed", "stack_diagonals", "tune_spmv_group"]
+
+SPMV_GROUPS = (2, 4, 8, 16, 32)
+
+
+def tune_spmv_group(mat, nvec=1, dtype=0, reps=5, vals=None, diag=None):
+    """Autotuner: threads per matvec row that is fastest on this matrix.
+
+    Times ``edg_spmv_group`` for every group size with CUDA events (after one
+    warm-up launch each) on the real matrix and the requested precision and
+    batch width; the choice is cached on the matrix object.
+    """
+    key = (dtype, nvec)
+    cache = getattr(mat, "_tuned_groups", None)
+    if cache is None:
+        cache = mat._tuned_groups = {}
+    if key in cache:
+        return cache[key]
+    dev = mat.rowptr.device
+    tdt = {0: torch.float64, 1: torch.float32}[dtype]
+    if vals is None:
+        vals = mat.vals.to(tdt)
+    if diag is None:
+        diag = torch.zeros((mat.n, nvec), dtype=tdt, device=dev)
+    x = torch.ones((mat.n, nvec), dtype=tdt, device=dev)
+    y = torch.empty_like(x)
+    best, best_t = 0, float("inf")
+    for g in SPMV_GROUPS:
+        def launch():
+            check(lib.edg_spmv_group(dtype, mat.n, mat.nnz, ptr(mat.rowptr), ptr(mat.cols) if mat.nnz else None,
+                                     ptr(vals) if mat.nnz else None, ptr(diag), nvec, ptr(x), ptr(y), g,
+                                     stream_handle()), "edg_spmv_group")
+        launch()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            launch()
+        b.record()
+        torch.cuda.synchronize()
+        t = a.elapsed_time(b) / reps
+        if t < best_t:
+            best, best_t = g, t
+    cache[key] = best
+    return best
 
 
 class LanczosResult:
@@ -33,7 +76,8 @@ class LanczosResult:
         self.resid = resid      # (nvec, k)
 
 
-def _problem(dtype, n, nnz, rowptr, cols, vals, diag, nvec, k, max_iter, tol, check_every, seed, v0, stats=None):
+def _problem(dtype, n, nnz, rowptr, cols, vals, diag, nvec, k, max_iter, tol, check_every, seed, v0, stats=None,
+             group=0):
     p = _lib.LanczosProblem()
     p.dtype = dtype
     p.n_rows = n
@@ -50,18 +94,21 @@ def _problem(dtype, n, nnz, rowptr, cols, vals, diag, nvec, k, max_iter, tol, ch
     p.seed = seed
     p.v0 = ptr(v0) if v0 is not None else None
     p.stats = stats.ctypes.data if stats is not None else None
+    p.spmv_group = group
     return p
 
 
 def run_lanczos(dtype, n, nnz, rowptr, cols, vals, diag, nvec=1, k=1, max_iter=300, tol=1e-12, check_every=5,
-                seed=1234, v0=None, want_vectors=True, allow_unconverged=False, workspace=None, stats=None):
+                seed=1234, v0=None, want_vectors=True, allow_unconverged=False, workspace=None, stats=None,
+                group=0):
     """Low-level call of ``edg_lanczos``; ``diag`` is ``[n][nvec]`` in the dtype.
 
     ``stats``: optional float64 numpy array of 6 entries filled with the
     phase timings of the run (see edg_lanczos_problem.stats).
     """
     max_iter = int(min(max_iter, n))
-    p = _problem(dtype, n, nnz, rowptr, cols, vals, diag, nvec, k, max_iter, tol, check_every, seed, v0, stats)
+    p = _problem(dtype, n, nnz, rowptr, cols, vals, diag, nvec, k, max_iter, tol, check_every, seed, v0, stats,
+                 group)
     wb = lib.edg_lanczos_workspace_bytes(ctypes.byref(p))
     if wb < 0:
         raise _lib.EdgError(-1, _lib.last_error())
@@ -81,12 +128,13 @@ def run_lanczos(dtype, n, nnz, rowptr, cols, vals, diag, nvec=1, k=1, max_iter=3
     return LanczosResult(evals.reshape(nvec, k), evecs, iters, resid.reshape(nvec, k))
 
 
-def lanczos(mat, k=1, tol=1e-12, max_iter=400, check_every=5, seed=1234, v0=None):
+def lanczos(mat, k=1, tol=1e-12, max_iter=400, check_every=5, seed=1234, v0=None, stats=None, tune=True, group=0):
     """f64 Lanczos on a real DeviceMatrix; returns (evals[k], evecs (n, k) device)."""
     if mat.is_complex:
         raise NotImplementedError("complex Hermitian Lanczos: assemble the real form of the model")
+    g = group or (tune_spmv_group(mat, 1, 0, vals=mat.vals) if tune else 0)
     r = run_lanczos(0, mat.n, mat.nnz, mat.rowptr, mat.cols, mat.vals, mat.diag, nvec=1, k=k, max_iter=max_iter,
-                    tol=tol, check_every=check_every, seed=seed, v0=v0)
+                    tol=tol, check_every=check_every, seed=seed, v0=v0, stats=stats, group=g)
     return r.evals[0], r.evecs[:, :, 0].T.contiguous(), r
 
 
@@ -95,8 +143,9 @@ def stack_diagonals(diags, dtype):
     return torch.stack([d.to(dtype) for d in diags], dim=1).contiguous()
 
 
-def lanczos_mixed(mat, diags=None, k=1, tol32=1e-6, tol=1e-12, max_iter=400, refine_iter=8, check_every=5,
-                  seed=1234, stats32=None, stats64=None, vals32=None, diag32=None, diag64=None):
+def lanczos_mixed(mat, diags=None, k=1, tol32=1e-5, tol=1e-12, max_iter=400, refine_iter=5, check_every=5,
+                  seed=1234, stats32=None, stats64=None, vals32=None, diag32=None, diag64=None, tune=True,
+                  group32=0, group64=0):
     """Mixed-precision (f32 Krylov, f64 recurrence) Lanczos + f64 refinement.
 
     ``diags``: list of f64 device diagonals (one per problem, <= 4) sharing the
@@ -113,12 +162,14 @@ def lanczos_mixed(mat, diags=None, k=1, tol32=1e-6, tol=1e-12, max_iter=400, ref
         diag32 = stack_diagonals(diags, torch.float32)
     if diag64 is None:
         diag64 = stack_diagonals(diags, torch.float64)
+    g32 = group32 or (tune_spmv_group(mat, nvec, 1, vals=vals32) if tune else 0)
+    g64 = group64 or (tune_spmv_group(mat, nvec, 0, vals=mat.vals) if tune else 0)
     r32 = run_lanczos(1, mat.n, mat.nnz, mat.rowptr, mat.cols, vals32, diag32, nvec=nvec, k=k, max_iter=max_iter,
-                      tol=tol32, check_every=check_every, seed=seed, stats=stats32)
+                      tol=tol32, check_every=check_every, seed=seed, stats=stats32, group=g32)
     # f64 refinement: short Lanczos restarted from the f32 Ritz vector (ground state)
     v0 = torch.empty((mat.n, nvec), dtype=torch.float64, device=diag64.device)
     check(lib.edg_convert(1, ptr(r32.evecs), 0, ptr(v0), mat.n * nvec, stream_handle()), "edg_convert")
     r64 = run_lanczos(0, mat.n, mat.nnz, mat.rowptr, mat.cols, mat.vals, diag64, nvec=nvec, k=1,
                       max_iter=refine_iter, tol=tol, check_every=refine_iter, seed=seed, v0=v0,
-                      allow_unconverged=True, stats=stats64)
+                      allow_unconverged=True, stats=stats64, group=g64)
     return r64, r32

@@ -225,6 +225,14 @@ int edg_spmv(int32_t dtype, int64_t n_rows, int64_t nnz,
              const void* diag, int32_t nvec, const void* x, void* y,
              cudaStream_t stream);
 
+/* Same with an explicit number of threads cooperating on a row (2, 4, 8, 16
+ * or 32; 0 = heuristic from the mean row length): the knob the autotuner in
+ * edgpu.solvers.tune_spmv_group sets. */
+int edg_spmv_group(int32_t dtype, int64_t n_rows, int64_t nnz,
+                   const int64_t* rowptr, const int32_t* cols, const void* vals,
+                   const void* diag, int32_t nvec, const void* x, void* y,
+                   int32_t group, cudaStream_t stream);
+
 /* Casts between f64 <-> f32 (or c128 <-> c64) arrays of n scalars. */
 int edg_convert(int32_t dtype_in, const void* in, int32_t dtype_out, void* out,
                 int64_t n_scalars, cudaStream_t stream);
@@ -256,6 +264,7 @@ typedef struct {
   int32_t check_every;    /* steps between convergence checks               */
   uint64_t seed;          /* start vector: uniform(-1,1) from this seed     */
   const void* v0;         /* optional start vectors [n_rows][nvec] or NULL  */
+  int32_t spmv_group;     /* threads per matvec row, 0 = heuristic         */
   double* stats;          /* optional HOST array of 6 doubles, or NULL:     */
                           /* [0] matvec ms, [1] matvec launches, [2] reorth */
                           /* ms, [3] kernel launches, [4] Lanczos steps,    */
@@ -294,6 +303,46 @@ int edg_tridiag_lowest_noalloc(const double* alpha, const double* beta,
                                double* evecs, cudaStream_t stream);
 
 /* ------------------------------------------------------------------------ */
+/* Batched Lanczos for many small instances (charge sectors, coupling        */
+/* sweeps) in one persistent launch: CTAs pull instances from a device work  */
+/* queue.  Replaces the sequential loop of eigsh calls (one per instance) of  */
+/* QMB_hamiltonian.diagonalize (edlgt/modeling/qmb_hamiltonian.py:260-332)   */
+/* that a sweep over instances performs.  f64 throughout, full               */
+/* reorthogonalisation, device tridiagonal eigen-solve per instance.  The    */
+/* launch (a queue reset + one kernel) can be captured in a CUDA graph.      */
+/* ------------------------------------------------------------------------ */
+
+typedef struct {
+  int32_t n_inst;
+  int32_t max_dim;            /* largest instance dimension (<= 4096)       */
+  const int64_t* dims;        /* [n_inst]                                   */
+  const int64_t* row_off;     /* [n_inst] first row of the instance in      */
+                              /* diag / evecs                               */
+  const int64_t* rowptr_off;  /* [n_inst] start of the instance's rowptr    */
+                              /* block (dim+1 entries into cols / vals)     */
+  const int64_t* rowptr;
+  const int32_t* cols;        /* column indices local to the instance       */
+  const double* vals;
+  const double* diag;         /* [sum of dims]                              */
+  double* work;               /* per-instance scratch, see                  */
+  const int64_t* work_off;    /* edg_small_batch_work_elems; [n_inst]       */
+  int32_t k;                  /* eigenvalues per instance (<= 16)           */
+  int32_t max_iter;
+  int32_t check_every;
+  double tol;
+  uint64_t seed;
+  double* evals;              /* [n_inst][k]                                */
+  double* evecs;              /* [sum of dims] ground states, or NULL       */
+  int32_t* iters;             /* [n_inst] Krylov dimension used, or NULL    */
+} edg_small_batch;
+
+/* Scratch doubles one instance of dimension dim needs. */
+int64_t edg_small_batch_work_elems(int64_t dim, int32_t max_iter, int32_t k);
+/* queue: one int32 of device memory (reset by the call). */
+int edg_lanczos_small_batched(const edg_small_batch* b, int32_t* queue,
+                              cudaStream_t stream);
+
+/* ------------------------------------------------------------------------ */
 /* Krylov time evolution psi <- exp(-i H dt) psi                             */
 /* Replaces scipy.sparse.linalg.expm_multiply(-iH, psi0, ...) as called from */
 /* QMB_hamiltonian.time_evolution (edlgt/modeling/qmb_hamiltonian.py:        */
@@ -314,6 +363,7 @@ typedef struct {
   const void* diag;       /* [n_rows]                                       */
   int32_t m;              /* Krylov dimension, <= 64                        */
   int32_t reorth_passes;  /* 0 local recurrence, 1 or 2 full Gram-Schmidt   */
+  int32_t spmv_group;     /* threads per matvec row, 0 = heuristic         */
 } edg_krylov_problem;
 
 int64_t edg_krylov_workspace_bytes(const edg_krylov_problem* p);

@@ -257,3 +257,51 @@ def test_krylov_states_are_unitary_and_match_dense(dev):
         got = model.H.psi_time[k].psi
         assert abs(np.vdot(got, got) - 1) < 1e-12
         assert np.max(np.abs(got - ref)) < 1e-10
+
+
+def _c3_instances(dev, n_coupling=64, seed=0):
+    """QED 3x2 OBC instances: couplings in the Q = 0 sector plus Q = -2..2."""
+    from cases import build as _b
+
+    rng = np.random.default_rng(seed)
+    gs = np.exp(rng.uniform(np.log(0.1), np.log(5.0), n_coupling))
+    ms = rng.uniform(0.0, 2.0, n_coupling)
+    model, _, _ = _b("qed2d_3x2_q0", device=dev)
+    mats, meta = [], []
+    for g, m in zip(gs, ms):
+        model.build_Hamiltonian(float(g), float(m))
+        mats.append(model.H.mat)
+        meta.append(("qed2d_3x2_q0", float(g), float(m)))
+    for q in (-2, -1, 1, 2):
+        name = f"qed2d_3x2_Q{q:+d}"
+        mq, g, m = _b(name, device=dev)
+        mq.build_Hamiltonian(g, m)
+        mats.append(mq.H.mat)
+        meta.append((name, g, m))
+    return mats, meta
+
+
+def test_batched_small_instances_match_oracle(golden_small, dev):
+    from edgpu.batch import SmallBatch
+
+    mats, meta = _c3_instances(dev)
+    batch = SmallBatch(mats, k=2, want_vectors=True)
+    batch.capture()
+    e_graph = batch.solve(use_graph=True).cpu().numpy().copy()
+    e_direct = batch.solve(use_graph=False).cpu().numpy()
+    assert np.array_equal(e_graph, e_direct)
+    for i, (name, g, m) in enumerate(meta):
+        H = mats[i].to_scipy().toarray()
+        w = np.linalg.eigvalsh(H)
+        assert np.allclose(e_direct[i], w[:2], atol=1e-10, rtol=0), (i, name)
+        if name.startswith("qed2d_3x2_Q"):
+            assert abs(e_direct[i, 0] / 6 - golden_small[f"{name}/energies"][0]) < 1e-10
+    # ground-state vectors: normalised and H x = E x
+    ev = batch.evecs.cpu().numpy()
+    off = 0
+    for i, mat in enumerate(mats):
+        x = ev[off: off + mat.n]
+        off += mat.n
+        H = mat.to_scipy()
+        assert abs(np.linalg.norm(x) - 1) < 1e-12
+        assert np.linalg.norm(H @ x - e_direct[i, 0] * x) < 1e-8
