@@ -1,0 +1,318 @@
+// Batched interleaved vectors: nvec instances stored [row][nvec], so one row
+// of all instances is one contiguous 32-byte sector (8 f32) and the
+// matrix-free matvec gathers every instance of a column with one load.
+//
+// Kernels for the Gram-Schmidt steps of a batched (thick-restart) Lanczos:
+// each thread owns slots of 4 consecutive elements (one float4 / two
+// double2), so the instance of slot element j is (4 * slot + j) % nvec; for
+// nvec = 8 that is fixed by the slot parity, which the grid-stride loop keeps.
+// Dots accumulate in f64 and reduce deterministically (per-CTA partials, then
+// one CTA per output in a fixed order).
+#include "internal.cuh"
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+constexpr int kTile = 8;   // basis vectors per dots CTA
+constexpr int kMaxM = 32;  // basis vectors per combine
+
+template <typename T>
+struct Slot;
+template <>
+struct Slot<float> {
+  __device__ static __forceinline__ void load(const float* p, double (&v)[4]) {
+    const float4 a = *reinterpret_cast<const float4*>(p);
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+  }
+  __device__ static __forceinline__ void store(float* p, const double (&v)[4]) {
+    *reinterpret_cast<float4*>(p) = make_float4((float)v[0], (float)v[1], (float)v[2], (float)v[3]);
+  }
+};
+template <>
+struct Slot<double> {
+  __device__ static __forceinline__ void load(const double* p, double (&v)[4]) {
+    const double2 a = reinterpret_cast<const double2*>(p)[0];
+    const double2 b = reinterpret_cast<const double2*>(p)[1];
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+  }
+  __device__ static __forceinline__ void store(double* p, const double (&v)[4]) {
+    reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
+    reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
+  }
+};
+
+// Number of lane classes: slots with different instance maps (2 for nvec 8).
+template <int NV>
+constexpr int classes() { return NV > 4 ? NV / 4 : 1; }
+
+// partial[block][i][class][4] over a tile of basis vectors [i0, i0 + kTile).
+template <typename T, int NV>
+__global__ void __launch_bounds__(kThreads) dots_k(const T* __restrict__ V, int64_t stride, int m,
+                                                   const T* __restrict__ w, int64_t n_slots,
+                                                   double* __restrict__ partial) {
+  constexpr int P = classes<NV>();
+  __shared__ double red[kWarps][kTile][P][4];
+  const int i0 = blockIdx.y * kTile;
+  const int ni = min(kTile, m - i0);
+  double acc[kTile][4];
+#pragma unroll
+  for (int i = 0; i < kTile; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+  for (int64_t s = (int64_t)blockIdx.x * kThreads + threadIdx.x; s < n_slots; s += (int64_t)gridDim.x * kThreads) {
+    double wv[4], vv[4];
+    Slot<T>::load(w + 4 * s, wv);
+#pragma unroll
+    for (int i = 0; i < kTile; ++i) {
+      if (i < ni) {
+        Slot<T>::load(V + (int64_t)(i0 + i) * stride + 4 * s, vv);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = fma(vv[j], wv[j], acc[i][j]);
+      }
+    }
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int i = 0; i < kTile; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      double a = acc[i][j];
+#pragma unroll
+      for (int o = 16; o >= P; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+      if (lane < P) red[warp][i][lane][j] = a;
+    }
+  __syncthreads();
+  for (int t = threadIdx.x; t < kTile * P * 4; t += kThreads) {
+    const int i = t / (P * 4), c = (t / 4) % P, j = t % 4;
+    double a = 0.0;
+    for (int k = 0; k < kWarps; ++k) a += red[k][i][c][j];
+    if (i < ni) partial[((int64_t)blockIdx.x * m + i0 + i) * (P * 4) + c * 4 + j] = a;
+  }
+}
+
+// h[i * nvec + v] = sum over CTAs and over the slot entries of instance v.
+template <int NV>
+__global__ void __launch_bounds__(kThreads) dots_reduce_k(const double* __restrict__ partial, int nblk, int m,
+                                                          double* __restrict__ h) {
+  constexpr int P = classes<NV>();
+  __shared__ double red[kWarps][P * 4];
+  const int i = blockIdx.x;
+  double a[P * 4];
+#pragma unroll
+  for (int q = 0; q < P * 4; ++q) a[q] = 0.0;
+  for (int b = threadIdx.x; b < nblk; b += kThreads)
+#pragma unroll
+    for (int q = 0; q < P * 4; ++q) a[q] += partial[((int64_t)b * m + i) * (P * 4) + q];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < P * 4; ++q) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) a[q] += __shfl_xor_sync(0xffffffffu, a[q], o);
+    if (lane == 0) red[warp][q] = a[q];
+  }
+  __syncthreads();
+  if (threadIdx.x < NV) {
+    const int v = threadIdx.x;
+    double t = 0.0;
+    // slot entry q = 4 c + j holds instance (4 c + j) % NV
+    for (int q = 0; q < P * 4; ++q)
+      if (q % NV == v)
+        for (int k = 0; k < kWarps; ++k) t += red[k][q];
+    h[(int64_t)i * NV + v] = t;
+  }
+}
+
+template <typename T, int NV>
+__global__ void __launch_bounds__(kThreads) update_k(const T* __restrict__ V, int64_t stride, int m,
+                                                     const double* __restrict__ h, T* __restrict__ w,
+                                                     int64_t n_slots) {
+  __shared__ double hs[kMaxM * 8];
+  for (int t = threadIdx.x; t < m * NV; t += kThreads) hs[t] = h[t];
+  __syncthreads();
+  for (int64_t s = (int64_t)blockIdx.x * kThreads + threadIdx.x; s < n_slots; s += (int64_t)gridDim.x * kThreads) {
+    double wv[4], vv[4];
+    Slot<T>::load(w + 4 * s, wv);
+    const int base = (int)((4 * s) % NV);
+    for (int i = 0; i < m; ++i) {
+      Slot<T>::load(V + (int64_t)i * stride + 4 * s, vv);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) wv[j] = fma(-vv[j], hs[i * NV + (base + j) % NV], wv[j]);
+    }
+    Slot<T>::store(w + 4 * s, wv);
+  }
+}
+
+template <typename T, int NV>
+__global__ void __launch_bounds__(kThreads) scale_k(const T* __restrict__ w, const double* __restrict__ sq,
+                                                    T* __restrict__ out, int64_t n_slots) {
+  __shared__ double inv[8];
+  if (threadIdx.x < NV) inv[threadIdx.x] = sq[threadIdx.x] > 0.0 ? 1.0 / sqrt(sq[threadIdx.x]) : 0.0;
+  __syncthreads();
+  for (int64_t s = (int64_t)blockIdx.x * kThreads + threadIdx.x; s < n_slots; s += (int64_t)gridDim.x * kThreads) {
+    double wv[4];
+    Slot<T>::load(w + 4 * s, wv);
+    const int base = (int)((4 * s) % NV);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) wv[j] *= inv[(base + j) % NV];
+    Slot<T>::store(out + 4 * s, wv);
+  }
+}
+
+// In place per element: V_q <- sum_i V_i S[v][i][q], q < k.
+template <typename T, int NV>
+__global__ void __launch_bounds__(kThreads) combine_k(T* __restrict__ V, int64_t stride, int m,
+                                                      const double* __restrict__ S, int k, int64_t n_elems) {
+  extern __shared__ double Ss[];  // [NV][m][k]
+  for (int t = threadIdx.x; t < NV * m * k; t += kThreads) Ss[t] = S[t];
+  __syncthreads();
+  for (int64_t e = (int64_t)blockIdx.x * kThreads + threadIdx.x; e < n_elems; e += (int64_t)gridDim.x * kThreads) {
+    const int v = (int)(e % NV);
+    double vals[kMaxM];
+#pragma unroll
+    for (int i = 0; i < kMaxM; ++i)
+      if (i < m) vals[i] = (double)V[(int64_t)i * stride + e];
+    for (int q = 0; q < k; ++q) {
+      double a = 0.0;
+#pragma unroll
+      for (int i = 0; i < kMaxM; ++i)
+        if (i < m) a = fma(vals[i], Ss[(v * m + i) * k + q], a);
+      V[(int64_t)q * stride + e] = (T)a;
+    }
+  }
+}
+
+__device__ __forceinline__ uint64_t mix64(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+
+template <typename T>
+__global__ void random_k(T* __restrict__ x, int64_t n_valid, int64_t n_elems, uint64_t seed) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n_elems; e += (int64_t)gridDim.x * blockDim.x) {
+    const double u = (double)(mix64(seed ^ mix64((uint64_t)e)) >> 11) * (1.0 / 9007199254740992.0);
+    x[e] = e < n_valid ? (T)(2.0 * u - 1.0) : (T)0;
+  }
+}
+
+int check_common(int dtype, int64_t n_elems, int nvec, const char* where) {
+  EDG_REQUIRE(dtype == 0 || dtype == 1, "%s: dtype must be 0 (f64) or 1 (f32)", where);
+  EDG_REQUIRE(nvec == 1 || nvec == 2 || nvec == 4 || nvec == 8, "%s: nvec must be 1, 2, 4 or 8", where);
+  EDG_REQUIRE(n_elems >= 0 && n_elems % 4 == 0 && n_elems % nvec == 0,
+              "%s: n_elems must be a multiple of 4 and of nvec", where);
+  return EDG_OK;
+}
+
+template <typename T, int NV>
+int run_dots(int64_t n_elems, const void* V, int64_t stride, int m, const void* w, double* h, double* scratch,
+             cudaStream_t stream) {
+  const int64_t n_slots = n_elems / 4;
+  const int tiles = (m + kTile - 1) / kTile;
+  unsigned nbx = edg::grid_for(n_slots, kThreads, 8);
+  const unsigned cap = (unsigned)(edg::kSmCount * 8 / tiles);
+  if (nbx > cap && cap >= (unsigned)edg::kSmCount) nbx = cap;
+  dots_k<T, NV><<<dim3(nbx, tiles), kThreads, 0, stream>>>((const T*)V, stride, m, (const T*)w, n_slots, scratch);
+  dots_reduce_k<NV><<<m, kThreads, 0, stream>>>(scratch, (int)nbx, m, h);
+  return EDG_OK;
+}
+
+}  // namespace
+
+extern "C" int64_t edg_iv_scratch_elems(int64_t n_elems, int32_t m) {
+  if (n_elems < 0 || m < 1) return -1;
+  return (int64_t)edg::kSmCount * 8 * m * 8;  // blocks * m * (P * 4) with P * 4 <= 8
+}
+
+#define EDG_IV_DISPATCH(CALL)                                \
+  switch (nvec) {                                            \
+    case 1: st = dtype ? CALL(float, 1) : CALL(double, 1); break; \
+    case 2: st = dtype ? CALL(float, 2) : CALL(double, 2); break; \
+    case 4: st = dtype ? CALL(float, 4) : CALL(double, 4); break; \
+    default: st = dtype ? CALL(float, 8) : CALL(double, 8); break; \
+  }
+
+extern "C" int edg_iv_dots(int32_t dtype, int64_t n_elems, int32_t nvec, const void* V, int64_t stride, int32_t m,
+                           const void* w, double* h, double* scratch, cudaStream_t stream) {
+  int st = check_common(dtype, n_elems, nvec, "edg_iv_dots");
+  if (st != EDG_OK) return st;
+  EDG_REQUIRE(m >= 1 && V != nullptr && w != nullptr && h != nullptr && scratch != nullptr,
+              "edg_iv_dots: need m >= 1 and non-null buffers");
+  EDG_REQUIRE(stride % 4 == 0, "edg_iv_dots: stride must be a multiple of 4");
+  if (n_elems == 0) {
+    cudaError_t e = cudaMemsetAsync(h, 0, sizeof(double) * (size_t)m * nvec, stream);
+    return e == cudaSuccess ? EDG_OK : edg::cuda_status(e, "edg_iv_dots");
+  }
+#define CALL(T, NV) run_dots<T, NV>(n_elems, V, stride, m, w, h, scratch, stream)
+  EDG_IV_DISPATCH(CALL)
+#undef CALL
+  if (st != EDG_OK) return st;
+  EDG_CHECK_LAUNCH("edg_iv_dots");
+  return EDG_OK;
+}
+
+extern "C" int edg_iv_update(int32_t dtype, int64_t n_elems, int32_t nvec, const void* V, int64_t stride, int32_t m,
+                             const double* h, void* w, cudaStream_t stream) {
+  int st = check_common(dtype, n_elems, nvec, "edg_iv_update");
+  if (st != EDG_OK) return st;
+  EDG_REQUIRE(m >= 1 && m <= kMaxM && V != nullptr && w != nullptr && h != nullptr,
+              "edg_iv_update: need 1 <= m <= %d and non-null buffers", kMaxM);
+  EDG_REQUIRE(stride % 4 == 0, "edg_iv_update: stride must be a multiple of 4");
+  if (n_elems == 0) return EDG_OK;
+  const int64_t n_slots = n_elems / 4;
+  const unsigned grid = edg::grid_for(n_slots, kThreads, 8);
+#define CALL(T, NV) (update_k<T, NV><<<grid, kThreads, 0, stream>>>((const T*)V, stride, m, h, (T*)w, n_slots), EDG_OK)
+  EDG_IV_DISPATCH(CALL)
+#undef CALL
+  EDG_CHECK_LAUNCH("edg_iv_update");
+  return st;
+}
+
+extern "C" int edg_iv_scale(int32_t dtype, int64_t n_elems, int32_t nvec, const void* w, const double* sq, void* out,
+                            cudaStream_t stream) {
+  int st = check_common(dtype, n_elems, nvec, "edg_iv_scale");
+  if (st != EDG_OK) return st;
+  EDG_REQUIRE(w != nullptr && sq != nullptr && out != nullptr, "edg_iv_scale: null argument");
+  if (n_elems == 0) return EDG_OK;
+  const int64_t n_slots = n_elems / 4;
+  const unsigned grid = edg::grid_for(n_slots, kThreads, 8);
+#define CALL(T, NV) (scale_k<T, NV><<<grid, kThreads, 0, stream>>>((const T*)w, sq, (T*)out, n_slots), EDG_OK)
+  EDG_IV_DISPATCH(CALL)
+#undef CALL
+  EDG_CHECK_LAUNCH("edg_iv_scale");
+  return st;
+}
+
+extern "C" int edg_iv_combine(int32_t dtype, int64_t n_elems, int32_t nvec, void* V, int64_t stride, int32_t m,
+                              const double* S, int32_t k, cudaStream_t stream) {
+  int st = check_common(dtype, n_elems, nvec, "edg_iv_combine");
+  if (st != EDG_OK) return st;
+  EDG_REQUIRE(m >= 1 && m <= kMaxM && k >= 1 && k <= m, "edg_iv_combine: need 1 <= k <= m <= %d", kMaxM);
+  EDG_REQUIRE(V != nullptr && S != nullptr, "edg_iv_combine: null argument");
+  if (n_elems == 0) return EDG_OK;
+  const size_t smem = sizeof(double) * (size_t)nvec * m * k;
+  EDG_REQUIRE(smem <= 48 * 1024, "edg_iv_combine: nvec * m * k must be at most 6144");
+  const unsigned grid = edg::grid_for(n_elems, kThreads, 8);
+#define CALL(T, NV) \
+  (combine_k<T, NV><<<grid, kThreads, smem, stream>>>((T*)V, stride, m, S, k, n_elems), EDG_OK)
+  EDG_IV_DISPATCH(CALL)
+#undef CALL
+  EDG_CHECK_LAUNCH("edg_iv_combine");
+  return st;
+}
+
+extern "C" int edg_iv_random(int32_t dtype, int64_t n_rows, int64_t n_elems, int32_t nvec, uint64_t seed, void* x,
+                             cudaStream_t stream) {
+  int st = check_common(dtype, n_elems, nvec, "edg_iv_random");
+  if (st != EDG_OK) return st;
+  EDG_REQUIRE(x != nullptr && n_rows >= 0 && n_rows * nvec <= n_elems, "edg_iv_random: bad sizes");
+  if (n_elems == 0) return EDG_OK;
+  const unsigned grid = edg::grid_for(n_elems, kThreads, 8);
+  if (dtype == 0)
+    random_k<double><<<grid, kThreads, 0, stream>>>((double*)x, n_rows * nvec, n_elems, seed);
+  else
+    random_k<float><<<grid, kThreads, 0, stream>>>((float*)x, n_rows * nvec, n_elems, seed);
+  EDG_CHECK_LAUNCH("edg_iv_random");
+  return EDG_OK;
+}

@@ -13,10 +13,13 @@ from pathlib import Path
 from ._build import LIB_PATH
 
 __all__ = ["lib", "check", "EdgError", "MAX_SITES", "MAX_OPS", "SectorTables", "LookupTable", "Assembly",
-           "LanczosProblem", "SiteDims", "KrylovProblem", "SmallBatch", "EXPORTED_SYMBOLS", "ptr", "stream_handle"]
+           "LanczosProblem", "SiteDims", "KrylovProblem", "SmallBatch", "ZnTranslation", "ZnLattice", "ZnBasis",
+           "ZN_MAX_SITES", "ZN_MAX_GROUP", "EXPORTED_SYMBOLS", "ptr", "stream_handle"]
 
 MAX_SITES = 64
 MAX_OPS = 4
+ZN_MAX_SITES = 14
+ZN_MAX_GROUP = 32
 
 EDG_OK = 0
 STATUS_NAMES = {
@@ -39,6 +42,7 @@ P = C.c_void_p
 I32 = C.c_int32
 I64 = C.c_int64
 U64 = C.c_uint64
+U32 = C.c_uint32
 F64 = C.c_double
 
 
@@ -170,6 +174,41 @@ class SmallBatch(C.Structure):
     ]
 
 
+class ZnTranslation(C.Structure):
+    _fields_ = [
+        ("sf", I32), ("sx", I32), ("sm", I32), ("smx", I32),
+        ("hif", U64), ("lof", U64),
+        ("him", U32), ("lom", U32),
+        ("ylow", U32), ("yhigh", U32),
+        ("xhead", U32), ("xtail", U32),
+    ]
+
+
+class ZnLattice(C.Structure):
+    _fields_ = [
+        ("lx", I32), ("ly", I32), ("zn", I32), ("link_bits", I32),
+        ("n_sites", I32), ("n_links", I32), ("field_bits", I32), ("n_cot", I32),
+        ("n_gauss", I64), ("pow_cot", I64),
+        ("odd_mask", U32), ("even_mask", U32),
+        ("n_group", I32), ("n_div", I32),
+        ("divisors", I32 * 8),
+        ("group", ZnTranslation * ZN_MAX_GROUP),
+        ("cot_link", I32 * (2 * ZN_MAX_SITES)),
+        ("peel_site", I32 * ZN_MAX_SITES), ("peel_link", I32 * ZN_MAX_SITES), ("peel_sign", I32 * ZN_MAX_SITES),
+        ("peel_other", (I32 * 3) * ZN_MAX_SITES), ("peel_osign", (I32 * 3) * ZN_MAX_SITES),
+        ("link_tail", I32 * (2 * ZN_MAX_SITES)), ("link_head", I32 * (2 * ZN_MAX_SITES)),
+        ("link_eta", I32 * (2 * ZN_MAX_SITES)),
+        ("link_between", U32 * (2 * ZN_MAX_SITES)),
+        ("plaq", (I32 * 4) * ZN_MAX_SITES),
+        ("esq", F64 * 4),
+        ("chunk_lut", P), ("occ_rank", P), ("rank_occ", P),
+    ]
+
+
+class ZnBasis(C.Structure):
+    _fields_ = [("n_rows", I64), ("keys", P), ("orbit", P)]
+
+
 _SIGS = {
     "edg_get_last_error": (I32, [C.c_char_p, I32]),
     "edg_version": (I32, []),
@@ -197,6 +236,17 @@ _SIGS = {
     "edg_lanczos_small_batched": (I32, [C.POINTER(SmallBatch), P, P]),
     "edg_krylov_workspace_bytes": (I64, [C.POINTER(KrylovProblem)]),
     "edg_krylov_step": (I32, [C.POINTER(KrylovProblem), P, F64, P, I64, P, P]),
+    "edg_zn_bitmap_words": (I64, [C.POINTER(ZnLattice)]),
+    "edg_zn_mark": (I32, [C.POINTER(ZnLattice), P, P, P]),
+    "edg_zn_fill": (I32, [C.POINTER(ZnLattice), P, P, P, P]),
+    "edg_zn_orbit_table": (I32, [C.POINTER(ZnLattice), P, I64, P, P]),
+    "edg_zn_matvec": (I32, [C.POINTER(ZnLattice), C.POINTER(ZnBasis), P, I32, I32, P, P, P]),
+    "edg_iv_scratch_elems": (I64, [I64, I32]),
+    "edg_iv_dots": (I32, [I32, I64, I32, P, I64, I32, P, P, P, P]),
+    "edg_iv_update": (I32, [I32, I64, I32, P, I64, I32, P, P, P]),
+    "edg_iv_scale": (I32, [I32, I64, I32, P, P, P, P]),
+    "edg_iv_combine": (I32, [I32, I64, I32, P, I64, I32, P, I32, P]),
+    "edg_iv_random": (I32, [I32, I64, I64, I32, U64, P, P]),
 }
 
 EXPORTED_SYMBOLS = tuple(_SIGS)

@@ -391,6 +391,114 @@ int edg_local_expval(const uint64_t* keys, int64_t n, const edg_site_dims* dims,
                      int64_t psi_stride, const double* diag, int32_t dmax,
                      double* out, cudaStream_t stream);
 
+/* ------------------------------------------------------------------------
+ * Matrix-free Z_n lattice gauge theory with staggered fermions (periodic
+ * Lx x Ly, Gauss law, zero charge, optional zero momentum).
+ *
+ * No reference counterpart computes this model: ed-lgt raises for odd n
+ * with matter (edlgt/operators/Zn_operators.py:153-157).  The pieces it
+ * replaces are the momentum-basis builders (get_momentum_basis,
+ * edlgt/symmetries/translational_sym.py:1307-1358; build_all_translations
+ * :567-617; select_references :620-694; momentum_basis_zero_k :697-819), the
+ * sector enumeration (symmetry_sector.py:785-967) and the projected n-body
+ * triplets with their CSR matvec (nbody_data_momentum*,
+ * translational_sym.py:1394-1969; csr_spmv, qmb_hamiltonian.py:705-730):
+ * the Hamiltonian is never stored, each matvec recomputes its elements from
+ * the packed representative configurations.
+ *
+ * Packed key: link l = 2 s + mu has its field at bits
+ * [link_bits * l, link_bits * (l + 1)); site s's occupation at bit
+ * field_bits + s.  Gauss index: colex rank of the occupied-site set times
+ * zn^n_cot plus the cotree fields as base-zn digits.
+ * ------------------------------------------------------------------------ */
+#define EDG_ZN_MAX_SITES 14
+#define EDG_ZN_MAX_GROUP 32
+
+typedef struct {
+  int32_t sf, sx;   /* field bits: lane-array rotation, rotation inside each lane */
+  int32_t sm, smx;  /* occupation bits: the same two rotations */
+  uint64_t hif, lof; /* field bits at lane positions >= sx / < sx */
+  uint32_t him, lom; /* occupation bits at lane positions >= smx / < smx */
+  uint32_t ylow, yhigh; /* occupied rows that stay below / wrap around in y */
+  uint32_t xhead, xtail; /* row-0 sites that stay / wrap around in x */
+} edg_zn_translation;
+
+typedef struct {
+  int32_t lx, ly, zn, link_bits;
+  int32_t n_sites, n_links, field_bits, n_cot;
+  int64_t n_gauss;  /* sector size before momentum: n_matter * zn^n_cot (< 2^32) */
+  int64_t pow_cot;  /* zn^n_cot */
+  uint32_t odd_mask;  /* sites with static charge offset 1 (x odd) */
+  uint32_t even_mask; /* sites with eta = +1 */
+  int32_t n_group;    /* translations, element 0 the identity */
+  int32_t n_div;      /* stabiliser sizes (divisors of n_group), at most 8 */
+  int32_t divisors[8];
+  edg_zn_translation group[EDG_ZN_MAX_GROUP];
+  int32_t cot_link[2 * EDG_ZN_MAX_SITES]; /* cotree link of digit c */
+  /* Gauss-law peeling order, children before parents */
+  int32_t peel_site[EDG_ZN_MAX_SITES], peel_link[EDG_ZN_MAX_SITES], peel_sign[EDG_ZN_MAX_SITES];
+  int32_t peel_other[EDG_ZN_MAX_SITES][3], peel_osign[EDG_ZN_MAX_SITES][3];
+  /* Hamiltonian geometry: link tail/head sites, Kogut-Susskind phase,
+   * occupation mask strictly between tail and head (Jordan-Wigner order) */
+  int32_t link_tail[2 * EDG_ZN_MAX_SITES], link_head[2 * EDG_ZN_MAX_SITES];
+  int32_t link_eta[2 * EDG_ZN_MAX_SITES];
+  uint32_t link_between[2 * EDG_ZN_MAX_SITES];
+  int32_t plaq[EDG_ZN_MAX_SITES][4]; /* links raised, raised, lowered, lowered by U_p */
+  double esq[4];                     /* E^2 of each field value */
+  const uint64_t* chunk_lut;  /* device [ceil(field_bits / 8)][256]: cotree digits of a key byte */
+  const uint32_t* occ_rank;   /* device [2^n_sites]: colex rank, 0xFFFFFFFF off-sector */
+  const uint32_t* rank_occ;   /* device [n_matter]: occupation bits of a rank */
+} edg_zn_lattice;
+
+typedef struct {
+  int64_t n_rows;
+  const uint64_t* keys;   /* [n_rows] representatives, ascending Gauss index */
+  const uint32_t* orbit;  /* [n_gauss] row | divisor index << 28 | sign << 31, or 0xFFFFFFFF */
+} edg_zn_basis;
+
+/* Number of 64-bit bitmap words over the Gauss index range. */
+int64_t edg_zn_bitmap_words(const edg_zn_lattice* L);
+/* Marks the zero-momentum representatives (smallest key of their orbit, no
+ * stabiliser element of sign -1): bitmap [words], counts [words] = popcount. */
+int edg_zn_mark(const edg_zn_lattice* L, uint64_t* bitmap, int64_t* counts, cudaStream_t stream);
+/* keys[offsets[w] + j] = the j-th representative of word w (offsets: exclusive scan of counts). */
+int edg_zn_fill(const edg_zn_lattice* L, const uint64_t* bitmap, const int64_t* offsets,
+                uint64_t* keys, cudaStream_t stream);
+/* orbit[gidx(T_g r)] = (row of r, stabiliser size, sign of T_g on r) for all g;
+ * 0xFFFFFFFF elsewhere.  n_rows < 2^28 - 1. */
+int edg_zn_orbit_table(const edg_zn_lattice* L, const uint64_t* keys, int64_t n_rows,
+                       uint32_t* orbit, cudaStream_t stream);
+/* y = H x for nvec instances at once, x and y interleaved [row][nvec]
+ * (dtype 0 f64, 1 f32; nvec 1, 2, 4 or 8); couplings [nvec][4] = (t, m,
+ * g^2/2, -1/(2 g^2)) in device memory; f64 accumulation. */
+int edg_zn_matvec(const edg_zn_lattice* L, const edg_zn_basis* B, const double* couplings,
+                  int32_t nvec, int32_t dtype, const void* x, void* y, cudaStream_t stream);
+
+/* ------------------------------------------------------------------------
+ * Batched interleaved vectors: nvec instances stored [row][nvec], the total
+ * element count n_elems a multiple of 4 with padding entries zero; basis
+ * vector i at V + i * stride elements (stride a multiple of 4).
+ * Building blocks of the thick-restart Lanczos that drives the matrix-free
+ * matvec (scipy eigsh's role, qmb_hamiltonian.py:313).
+ * ------------------------------------------------------------------------ */
+int64_t edg_iv_scratch_elems(int64_t n_elems, int32_t m);
+/* h[i * nvec + v] = sum over rows of V_i * w for instance v, i < m (f64). */
+int edg_iv_dots(int32_t dtype, int64_t n_elems, int32_t nvec, const void* V, int64_t stride,
+                int32_t m, const void* w, double* h, double* scratch, cudaStream_t stream);
+/* w -= sum_i V_i h[i * nvec + v] per instance v. */
+int edg_iv_update(int32_t dtype, int64_t n_elems, int32_t nvec, const void* V, int64_t stride,
+                  int32_t m, const double* h, void* w, cudaStream_t stream);
+/* out = w / sqrt(sq[v]) per instance (0 where sq <= 0). */
+int edg_iv_scale(int32_t dtype, int64_t n_elems, int32_t nvec, const void* w, const double* sq,
+                 void* out, cudaStream_t stream);
+/* In place, per row: V_q <- sum_{i<m} V_i S[v][i][q] for q < k (S device f64 [nvec][m][k]);
+ * m <= 32, k <= m. */
+int edg_iv_combine(int32_t dtype, int64_t n_elems, int32_t nvec, void* V, int64_t stride,
+                   int32_t m, const double* S, int32_t k, cudaStream_t stream);
+/* x = uniform(-1, 1) from (seed, element) for rows < n_rows, 0 in the padding. */
+int edg_iv_random(int32_t dtype, int64_t n_rows, int64_t n_elems, int32_t nvec, uint64_t seed,
+                  void* x, cudaStream_t stream);
+
 #ifdef __cplusplus
 }
 #endif
