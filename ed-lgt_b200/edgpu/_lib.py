@@ -256,7 +256,7 @@ def _load():
     path = Path(LIB_PATH)
     if not path.exists():
         raise ImportError(
-            f"libedgpu.so not found at {path}; build it with `python -m edgpu._build` "
+            f"libedgpu.so not found at {path}; build it with `python ed-lgt_b200/edgpu/_build.py` "
             "(there is no CPU fallback for the engine)"
         )
     handle = C.CDLL(str(path))
