@@ -111,3 +111,28 @@ def test_lattice_rejects_bad_shapes():
         ZnLattice((4, 4), 3)
     with pytest.raises(ValueError):
         ZnLattice((2, 2), 5)
+
+
+@pytest.mark.parametrize("lx,ly,n", [(2, 2, 3), (2, 3, 3), (2, 2, 2), (2, 3, 2), (2, 2, 4)])
+def test_oracle_pinned_by_reference_kernels(lx, ly, n):
+    """The oracle's full Gauss-law sector Hamiltonian against the one ed-lgt's
+    own sector builder and nbody_term produce from dressed-site Z_n tables
+    (tests/golden/make_zn_golden.py): dimension, tr H, ||H||_F^2 and the three
+    lowest eigenvalues, all basis independent."""
+    import os
+
+    from scipy.sparse.linalg import eigsh
+
+    gold = np.load(os.path.join(os.path.dirname(__file__), "golden", "zn_cases.npz"))
+    tag = f"{lx}x{ly}_z{n}"
+    o = ZnOracle(lx, ly, n, momentum=False)
+    assert o.dim == int(gold[f"{tag}_dim"])
+    for i, (t, m, g) in enumerate(gold["couplings"]):
+        H = o.hamiltonian(t, m, g, momentum=False)
+        assert np.isclose(H.diagonal().sum(), gold[f"{tag}_trace"][i], rtol=1e-12, atol=1e-9)
+        assert np.isclose((abs(H).power(2)).sum(), gold[f"{tag}_fro2"][i], rtol=1e-12)
+        if o.dim <= 3000:
+            e = np.linalg.eigvalsh(H.toarray())[:3]
+        else:
+            e = np.sort(eigsh(H, k=3, which="SA", tol=0, return_eigenvectors=False))
+        assert np.allclose(e, gold[f"{tag}_energies"][i], rtol=1e-10, atol=1e-10)
