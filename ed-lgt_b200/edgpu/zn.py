@@ -188,6 +188,7 @@ def trlan_batched(apply, n_rows, nvec, dtype, m, k_keep, k_want, tol, max_cycles
     T = np.zeros((nvec, m, m))
     j0 = 0
     n_mv = 0
+    launches = 4  # random start, norm (dots + reduce), scale
     mv_events = []
     converged = np.zeros(nvec, dtype=bool)
     theta = np.zeros((nvec, k_want))
@@ -197,12 +198,11 @@ def trlan_batched(apply, n_rows, nvec, dtype, m, k_keep, k_want, tol, max_cycles
     cycles = 0
     for cycles in range(1, max_cycles + 1):
         for j in range(j0, m):
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
+            e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
             e0.record()
             apply(V[j], w)
             e1.record()
-            mv_events.append((e0, e1))
+            mv_events.append((e0, e1, e2))
             n_mv += 1
             for p in range(2):
                 h = rec[j, p]
@@ -211,6 +211,8 @@ def trlan_batched(apply, n_rows, nvec, dtype, m, k_keep, k_want, tol, max_cycles
             sq = rec[j, 2, 0]
             _ivec("edg_iv_dots", dtype, E, nvec, ptr(w), E, 1, ptr(w), ptr(sq), ptr(scratch), st)
             _ivec("edg_iv_scale", dtype, E, nvec, ptr(w), ptr(sq), ptr(V[j + 1]), st)
+            e2.record()
+            launches += 10  # matvec, 3 x (dots + reduce), 2 x update, scale
         R = rec.cpu().numpy()
         for j in range(j0, m):
             hcol = R[j, 0, : j + 1] + R[j, 1, : j + 1]  # [j+1, nvec]
@@ -236,6 +238,7 @@ def trlan_batched(apply, n_rows, nvec, dtype, m, k_keep, k_want, tol, max_cycles
         # thick restart: keep the k_keep lowest Ritz vectors, continue from V[m]
         Sk = torch.from_numpy(np.ascontiguousarray(S_all[:, :, :k_keep])).to(dev)
         _ivec("edg_iv_combine", dtype, E, nvec, ptr(V), E, m, ptr(Sk), k_keep, st)
+        launches += 1
         V[k_keep].copy_(V[m])
         T[:] = 0.0
         for v in range(nvec):
@@ -244,11 +247,15 @@ def trlan_batched(apply, n_rows, nvec, dtype, m, k_keep, k_want, tol, max_cycles
         j0 = k_keep
     Sk = torch.from_numpy(np.ascontiguousarray(S_all[:, :, :k_want])).to(dev)
     _ivec("edg_iv_combine", dtype, E, nvec, ptr(V), E, m, ptr(Sk), k_want, st)
+    launches += 1
     torch.cuda.synchronize()
-    mv_ms = sum(a.elapsed_time(b) for a, b in mv_events)
+    mv_ms = sum(a.elapsed_time(b) for a, b, _ in mv_events)
+    ro_ms = sum(b.elapsed_time(c) for _, b, c in mv_events)
     if stats is not None:
         stats["matvec_ms"] = stats.get("matvec_ms", 0.0) + mv_ms
+        stats["reorth_ms"] = stats.get("reorth_ms", 0.0) + ro_ms
         stats["matvecs"] = stats.get("matvecs", 0) + n_mv
+        stats["launches"] = stats.get("launches", 0) + launches
     out = V[:k_want].clone()
     return theta, res, out, n_mv, cycles, converged
 
@@ -256,6 +263,7 @@ def trlan_batched(apply, n_rows, nvec, dtype, m, k_keep, k_want, tol, max_cycles
 def _auto_m(vec_bytes, cap, reserve_vectors=3):
     """Basis length that fits the free device memory (w, a copy and a margin
     besides the basis), at most cap."""
+    torch.cuda.empty_cache()  # blocks cached by torch count as free here
     free, _ = torch.cuda.mem_get_info()
     fit = int((free - (1 << 30)) // max(vec_bytes, 1)) - reserve_vectors
     return max(4, min(cap, fit))
@@ -315,7 +323,10 @@ def zn_lowest(engine, couplings, k=1, precision="mixed", m=None, k_keep=None, to
                      matvecs64=nmv64, cycles64=cyc64, matvec64_ms=s64.get("matvec_ms", 0.0),
                      theta32=th32[:n_inst].copy(), res32=res32[:n_inst].copy())
         stats["matvec_ms"] = s32.get("matvec_ms", 0.0) + s64.get("matvec_ms", 0.0)
+        stats["reorth_ms"] = s32.get("reorth_ms", 0.0) + s64.get("reorth_ms", 0.0)
+        stats["reorth32_ms"] = s32.get("reorth_ms", 0.0)
         stats["matvecs"] = nmv32 + nmv64
+        stats["launches"] = s32.get("launches", 0) + s64.get("launches", 0) + 1  # + convert
         cycles = cyc32 + cyc64
     else:
         raise ValueError("precision must be 'mixed' or 'fp64'")
