@@ -2,10 +2,11 @@
 // of all instances is one contiguous 32-byte sector (8 f32) and the
 // matrix-free matvec gathers every instance of a column with one load.
 //
-// Kernels for the Gram-Schmidt steps of a batched (thick-restart) Lanczos:
-// each thread owns slots of 4 consecutive elements (one float4 / two
+// Kernels for the Gram-Schmidt steps of a batched (thick-restart) Lanczos.
+// The streaming updates own slots of 4 consecutive elements (one float4 / two
 // double2), so the instance of slot element j is (4 * slot + j) % nvec; for
 // nvec = 8 that is fixed by the slot parity, which the grid-stride loop keeps.
+// Dots tile the basis (grid y) so that their f64 accumulators stay few.
 // Dots accumulate in f64 and reduce deterministically (per-CTA partials, then
 // one CTA per output in a fixed order).
 #include "internal.cuh"
@@ -14,7 +15,6 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
-constexpr int kTile = 8;   // basis vectors per dots CTA
 constexpr int kMaxM = 32;  // basis vectors per combine
 
 template <typename T>
@@ -46,51 +46,6 @@ struct Slot<double> {
 template <int NV>
 constexpr int classes() { return NV > 4 ? NV / 4 : 1; }
 
-// partial[block][i][class][4] over a tile of basis vectors [i0, i0 + kTile).
-template <typename T, int NV>
-__global__ void __launch_bounds__(kThreads) dots_k(const T* __restrict__ V, int64_t stride, int m,
-                                                   const T* __restrict__ w, int64_t n_slots,
-                                                   double* __restrict__ partial) {
-  constexpr int P = classes<NV>();
-  __shared__ double red[kWarps][kTile][P][4];
-  const int i0 = blockIdx.y * kTile;
-  const int ni = min(kTile, m - i0);
-  double acc[kTile][4];
-#pragma unroll
-  for (int i = 0; i < kTile; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
-  for (int64_t s = (int64_t)blockIdx.x * kThreads + threadIdx.x; s < n_slots; s += (int64_t)gridDim.x * kThreads) {
-    double wv[4], vv[4];
-    Slot<T>::load(w + 4 * s, wv);
-#pragma unroll
-    for (int i = 0; i < kTile; ++i) {
-      if (i < ni) {
-        Slot<T>::load(V + (int64_t)(i0 + i) * stride + 4 * s, vv);
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = fma(vv[j], wv[j], acc[i][j]);
-      }
-    }
-  }
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-  for (int i = 0; i < kTile; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      double a = acc[i][j];
-#pragma unroll
-      for (int o = 16; o >= P; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
-      if (lane < P) red[warp][i][lane][j] = a;
-    }
-  __syncthreads();
-  for (int t = threadIdx.x; t < kTile * P * 4; t += kThreads) {
-    const int i = t / (P * 4), c = (t / 4) % P, j = t % 4;
-    double a = 0.0;
-    for (int k = 0; k < kWarps; ++k) a += red[k][i][c][j];
-    if (i < ni) partial[((int64_t)blockIdx.x * m + i0 + i) * (P * 4) + c * 4 + j] = a;
-  }
-}
-
 // h[i * nvec + v] = sum over CTAs and over the slot entries of instance v.
 template <int NV>
 __global__ void __launch_bounds__(kThreads) dots_reduce_k(const double* __restrict__ partial, int nblk, int m,
@@ -120,6 +75,54 @@ __global__ void __launch_bounds__(kThreads) dots_reduce_k(const double* __restri
       if (q % NV == v)
         for (int k = 0; k < kWarps; ++k) t += red[k][q];
     h[(int64_t)i * NV + v] = t;
+  }
+}
+
+// partial[block][i][class][4] over a tile of KT basis vectors [i0, i0 + KT):
+// float4 / double2 slot loads (narrower loads do not keep HBM busy), f64
+// accumulators; KT = 4 keeps them to 16 registers pairs, KT = 8 reads w once
+// for m <= 8.
+template <typename T, int NV, int KT>
+__global__ void __launch_bounds__(kThreads) dots_k(const T* __restrict__ V, int64_t stride, int m,
+                                                   const T* __restrict__ w, int64_t n_slots,
+                                                   double* __restrict__ partial) {
+  constexpr int P = classes<NV>();
+  __shared__ double red[kWarps][KT][P][4];
+  const int i0 = blockIdx.y * KT;
+  const int ni = min(KT, m - i0);
+  double acc[KT][4];
+#pragma unroll
+  for (int i = 0; i < KT; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+  for (int64_t s = (int64_t)blockIdx.x * kThreads + threadIdx.x; s < n_slots; s += (int64_t)gridDim.x * kThreads) {
+    double wv[4], vv[4];
+    Slot<T>::load(w + 4 * s, wv);
+#pragma unroll
+    for (int i = 0; i < KT; ++i) {
+      if (i < ni) {
+        Slot<T>::load(V + (int64_t)(i0 + i) * stride + 4 * s, vv);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = fma(vv[j], wv[j], acc[i][j]);
+      }
+    }
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int i = 0; i < KT; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      double a = acc[i][j];
+#pragma unroll
+      for (int o = 16; o >= P; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+      if (lane < P) red[warp][i][lane][j] = a;
+    }
+  __syncthreads();
+  for (int t = threadIdx.x; t < KT * P * 4; t += kThreads) {
+    const int i = t / (P * 4), c = (t / 4) % P, j = t % 4;
+    double a = 0.0;
+    for (int k = 0; k < kWarps; ++k) a += red[k][i][c][j];
+    if (i < ni) partial[((int64_t)blockIdx.x * m + i0 + i) * (P * 4) + c * 4 + j] = a;
   }
 }
 
@@ -159,26 +162,107 @@ __global__ void __launch_bounds__(kThreads) scale_k(const T* __restrict__ w, con
   }
 }
 
-// In place per element: V_q <- sum_i V_i S[v][i][q], q < k.
-template <typename T, int NV>
+// In place per element: V_q <- sum_i V_i S[v][i][q], q < k.  Streams over
+// the m inputs with the k outputs in f64 registers (KB >= k); every input of
+// an element is read before any output of it is written.  The coefficient
+// blocks of the instances are stored with an odd stride (m k + 1) so the
+// eight instances of a warp read different shared-memory banks.
+template <typename T, int NV, int KB>
 __global__ void __launch_bounds__(kThreads) combine_k(T* __restrict__ V, int64_t stride, int m,
                                                       const double* __restrict__ S, int k, int64_t n_elems) {
-  extern __shared__ double Ss[];  // [NV][m][k]
-  for (int t = threadIdx.x; t < NV * m * k; t += kThreads) Ss[t] = S[t];
+  extern __shared__ double Ss[];  // [NV][m k + 1]
+  const int sp = m * k + 1;
+  for (int t = threadIdx.x; t < NV * m * k; t += kThreads) Ss[(t / (m * k)) * sp + t % (m * k)] = S[t];
   __syncthreads();
   for (int64_t e = (int64_t)blockIdx.x * kThreads + threadIdx.x; e < n_elems; e += (int64_t)gridDim.x * kThreads) {
-    const int v = (int)(e % NV);
-    double vals[kMaxM];
+    const double* Sv = Ss + (int)(e % NV) * sp;
+    double acc[KB];
 #pragma unroll
-    for (int i = 0; i < kMaxM; ++i)
-      if (i < m) vals[i] = (double)V[(int64_t)i * stride + e];
-    for (int q = 0; q < k; ++q) {
-      double a = 0.0;
+    for (int q = 0; q < KB; ++q) acc[q] = 0.0;
+#pragma unroll 4
+    for (int i = 0; i < m; ++i) {
+      const double x = (double)V[(int64_t)i * stride + e];
 #pragma unroll
-      for (int i = 0; i < kMaxM; ++i)
-        if (i < m) a = fma(vals[i], Ss[(v * m + i) * k + q], a);
-      V[(int64_t)q * stride + e] = (T)a;
+      for (int q = 0; q < KB; ++q)
+        if (q < k) acc[q] = fma(x, Sv[i * k + q], acc[q]);
     }
+#pragma unroll
+    for (int q = 0; q < KB; ++q)
+      if (q < k) V[(int64_t)q * stride + e] = (T)acc[q];
+  }
+}
+
+// Second Gram-Schmidt pass fused with the norm (update_k's slot layout):
+// w <- w - sum_{i<m} V_i h[i][v], and per CTA the squared norms of the
+// stored (rounded) w by slot class, partial[blk][class * 4 + j], reduced by
+// dots_reduce_k like a one-vector dot.
+template <typename T, int NV>
+__global__ void __launch_bounds__(kThreads) update_norm_k(const T* __restrict__ V, int64_t stride, int m,
+                                                          const double* __restrict__ h, T* __restrict__ w,
+                                                          int64_t n_slots, double* __restrict__ partial) {
+  constexpr int P = classes<NV>();
+  __shared__ double hs[kMaxM * 8];
+  __shared__ double red[kWarps][P][4];
+  for (int t = threadIdx.x; t < m * NV; t += kThreads) hs[t] = h[t];
+  __syncthreads();
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int64_t s = (int64_t)blockIdx.x * kThreads + threadIdx.x; s < n_slots; s += (int64_t)gridDim.x * kThreads) {
+    double wv[4], vv[4];
+    Slot<T>::load(w + 4 * s, wv);
+    const int base = (int)((4 * s) % NV);
+    for (int i = 0; i < m; ++i) {
+      Slot<T>::load(V + (int64_t)i * stride + 4 * s, vv);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) wv[j] = fma(-vv[j], hs[i * NV + (base + j) % NV], wv[j]);
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      wv[j] = (double)(T)wv[j];
+      acc[j] = fma(wv[j], wv[j], acc[j]);
+    }
+    Slot<T>::store(w + 4 * s, wv);
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    double a = acc[j];
+#pragma unroll
+    for (int o = 16; o >= P; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    if (lane < P) red[warp][lane][j] = a;
+  }
+  __syncthreads();
+  if (threadIdx.x < P * 4) {
+    const int c = threadIdx.x / 4, j = threadIdx.x % 4;
+    double a = 0.0;
+    for (int k = 0; k < kWarps; ++k) a += red[k][c][j];
+    partial[(int64_t)blockIdx.x * (P * 4) + threadIdx.x] = a;
+  }
+}
+
+// out[o * NV + v] = sum over blocks of partial[blk][o][v]; one CTA per o.
+template <int NV>
+__global__ void __launch_bounds__(kThreads) reduce_nv_k(const double* __restrict__ partial, int nblk, int n_out,
+                                                        double* __restrict__ out) {
+  __shared__ double red[kWarps][NV];
+  const int o = blockIdx.x;
+  double a[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) a[v] = 0.0;
+  for (int b = threadIdx.x; b < nblk; b += kThreads)
+#pragma unroll
+    for (int v = 0; v < NV; ++v) a[v] += partial[((int64_t)b * n_out + o) * NV + v];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) a[v] += __shfl_xor_sync(0xffffffffu, a[v], off);
+    if (lane == 0) red[warp][v] = a[v];
+  }
+  __syncthreads();
+  if (threadIdx.x < NV) {
+    double t = 0.0;
+    for (int k = 0; k < kWarps; ++k) t += red[k][threadIdx.x];
+    out[(int64_t)o * NV + threadIdx.x] = t;
   }
 }
 
@@ -205,16 +289,55 @@ int check_common(int dtype, int64_t n_elems, int nvec, const char* where) {
   return EDG_OK;
 }
 
+template <typename T, int NV, int KT>
+int run_dots_kt(int64_t n_elems, const void* V, int64_t stride, int m, const void* w, double* h, double* scratch,
+                cudaStream_t stream) {
+  const int64_t n_slots = n_elems / 4;
+  const int tiles = (m + KT - 1) / KT;
+  int per_sm = 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dots_k<T, NV, KT>, kThreads, 0) != cudaSuccess ||
+      per_sm < 1)
+    per_sm = 1;
+  int64_t nbx = edg::ceil_div(n_slots, kThreads);
+  const int64_t cap = (int64_t)edg::kSmCount * (per_sm < 8 ? per_sm : 8);
+  const int64_t cap_t = cap / tiles > edg::kSmCount ? cap / tiles : edg::kSmCount;
+  if (nbx > cap_t) nbx = cap_t;
+  if (nbx < 1) nbx = 1;
+  dots_k<T, NV, KT><<<dim3((unsigned)nbx, tiles), kThreads, 0, stream>>>((const T*)V, stride, m, (const T*)w,
+                                                                        n_slots, scratch);
+  dots_reduce_k<NV><<<m, kThreads, 0, stream>>>(scratch, (int)nbx, m, h);
+  return EDG_OK;
+}
+
 template <typename T, int NV>
 int run_dots(int64_t n_elems, const void* V, int64_t stride, int m, const void* w, double* h, double* scratch,
              cudaStream_t stream) {
+  if (m <= 8) return run_dots_kt<T, NV, 8>(n_elems, V, stride, m, w, h, scratch, stream);
+  return run_dots_kt<T, NV, 4>(n_elems, V, stride, m, w, h, scratch, stream);
+}
+
+template <typename T, int NV>
+int run_norm(int64_t n_elems, const void* V, int64_t stride, int m, const double* h, void* w, double* out,
+             double* scratch, cudaStream_t stream) {
   const int64_t n_slots = n_elems / 4;
-  const int tiles = (m + kTile - 1) / kTile;
-  unsigned nbx = edg::grid_for(n_slots, kThreads, 8);
-  const unsigned cap = (unsigned)(edg::kSmCount * 8 / tiles);
-  if (nbx > cap && cap >= (unsigned)edg::kSmCount) nbx = cap;
-  dots_k<T, NV><<<dim3(nbx, tiles), kThreads, 0, stream>>>((const T*)V, stride, m, (const T*)w, n_slots, scratch);
-  dots_reduce_k<NV><<<m, kThreads, 0, stream>>>(scratch, (int)nbx, m, h);
+  const unsigned nblk = edg::grid_for(n_slots, kThreads, 8);
+  update_norm_k<T, NV><<<nblk, kThreads, 0, stream>>>((const T*)V, stride, m, h, (T*)w, n_slots, scratch);
+  dots_reduce_k<NV><<<1, kThreads, 0, stream>>>(scratch, (int)nblk, 1, out);
+  return EDG_OK;
+}
+
+template <typename T, int NV>
+int run_combine(int64_t n_elems, void* V, int64_t stride, int m, const double* S, int k, size_t smem,
+                cudaStream_t stream) {
+  const unsigned grid = edg::grid_for(n_elems, kThreads, 8);
+  if (k <= 4)
+    combine_k<T, NV, 4><<<grid, kThreads, smem, stream>>>((T*)V, stride, m, S, k, n_elems);
+  else if (k <= 8)
+    combine_k<T, NV, 8><<<grid, kThreads, smem, stream>>>((T*)V, stride, m, S, k, n_elems);
+  else if (k <= 16)
+    combine_k<T, NV, 16><<<grid, kThreads, smem, stream>>>((T*)V, stride, m, S, k, n_elems);
+  else
+    combine_k<T, NV, 32><<<grid, kThreads, smem, stream>>>((T*)V, stride, m, S, k, n_elems);
   return EDG_OK;
 }
 
@@ -291,11 +414,9 @@ extern "C" int edg_iv_combine(int32_t dtype, int64_t n_elems, int32_t nvec, void
   EDG_REQUIRE(m >= 1 && m <= kMaxM && k >= 1 && k <= m, "edg_iv_combine: need 1 <= k <= m <= %d", kMaxM);
   EDG_REQUIRE(V != nullptr && S != nullptr, "edg_iv_combine: null argument");
   if (n_elems == 0) return EDG_OK;
-  const size_t smem = sizeof(double) * (size_t)nvec * m * k;
-  EDG_REQUIRE(smem <= 48 * 1024, "edg_iv_combine: nvec * m * k must be at most 6144");
-  const unsigned grid = edg::grid_for(n_elems, kThreads, 8);
-#define CALL(T, NV) \
-  (combine_k<T, NV><<<grid, kThreads, smem, stream>>>((T*)V, stride, m, S, k, n_elems), EDG_OK)
+  const size_t smem = sizeof(double) * ((size_t)nvec * (m * k + 1));
+  EDG_REQUIRE(smem <= 48 * 1024, "edg_iv_combine: nvec * m * k too large for shared memory");
+#define CALL(T, NV) run_combine<T, NV>(n_elems, V, stride, m, S, k, smem, stream)
   EDG_IV_DISPATCH(CALL)
 #undef CALL
   EDG_CHECK_LAUNCH("edg_iv_combine");
@@ -314,5 +435,25 @@ extern "C" int edg_iv_random(int32_t dtype, int64_t n_rows, int64_t n_elems, int
   else
     random_k<float><<<grid, kThreads, 0, stream>>>((float*)x, n_rows * nvec, n_elems, seed);
   EDG_CHECK_LAUNCH("edg_iv_random");
+  return EDG_OK;
+}
+
+extern "C" int edg_iv_update_norm(int32_t dtype, int64_t n_elems, int32_t nvec, const void* V, int64_t stride,
+                                  int32_t m, const double* h, void* w, double* sq, double* scratch,
+                                  cudaStream_t stream) {
+  int st = check_common(dtype, n_elems, nvec, "edg_iv_update_norm");
+  if (st != EDG_OK) return st;
+  EDG_REQUIRE(m >= 1 && m <= kMaxM && V != nullptr && h != nullptr && w != nullptr && sq != nullptr &&
+                  scratch != nullptr,
+              "edg_iv_update_norm: need 1 <= m <= %d and non-null buffers", kMaxM);
+  if (n_elems == 0) {
+    cudaError_t e = cudaMemsetAsync(sq, 0, sizeof(double) * (size_t)nvec, stream);
+    return e == cudaSuccess ? EDG_OK : edg::cuda_status(e, "edg_iv_update_norm");
+  }
+#define CALL(T, NV) run_norm<T, NV>(n_elems, V, stride, m, h, w, sq, scratch, stream)
+  EDG_IV_DISPATCH(CALL)
+#undef CALL
+  if (st != EDG_OK) return st;
+  EDG_CHECK_LAUNCH("edg_iv_update_norm");
   return EDG_OK;
 }

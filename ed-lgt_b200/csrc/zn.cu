@@ -183,59 +183,44 @@ __global__ void __launch_bounds__(256) zn_orbit_k(const __grid_constant__ edg_zn
 }
 
 // ---------------------------------------------------------------- matvec
+// One x row (the nvec interleaved instances of a column) in 16-byte loads.
 template <typename T, int NV>
-struct Row {
-  __device__ static __forceinline__ void load(const T* __restrict__ p, double (&v)[NV]) {
+__device__ __forceinline__ void load_row(const T* __restrict__ p, T (&v)[NV]) {
+  if constexpr (NV * sizeof(T) >= 16) {
+    constexpr int kVec = 16 / sizeof(T);
 #pragma unroll
-    for (int i = 0; i < NV; ++i) v[i] = (double)p[i];
-  }
-};
-template <>
-struct Row<float, 8> {
-  __device__ static __forceinline__ void load(const float* __restrict__ p, double (&v)[8]) {
-    const float4 a = __ldg(reinterpret_cast<const float4*>(p));
-    const float4 b = __ldg(reinterpret_cast<const float4*>(p) + 1);
-    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
-    v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
-  }
-};
-template <>
-struct Row<float, 4> {
-  __device__ static __forceinline__ void load(const float* __restrict__ p, double (&v)[4]) {
-    const float4 a = __ldg(reinterpret_cast<const float4*>(p));
-    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
-  }
-};
-template <>
-struct Row<double, 8> {
-  __device__ static __forceinline__ void load(const double* __restrict__ p, double (&v)[8]) {
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const double2 a = __ldg(reinterpret_cast<const double2*>(p) + i);
-      v[2 * i] = a.x;
-      v[2 * i + 1] = a.y;
+    for (int i = 0; i < NV / kVec; ++i) {
+      if constexpr (sizeof(T) == 4) {
+        const float4 a = __ldg(reinterpret_cast<const float4*>(p) + i);
+        v[4 * i] = a.x; v[4 * i + 1] = a.y; v[4 * i + 2] = a.z; v[4 * i + 3] = a.w;
+      } else {
+        const double2 a = __ldg(reinterpret_cast<const double2*>(p) + i);
+        v[2 * i] = a.x; v[2 * i + 1] = a.y;
+      }
     }
-  }
-};
-template <>
-struct Row<double, 4> {
-  __device__ static __forceinline__ void load(const double* __restrict__ p, double (&v)[4]) {
+  } else {
 #pragma unroll
-    for (int i = 0; i < 2; ++i) {
-      const double2 a = __ldg(reinterpret_cast<const double2*>(p) + i);
-      v[2 * i] = a.x;
-      v[2 * i + 1] = a.y;
-    }
+    for (int i = 0; i < NV; ++i) v[i] = __ldg(p + i);
   }
-};
+}
 
 constexpr int kMvThreads = 256;
 
+// Images whose loads are in flight together: four for f32 rows, two for f64
+// rows (register budget).
+template <typename T>
+constexpr int group_of() { return sizeof(T) == 4 ? 4 : 2; }
+
+// Images are handled a group at a time (G links, or G/2 plaquettes in both
+// directions): the G orbit-table loads are issued together, then the G x-row
+// loads, then the arithmetic, so that each thread keeps several independent
+// gathers in flight instead of one dependent pair per image.
 template <int ZN, typename T, int NV>
-__global__ void __launch_bounds__(kMvThreads) zn_matvec_k(const __grid_constant__ edg_zn_lattice L, const edg_zn_basis B,
+__global__ void __launch_bounds__(kMvThreads, 2) zn_matvec_k(const __grid_constant__ edg_zn_lattice L, const edg_zn_basis B,
                                                           const double* __restrict__ coup, const T* __restrict__ x,
                                                           T* __restrict__ y) {
   using Z = Zn<ZN>;
+  constexpr int kGroup = group_of<T>();
   extern __shared__ uint64_t zsm[];
   __shared__ double c_t[NV], c_m[NV], c_e[NV], c_b[NV];
   __shared__ double sq_div[8], isq_div[8];
@@ -261,52 +246,77 @@ __global__ void __launch_bounds__(kMvThreads) zn_matvec_k(const __grid_constant_
     const uint32_t occ = (uint32_t)(key >> F);
     const uint32_t self = B.orbit[gauss_index(lut, rank, key, F, n_chunks, pc)];
     const double inv_s = isq_div[(self >> 28) & 7u];
+    double ah[NV], ap[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) ah[v] = ap[v] = 0.0;
+    // hopping: c^dag_tail U c_head (tail empty, head full) and its conjugate;
+    // links in groups (n_links = 2 * n_sites is a multiple of four)
+    for (int l0 = 0; l0 < L.n_links; l0 += kGroup) {
+      uint32_t e[kGroup];
+      int neg[kGroup];
+#pragma unroll
+      for (int c = 0; c < kGroup; ++c) {
+        const int l = l0 + c;
+        const int ta = L.link_tail[l], he = L.link_head[l];
+        const uint32_t nt = (occ >> ta) & 1u, nh = (occ >> he) & 1u;
+        e[c] = 0xFFFFFFFFu;
+        neg[c] = (int)(__popc(occ & L.link_between[l]) & 1) ^ (L.link_eta[l] < 0);
+        if (nt != nh) {
+          const int f = Z::field(key, l);
+          uint64_t k2 = Z::set(key, l, nt == 0 ? Z::inc(f) : Z::dec(f));
+          k2 ^= ((1ull << ta) | (1ull << he)) << F;
+          e[c] = B.orbit[gauss_index(lut, rank, k2, F, n_chunks, pc)];
+        }
+      }
+      T xv[kGroup][NV];
+#pragma unroll
+      for (int c = 0; c < kGroup; ++c)
+        if (e[c] != 0xFFFFFFFFu) load_row<T, NV>(x + (int64_t)(e[c] & 0x0FFFFFFFu) * NV, xv[c]);
+#pragma unroll
+      for (int c = 0; c < kGroup; ++c)
+        if (e[c] != 0xFFFFFFFFu) {
+          const double s = sq_div[(e[c] >> 28) & 7u] * inv_s;
+          const double a = (neg[c] ^ (int)(e[c] >> 31)) ? -s : s;
+#pragma unroll
+          for (int v = 0; v < NV; ++v) ah[v] = fma(a, (double)xv[c][v], ah[v]);
+        }
+    }
+    // plaquettes U_p and U_p^dag, kGroup / 2 plaquettes per group
+    for (int p0 = 0; p0 < L.n_sites; p0 += kGroup / 2) {
+      uint32_t e[kGroup];
+#pragma unroll
+      for (int c = 0; c < kGroup; ++c) {
+        const int p = p0 + c / 2, dir = c & 1;
+        const int l0 = L.plaq[p][0], l1 = L.plaq[p][1], l2 = L.plaq[p][2], l3 = L.plaq[p][3];
+        uint64_t k2 = key;
+        k2 = Z::set(k2, l0, dir == 0 ? Z::inc(Z::field(key, l0)) : Z::dec(Z::field(key, l0)));
+        k2 = Z::set(k2, l1, dir == 0 ? Z::inc(Z::field(key, l1)) : Z::dec(Z::field(key, l1)));
+        k2 = Z::set(k2, l2, dir == 0 ? Z::dec(Z::field(key, l2)) : Z::inc(Z::field(key, l2)));
+        k2 = Z::set(k2, l3, dir == 0 ? Z::dec(Z::field(key, l3)) : Z::inc(Z::field(key, l3)));
+        e[c] = B.orbit[gauss_index(lut, rank, k2, F, n_chunks, pc)];
+      }
+      T xv[kGroup][NV];
+#pragma unroll
+      for (int c = 0; c < kGroup; ++c)
+        if (e[c] != 0xFFFFFFFFu) load_row<T, NV>(x + (int64_t)(e[c] & 0x0FFFFFFFu) * NV, xv[c]);
+#pragma unroll
+      for (int c = 0; c < kGroup; ++c)
+        if (e[c] != 0xFFFFFFFFu) {
+          const double s = sq_div[(e[c] >> 28) & 7u] * inv_s;
+          const double a = (e[c] >> 31) ? -s : s;
+#pragma unroll
+          for (int v = 0; v < NV; ++v) ap[v] = fma(a, (double)xv[c][v], ap[v]);
+        }
+    }
     double esq = 0.0;
     for (int l = 0; l < L.n_links; ++l) esq += L.esq[Z::field(key, l)];
     const double mass = (double)(__popc(occ & L.even_mask) - __popc(occ & ~L.even_mask));
-    double ah[NV], ap[NV], xv[NV];
-#pragma unroll
-    for (int v = 0; v < NV; ++v) ah[v] = ap[v] = 0.0;
-    // hopping: c^dag_tail U c_head (tail empty, head full) and its conjugate
-    for (int l = 0; l < L.n_links; ++l) {
-      const int ta = L.link_tail[l], he = L.link_head[l];
-      const uint32_t nt = (occ >> ta) & 1u, nh = (occ >> he) & 1u;
-      if (nt == nh) continue;
-      const int f = Z::field(key, l);
-      uint64_t k2 = Z::set(key, l, nt == 0 ? Z::inc(f) : Z::dec(f));
-      k2 ^= ((1ull << ta) | (1ull << he)) << F;
-      const uint32_t e = B.orbit[gauss_index(lut, rank, k2, F, n_chunks, pc)];
-      if (e == 0xFFFFFFFFu) continue;
-      const int neg = (int)(__popc(occ & L.link_between[l]) & 1) ^ (int)(e >> 31) ^ (L.link_eta[l] < 0);
-      const double a = (neg ? -sq_div[(e >> 28) & 7u] : sq_div[(e >> 28) & 7u]) * inv_s;
-      Row<T, NV>::load(x + (int64_t)(e & 0x0FFFFFFFu) * NV, xv);
-#pragma unroll
-      for (int v = 0; v < NV; ++v) ah[v] = fma(a, xv[v], ah[v]);
-    }
-    // plaquettes U_p and U_p^dag
-    for (int p = 0; p < L.n_sites; ++p) {
-      const int l0 = L.plaq[p][0], l1 = L.plaq[p][1], l2 = L.plaq[p][2], l3 = L.plaq[p][3];
-      const int f0 = Z::field(key, l0), f1 = Z::field(key, l1), f2 = Z::field(key, l2), f3 = Z::field(key, l3);
-#pragma unroll
-      for (int dir = 0; dir < 2; ++dir) {
-        uint64_t k2 = key;
-        k2 = Z::set(k2, l0, dir == 0 ? Z::inc(f0) : Z::dec(f0));
-        k2 = Z::set(k2, l1, dir == 0 ? Z::inc(f1) : Z::dec(f1));
-        k2 = Z::set(k2, l2, dir == 0 ? Z::dec(f2) : Z::inc(f2));
-        k2 = Z::set(k2, l3, dir == 0 ? Z::dec(f3) : Z::inc(f3));
-        const uint32_t e = B.orbit[gauss_index(lut, rank, k2, F, n_chunks, pc)];
-        if (e == 0xFFFFFFFFu) continue;
-        const double a = ((e >> 31) ? -sq_div[(e >> 28) & 7u] : sq_div[(e >> 28) & 7u]) * inv_s;
-        Row<T, NV>::load(x + (int64_t)(e & 0x0FFFFFFFu) * NV, xv);
-#pragma unroll
-        for (int v = 0; v < NV; ++v) ap[v] = fma(a, xv[v], ap[v]);
-      }
-    }
-    Row<T, NV>::load(x + r * NV, xv);
+    T xr[NV];
+    load_row<T, NV>(x + r * NV, xr);
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
       const double d = c_e[v] * esq + c_m[v] * mass;
-      y[r * NV + v] = (T)(fma(d, xv[v], fma(c_t[v], ah[v], c_b[v] * ap[v])));
+      y[r * NV + v] = (T)(fma(d, (double)xr[v], fma(c_t[v], ah[v], c_b[v] * ap[v])));
     }
   }
 }
@@ -317,6 +327,7 @@ int check_lattice(const edg_zn_lattice* L, const char* where) {
   EDG_REQUIRE(L->link_bits == (L->zn == 2 ? 1 : 2), "%s: link_bits must be %d", where, L->zn == 2 ? 1 : 2);
   EDG_REQUIRE(L->n_sites >= 4 && L->n_sites <= EDG_ZN_MAX_SITES && L->n_sites == L->lx * L->ly,
               "%s: need 4 <= lx * ly <= %d", where, EDG_ZN_MAX_SITES);
+  EDG_REQUIRE(L->lx % 2 == 0 && L->ly >= 2, "%s: need lx even and ly >= 2", where);
   EDG_REQUIRE(L->n_links == 2 * L->n_sites && L->field_bits == L->link_bits * L->n_links &&
                   L->field_bits + L->n_sites <= 64,
               "%s: inconsistent link/field sizes", where);

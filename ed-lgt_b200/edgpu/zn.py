@@ -7,7 +7,8 @@ representative keys and a 4-byte orbit table, for up to 8 coupling sets at
 once (vectors interleaved [row][instance]).  The eigensolver replaces
 ``eigsh(H, k, which="SA")`` (edlgt/modeling/qmb_hamiltonian.py:313): a
 thick-restart Lanczos (Wu and Simon, SIAM J. Matrix Anal. Appl. 22 (2000)
-602) with classical Gram-Schmidt applied twice against the whole basis, the
+602) with classical Gram-Schmidt applied twice against the whole basis (the
+norm fused with the second update), the
 basis length chosen from the free device memory, all inner products in f64.
 ``precision="mixed"`` runs the Krylov vectors and the matvec input/output in
 f32, then refines the Ritz vectors with a short f64 thick-restart run started
@@ -144,6 +145,23 @@ class ZnEngine:
         check(lib.edg_zn_matvec(ctypes.byref(self.struct), ctypes.byref(self.basis), ptr(couplings), nvec, dt,
                                 ptr(x), ptr(y), stream_handle()), "edg_zn_matvec")
 
+    def time_matvec(self, nvec=8, dtype=torch.float32, reps=3, warmup=2, g=1.0, m=0.5):
+        """Average device time (ms) of one batched matvec on random vectors,
+        measured with CUDA events after warm-up launches."""
+        cp = np.tile([1.0, m, g * g / 2, -1.0 / (2 * g * g)], (nvec, 1))
+        coup = torch.from_numpy(cp).to(self.device)
+        x = torch.rand((self.n_rows, nvec), dtype=dtype, device=self.device)
+        y = torch.empty_like(x)
+        for _ in range(warmup):
+            self.matvec(x, y, coup, nvec)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            self.matvec(x, y, coup, nvec)
+        b.record()
+        b.synchronize()
+        return a.elapsed_time(b) / max(reps, 1)
+
 
 # --------------------------------------------------------------- eigensolver
 @dataclass
@@ -204,15 +222,15 @@ def trlan_batched(apply, n_rows, nvec, dtype, m, k_keep, k_want, tol, max_cycles
             e1.record()
             mv_events.append((e0, e1, e2))
             n_mv += 1
-            for p in range(2):
-                h = rec[j, p]
-                _ivec("edg_iv_dots", dtype, E, nvec, ptr(V), E, j + 1, ptr(w), ptr(h), ptr(scratch), st)
-                _ivec("edg_iv_update", dtype, E, nvec, ptr(V), E, j + 1, ptr(h), ptr(w), st)
-            sq = rec[j, 2, 0]
-            _ivec("edg_iv_dots", dtype, E, nvec, ptr(w), E, 1, ptr(w), ptr(sq), ptr(scratch), st)
+            # classical Gram-Schmidt twice; the second update carries the norm
+            h1, h2, sq = rec[j, 0], rec[j, 1], rec[j, 2, 0]
+            _ivec("edg_iv_dots", dtype, E, nvec, ptr(V), E, j + 1, ptr(w), ptr(h1), ptr(scratch), st)
+            _ivec("edg_iv_update", dtype, E, nvec, ptr(V), E, j + 1, ptr(h1), ptr(w), st)
+            _ivec("edg_iv_dots", dtype, E, nvec, ptr(V), E, j + 1, ptr(w), ptr(h2), ptr(scratch), st)
+            _ivec("edg_iv_update_norm", dtype, E, nvec, ptr(V), E, j + 1, ptr(h2), ptr(w), ptr(sq), ptr(scratch), st)
             _ivec("edg_iv_scale", dtype, E, nvec, ptr(w), ptr(sq), ptr(V[j + 1]), st)
             e2.record()
-            launches += 10  # matvec, 3 x (dots + reduce), 2 x update, scale
+            launches += 9  # matvec, 2 x (dots + reduce), update, update+norm + reduce, scale
         R = rec.cpu().numpy()
         for j in range(j0, m):
             hcol = R[j, 0, : j + 1] + R[j, 1, : j + 1]  # [j+1, nvec]

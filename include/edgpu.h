@@ -488,6 +488,11 @@ int edg_iv_dots(int32_t dtype, int64_t n_elems, int32_t nvec, const void* V, int
 /* w -= sum_i V_i h[i * nvec + v] per instance v. */
 int edg_iv_update(int32_t dtype, int64_t n_elems, int32_t nvec, const void* V, int64_t stride,
                   int32_t m, const double* h, void* w, cudaStream_t stream);
+/* Second Gram-Schmidt pass fused with the norm: w -= sum_i V_i h[i * nvec + v]
+ * (i < m), then sq[v] = w . w per instance. */
+int edg_iv_update_norm(int32_t dtype, int64_t n_elems, int32_t nvec, const void* V, int64_t stride,
+                       int32_t m, const double* h, void* w, double* sq, double* scratch,
+                       cudaStream_t stream);
 /* out = w / sqrt(sq[v]) per instance (0 where sq <= 0). */
 int edg_iv_scale(int32_t dtype, int64_t n_elems, int32_t nvec, const void* w, const double* sq,
                  void* out, cudaStream_t stream);

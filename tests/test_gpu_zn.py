@@ -124,14 +124,15 @@ def test_matvec_full_sector_matches_oracle(lx, ly, n):
     assert np.abs(y.cpu().numpy()[:, 0] - want).max() <= 1e-12 * np.abs(want).max()
 
 
+@pytest.mark.parametrize("m", [7, 20])
 @pytest.mark.parametrize("dt", [torch.float64, torch.float32])
 @pytest.mark.parametrize("nvec", [1, 2, 4, 8])
-def test_interleaved_vector_kernels(nvec, dt):
+def test_interleaved_vector_kernels(nvec, dt, m):
     from edgpu._lib import lib, ptr, stream_handle
 
     dtype = 0 if dt == torch.float64 else 1
     rng = np.random.default_rng(nvec)
-    n_rows, m = 1001, 7
+    n_rows = 1001
     n_pad = (n_rows + 3) // 4 * 4
     E = n_pad * nvec
     Vh = np.zeros((m, n_pad, nvec))
@@ -148,6 +149,15 @@ def test_interleaved_vector_kernels(nvec, dt):
     assert lib.edg_iv_dots(dtype, E, nvec, ptr(V), E, m, ptr(w), ptr(h), ptr(scratch), st) == 0
     want_h = np.einsum("irv,rv->iv", Vr, wr)
     assert np.allclose(h.cpu().numpy(), want_h, rtol=1e-12, atol=1e-9)
+    # fused second pass on a copy: w1 = w - V h, sq = |w1|^2
+    w1 = w.clone()
+    sq1 = torch.zeros(nvec, dtype=torch.float64, device="cuda")
+    assert lib.edg_iv_update_norm(dtype, E, nvec, ptr(V), E, m, ptr(h), ptr(w1), ptr(sq1), ptr(scratch), st) == 0
+    w1r = w1.double().cpu().numpy().reshape(n_pad, nvec)
+    want_w1 = wr - np.einsum("irv,iv->rv", Vr, h.cpu().numpy())
+    tol = 1e-12 if dtype == 0 else 1e-5
+    assert np.abs(w1r - want_w1).max() <= tol * np.abs(want_w1).max()
+    assert np.allclose(sq1.cpu().numpy(), (w1r**2).sum(axis=0), rtol=1e-11)
     assert lib.edg_iv_update(dtype, E, nvec, ptr(V), E, m, ptr(h), ptr(w), st) == 0
     want_w = wr - np.einsum("irv,iv->rv", Vr, want_h)
     tol = 1e-12 if dtype == 0 else 1e-4
