@@ -192,6 +192,166 @@ __global__ void __launch_bounds__(kThreads) combine_k(T* __restrict__ V, int64_t
   }
 }
 
+// Dots of a tile of KT basis vectors against two vectors at once (the
+// lagged candidate u and the new matvec result w of a delayed Gram-Schmidt
+// step): partial[block][i][r][class][4], r = 0 for x1, 1 for x2.
+template <typename T, int NV, int KT>
+__global__ void __launch_bounds__(kThreads) dots2_k(const T* __restrict__ V, int64_t stride, int m,
+                                                    const T* __restrict__ x1, const T* __restrict__ x2,
+                                                    int64_t n_slots, double* __restrict__ partial) {
+  constexpr int P = classes<NV>();
+  __shared__ double red[kWarps][KT][2][P][4];
+  const int i0 = blockIdx.y * KT;
+  const int ni = min(KT, m - i0);
+  double acc[KT][2][4];
+#pragma unroll
+  for (int i = 0; i < KT; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][0][j] = acc[i][1][j] = 0.0;
+  for (int64_t s = (int64_t)blockIdx.x * kThreads + threadIdx.x; s < n_slots; s += (int64_t)gridDim.x * kThreads) {
+    double a[4], b[4], vv[4];
+    Slot<T>::load(x1 + 4 * s, a);
+    Slot<T>::load(x2 + 4 * s, b);
+#pragma unroll
+    for (int i = 0; i < KT; ++i) {
+      if (i < ni) {
+        Slot<T>::load(V + (int64_t)(i0 + i) * stride + 4 * s, vv);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          acc[i][0][j] = fma(vv[j], a[j], acc[i][0][j]);
+          acc[i][1][j] = fma(vv[j], b[j], acc[i][1][j]);
+        }
+      }
+    }
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int i = 0; i < KT; ++i)
+#pragma unroll
+    for (int r = 0; r < 2; ++r)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        double x = acc[i][r][j];
+#pragma unroll
+        for (int o = 16; o >= P; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane < P) red[warp][i][r][lane][j] = x;
+      }
+  __syncthreads();
+  for (int t = threadIdx.x; t < KT * 2 * P * 4; t += kThreads) {
+    const int i = t / (2 * P * 4), r = (t / (P * 4)) % 2, q = t % (P * 4);
+    double x = 0.0;
+    for (int k = 0; k < kWarps; ++k) x += red[k][i][r][q / 4][q % 4];
+    if (i < ni) partial[(((int64_t)blockIdx.x * m + i0 + i) * 2 + r) * (P * 4) + q] = x;
+  }
+}
+
+// h_r[i * NV + v] from the dots2_k partials; one CTA per (i, r).
+template <int NV>
+__global__ void __launch_bounds__(kThreads) dots2_reduce_k(const double* __restrict__ partial, int nblk, int m,
+                                                           double* __restrict__ h1, double* __restrict__ h2) {
+  constexpr int P = classes<NV>();
+  __shared__ double red[kWarps][P * 4];
+  const int i = blockIdx.x / 2, r = blockIdx.x % 2;
+  double a[P * 4];
+#pragma unroll
+  for (int q = 0; q < P * 4; ++q) a[q] = 0.0;
+  for (int b = threadIdx.x; b < nblk; b += kThreads)
+#pragma unroll
+    for (int q = 0; q < P * 4; ++q) a[q] += partial[(((int64_t)b * m + i) * 2 + r) * (P * 4) + q];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < P * 4; ++q) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) a[q] += __shfl_xor_sync(0xffffffffu, a[q], o);
+    if (lane == 0) red[warp][q] = a[q];
+  }
+  __syncthreads();
+  if (threadIdx.x < NV) {
+    const int v = threadIdx.x;
+    double t = 0.0;
+    for (int q = 0; q < P * 4; ++q)
+      if (q % NV == v)
+        for (int k = 0; k < kWarps; ++k) t += red[k][q];
+    (r == 0 ? h1 : h2)[(int64_t)i * NV + v] = t;
+  }
+}
+
+// One delayed classical Gram-Schmidt step in one pass over V_0..V_{j-1}.
+// With s = hu[0..j), alpha = hu[j] (= u.u), z = hw[0..j), omega = hw[j]
+// (= u.w), u = V_j:  r = sqrt(alpha - s.s), q = (u - sum_i V_i s_i) / r is
+// written to V_j (u's lagged second pass), c = (omega - s.z) / r, and
+// w <- w - sum_i V_i z_i - q c (one pass of w against V_0..V_j), with the
+// squared norm of the stored w per CTA and slot class (reduced by
+// dots_reduce_k).
+template <typename T, int NV>
+__global__ void __launch_bounds__(kThreads) dcgs_update_k(T* __restrict__ V, int64_t stride, int j,
+                                                          const double* __restrict__ hu,
+                                                          const double* __restrict__ hw, T* __restrict__ w,
+                                                          int64_t n_slots, double* __restrict__ partial) {
+  constexpr int P = classes<NV>();
+  __shared__ double ss[kMaxM * 8], zs[kMaxM * 8];
+  __shared__ double rinv[8], cq[8];
+  __shared__ double red[kWarps][P][4];
+  for (int t = threadIdx.x; t < j * NV; t += kThreads) {
+    ss[t] = hu[t];
+    zs[t] = hw[t];
+  }
+  if (threadIdx.x < NV) {
+    const int v = threadIdx.x;
+    double s2 = 0.0, sz = 0.0;
+    for (int i = 0; i < j; ++i) {
+      s2 = fma(hu[i * NV + v], hu[i * NV + v], s2);
+      sz = fma(hu[i * NV + v], hw[i * NV + v], sz);
+    }
+    const double r2 = hu[j * NV + v] - s2;
+    const double ri = r2 > 0.0 ? 1.0 / sqrt(r2) : 0.0;
+    rinv[v] = ri;
+    cq[v] = (hw[j * NV + v] - sz) * ri;
+  }
+  __syncthreads();
+  T* U = V + (int64_t)j * stride;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int64_t s = (int64_t)blockIdx.x * kThreads + threadIdx.x; s < n_slots; s += (int64_t)gridDim.x * kThreads) {
+    double uv[4], wv[4], vv[4];
+    Slot<T>::load(U + 4 * s, uv);
+    Slot<T>::load(w + 4 * s, wv);
+    const int base = (int)((4 * s) % NV);
+    for (int i = 0; i < j; ++i) {
+      Slot<T>::load(V + (int64_t)i * stride + 4 * s, vv);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int v = (base + k) % NV;
+        uv[k] = fma(-vv[k], ss[i * NV + v], uv[k]);
+        wv[k] = fma(-vv[k], zs[i * NV + v], wv[k]);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int v = (base + k) % NV;
+      uv[k] = (double)(T)(uv[k] * rinv[v]);
+      wv[k] = (double)(T)fma(-uv[k], cq[v], wv[k]);
+      acc[k] = fma(wv[k], wv[k], acc[k]);
+    }
+    Slot<T>::store(U + 4 * s, uv);
+    Slot<T>::store(w + 4 * s, wv);
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    double a = acc[k];
+#pragma unroll
+    for (int o = 16; o >= P; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    if (lane < P) red[warp][lane][k] = a;
+  }
+  __syncthreads();
+  if (threadIdx.x < P * 4) {
+    const int c = threadIdx.x / 4, k = threadIdx.x % 4;
+    double a = 0.0;
+    for (int q = 0; q < kWarps; ++q) a += red[q][c][k];
+    partial[(int64_t)blockIdx.x * (P * 4) + threadIdx.x] = a;
+  }
+}
+
 // Second Gram-Schmidt pass fused with the norm (update_k's slot layout):
 // w <- w - sum_{i<m} V_i h[i][v], and per CTA the squared norms of the
 // stored (rounded) w by slot class, partial[blk][class * 4 + j], reduced by
@@ -316,6 +476,36 @@ int run_dots(int64_t n_elems, const void* V, int64_t stride, int m, const void* 
   return run_dots_kt<T, NV, 4>(n_elems, V, stride, m, w, h, scratch, stream);
 }
 
+template <typename T, int NV, int KT>
+int run_dots2(int64_t n_elems, const void* V, int64_t stride, int m, const void* x1, const void* x2, double* h1,
+              double* h2, double* scratch, cudaStream_t stream) {
+  const int64_t n_slots = n_elems / 4;
+  const int tiles = (m + KT - 1) / KT;
+  int per_sm = 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dots2_k<T, NV, KT>, kThreads, 0) != cudaSuccess ||
+      per_sm < 1)
+    per_sm = 1;
+  int64_t nbx = edg::ceil_div(n_slots, kThreads);
+  const int64_t cap = (int64_t)edg::kSmCount * (per_sm < 8 ? per_sm : 8);
+  const int64_t cap_t = cap / tiles > edg::kSmCount ? cap / tiles : edg::kSmCount;
+  if (nbx > cap_t) nbx = cap_t;
+  if (nbx < 1) nbx = 1;
+  dots2_k<T, NV, KT><<<dim3((unsigned)nbx, tiles), kThreads, 0, stream>>>((const T*)V, stride, m, (const T*)x1,
+                                                                         (const T*)x2, n_slots, scratch);
+  dots2_reduce_k<NV><<<2 * m, kThreads, 0, stream>>>(scratch, (int)nbx, m, h1, h2);
+  return EDG_OK;
+}
+
+template <typename T, int NV>
+int run_dcgs(int64_t n_elems, void* V, int64_t stride, int j, const double* hu, const double* hw, void* w,
+             double* sq, double* scratch, cudaStream_t stream) {
+  const int64_t n_slots = n_elems / 4;
+  const unsigned nblk = edg::grid_for(n_slots, kThreads, 8);
+  dcgs_update_k<T, NV><<<nblk, kThreads, 0, stream>>>((T*)V, stride, j, hu, hw, (T*)w, n_slots, scratch);
+  dots_reduce_k<NV><<<1, kThreads, 0, stream>>>(scratch, (int)nblk, 1, sq);
+  return EDG_OK;
+}
+
 template <typename T, int NV>
 int run_norm(int64_t n_elems, const void* V, int64_t stride, int m, const double* h, void* w, double* out,
              double* scratch, cudaStream_t stream) {
@@ -345,7 +535,7 @@ int run_combine(int64_t n_elems, void* V, int64_t stride, int m, const double* S
 
 extern "C" int64_t edg_iv_scratch_elems(int64_t n_elems, int32_t m) {
   if (n_elems < 0 || m < 1) return -1;
-  return (int64_t)edg::kSmCount * 8 * m * 8;  // blocks * m * (P * 4) with P * 4 <= 8
+  return (int64_t)edg::kSmCount * 8 * m * 2 * 8;  // blocks * m * 2 right-hand sides * (P * 4 <= 8)
 }
 
 #define EDG_IV_DISPATCH(CALL)                                \
@@ -455,5 +645,48 @@ extern "C" int edg_iv_update_norm(int32_t dtype, int64_t n_elems, int32_t nvec, 
 #undef CALL
   if (st != EDG_OK) return st;
   EDG_CHECK_LAUNCH("edg_iv_update_norm");
+  return EDG_OK;
+}
+
+extern "C" int edg_iv_dots2(int32_t dtype, int64_t n_elems, int32_t nvec, const void* V, int64_t stride, int32_t m,
+                            const void* x1, const void* x2, double* h1, double* h2, double* scratch,
+                            cudaStream_t stream) {
+  int st = check_common(dtype, n_elems, nvec, "edg_iv_dots2");
+  if (st != EDG_OK) return st;
+  EDG_REQUIRE(m >= 1 && V != nullptr && x1 != nullptr && x2 != nullptr && h1 != nullptr && h2 != nullptr &&
+                  scratch != nullptr,
+              "edg_iv_dots2: need m >= 1 and non-null buffers");
+  EDG_REQUIRE(stride % 4 == 0, "edg_iv_dots2: stride must be a multiple of 4");
+  if (n_elems == 0) {
+    cudaError_t e = cudaMemsetAsync(h1, 0, sizeof(double) * (size_t)m * nvec, stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(h2, 0, sizeof(double) * (size_t)m * nvec, stream);
+    return e == cudaSuccess ? EDG_OK : edg::cuda_status(e, "edg_iv_dots2");
+  }
+#define CALL(T, NV) run_dots2<T, NV, 4>(n_elems, V, stride, m, x1, x2, h1, h2, scratch, stream)
+  EDG_IV_DISPATCH(CALL)
+#undef CALL
+  if (st != EDG_OK) return st;
+  EDG_CHECK_LAUNCH("edg_iv_dots2");
+  return EDG_OK;
+}
+
+extern "C" int edg_iv_dcgs_update(int32_t dtype, int64_t n_elems, int32_t nvec, void* V, int64_t stride, int32_t j,
+                                  const double* hu, const double* hw, void* w, double* sq, double* scratch,
+                                  cudaStream_t stream) {
+  int st = check_common(dtype, n_elems, nvec, "edg_iv_dcgs_update");
+  if (st != EDG_OK) return st;
+  EDG_REQUIRE(j >= 0 && j < kMaxM && V != nullptr && hu != nullptr && hw != nullptr && w != nullptr &&
+                  sq != nullptr && scratch != nullptr,
+              "edg_iv_dcgs_update: need 0 <= j < %d and non-null buffers", kMaxM);
+  EDG_REQUIRE(stride % 4 == 0, "edg_iv_dcgs_update: stride must be a multiple of 4");
+  if (n_elems == 0) {
+    cudaError_t e = cudaMemsetAsync(sq, 0, sizeof(double) * (size_t)nvec, stream);
+    return e == cudaSuccess ? EDG_OK : edg::cuda_status(e, "edg_iv_dcgs_update");
+  }
+#define CALL(T, NV) run_dcgs<T, NV>(n_elems, V, stride, j, hu, hw, w, sq, scratch, stream)
+  EDG_IV_DISPATCH(CALL)
+#undef CALL
+  if (st != EDG_OK) return st;
+  EDG_CHECK_LAUNCH("edg_iv_dcgs_update");
   return EDG_OK;
 }

@@ -246,6 +246,8 @@ _SIGS = {
     "edg_iv_update": (I32, [I32, I64, I32, P, I64, I32, P, P, P]),
     "edg_iv_scale": (I32, [I32, I64, I32, P, P, P, P]),
     "edg_iv_update_norm": (I32, [I32, I64, I32, P, I64, I32, P, P, P, P, P]),
+    "edg_iv_dots2": (I32, [I32, I64, I32, P, I64, I32, P, P, P, P, P, P]),
+    "edg_iv_dcgs_update": (I32, [I32, I64, I32, P, I64, I32, P, P, P, P, P, P]),
     "edg_iv_combine": (I32, [I32, I64, I32, P, I64, I32, P, I32, P]),
     "edg_iv_random": (I32, [I32, I64, I64, I32, U64, P, P]),
 }

@@ -7,9 +7,9 @@ representative keys and a 4-byte orbit table, for up to 8 coupling sets at
 once (vectors interleaved [row][instance]).  The eigensolver replaces
 ``eigsh(H, k, which="SA")`` (edlgt/modeling/qmb_hamiltonian.py:313): a
 thick-restart Lanczos (Wu and Simon, SIAM J. Matrix Anal. Appl. 22 (2000)
-602) with classical Gram-Schmidt applied twice against the whole basis (the
-norm fused with the second update), the
-basis length chosen from the free device memory, all inner products in f64.
+602) with delayed classical Gram-Schmidt reorthogonalisation against the
+whole basis (two reads of the basis per step), the basis length chosen from
+the free device memory, all inner products in f64.
 ``precision="mixed"`` runs the Krylov vectors and the matvec input/output in
 f32, then refines the Ritz vectors with a short f64 thick-restart run started
 from them; ``precision="fp64"`` is the plain f64 solver.
@@ -181,6 +181,16 @@ def _ivec(op, *args):
 def trlan_batched(apply, n_rows, nvec, dtype, m, k_keep, k_want, tol, max_cycles, v0=None, seed=1, stats=None):
     """Batched thick-restart Lanczos on interleaved vectors.
 
+    Orthogonalisation is delayed classical Gram-Schmidt with
+    reorthogonalisation (DCGS2: Swirydowicz, Langou, Ananthan, Yang, Thomas,
+    Numer. Linear Algebra Appl. 28 (2021) e2343): step j takes the matvec of
+    the candidate u_j that has had one Gram-Schmidt pass, and in one read of
+    the basis (``edg_iv_dots2``) gets u_j's second-pass coefficients s and the
+    projections z of w = H u_j; one more read (``edg_iv_dcgs_update``)
+    finishes q_j = (u_j - Q s) / r and projects w against Q and q_j.  The
+    projected matrix follows from the recorded dots without further passes:
+    T[:j, j] = (z - T s) / r, T[j, j] = (omega - 2 z.s + s.T s) / r^2.
+
     apply(x, y): y = H x for all instances.  Returns (theta [nvec, k_want],
     residual estimates [nvec, k_want] relative to |theta|, Ritz vectors
     (tensor [k_want, n_elems]), matvec count, cycles, converged flags)."""
@@ -196,17 +206,15 @@ def trlan_batched(apply, n_rows, nvec, dtype, m, k_keep, k_want, tol, max_cycles
     rec = torch.zeros((m, 3, m + 1, nvec), dtype=torch.float64, device=dev)
     scratch = torch.empty(lib.edg_iv_scratch_elems(E, m + 1), dtype=torch.float64, device=dev)
     st = stream_handle()
+    launches = 0
     if v0 is None:
         _ivec("edg_iv_random", dtype, n_rows, E, nvec, seed, ptr(V[0]), st)
+        launches += 1
     else:
         V[0].copy_(v0)
-    sq0 = torch.zeros(nvec, dtype=torch.float64, device=dev)
-    _ivec("edg_iv_dots", dtype, E, nvec, ptr(V[0]), E, 1, ptr(V[0]), ptr(sq0), ptr(scratch), st)
-    _ivec("edg_iv_scale", dtype, E, nvec, ptr(V[0]), ptr(sq0), ptr(V[0]), st)
     T = np.zeros((nvec, m, m))
     j0 = 0
     n_mv = 0
-    launches = 4  # random start, norm (dots + reduce), scale
     mv_events = []
     converged = np.zeros(nvec, dtype=bool)
     theta = np.zeros((nvec, k_want))
@@ -222,38 +230,43 @@ def trlan_batched(apply, n_rows, nvec, dtype, m, k_keep, k_want, tol, max_cycles
             e1.record()
             mv_events.append((e0, e1, e2))
             n_mv += 1
-            # classical Gram-Schmidt twice; the second update carries the norm
-            h1, h2, sq = rec[j, 0], rec[j, 1], rec[j, 2, 0]
-            _ivec("edg_iv_dots", dtype, E, nvec, ptr(V), E, j + 1, ptr(w), ptr(h1), ptr(scratch), st)
-            _ivec("edg_iv_update", dtype, E, nvec, ptr(V), E, j + 1, ptr(h1), ptr(w), st)
-            _ivec("edg_iv_dots", dtype, E, nvec, ptr(V), E, j + 1, ptr(w), ptr(h2), ptr(scratch), st)
-            _ivec("edg_iv_update_norm", dtype, E, nvec, ptr(V), E, j + 1, ptr(h2), ptr(w), ptr(sq), ptr(scratch), st)
+            hu, hw, sq = rec[j, 0], rec[j, 1], rec[j, 2, 0]
+            _ivec("edg_iv_dots2", dtype, E, nvec, ptr(V), E, j + 1, ptr(V[j]), ptr(w), ptr(hu), ptr(hw),
+                  ptr(scratch), st)
+            _ivec("edg_iv_dcgs_update", dtype, E, nvec, ptr(V), E, j, ptr(hu), ptr(hw), ptr(w), ptr(sq),
+                  ptr(scratch), st)
             _ivec("edg_iv_scale", dtype, E, nvec, ptr(w), ptr(sq), ptr(V[j + 1]), st)
             e2.record()
-            launches += 9  # matvec, 2 x (dots + reduce), update, update+norm + reduce, scale
+            launches += 6  # matvec, dots2 + reduce, update + reduce, scale
         R = rec.cpu().numpy()
+        beta = np.zeros((m, nvec))
         for j in range(j0, m):
-            hcol = R[j, 0, : j + 1] + R[j, 1, : j + 1]  # [j+1, nvec]
-            T[:, : j + 1, j] = hcol.T
-            T[:, j, : j + 1] = hcol.T
-        beta = np.sqrt(np.maximum(R[m - 1, 2, 0], 0.0))
+            s_, alpha = R[j, 0, :j], R[j, 0, j]       # [j, nvec], [nvec]
+            z, omega = R[j, 1, :j], R[j, 1, j]
+            r = np.sqrt(np.maximum(alpha - np.einsum("iv,iv->v", s_, s_), 1e-300))
+            Ts = np.einsum("vik,kv->iv", T[:, :j, :j], s_)  # [j, nvec]
+            col = (z - Ts) / r
+            T[:, :j, j] = col.T
+            T[:, j, :j] = col.T
+            T[:, j, j] = (omega - 2 * np.einsum("iv,iv->v", z, s_) + np.einsum("iv,iv->v", s_, Ts)) / r**2
+            beta[j] = np.sqrt(np.maximum(R[j, 2, 0], 0.0)) / r
         for v in range(nvec):
             # an invariant subspace ends the recurrence early for this instance
-            sqs = R[:, 2, 0, v]
             scale = max(np.abs(np.diag(T[v])).max(), 1e-300)
-            tiny = np.nonzero(np.sqrt(np.maximum(sqs[j0:m], 0.0)) <= 1e-12 * scale)[0]
+            tiny = np.nonzero(beta[j0:m, v] <= 1e-12 * scale)[0]
             me = j0 + int(tiny[0]) + 1 if len(tiny) else m
             th, S = np.linalg.eigh(T[v, :me, :me])
             S_all[v] = 0.0
             S_all[v, :me, :me] = S
             theta[v] = th[:k_want]
             th_keep[v, : min(k_keep, me)] = th[:k_keep]
-            bv = 0.0 if me < m else beta[v]
+            bv = 0.0 if me < m else beta[m - 1, v]
             res[v] = bv * np.abs(S[me - 1, :k_want]) / np.maximum(np.abs(th[:k_want]), 1e-300)
             converged[v] = bool(np.all(res[v] <= tol)) or me < m
         if converged.all() or cycles == max_cycles:
             break
-        # thick restart: keep the k_keep lowest Ritz vectors, continue from V[m]
+        # thick restart: keep the k_keep lowest Ritz vectors, continue from the
+        # candidate V[m] (its second Gram-Schmidt pass happens in the next step)
         Sk = torch.from_numpy(np.ascontiguousarray(S_all[:, :, :k_keep])).to(dev)
         _ivec("edg_iv_combine", dtype, E, nvec, ptr(V), E, m, ptr(Sk), k_keep, st)
         launches += 1

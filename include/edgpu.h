@@ -493,6 +493,20 @@ int edg_iv_update(int32_t dtype, int64_t n_elems, int32_t nvec, const void* V, i
 int edg_iv_update_norm(int32_t dtype, int64_t n_elems, int32_t nvec, const void* V, int64_t stride,
                        int32_t m, const double* h, void* w, double* sq, double* scratch,
                        cudaStream_t stream);
+/* Dots against two vectors in one read of the basis: h1[i * nvec + v] = V_i . x1,
+ * h2[i * nvec + v] = V_i . x2 (i < m).  scratch: edg_iv_scratch_elems(n_elems, m). */
+int edg_iv_dots2(int32_t dtype, int64_t n_elems, int32_t nvec, const void* V, int64_t stride,
+                 int32_t m, const void* x1, const void* x2, double* h1, double* h2, double* scratch,
+                 cudaStream_t stream);
+/* One delayed classical Gram-Schmidt step (the second pass of the previous
+ * vector lagged into this one), one read of V_0..V_{j-1}.  Inputs: hu = dots
+ * of V_0..V_j with u = V_j (s = hu[0..j), alpha = hu[j]), hw = dots of
+ * V_0..V_j with w (z = hw[0..j), omega = hw[j]).  Writes
+ * V_j = (u - sum_i V_i s_i) / r with r = sqrt(alpha - s.s), then
+ * w -= sum_i V_i z_i + V_j (omega - s.z) / r, and sq[v] = w . w.  j < 32. */
+int edg_iv_dcgs_update(int32_t dtype, int64_t n_elems, int32_t nvec, void* V, int64_t stride,
+                       int32_t j, const double* hu, const double* hw, void* w, double* sq,
+                       double* scratch, cudaStream_t stream);
 /* out = w / sqrt(sq[v]) per instance (0 where sq <= 0). */
 int edg_iv_scale(int32_t dtype, int64_t n_elems, int32_t nvec, const void* w, const double* sq,
                  void* out, cudaStream_t stream);

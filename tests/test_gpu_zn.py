@@ -135,8 +135,12 @@ def test_interleaved_vector_kernels(nvec, dt, m):
     n_rows = 1001
     n_pad = (n_rows + 3) // 4 * 4
     E = n_pad * nvec
+    # an orthonormal basis per instance plus one more random vector (what a
+    # delayed Gram-Schmidt step sees: Q orthonormal, u not yet orthogonalised)
     Vh = np.zeros((m, n_pad, nvec))
-    Vh[:, :n_rows] = rng.standard_normal((m, n_rows, nvec))
+    for v in range(nvec):
+        Vh[: m - 1, :n_rows, v] = np.linalg.qr(rng.standard_normal((n_rows, m - 1)))[0].T
+    Vh[m - 1, :n_rows] = rng.standard_normal((n_rows, nvec)) / np.sqrt(n_rows)
     wh = np.zeros((n_pad, nvec))
     wh[:n_rows] = rng.standard_normal((n_rows, nvec))
     V = torch.from_numpy(Vh.reshape(m, E)).to("cuda", dt).contiguous()
@@ -149,6 +153,31 @@ def test_interleaved_vector_kernels(nvec, dt, m):
     assert lib.edg_iv_dots(dtype, E, nvec, ptr(V), E, m, ptr(w), ptr(h), ptr(scratch), st) == 0
     want_h = np.einsum("irv,rv->iv", Vr, wr)
     assert np.allclose(h.cpu().numpy(), want_h, rtol=1e-12, atol=1e-9)
+    # two right-hand-side dots and one delayed Gram-Schmidt step with u = V[m-1]
+    hu = torch.zeros((m, nvec), dtype=torch.float64, device="cuda")
+    hw = torch.zeros((m, nvec), dtype=torch.float64, device="cuda")
+    assert lib.edg_iv_dots2(dtype, E, nvec, ptr(V), E, m, ptr(V[m - 1]), ptr(w), ptr(hu), ptr(hw),
+                            ptr(scratch), st) == 0
+    assert np.allclose(hu.cpu().numpy(), np.einsum("irv,rv->iv", Vr, Vr[m - 1]), rtol=1e-12, atol=1e-9)
+    assert np.allclose(hw.cpu().numpy(), want_h, rtol=1e-12, atol=1e-9)
+    Vd, wd = V.clone(), w.clone()
+    sqd = torch.zeros(nvec, dtype=torch.float64, device="cuda")
+    j = m - 1
+    assert lib.edg_iv_dcgs_update(dtype, E, nvec, ptr(Vd), E, j, ptr(hu), ptr(hw), ptr(wd), ptr(sqd),
+                                  ptr(scratch), st) == 0
+    hun, hwn = hu.cpu().numpy(), hw.cpu().numpy()
+    s_, z_ = hun[:j], hwn[:j]
+    r = np.sqrt(hun[j] - (s_ * s_).sum(axis=0))
+    q = (Vr[j] - np.einsum("irv,iv->rv", Vr[:j], s_)) / r
+    c = (hwn[j] - (s_ * z_).sum(axis=0)) / r
+    want_wd = wr - np.einsum("irv,iv->rv", Vr[:j], z_) - q * c
+    got_q = Vd[j].double().cpu().numpy().reshape(n_pad, nvec)
+    got_w = wd.double().cpu().numpy().reshape(n_pad, nvec)
+    tq = 1e-12 if dtype == 0 else 2e-6
+    assert np.abs(got_q - q).max() <= tq * np.abs(q).max()
+    assert np.abs(got_w - want_wd).max() <= tq * 10 * np.abs(want_wd).max()
+    assert np.allclose(sqd.cpu().numpy(), (got_w**2).sum(axis=0), rtol=1e-11)
+    assert torch.equal(Vd[:j], V[:j])
     # fused second pass on a copy: w1 = w - V h, sq = |w1|^2
     w1 = w.clone()
     sq1 = torch.zeros(nvec, dtype=torch.float64, device="cuda")
