@@ -4,10 +4,18 @@
 // [row][vec]; the working vector w, every inner product, the recurrence
 // coefficients and the tridiagonal eigen-solve are double precision.
 //
-// Step j (v_j in V[j]):
-//   w = H v_j                                  (spmv, double output)
-//   two classical Gram-Schmidt passes:         h = V[0..j]^T w ; w -= V h
-//   alpha_j = h1_j + h2_j ; beta_{j+1} = |w| ; V[j+1] = w / beta_{j+1}
+// Step j, delayed classical Gram-Schmidt with reorthogonalisation (DCGS2,
+// Swirydowicz, Langou, Ananthan, Yang, Thomas, Numer. Linear Algebra Appl.
+// 28 (2021) e2343): V[j] holds the candidate u_j, which has had one
+// Gram-Schmidt pass; its second pass is done in this step.
+//   w = H u_j                                   (spmv, double output)
+//   one read of V[0..j]: s = V[0..j)^T u_j, alpha_u = u_j.u_j,
+//                        z = V[0..j)^T w,   omega = u_j.w
+//   r = sqrt(alpha_u - s.s), c = (omega - s.z) / r
+//   alpha_j = (omega - 2 z.s + s.T s) / r^2, beta_j = (z_{j-1} - (T s)_{j-1}) / r
+//   one read of V[0..j): V[j] = q_j = (u_j - V s) / r ; w -= V z + q_j c
+//   V[j+1] = w / |w| (the next candidate), beta_{j+1} = |w| / r (refined at j+1)
+// T is the j x j tridiagonal block of the previous steps.
 // Every check_every steps the k lowest Ritz pairs of the tridiagonal matrix are
 // computed on the device (multisection + inverse iteration) and the residual
 // bound |beta_{j+1} s_{j}| is compared with tol * max(1, |theta|).
@@ -89,129 +97,6 @@ __device__ __forceinline__ void block_sum(double* vals, double* smem /*[kThreads
   __syncthreads();
 }
 
-// partial[bx][i][v] = sum over the rows of chunk bx of V[i][v][r] w[v][r], for
-// the Krylov tile i in [blockIdx.y*kItile, ...] (i <= j).  Rows are read in
-// quads (16-byte loads); blockIdx.x strides over row chunks.
-template <typename T, int NV>
-__global__ void __launch_bounds__(kThreads, 4) dots_k(const T* __restrict__ V, int64_t n_pad, int j,
-                                                   const double* __restrict__ w, double* __restrict__ partial,
-                                                   int ld_i, int64_t stride_i) {
-  __shared__ double red[(kThreads / 32) * kItile];
-  const int i0 = blockIdx.y * kItile;
-  const int nt = min(kItile, j + 1 - i0);
-  const int64_t nq = n_pad / 4;
-  const int64_t cq = (nq + gridDim.x - 1) / gridDim.x;
-  const int64_t q0 = blockIdx.x * cq, q1 = min(nq, q0 + cq);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll 1
-  for (int v = 0; v < NV; ++v) {
-    double acc[kItile];
-#pragma unroll
-    for (int t = 0; t < kItile; ++t) acc[t] = 0.0;
-    const double* wv = w + (int64_t)v * n_pad;
-    const T* Vv = V + (int64_t)i0 * stride_i + (int64_t)v * n_pad;
-    for (int64_t q = q0 + threadIdx.x; q < q1; q += kThreads) {
-      double w4[4];
-      ld4(wv + 4 * q, w4);
-#pragma unroll
-      for (int t = 0; t < kItile; ++t) {
-        if (t < nt) {
-          double x4[4];
-          ld4(Vv + (int64_t)t * stride_i + 4 * q, x4);
-          acc[t] = fma(x4[0], w4[0], fma(x4[1], w4[1], fma(x4[2], w4[2], fma(x4[3], w4[3], acc[t]))));
-        }
-      }
-    }
-#pragma unroll
-    for (int t = 0; t < kItile; ++t) {
-      double a = acc[t];
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
-      if (lane == 0) red[warp * kItile + t] = a;
-    }
-    __syncthreads();
-    if (threadIdx.x < nt) {
-      double a = 0.0;
-      for (int wi = 0; wi < kThreads / 32; ++wi) a += red[wi * kItile + threadIdx.x];
-      partial[((int64_t)blockIdx.x * ld_i + i0 + threadIdx.x) * NV + v] = a;
-    }
-    __syncthreads();
-  }
-}
-
-// h[i][v] = sum_b partial[b][i][v] (one CTA per Krylov index i, fixed order);
-// alpha accumulates h[j].
-template <int NV>
-__global__ void __launch_bounds__(kThreads) reduce_h_k(const double* __restrict__ partial, int nblocks, int ld_i,
-                                                       int j, double* __restrict__ h, double* __restrict__ alpha_j) {
-  __shared__ double red[(kThreads / 32) * NV];
-  const int i = blockIdx.x;
-  double a[NV];
-#pragma unroll
-  for (int v = 0; v < NV; ++v) a[v] = 0.0;
-  for (int b = threadIdx.x; b < nblocks; b += kThreads)
-#pragma unroll
-    for (int v = 0; v < NV; ++v) a[v] += partial[((int64_t)b * ld_i + i) * NV + v];
-  block_sum<NV>(a, red);
-  if (threadIdx.x < NV) {
-    h[i * NV + threadIdx.x] = a[threadIdx.x];
-    if (alpha_j && i == j) alpha_j[threadIdx.x] += a[threadIdx.x];
-  }
-}
-
-// w[v][r] -= sum_{i<=j} V[i][v][r] h[i][v] over row quads; block partials of
-// |w_v|^2 (padding rows are zero in V and w and stay zero).
-template <typename T, int NV>
-__global__ void __launch_bounds__(kThreads) update_k(const T* __restrict__ V, int64_t n_pad, int j,
-                                                     const double* __restrict__ h, double* __restrict__ w,
-                                                     double* __restrict__ norm_partial, int64_t stride_i) {
-  extern __shared__ double hs[];  // [(j+1)][NV]
-  __shared__ double red[(kThreads / 32) * NV];
-  for (int t = threadIdx.x; t < (j + 1) * NV; t += kThreads) hs[t] = h[t];
-  __syncthreads();
-  double nrm[NV];
-#pragma unroll
-  for (int v = 0; v < NV; ++v) nrm[v] = 0.0;
-  const int64_t nq = n_pad / 4;
-  for (int64_t g = blockIdx.x * (int64_t)kThreads + threadIdx.x; g < nq * NV; g += (int64_t)gridDim.x * kThreads) {
-    const int v = (int)(g / nq);
-    const int64_t q = g - v * nq;
-    const T* Vp = V + (int64_t)v * n_pad + 4 * q;
-    double s[4] = {0.0, 0.0, 0.0, 0.0};
-    int i = 0;
-    for (; i + 1 <= j; i += 2) {
-      double a4[4], b4[4];
-      ld4(Vp + (int64_t)i * stride_i, a4);
-      ld4(Vp + (int64_t)(i + 1) * stride_i, b4);
-      const double ha = hs[i * NV + v], hb = hs[(i + 1) * NV + v];
-#pragma unroll
-      for (int k = 0; k < 4; ++k) s[k] = fma(a4[k], ha, fma(b4[k], hb, s[k]));
-    }
-    for (; i <= j; ++i) {
-      double a4[4];
-      ld4(Vp + (int64_t)i * stride_i, a4);
-      const double ha = hs[i * NV + v];
-#pragma unroll
-      for (int k = 0; k < 4; ++k) s[k] = fma(a4[k], ha, s[k]);
-    }
-    double* wp = w + (int64_t)v * n_pad + 4 * q;
-    double w4[4];
-    ld4(wp, w4);
-    double sq = 0.0;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      w4[k] -= s[k];
-      sq = fma(w4[k], w4[k], sq);
-    }
-    st4(wp, w4);
-#pragma unroll
-    for (int vv = 0; vv < NV; ++vv)
-      if (vv == v) nrm[vv] += sq;
-  }
-  block_sum<NV>(nrm, red);
-  if (threadIdx.x < NV) norm_partial[blockIdx.x * NV + threadIdx.x] = nrm[threadIdx.x];
-}
-
 // |w_v|^2 block partials (planar w)
 template <int NV>
 __global__ void __launch_bounds__(kThreads) norm_k(const double* __restrict__ w, int64_t n_pad,
@@ -264,6 +149,178 @@ __global__ void scale_store_k(const double* __restrict__ w, int64_t n, int64_t n
   }
 }
 
+// partial[bx][i][r][v] over the Krylov tile i in [blockIdx.y*kItile, ...]
+// (i <= j): dots of V[i] with the candidate u = V[j] (r = 0) and with w (r = 1).
+template <typename T, int NV>
+__global__ void __launch_bounds__(kThreads, NV == 1 ? 2 : 3) dots2_k(const T* __restrict__ V, int64_t n_pad, int j,
+                                                    const double* __restrict__ w, double* __restrict__ partial,
+                                                    int ld_i, int64_t stride_i) {
+  __shared__ double red[(kThreads / 32) * kItile * 2];
+  const int i0 = blockIdx.y * kItile;
+  const int nt = min(kItile, j + 1 - i0);
+  const int64_t nq = n_pad / 4;
+  const int64_t cq = (nq + gridDim.x - 1) / gridDim.x;
+  const int64_t q0 = blockIdx.x * cq, q1 = min(nq, q0 + cq);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll 1
+  for (int v = 0; v < NV; ++v) {
+    double au[kItile], aw[kItile];
+#pragma unroll
+    for (int t = 0; t < kItile; ++t) au[t] = aw[t] = 0.0;
+    const double* wv = w + (int64_t)v * n_pad;
+    const T* U = V + (int64_t)j * stride_i + (int64_t)v * n_pad;
+    const T* Vv = V + (int64_t)i0 * stride_i + (int64_t)v * n_pad;
+#pragma unroll 1
+    for (int64_t q = q0 + threadIdx.x; q < q1; q += kThreads) {
+      double w4[4], u4[4];
+      ld4(wv + 4 * q, w4);
+      ld4(U + 4 * q, u4);
+#pragma unroll
+      for (int t = 0; t < kItile; ++t) {
+        if (t < nt) {
+          double x4[4];
+          ld4(Vv + (int64_t)t * stride_i + 4 * q, x4);
+          au[t] = fma(x4[0], u4[0], fma(x4[1], u4[1], fma(x4[2], u4[2], fma(x4[3], u4[3], au[t]))));
+          aw[t] = fma(x4[0], w4[0], fma(x4[1], w4[1], fma(x4[2], w4[2], fma(x4[3], w4[3], aw[t]))));
+        }
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < kItile; ++t) {
+      double a = au[t], b = aw[t];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_down_sync(0xffffffffu, a, o);
+        b += __shfl_down_sync(0xffffffffu, b, o);
+      }
+      if (lane == 0) {
+        red[(warp * kItile + t) * 2 + 0] = a;
+        red[(warp * kItile + t) * 2 + 1] = b;
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x < 2 * nt) {
+      const int t = threadIdx.x / 2, r = threadIdx.x % 2;
+      double a = 0.0;
+      for (int wi = 0; wi < kThreads / 32; ++wi) a += red[(wi * kItile + t) * 2 + r];
+      partial[(((int64_t)blockIdx.x * ld_i + i0 + t) * 2 + r) * NV + v] = a;
+    }
+    __syncthreads();
+  }
+}
+
+// hu[i][v] (r = 0), hw[i][v] (r = 1) = sum over row chunks (one CTA per (i, r)).
+template <int NV>
+__global__ void __launch_bounds__(kThreads) reduce2_k(const double* __restrict__ partial, int nblocks, int ld_i,
+                                                      double* __restrict__ hu, double* __restrict__ hw) {
+  __shared__ double red[(kThreads / 32) * NV];
+  const int i = blockIdx.x / 2, r = blockIdx.x % 2;
+  double a[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) a[v] = 0.0;
+  for (int b = threadIdx.x; b < nblocks; b += kThreads)
+#pragma unroll
+    for (int v = 0; v < NV; ++v) a[v] += partial[(((int64_t)b * ld_i + i) * 2 + r) * NV + v];
+  block_sum<NV>(a, red);
+  if (threadIdx.x < NV) (r == 0 ? hu : hw)[i * NV + threadIdx.x] = a[threadIdx.x];
+}
+
+// Per problem (thread v): r, c of the delayed step and the new tridiagonal
+// entries alpha_j, beta_j from the dots hu, hw and the previous alpha, beta.
+template <int NV>
+__global__ void dcgs_coef_k(const double* __restrict__ hu, const double* __restrict__ hw, int j,
+                            double* __restrict__ alpha, int lda, double* __restrict__ beta, int ldb,
+                            double* __restrict__ rc) {
+  const int v = threadIdx.x;
+  if (v >= NV) return;
+  const double* a = alpha + (int64_t)v * lda;
+  double* b = beta + (int64_t)v * ldb;
+  double ss = 0.0, sz = 0.0, sts = 0.0, ts_last = 0.0;
+  for (int i = 0; i < j; ++i) {
+    const double si = hu[i * NV + v], zi = hw[i * NV + v];
+    // (T s)_i over the leading j x j tridiagonal block
+    double ts = a[i] * si;
+    if (i > 0) ts = fma(b[i], hu[(i - 1) * NV + v], ts);
+    if (i + 1 < j) ts = fma(b[i + 1], hu[(i + 1) * NV + v], ts);
+    ss = fma(si, si, ss);
+    sz = fma(si, zi, sz);
+    sts = fma(si, ts, sts);
+    ts_last = ts;
+  }
+  const double r2 = hu[j * NV + v] - ss;
+  const double r = r2 > 0.0 ? sqrt(r2) : 0.0;
+  const double ri = r > 0.0 ? 1.0 / r : 0.0;
+  const double omega = hw[j * NV + v];
+  rc[v] = ri;
+  rc[NV + v] = (omega - sz) * ri;
+  alpha[(int64_t)v * lda + j] = (omega - 2.0 * sz + sts) * ri * ri;
+  if (j > 0) b[j] = (hw[(j - 1) * NV + v] - ts_last) * ri;
+}
+
+// One read of V[0..j): V[j] <- (u_j - sum_i V[i] s_i) / r, w <- w - sum_i V[i] z_i
+// - V[j] c, with block partials of |w_v|^2 (planar layouts, row quads).
+template <typename T, int NV>
+__global__ void __launch_bounds__(kThreads) dcgs_update_k(T* __restrict__ V, int64_t n_pad, int j,
+                                                          const double* __restrict__ hu,
+                                                          const double* __restrict__ hw,
+                                                          const double* __restrict__ rc, double* __restrict__ w,
+                                                          double* __restrict__ norm_partial, int64_t stride_i) {
+  extern __shared__ double sz[];  // s [j][NV] | z [j][NV]
+  __shared__ double red[(kThreads / 32) * NV];
+  for (int t = threadIdx.x; t < j * NV; t += kThreads) {
+    sz[t] = hu[t];
+    sz[j * NV + t] = hw[t];
+  }
+  __syncthreads();
+  double nrm[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) nrm[v] = 0.0;
+  const int64_t nq = n_pad / 4;
+  for (int64_t g = blockIdx.x * (int64_t)kThreads + threadIdx.x; g < nq * NV; g += (int64_t)gridDim.x * kThreads) {
+    const int v = (int)(g / nq);
+    const int64_t q = g - v * nq;
+    const T* Vp = V + (int64_t)v * n_pad + 4 * q;
+    T* Up = V + (int64_t)j * stride_i + (int64_t)v * n_pad + 4 * q;
+    double u4[4], w4[4];
+    ld4(Up, u4);
+    double* wp = w + (int64_t)v * n_pad + 4 * q;
+    ld4(wp, w4);
+    for (int i = 0; i < j; ++i) {
+      double a4[4];
+      ld4(Vp + (int64_t)i * stride_i, a4);
+      const double si = sz[i * NV + v], zi = sz[(j + i) * NV + v];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        u4[k] = fma(-a4[k], si, u4[k]);
+        w4[k] = fma(-a4[k], zi, w4[k]);
+      }
+    }
+    const double ri = rc[v], c = rc[NV + v];
+    double sq = 0.0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const T qk = (T)(u4[k] * ri);
+      Up[k] = qk;
+      w4[k] = fma(-(double)qk, c, w4[k]);
+      sq = fma(w4[k], w4[k], sq);
+    }
+    st4(wp, w4);
+#pragma unroll
+    for (int vv = 0; vv < NV; ++vv)
+      if (vv == v) nrm[vv] += sq;
+  }
+  block_sum<NV>(nrm, red);
+  if (threadIdx.x < NV) norm_partial[blockIdx.x * NV + threadIdx.x] = nrm[threadIdx.x];
+}
+
+// beta[v][j+1] = |w_v| / r_v (the coupling to the next candidate)
+template <int NV>
+__global__ void beta_next_k(const double* __restrict__ wnorm, const double* __restrict__ rc, double* __restrict__ beta,
+                            int ldb, int j1) {
+  const int v = threadIdx.x;
+  if (v < NV) beta[(int64_t)v * ldb + j1] = wnorm[v] * rc[v];
+}
+
 // ---------------------------------------------------------------------------
 // Tridiagonal eigen-solve (one CTA per problem)
 // ---------------------------------------------------------------------------
@@ -313,8 +370,8 @@ Layout make_layout(const edg_lanczos_problem* p) {
   L.V = off; off = align256(off + (int64_t)(L.m_max + 1) * L.n_pad * nv * esz);
   L.X = off; off = align256(off + n * nv * esz);
   L.w = off; off = align256(off + L.n_pad * nv * 8);
-  L.h = off; off = align256(off + (int64_t)(L.m_max + 1) * nv * 8);
-  L.partial = off; off = align256(off + (int64_t)L.nblk_dot * (L.m_max + 1) * nv * 8);
+  L.h = off; off = align256(off + (int64_t)(2 * (L.m_max + 1) + 3) * nv * 8);  // hu | hw | rc | |w|
+  L.partial = off; off = align256(off + (int64_t)L.nblk_dot * (L.m_max + 1) * 2 * nv * 8);
   L.normp = off; off = align256(off + (int64_t)L.nblk_upd * nv * 8);
   L.alpha = off; off = align256(off + (int64_t)nv * (L.m_max + 1) * 8);   // [nv][m_max+1]
   L.beta = off; off = align256(off + (int64_t)nv * (L.m_max + 2) * 8);    // [nv][m_max+2]
@@ -323,13 +380,6 @@ Layout make_layout(const edg_lanczos_problem* p) {
   L.tri_work = off; off = align256(off + (int64_t)nv * 6 * (L.m_max + 1) * 8);
   L.total = off;
   return L;
-}
-
-// column-major per-problem recurrence storage: alpha[v][i], beta[v][i]
-template <int NV>
-__global__ void scatter_coef_k(const double* __restrict__ src, double* __restrict__ dst, int ld, int i) {
-  int v = threadIdx.x;
-  if (v < NV) dst[(int64_t)v * ld + i] = src[v];
 }
 
 template <int NV>
@@ -379,7 +429,10 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
   double* tri_work = (double*)(ws + L.tri_work);
   const int ld_a = L.m_max + 1, ld_b = L.m_max + 2, ld_s = L.m_max + 1;
   const int64_t stride_i = n_pad * NV;  // entries per Krylov vector (all problems)
-  double* alpha_cur = h + (int64_t)L.m_max * NV;  // last NV slots of h (h[i] only used for i < m_max)
+  double* hu = h;                                   // [m_max+1][NV] dots with the candidate
+  double* hw = h + (int64_t)(L.m_max + 1) * NV;      // [m_max+1][NV] dots with w
+  double* rc = hw + (int64_t)(L.m_max + 1) * NV;     // [2][NV]: 1/r, c of the current step
+  double* wnorm = rc + 2 * NV;                        // [NV]: |w| of the next candidate
   const unsigned g_vec = edg::grid_for(n_pad, 256);
   cudaError_t e;
   // padding rows (r >= n) of w are zero from start_k on, so every Krylov plane
@@ -391,9 +444,9 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
   zero_k<NV><<<(NV * ld_b + 255) / 256, 256, 0, s>>>(beta, NV * ld_b);
   zero_k<NV><<<(NV * ld_a + 255) / 256, 256, 0, s>>>(alpha, NV * ld_a);
   if ((e = cudaGetLastError()) != cudaSuccess) return edg::cuda_status(e, "edg_lanczos: start");
-  const size_t upd_smem = (size_t)(L.m_max + 1) * NV * sizeof(double);
+  const size_t upd_smem = (size_t)2 * (L.m_max + 1) * NV * sizeof(double);
   if (upd_smem > 40 * 1024) {
-    e = cudaFuncSetAttribute(update_k<T, NV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)upd_smem);
+    e = cudaFuncSetAttribute(dcgs_update_k<T, NV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)upd_smem);
     if (e != cudaSuccess) return edg::cuda_status(e, "edg_lanczos: smem attribute");
   }
   std::vector<double> hb((size_t)NV * ld_b), ha((size_t)NV * ld_a), hev((size_t)NV * kMaxK),
@@ -451,23 +504,20 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
                                             X, w, s, n_pad, p->spmv_group);
     if (st) return st;
     if (timing) cudaEventRecord(event_at(3 * j + 1), s);
-    launches += 11;
-    zero_k<NV><<<1, 32, 0, s>>>(alpha_cur, NV);
-    // classical Gram-Schmidt twice against V[0..j]; the row-chunk grid shrinks
-    // as the Krylov tiles grow so that about 8 CTAs per SM are in flight
+    launches += 8;
+    // one delayed Gram-Schmidt step: two reads of V[0..j]; the row-chunk grid
+    // of the dots shrinks as the Krylov tiles grow (about 8 CTAs per SM)
     const int tiles = (j + kItile) / kItile;
     int nx = L.nblk_dot / tiles;
     if (nx < edg::kSmCount) nx = edg::kSmCount;
     const dim3 gd(nx, tiles);
-    for (int pass = 0; pass < 2; ++pass) {
-      dots_k<T, NV><<<gd, kThreads, 0, s>>>(V, n_pad, j, w, partial, ld_a, stride_i);
-      reduce_h_k<NV><<<j + 1, kThreads, 0, s>>>(partial, nx, ld_a, j, h, alpha_cur);
-      update_k<T, NV><<<L.nblk_upd, kThreads, upd_smem, s>>>(V, n_pad, j, h, w, normp, stride_i);
-    }
-    scatter_coef_k<NV><<<1, 32, 0, s>>>(alpha_cur, alpha, ld_a, j);
-    beta_k<NV><<<1, kThreads, 0, s>>>(normp, L.nblk_upd, h);  // h[0..NV) = beta_{j+1}
-    scatter_coef_k<NV><<<1, 32, 0, s>>>(h, beta, ld_b, j + 1);
-    scale_store_k<T, NV><<<g_vec, 256, 0, s>>>(w, n, n_pad, h, V + (int64_t)(j + 1) * stride_i, X);
+    dots2_k<T, NV><<<gd, kThreads, 0, s>>>(V, n_pad, j, w, partial, ld_a, stride_i);
+    reduce2_k<NV><<<2 * (j + 1), kThreads, 0, s>>>(partial, nx, ld_a, hu, hw);
+    dcgs_coef_k<NV><<<1, 32, 0, s>>>(hu, hw, j, alpha, ld_a, beta, ld_b, rc);
+    dcgs_update_k<T, NV><<<L.nblk_upd, kThreads, upd_smem, s>>>(V, n_pad, j, hu, hw, rc, w, normp, stride_i);
+    beta_k<NV><<<1, kThreads, 0, s>>>(normp, L.nblk_upd, wnorm);  // |w| of the next candidate
+    beta_next_k<NV><<<1, 32, 0, s>>>(wnorm, rc, beta, ld_b, j + 1);
+    scale_store_k<T, NV><<<g_vec, 256, 0, s>>>(w, n, n_pad, wnorm, V + (int64_t)(j + 1) * stride_i, X);
     if (timing) cudaEventRecord(event_at(3 * j + 2), s);
     if ((e = cudaGetLastError()) != cudaSuccess) return edg::cuda_status(e, "edg_lanczos: step");
     const int m = j + 1;

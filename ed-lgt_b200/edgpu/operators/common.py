@@ -95,7 +95,12 @@ def selection_basis(rows: list[int], full_dim: int) -> csr_matrix:
     return csr_matrix((data, (np.asarray(rows, dtype=np.int64), np.arange(k))), shape=(full_dim, k))
 
 
+def _dense(a) -> np.ndarray:
+    return a.toarray() if hasattr(a, "toarray") else np.asarray(a)
+
+
 def project(basis, operator) -> np.ndarray:
-    """Dense ``B^dagger O B`` for a column basis ``B``."""
-    b = csr_matrix(basis)
-    return np.asarray((b.conj().T @ csr_matrix(operator) @ b).toarray())
+    """Dense ``B^dagger O B`` for a column basis ``B`` (local spaces are a few
+    dozen states, so dense products beat sparse ones here)."""
+    b = _dense(basis)
+    return b.conj().T @ _dense(operator) @ b

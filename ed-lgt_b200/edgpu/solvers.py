@@ -25,6 +25,7 @@ from ._lib import check, lib, ptr, stream_handle
 __all__ = ["LanczosResult", "lanczos", "lanczos_mixed", "stack_diagonals", "tune_spmv_group"]
 
 SPMV_GROUPS = (2, 4, 8, 16, 32)
+_TUNED_BY_SHAPE = {}  # (n, nnz, dtype, nvec, device) -> threads per row
 
 
 def tune_spmv_group(mat, nvec=1, dtype=0, reps=5, vals=None, diag=None):
@@ -32,13 +33,21 @@ def tune_spmv_group(mat, nvec=1, dtype=0, reps=5, vals=None, diag=None):
 
     Times ``edg_spmv_group`` for every group size with CUDA events (after one
     warm-up launch each) on the real matrix and the requested precision and
-    batch width; the choice is cached on the matrix object.
+    batch width; the choice is cached on the matrix object and, for the rest
+    of the process, for every matrix of the same shape (a performance choice
+    only: every group size gives the same result).
     """
     key = (dtype, nvec)
     cache = getattr(mat, "_tuned_groups", None)
     if cache is None:
         cache = mat._tuned_groups = {}
     if key in cache:
+        return cache[key]
+    # a matrix of the same shape (n, nnz) was tuned before in this process:
+    # the choice depends on the sparsity structure only, reuse it
+    shape_key = (mat.n, mat.nnz, dtype, nvec, mat.rowptr.device.index)
+    if shape_key in _TUNED_BY_SHAPE:
+        cache[key] = _TUNED_BY_SHAPE[shape_key]
         return cache[key]
     dev = mat.rowptr.device
     tdt = {0: torch.float64, 1: torch.float32}[dtype]
@@ -65,6 +74,7 @@ def tune_spmv_group(mat, nvec=1, dtype=0, reps=5, vals=None, diag=None):
         if t < best_t:
             best, best_t = g, t
     cache[key] = best
+    _TUNED_BY_SHAPE[shape_key] = best
     return best
 
 
