@@ -209,11 +209,18 @@ __global__ void __launch_bounds__(kThreads, NV == 1 ? 2 : 3) dots2_k(const T* __
   }
 }
 
-// hu[i][v] (r = 0), hw[i][v] (r = 1) = sum over row chunks (one CTA per (i, r)).
+// hu[i][v] (r = 0), hw[i][v] (r = 1) = sum over row chunks (one CTA per (i, r),
+// fixed order).  The last CTA to finish (ticket counter, reset by it) then
+// computes, one warp per problem, r and c of the delayed step and the new
+// tridiagonal entries alpha_j, beta_j from hu, hw and the previous alpha, beta.
 template <int NV>
-__global__ void __launch_bounds__(kThreads) reduce2_k(const double* __restrict__ partial, int nblocks, int ld_i,
-                                                      double* __restrict__ hu, double* __restrict__ hw) {
+__global__ void __launch_bounds__(kThreads) reduce2_coef_k(const double* __restrict__ partial, int nblocks, int ld_i,
+                                                           int j, double* __restrict__ hu, double* __restrict__ hw,
+                                                           double* __restrict__ alpha, int lda,
+                                                           double* __restrict__ beta, int ldb,
+                                                           double* __restrict__ rc, int* __restrict__ counter) {
   __shared__ double red[(kThreads / 32) * NV];
+  __shared__ int last;
   const int i = blockIdx.x / 2, r = blockIdx.x % 2;
   double a[NV];
 #pragma unroll
@@ -223,38 +230,50 @@ __global__ void __launch_bounds__(kThreads) reduce2_k(const double* __restrict__
     for (int v = 0; v < NV; ++v) a[v] += partial[(((int64_t)b * ld_i + i) * 2 + r) * NV + v];
   block_sum<NV>(a, red);
   if (threadIdx.x < NV) (r == 0 ? hu : hw)[i * NV + threadIdx.x] = a[threadIdx.x];
-}
-
-// Per problem (thread v): r, c of the delayed step and the new tridiagonal
-// entries alpha_j, beta_j from the dots hu, hw and the previous alpha, beta.
-template <int NV>
-__global__ void dcgs_coef_k(const double* __restrict__ hu, const double* __restrict__ hw, int j,
-                            double* __restrict__ alpha, int lda, double* __restrict__ beta, int ldb,
-                            double* __restrict__ rc) {
-  const int v = threadIdx.x;
-  if (v >= NV) return;
-  const double* a = alpha + (int64_t)v * lda;
-  double* b = beta + (int64_t)v * ldb;
-  double ss = 0.0, sz = 0.0, sts = 0.0, ts_last = 0.0;
-  for (int i = 0; i < j; ++i) {
-    const double si = hu[i * NV + v], zi = hw[i * NV + v];
-    // (T s)_i over the leading j x j tridiagonal block
-    double ts = a[i] * si;
-    if (i > 0) ts = fma(b[i], hu[(i - 1) * NV + v], ts);
-    if (i + 1 < j) ts = fma(b[i + 1], hu[(i + 1) * NV + v], ts);
-    ss = fma(si, si, ss);
-    sz = fma(si, zi, sz);
-    sts = fma(si, ts, sts);
-    ts_last = ts;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(counter, 1) == (int)gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  const int lane = threadIdx.x & 31, v = threadIdx.x >> 5;
+  if (v < NV) {
+    const double* al = alpha + (int64_t)v * lda;
+    double* be = beta + (int64_t)v * ldb;
+    double ss = 0.0, sz = 0.0, sts = 0.0;
+    for (int k = lane; k < j; k += 32) {
+      const double sk = __ldcg(hu + k * NV + v), zk = __ldcg(hw + k * NV + v);
+      // (T s)_k over the leading j x j tridiagonal block
+      double ts = al[k] * sk;
+      if (k > 0) ts = fma(be[k], __ldcg(hu + (k - 1) * NV + v), ts);
+      if (k + 1 < j) ts = fma(be[k + 1], __ldcg(hu + (k + 1) * NV + v), ts);
+      ss = fma(sk, sk, ss);
+      sz = fma(sk, zk, sz);
+      sts = fma(sk, ts, sts);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      ss += __shfl_xor_sync(0xffffffffu, ss, o);
+      sz += __shfl_xor_sync(0xffffffffu, sz, o);
+      sts += __shfl_xor_sync(0xffffffffu, sts, o);
+    }
+    if (lane == 0) {
+      double ts_last = 0.0;
+      if (j > 0) {
+        ts_last = al[j - 1] * __ldcg(hu + (j - 1) * NV + v);
+        if (j > 1) ts_last = fma(be[j - 1], __ldcg(hu + (j - 2) * NV + v), ts_last);
+      }
+      const double r2 = __ldcg(hu + j * NV + v) - ss;
+      const double rr = r2 > 0.0 ? sqrt(r2) : 0.0;
+      const double ri = rr > 0.0 ? 1.0 / rr : 0.0;
+      const double omega = __ldcg(hw + j * NV + v);
+      rc[v] = ri;
+      rc[NV + v] = (omega - sz) * ri;
+      alpha[(int64_t)v * lda + j] = (omega - 2.0 * sz + sts) * ri * ri;
+      if (j > 0) be[j] = (__ldcg(hw + (j - 1) * NV + v) - ts_last) * ri;
+    }
   }
-  const double r2 = hu[j * NV + v] - ss;
-  const double r = r2 > 0.0 ? sqrt(r2) : 0.0;
-  const double ri = r > 0.0 ? 1.0 / r : 0.0;
-  const double omega = hw[j * NV + v];
-  rc[v] = ri;
-  rc[NV + v] = (omega - sz) * ri;
-  alpha[(int64_t)v * lda + j] = (omega - 2.0 * sz + sts) * ri * ri;
-  if (j > 0) b[j] = (hw[(j - 1) * NV + v] - ts_last) * ri;
+  if (threadIdx.x == 0) *counter = 0;
 }
 
 // One read of V[0..j): V[j] <- (u_j - sum_i V[i] s_i) / r, w <- w - sum_i V[i] z_i
@@ -264,7 +283,9 @@ __global__ void __launch_bounds__(kThreads) dcgs_update_k(T* __restrict__ V, int
                                                           const double* __restrict__ hu,
                                                           const double* __restrict__ hw,
                                                           const double* __restrict__ rc, double* __restrict__ w,
-                                                          double* __restrict__ norm_partial, int64_t stride_i) {
+                                                          double* __restrict__ norm_partial, int64_t stride_i,
+                                                          double* __restrict__ wnorm, double* __restrict__ beta,
+                                                          int ldb, int* __restrict__ counter) {
   extern __shared__ double sz[];  // s [j][NV] | z [j][NV]
   __shared__ double red[(kThreads / 32) * NV];
   for (int t = threadIdx.x; t < j * NV; t += kThreads) {
@@ -311,14 +332,28 @@ __global__ void __launch_bounds__(kThreads) dcgs_update_k(T* __restrict__ V, int
   }
   block_sum<NV>(nrm, red);
   if (threadIdx.x < NV) norm_partial[blockIdx.x * NV + threadIdx.x] = nrm[threadIdx.x];
-}
-
-// beta[v][j+1] = |w_v| / r_v (the coupling to the next candidate)
-template <int NV>
-__global__ void beta_next_k(const double* __restrict__ wnorm, const double* __restrict__ rc, double* __restrict__ beta,
-                            int ldb, int j1) {
-  const int v = threadIdx.x;
-  if (v < NV) beta[(int64_t)v * ldb + j1] = wnorm[v] * rc[v];
+  // the last CTA: |w_v| (fixed-order sum of the block partials) and
+  // beta[v][j+1] = |w_v| / r_v, the coupling to the next candidate
+  __shared__ int last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(counter, 1) == (int)gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  double tot[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) tot[v] = 0.0;
+  for (int b = threadIdx.x; b < (int)gridDim.x; b += kThreads)
+#pragma unroll
+    for (int v = 0; v < NV; ++v) tot[v] += __ldcg(norm_partial + b * NV + v);
+  block_sum<NV>(tot, red);
+  if (threadIdx.x < NV) {
+    const double nv = sqrt(tot[threadIdx.x]);
+    wnorm[threadIdx.x] = nv;
+    beta[(int64_t)threadIdx.x * ldb + j + 1] = nv * rc[threadIdx.x];
+  }
+  if (threadIdx.x == 0) *counter = 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -350,7 +385,7 @@ __global__ void ritz_k(const T* __restrict__ V, int64_t n_pad, int m, const doub
 // Workspace layout
 // ---------------------------------------------------------------------------
 struct Layout {
-  int64_t V, X, w, h, partial, normp, alpha, beta, tri_eval, tri_vec, tri_work, total;
+  int64_t V, X, w, h, partial, normp, alpha, beta, tri_eval, tri_vec, tri_work, sync, total;
   int nblk_dot, nblk_upd, m_max, ld_h;
   int64_t n_pad;
 };
@@ -378,6 +413,7 @@ Layout make_layout(const edg_lanczos_problem* p) {
   L.tri_eval = off; off = align256(off + (int64_t)nv * kMaxK * 8);
   L.tri_vec = off; off = align256(off + (int64_t)nv * kMaxK * (L.m_max + 1) * 8);
   L.tri_work = off; off = align256(off + (int64_t)nv * 6 * (L.m_max + 1) * 8);
+  L.sync = off; off = align256(off + 2 * (int64_t)sizeof(int));  // last-CTA tickets
   L.total = off;
   return L;
 }
@@ -433,6 +469,7 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
   double* hw = h + (int64_t)(L.m_max + 1) * NV;      // [m_max+1][NV] dots with w
   double* rc = hw + (int64_t)(L.m_max + 1) * NV;     // [2][NV]: 1/r, c of the current step
   double* wnorm = rc + 2 * NV;                        // [NV]: |w| of the next candidate
+  int* tickets = (int*)(ws + L.sync);                  // [2] last-CTA counters (left at 0)
   const unsigned g_vec = edg::grid_for(n_pad, 256);
   cudaError_t e;
   // padding rows (r >= n) of w are zero from start_k on, so every Krylov plane
@@ -443,6 +480,8 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
   scale_store_k<T, NV><<<g_vec, 256, 0, s>>>(w, n, n_pad, h, V, X);
   zero_k<NV><<<(NV * ld_b + 255) / 256, 256, 0, s>>>(beta, NV * ld_b);
   zero_k<NV><<<(NV * ld_a + 255) / 256, 256, 0, s>>>(alpha, NV * ld_a);
+  if ((e = cudaMemsetAsync(tickets, 0, 2 * sizeof(int), s)) != cudaSuccess)
+    return edg::cuda_status(e, "edg_lanczos: tickets");
   if ((e = cudaGetLastError()) != cudaSuccess) return edg::cuda_status(e, "edg_lanczos: start");
   const size_t upd_smem = (size_t)2 * (L.m_max + 1) * NV * sizeof(double);
   if (upd_smem > 40 * 1024) {
@@ -504,19 +543,22 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
                                             X, w, s, n_pad, p->spmv_group);
     if (st) return st;
     if (timing) cudaEventRecord(event_at(3 * j + 1), s);
-    launches += 8;
+    launches += 5;
     // one delayed Gram-Schmidt step: two reads of V[0..j]; the row-chunk grid
     // of the dots shrinks as the Krylov tiles grow (about 8 CTAs per SM)
+    // every thread of the dots handles at least 4 row quads per problem (the
+    // per-CTA reduction is then amortised), at most 8 CTAs per SM overall
     const int tiles = (j + kItile) / kItile;
+    const int64_t want = (n_pad / 4 + 4 * kThreads - 1) / (4 * kThreads);
     int nx = L.nblk_dot / tiles;
+    if (want < nx) nx = (int)want;
     if (nx < edg::kSmCount) nx = edg::kSmCount;
     const dim3 gd(nx, tiles);
     dots2_k<T, NV><<<gd, kThreads, 0, s>>>(V, n_pad, j, w, partial, ld_a, stride_i);
-    reduce2_k<NV><<<2 * (j + 1), kThreads, 0, s>>>(partial, nx, ld_a, hu, hw);
-    dcgs_coef_k<NV><<<1, 32, 0, s>>>(hu, hw, j, alpha, ld_a, beta, ld_b, rc);
-    dcgs_update_k<T, NV><<<L.nblk_upd, kThreads, upd_smem, s>>>(V, n_pad, j, hu, hw, rc, w, normp, stride_i);
-    beta_k<NV><<<1, kThreads, 0, s>>>(normp, L.nblk_upd, wnorm);  // |w| of the next candidate
-    beta_next_k<NV><<<1, 32, 0, s>>>(wnorm, rc, beta, ld_b, j + 1);
+    reduce2_coef_k<NV><<<2 * (j + 1), kThreads, 0, s>>>(partial, nx, ld_a, j, hu, hw, alpha, ld_a, beta, ld_b, rc,
+                                                         tickets);
+    dcgs_update_k<T, NV><<<L.nblk_upd, kThreads, upd_smem, s>>>(V, n_pad, j, hu, hw, rc, w, normp, stride_i, wnorm,
+                                                                beta, ld_b, tickets + 1);
     scale_store_k<T, NV><<<g_vec, 256, 0, s>>>(w, n, n_pad, wnorm, V + (int64_t)(j + 1) * stride_i, X);
     if (timing) cudaEventRecord(event_at(3 * j + 2), s);
     if ((e = cudaGetLastError()) != cudaSuccess) return edg::cuda_status(e, "edg_lanczos: step");
