@@ -642,7 +642,7 @@ def run_z3(args, world, rank, local):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=60)  # ~0.8 s timed: several 200 ms clock samples
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="edgpu", choices=["edgpu", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")

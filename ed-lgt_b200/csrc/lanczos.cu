@@ -150,9 +150,10 @@ __global__ void scale_store_k(const double* __restrict__ w, int64_t n, int64_t n
 }
 
 // partial[bx][i][r][v] over the Krylov tile i in [blockIdx.y*kItile, ...]
-// (i <= j): dots of V[i] with the candidate u = V[j] (r = 0) and with w (r = 1).
+// (i <= j) and the problem v = blockIdx.z: dots of V[i] with the candidate
+// u = V[j] (r = 0) and with w (r = 1).
 template <typename T, int NV>
-__global__ void __launch_bounds__(kThreads, NV == 1 ? 2 : 3) dots2_k(const T* __restrict__ V, int64_t n_pad, int j,
+__global__ void __launch_bounds__(kThreads, 2) dots2_k(const T* __restrict__ V, int64_t n_pad, int j,
                                                     const double* __restrict__ w, double* __restrict__ partial,
                                                     int ld_i, int64_t stride_i) {
   __shared__ double red[(kThreads / 32) * kItile * 2];
@@ -162,8 +163,8 @@ __global__ void __launch_bounds__(kThreads, NV == 1 ? 2 : 3) dots2_k(const T* __
   const int64_t cq = (nq + gridDim.x - 1) / gridDim.x;
   const int64_t q0 = blockIdx.x * cq, q1 = min(nq, q0 + cq);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll 1
-  for (int v = 0; v < NV; ++v) {
+  {
+    const int v = blockIdx.z;  // one problem per CTA: grid (row chunks, Krylov tiles, problems)
     double au[kItile], aw[kItile];
 #pragma unroll
     for (int t = 0; t < kItile; ++t) au[t] = aw[t] = 0.0;
@@ -229,8 +230,10 @@ __global__ void __launch_bounds__(kThreads) reduce2_coef_k(const double* __restr
 #pragma unroll
     for (int v = 0; v < NV; ++v) a[v] += partial[(((int64_t)b * ld_i + i) * 2 + r) * NV + v];
   block_sum<NV>(a, red);
-  if (threadIdx.x < NV) (r == 0 ? hu : hw)[i * NV + threadIdx.x] = a[threadIdx.x];
-  __threadfence();
+  if (threadIdx.x < NV) {
+    (r == 0 ? hu : hw)[i * NV + threadIdx.x] = a[threadIdx.x];
+    __threadfence();  // the writers publish before the ticket
+  }
   __syncthreads();
   if (threadIdx.x == 0) last = atomicAdd(counter, 1) == (int)gridDim.x - 1;
   __syncthreads();
@@ -331,11 +334,13 @@ __global__ void __launch_bounds__(kThreads) dcgs_update_k(T* __restrict__ V, int
       if (vv == v) nrm[vv] += sq;
   }
   block_sum<NV>(nrm, red);
-  if (threadIdx.x < NV) norm_partial[blockIdx.x * NV + threadIdx.x] = nrm[threadIdx.x];
+  if (threadIdx.x < NV) {
+    norm_partial[blockIdx.x * NV + threadIdx.x] = nrm[threadIdx.x];
+    __threadfence();  // the writers publish before the ticket
+  }
   // the last CTA: |w_v| (fixed-order sum of the block partials) and
   // beta[v][j+1] = |w_v| / r_v, the coupling to the next candidate
   __shared__ int last;
-  __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) last = atomicAdd(counter, 1) == (int)gridDim.x - 1;
   __syncthreads();
@@ -548,12 +553,15 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
     // of the dots shrinks as the Krylov tiles grow (about 8 CTAs per SM)
     // every thread of the dots handles at least 4 row quads per problem (the
     // per-CTA reduction is then amortised), at most 8 CTAs per SM overall
+    // grid (row chunks, Krylov tiles, problems): about four CTAs per SM in
+    // all, each thread at least two row quads, at most L.nblk_dot row chunks
     const int tiles = (j + kItile) / kItile;
-    const int64_t want = (n_pad / 4 + 4 * kThreads - 1) / (4 * kThreads);
-    int nx = L.nblk_dot / tiles;
-    if (want < nx) nx = (int)want;
-    if (nx < edg::kSmCount) nx = edg::kSmCount;
-    const dim3 gd(nx, tiles);
+    int nx = (4 * edg::kSmCount + tiles * NV - 1) / (tiles * NV);
+    const int64_t most = (n_pad / 4 + 2 * kThreads - 1) / (2 * kThreads);
+    if (nx > most) nx = (int)most;
+    if (nx > L.nblk_dot) nx = L.nblk_dot;
+    if (nx < 1) nx = 1;
+    const dim3 gd(nx, tiles, NV);
     dots2_k<T, NV><<<gd, kThreads, 0, s>>>(V, n_pad, j, w, partial, ld_a, stride_i);
     reduce2_coef_k<NV><<<2 * (j + 1), kThreads, 0, s>>>(partial, nx, ld_a, j, hu, hw, alpha, ld_a, beta, ld_b, rc,
                                                          tickets);
