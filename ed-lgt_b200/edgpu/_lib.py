@@ -236,6 +236,8 @@ _SIGS = {
     "edg_lanczos_small_batched": (I32, [C.POINTER(SmallBatch), P, P]),
     "edg_krylov_workspace_bytes": (I64, [C.POINTER(KrylovProblem)]),
     "edg_krylov_step": (I32, [C.POINTER(KrylovProblem), P, F64, P, I64, P, P]),
+    "edg_twobody_scratch_elems": (I64, [I32]),
+    "edg_twobody_expval": (I32, [C.POINTER(LookupTable), P, P, I32, P, P, P, I32, P, P, I32, P, I32, I64, P, P, I64, P]),
     "edg_zn_bitmap_words": (I64, [C.POINTER(ZnLattice)]),
     "edg_zn_mark": (I32, [C.POINTER(ZnLattice), P, P, P]),
     "edg_zn_fill": (I32, [C.POINTER(ZnLattice), P, P, P, P]),

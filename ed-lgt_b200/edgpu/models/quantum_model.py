@@ -57,6 +57,61 @@ def site_expval_device(sector, op, psi, out=None):
     return out
 
 
+def _transition_tables(ops, dmax, tol=1e-10):
+    """Per site and bra state, the kets with |<bra|op|ket>| > tol and their
+    amplitudes (the threshold of _prepare_local_transition_data,
+    edlgt/symmetries/sym_qmb_operations.py:32-92)."""
+    n_sites = ops.shape[0]
+    count = np.zeros((n_sites, dmax), dtype=np.int32)
+    ket = np.zeros((n_sites, dmax, dmax), dtype=np.uint8)
+    amp = np.zeros((n_sites, dmax, dmax, 2), dtype=np.float64)
+    for s in range(n_sites):
+        m = np.asarray(ops[s], dtype=np.complex128)
+        for b in range(min(dmax, m.shape[0])):
+            ks = np.nonzero(np.abs(m[b]) > tol)[0]
+            count[s, b] = len(ks)
+            ket[s, b, : len(ks)] = ks
+            amp[s, b, : len(ks), 0] = m[b, ks].real
+            amp[s, b, : len(ks), 1] = m[b, ks].imag
+    return count, ket, amp
+
+
+def twobody_corr_device(sector, op_a, op_b, psi, pairs=None):
+    """Device matrix corr[i][j] = corr[j][i] = Re <psi| A_i B_j |psi> over site
+    pairs i < j (all pairs by default), zero diagonal: TwoBodyTerm.get_expval
+    with lattice_twobody_exp_val (edlgt/modeling/twobody_term.py:160-264).
+    op_a, op_b: (n_sites, dmax, dmax) projected site operators; psi: device
+    vector in the sector basis."""
+    n_sites = sector.n_sites
+    dmax = int(op_a.shape[-1])
+    key = ("tb", id(op_a), id(op_b), sector.device, tuple(int(d) for d in sector.loc_dims))
+    if key not in _DIAG_CACHE:
+        ca, ka, aa = _transition_tables(op_a, dmax)
+        cb, kb, ab = _transition_tables(op_b, dmax)
+        dev = sector.device
+        up = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+        _DIAG_CACHE[key] = (op_a, op_b, up(np.stack([ca, cb])), up(np.stack([ka, kb])), up(np.stack([aa, ab])),
+                            up(sector.strides.astype(np.int64)), up(sector.loc_dims.astype(np.int32)))
+    _, _, t_count, t_ket, t_amp, strides, loc_dims = _DIAG_CACHE[key]
+    if pairs is None:
+        pairs = [(i, j) for i in range(n_sites) for j in range(i + 1, n_sites)]
+    pairs = np.asarray(pairs, dtype=np.int32).reshape(-1, 2)
+    pi = torch.from_numpy(np.ascontiguousarray(pairs[:, 0])).to(sector.device)
+    pj = torch.from_numpy(np.ascontiguousarray(pairs[:, 1])).to(sector.device)
+    codes = {torch.float64: 0, torch.float32: 1, torch.complex128: 2, torch.complex64: 3}
+    if psi.dtype not in codes:
+        psi = psi.to(torch.complex128)
+    p = psi.contiguous()
+    n_pairs = len(pairs)
+    ns = lib.edg_twobody_scratch_elems(n_pairs)
+    scratch = torch.empty(max(ns, 1), dtype=torch.float64, device=sector.device)
+    corr = torch.empty((n_sites, n_sites), dtype=torch.float64, device=sector.device)
+    check(lib.edg_twobody_expval(sector.lookup_table(), ptr(strides), ptr(loc_dims), n_sites, ptr(t_count),
+                                 ptr(t_ket), ptr(t_amp), dmax, ptr(pi), ptr(pj), n_pairs, ptr(p), codes[p.dtype], 1,
+                                 ptr(corr), ptr(scratch), ns, stream_handle()), "edg_twobody_expval")
+    return corr
+
+
 class QuantumModel:
     def __init__(self, lvals, has_obc, ham_format="gpu", basis_projector=None, device=None):
         self.lvals = list(lvals)
@@ -227,10 +282,19 @@ class QuantumModel:
             psi = torch.from_numpy(np.asarray(psi)).to(self.device)
         return site_expval_device(self.sector, op, psi).cpu().numpy()
 
+    def twobody_expval(self, op_a, op_b, psi) -> np.ndarray:
+        """Correlator matrix Re <psi| A_i B_j |psi>, i != j (TwoBodyTerm.get_expval)."""
+        if isinstance(psi, QMB_state):
+            psi = psi.device(self.device)
+        elif not isinstance(psi, torch.Tensor):
+            psi = torch.from_numpy(np.asarray(psi)).to(self.device)
+        return twobody_corr_device(self.sector, op_a, op_b, psi).cpu().numpy()
+
     def get_observables(self, local_obs=(), twobody_obs=(), plaquette_obs=(), nbody_obs=(), nbody_dist=(),
                         twobody_axes=None):
         self.local_obs = list(local_obs)
-        self.twobody_obs = list(twobody_obs)
+        self.twobody_obs = [list(x) for x in twobody_obs]
+        self.twobody_axes = twobody_axes
         self.plaquette_obs = [list(x) for x in plaquette_obs]
         self.obs_list = {}
         self._plaq_mats = {}
@@ -238,8 +302,6 @@ class QuantumModel:
             axes = [names[-1][3], names[-1][6]]
             term = PlaquetteTerm(axes, [self.ops[o] for o in names], names, **self.def_params)
             self.obs_list["_".join(names)] = term
-        if twobody_obs:
-            raise NotImplementedError("two-body correlators are not part of the device engine yet")
 
     def _state(self, index, dynamics):
         return self.H.Npsi[index] if not dynamics else self.H.psi_time[index]
@@ -248,6 +310,8 @@ class QuantumModel:
         st = self._state(index, dynamics)
         for obs in self.local_obs:
             self.res[obs] = self.local_expval(self.ops[obs], st)
+        for names in self.twobody_obs:
+            self.res["_".join(names)] = self.twobody_expval(self.ops[names[0]], self.ops[names[1]], st)
         for names in self.plaquette_obs:
             key = "_".join(names)
             self.res[key] = self.plaquette_avg(names, st)

@@ -391,6 +391,27 @@ int edg_local_expval(const uint64_t* keys, int64_t n, const edg_site_dims* dims,
                      int64_t psi_stride, const double* diag, int32_t dmax,
                      double* out, cudaStream_t stream);
 
+/* Two-body correlators, TwoBodyTerm.get_expval / lattice_twobody_exp_val
+ * (edlgt/modeling/twobody_term.py:160-264): corr[i * n_sites + j] =
+ * corr[j * n_sites + i] = Re <psi| A_i B_j |psi> for each listed pair i < j
+ * (pair_i, pair_j device arrays), 0 elsewhere.  A and B come as transition
+ * tables: t_count [2][n_sites][dmax], t_ket [2][n_sites][dmax][dmax] (uint8),
+ * t_amp [2][n_sites][dmax][dmax][2] (re, im), first index 0 for A, 1 for B.
+ * sector: the lookup table of the sorted sector keys; strides, loc_dims:
+ * [n_sites] device arrays of the key format.  psi: dtype 0 f64, 1 f32,
+ * 2 complex128, 3 complex64 at psi[r * psi_stride].  scratch: at least
+ * edg_twobody_scratch_elems(n_pairs) doubles; t_amp 16-byte aligned.
+ * Synchronizes the stream (one flag read); a ket outside the sector returns
+ * EDG_ERR_MISSING_KET (the reference would read psi[-1] there), a pair with a
+ * site outside [0, n_sites) or i == j returns EDG_ERR_ARG. */
+int64_t edg_twobody_scratch_elems(int32_t n_pairs);
+int edg_twobody_expval(const edg_lookup_table* sector, const uint64_t* strides,
+                       const int32_t* loc_dims, int32_t n_sites, const int32_t* t_count,
+                       const uint8_t* t_ket, const double* t_amp, int32_t dmax,
+                       const int32_t* pair_i, const int32_t* pair_j, int32_t n_pairs,
+                       const void* psi, int32_t psi_dtype, int64_t psi_stride, double* corr,
+                       double* scratch, int64_t scratch_elems, cudaStream_t stream);
+
 /* ------------------------------------------------------------------------
  * Matrix-free Z_n lattice gauge theory with staggered fermions (periodic
  * Lx x Ly, Gauss law, zero charge, optional zero momentum).

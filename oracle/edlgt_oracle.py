@@ -286,3 +286,20 @@ def local_expval(psi, op, cfg):
         d = np.real(np.diagonal(np.asarray(op[s])))
         out[s] = np.sum(p2 * d[cfg[:, s]])
     return out
+
+
+def twobody_expval(psi, op_a, op_b, cfg, loc_dims):
+    """corr[i, j] = corr[j, i] = Re <psi| A_i B_j |psi> for all pairs i < j, the
+    loop of lattice_twobody_exp_val (edlgt/modeling/twobody_term.py:232-264)
+    over the two-site triplets (nbody_data_2sites) and exp_val_data
+    (edlgt/modeling/qmb_state.py:631-654)."""
+    psi = np.asarray(psi, dtype=np.complex128)
+    n = cfg.shape[1]
+    corr = np.zeros((n, n))
+    for i in range(n):
+        for j in range(i + 1, n):
+            rows, cols, vals = nbody_triplets([op_a, op_b], [i, j], cfg, loc_dims)
+            ok = cols >= 0
+            e = np.sum(np.conj(psi[rows[ok]]) * vals[ok] * psi[cols[ok]])
+            corr[i, j] = corr[j, i] = float(np.real(e))
+    return corr

@@ -45,3 +45,10 @@ def build(name, device="cpu", big=False):
     kw, g, m = ALL_CASES[name]
     cls = QED_Model if name.startswith("qed") else SU2_Model
     return cls(**kw, device=device), g, m
+
+# two-body correlator fixtures: case name -> operator pairs measured on the ground state
+TWOBODY_CASES = {
+    "qed1d_L8_obc": [["N", "N"], ["E2_px", "N"]],
+    "qed2d_3x2_bg": [["N", "N"], ["E2_px", "E2_py"]],
+    "su2_1d_L8_obc": [["N_tot", "N_tot"], ["N_pair", "T2_px"]],
+}

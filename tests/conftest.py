@@ -44,3 +44,10 @@ def golden_dyn():
     import numpy as np
 
     return np.load(os.path.join(GOLDEN, "dynamics_cases.npz"))
+
+
+@pytest.fixture(scope="session")
+def golden_twobody():
+    import numpy as np
+
+    return np.load(os.path.join(GOLDEN, "twobody_cases.npz"))

@@ -5,7 +5,7 @@ Run in a container that has the reference checkout (EDLGT_PATH, default
 
     python tests/golden/make_golden.py [group ...]
 
-Groups: sectors, matrices, spectra, dynamics, big.  Output: .npz files next to
+Groups: small, pins, dynamics, big, twobody.  Output: .npz files next to
 this script.  Nothing here is imported by the library or by the GPU tests;
 the tests only read the .npz files.
 
@@ -284,8 +284,39 @@ def gen_dynamics():
     np.savez_compressed(os.path.join(HERE, "dynamics_cases.npz"), **out)
 
 
+TWOBODY_CASES = {
+    # name: (factory, kwargs, g, m, [operator pairs])
+    "qed1d_L8_obc": (qed_model, QED_CASES["qed1d_L8_obc"][0], 1.0, 1.0, [["N", "N"], ["E2_px", "N"]]),
+    "qed2d_3x2_bg": (qed_model, QED_CASES["qed2d_3x2_bg"][0], 1.0, 1.0, [["N", "N"], ["E2_px", "E2_py"]]),
+    "su2_1d_L8_obc": (su2_model, SU2_CASES["su2_1d_L8_obc"][0], 1.0, 0.5,
+                      [["N_tot", "N_tot"], ["N_pair", "T2_px"]]),
+}
+
+
+def gen_twobody():
+    """Two-body correlator matrices of the ground state through the
+    reference's get_observables(twobody_obs=...) / measure_observables path,
+    stored with the ground state and the sector keys they were measured on."""
+    out = {}
+    for name, (factory, kw, g, mass, pairs) in TWOBODY_CASES.items():
+        model = factory(kw)
+        model.build_Hamiltonian(g, mass)
+        model.diagonalize_Hamiltonian(1, "sparse")
+        model.get_observables([], pairs, [])
+        model.measure_observables(0)
+        out[f"{name}/keys"] = keys_of(model.sector_configs, model.loc_dims)
+        out[f"{name}/loc_dims"] = np.asarray(model.loc_dims, dtype=np.int64)
+        out[f"{name}/psi"] = np.asarray(model.H.Npsi[0].psi, dtype=np.complex128)
+        for a, b in pairs:
+            out[f"{name}/{a}_{b}"] = np.asarray(model.res[f"{a}_{b}"], dtype=np.float64)
+        print(name, len(model.sector_configs), flush=True)
+    np.savez_compressed(os.path.join(HERE, "twobody_cases.npz"), **out)
+
+
 if __name__ == "__main__":
-    groups = sys.argv[1:] or ["small", "pins", "dynamics", "big"]
+    groups = sys.argv[1:] or ["small", "pins", "dynamics", "big", "twobody"]
+    if "twobody" in groups:
+        gen_twobody()
     if "small" in groups:
         gen_small()
     if "pins" in groups:

@@ -5,7 +5,7 @@ the package feed both, so these tests also pin the host model layer."""
 import numpy as np
 import pytest
 
-from cases import ALL_CASES, build
+from cases import ALL_CASES, TWOBODY_CASES, build
 from oracle import edlgt_oracle as O
 
 
@@ -86,3 +86,19 @@ def test_dynamics_oracle(golden_dyn):
         psi_t = O.evolve(H, psi0, t)
         T2 = np.array([O.local_expval(p, model.ops["T2_px"], cfg) for p in psi_t])
         assert np.max(np.abs(T2 - golden_dyn[f"{key}/T2_px"])) < 1e-9
+
+
+@pytest.mark.parametrize("name", sorted(TWOBODY_CASES))
+def test_twobody_oracle(name, golden_twobody):
+    """Correlator matrices of the reference's TwoBodyTerm on its own ground
+    state, recomputed by the oracle from the package's projected operators."""
+    model, _, _ = build(name)
+    loc = golden_twobody[f"{name}/loc_dims"]
+    assert np.array_equal(model.loc_dims, loc)
+    cfg = O.sector_configs(**model.sector_inputs)
+    assert np.array_equal(O.keys_of(cfg, loc), golden_twobody[f"{name}/keys"])
+    psi = golden_twobody[f"{name}/psi"]
+    for a, b in TWOBODY_CASES[name]:
+        corr = O.twobody_expval(psi, model.ops[a], model.ops[b], cfg, loc)
+        ref = golden_twobody[f"{name}/{a}_{b}"]
+        assert np.max(np.abs(corr - ref)) <= 1e-12 * max(1.0, np.max(np.abs(ref))), (a, b)
