@@ -52,40 +52,77 @@ struct Args {
   double* partial;  // [kBlocks][n_pairs][2]
   int32_t* err;
   int n_sites, dmax, n_pairs;
-  int tables_in_smem;
+  int tables_in_smem, diag_in_smem;
 };
 
-// Dynamic shared memory: [amp | diagonal values | count | ket] (when they
-// fit), the row staging (keys, amplitudes, local states) and the per-warp pair
-// partials.  In shared memory a count carries kDiagBit when its bra state has
-// exactly one transition, to itself; the diagonal table then holds that
-// element, so a pair whose both factors are diagonal on a row costs two
-// table reads and |psi_row|^2 (a b).
+// Shared memory, in this order: the transition tables [amp | diagonal values
+// | count | ket] when they fit (kTableSmemCap); the real diagonal table when
+// it fits (kDiagCap entries); the local dimensions with their multiply-high
+// reciprocals; the row staging (keys, amplitudes, local states); the per-warp
+// pair partials.  In the transition tables a count carries kDiagBit when its
+// bra state has exactly one transition, to itself, and the diagonal values
+// hold that element.  The real diagonal table is stored local state major,
+// [b][operator * n_sites + site] with a row pitch rounded to 16 doubles: the
+// lanes of a warp read one row's values at different sites, which then fall
+// in different banks whatever the local states are.
 constexpr int kDiagBit = 1 << 16;
+constexpr int kDiagCap = 2048;
+__host__ __device__ inline int64_t round16(int64_t b) { return (b + 15) / 16 * 16; }
+__host__ __device__ inline int diag_pitch(int n_sites) { return (2 * n_sites + 15) / 16 * 16; }
 __host__ __device__ inline int64_t table_bytes(int n_sites, int dmax) {
   const int64_t e = 2LL * n_sites * dmax;
   return e * dmax * 16 + e * 16 + e * 4 + e * dmax;
 }
-__host__ __device__ inline int64_t staging_bytes(int n_sites) {
-  return (int64_t)kWarps * 32 * (8 + 16) + (((int64_t)kWarps * 32 * n_sites + 15) / 16) * 16;
+struct Layout {
+  int64_t tables, diag, aux, staging, red, total;
+};
+__host__ __device__ inline Layout layout(int ns, int dm, int tables_in_smem, int diag_in_smem) {
+  Layout l;
+  int64_t off = 0;
+  l.tables = off;
+  off += tables_in_smem ? round16(table_bytes(ns, dm)) : 0;
+  l.diag = off;
+  off += diag_in_smem ? (int64_t)dm * diag_pitch(ns) * 8 : 0;
+  l.aux = off;
+  off += round16((int64_t)ns * 12);
+  l.staging = off;
+  off += (int64_t)kWarps * 32 * (8 + 16) + round16((int64_t)kWarps * 32 * ns);
+  l.red = off;
+  off += (int64_t)kWarps * kTilePairs * 16;
+  l.total = off;
+  return l;
 }
-constexpr int64_t kRedBytes = (int64_t)kWarps * kTilePairs * 16;
 
 template <int PT>
 __global__ void __launch_bounds__(kThreads, 3) twobody_k(const Args a) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int ns = a.n_sites, dm = a.dmax;
-  const int64_t tb = a.tables_in_smem ? table_bytes(ns, dm) : 0;
   const int e = 2 * ns * dm;  // table entries (operator, site, bra state)
-  double2* s_amp = reinterpret_cast<double2*>(smem);
+  const Layout L = layout(ns, dm, a.tables_in_smem, a.diag_in_smem);
+  double2* s_amp = reinterpret_cast<double2*>(smem + L.tables);
   double2* s_dv = s_amp + (int64_t)e * dm;
   int32_t* s_count = reinterpret_cast<int32_t*>(s_dv + e);
   uint8_t* s_ket = reinterpret_cast<uint8_t*>(s_count + e);
-  uint64_t* s_key = reinterpret_cast<uint64_t*>(smem + ((tb + 15) / 16) * 16);
+  double* s_dre = reinterpret_cast<double*>(smem + L.diag);
+  uint64_t* s_magic = reinterpret_cast<uint64_t*>(smem + L.aux);
+  uint32_t* s_ld = reinterpret_cast<uint32_t*>(s_magic + ns);
+  uint64_t* s_key = reinterpret_cast<uint64_t*>(smem + L.staging);
   double2* s_psi = reinterpret_cast<double2*>(s_key + kWarps * 32);
   uint8_t* s_dig = reinterpret_cast<uint8_t*>(s_psi + kWarps * 32);
-  double2* s_red = reinterpret_cast<double2*>(smem + ((tb + 15) / 16) * 16 + staging_bytes(ns));
+  double2* s_red = reinterpret_cast<double2*>(smem + L.red);
 
+  // local dimensions and ceil(2^64 / d): floor(x / d) = umulhi(x, that) for
+  // every x < 2^32 (Lemire, Kaser, Kurz, "Faster remainder by direct
+  // computation", 2019, theorem 1 with N = 32, F = 64)
+  for (int s = threadIdx.x; s < ns; s += kThreads) {
+    uint32_t d = (uint32_t)a.loc_dims[s];
+    if (d < 1) {
+      atomicExch(a.err, 1);
+      d = 1;
+    }
+    s_ld[s] = d;
+    s_magic[s] = d > 1 ? ~0ull / d + 1 : 0;
+  }
   const double2* amp = a.amp;
   const int32_t* count = a.count;
   const uint8_t* ket = a.ket;
@@ -104,7 +141,19 @@ __global__ void __launch_bounds__(kThreads, 3) twobody_k(const Args a) {
     count = s_count;
     ket = s_ket;
   }
-  __syncthreads();
+  // both operators diagonal and real on every local state: the block takes
+  // the real diagonal path, <psi| A_i B_j |psi> = sum_r |psi_r|^2 a_i(r) b_j(r)
+  const int pitch = diag_pitch(ns);
+  int real_diag = a.diag_in_smem;
+  if (a.diag_in_smem) {
+    for (int k = threadIdx.x; k < e; k += kThreads) {
+      const int c = a.count[k];
+      const double2 v = c > 0 ? a.amp[k * dm] : make_double2(0.0, 0.0);
+      real_diag &= c == 0 || (c == 1 && a.ket[k * dm] == k % dm && v.y == 0.0);
+      s_dre[(k % dm) * pitch + k / dm] = v.x;  // k / dm = operator * n_sites + site
+    }
+  }
+  const bool fast = __syncthreads_and(real_diag) != 0;
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int64_t n = a.sec.n;
@@ -126,7 +175,7 @@ __global__ void __launch_bounds__(kThreads, 3) twobody_k(const Args a) {
       if (p < a.n_pairs && !ok && blockIdx.x == 0) atomicExch(a.err, 2);
       live[k] = p < a.n_pairs && ok;
       si[k] = live[k] ? pi : 0;
-      sj[k] = live[k] ? pj : 0;
+      sj[k] = live[k] ? pj : 1;
       acc_re[k] = 0.0;
       acc_im[k] = 0.0;
     }
@@ -137,64 +186,79 @@ __global__ void __launch_bounds__(kThreads, 3) twobody_k(const Args a) {
         uint64_t x = __ldg(a.sec.keys + r0 + lane);
         wkey[lane] = x;
         wpsi[lane] = load_psi<PT>(a.psi, r0 + lane, a.psi_stride);
-        for (int s = ns - 1; s >= 0; --s) {
-          const uint64_t d = (uint64_t)__ldg(a.loc_dims + s);
-          const uint64_t q = x / d;
-          wdig[lane * ns + s] = (uint8_t)(x - q * d);
+        for (int s = ns - 1; s >= 0; --s) {  // last site fastest
+          const uint32_t d = s_ld[s];
+          const uint64_t q = (x >> 32) ? x / d : (d > 1 ? __umul64hi(s_magic[s], x) : x);
+          uint32_t c = (uint32_t)(x - q * d);
+          if (c >= (uint32_t)dm) {  // a local state beyond the operators' dimension
+            atomicExch(a.err, 1);
+            c = 0;
+          }
+          wdig[lane * ns + s] = (uint8_t)c;
           x = q;
         }
       }
       __syncwarp();
-      for (int t = 0; t < rows; ++t) {
-        const uint64_t key = wkey[t];
-        const double2 pr = wpsi[t];
-        const double w = fma(pr.x, pr.x, pr.y * pr.y);
-        const uint8_t* drow = wdig + t * ns;
+      if (fast) {
+        for (int t = 0; t < rows; ++t) {
+          const double2 pr = wpsi[t];
+          const double w = fma(pr.x, pr.x, pr.y * pr.y);
+          const uint8_t* drow = wdig + t * ns;
 #pragma unroll
-        for (int k = 0; k < kPairsPerLane; ++k) {
-          if (!live[k]) continue;
-          const int ci = drow[si[k]], cj = drow[sj[k]];
-          if (ci >= dm || cj >= dm) {  // a local state beyond the operators' dimension
-            atomicExch(a.err, 1);
-            continue;
+          for (int k = 0; k < kPairsPerLane; ++k) {
+            const double va = s_dre[drow[si[k]] * pitch + si[k]];
+            const double vb = s_dre[drow[sj[k]] * pitch + ns + sj[k]];
+            acc_re[k] = fma(va * w, vb, acc_re[k]);
           }
-          const int ea = si[k] * dm + ci, eb = (ns + sj[k]) * dm + cj;
-          const int na = count[ea], nb = count[eb];
-          if (na & nb & kDiagBit) {  // both diagonal here: <r| a b |r> |psi_r|^2
-            const double2 av = s_dv[ea], bv = s_dv[eb];
-            acc_re[k] = fma(w, av.x * bv.x - av.y * bv.y, acc_re[k]);
-            acc_im[k] = fma(w, av.x * bv.y + av.y * bv.x, acc_im[k]);
-            continue;
-          }
-          const int ca = na & (kDiagBit - 1), cb = nb & (kDiagBit - 1);
-          for (int ta = 0; ta < ca; ++ta) {
-            const int ia = ea * dm + ta;
-            const int ka = ket[ia];
-            const double2 av = amp[ia];
-            for (int tbi = 0; tbi < cb; ++tbi) {
-              const int ib = eb * dm + tbi;
-              const int kb = ket[ib];
-              const double2 bv = amp[ib];
-              double2 pc;
-              if (ka == ci && kb == cj) {
-                pc = pr;  // both factors diagonal: the ket is this row
-              } else {
-                // a padded local state (beyond the site's dimension) is no configuration
-                const bool inside = ka < __ldg(a.loc_dims + si[k]) && kb < __ldg(a.loc_dims + sj[k]);
-                const uint64_t q = key + ((uint64_t)ka - (uint64_t)ci) * __ldg(a.strides + si[k]) +
-                                   ((uint64_t)kb - (uint64_t)cj) * __ldg(a.strides + sj[k]);
-                const int64_t col = inside ? edg::find_key(a.sec, q) : -1;
-                if (col < 0) {
-                  atomicExch(a.err, 1);
-                  continue;
+        }
+      } else {
+        for (int t = 0; t < rows; ++t) {
+          const uint64_t key = wkey[t];
+          const double2 pr = wpsi[t];
+          const double w = fma(pr.x, pr.x, pr.y * pr.y);
+          const uint8_t* drow = wdig + t * ns;
+#pragma unroll
+          for (int k = 0; k < kPairsPerLane; ++k) {
+            if (!live[k]) continue;
+            const int ci = drow[si[k]], cj = drow[sj[k]];
+            const int ea = si[k] * dm + ci, eb = (ns + sj[k]) * dm + cj;
+            const int na = count[ea], nb = count[eb];
+            if (na & nb & kDiagBit) {  // both diagonal here: <r| a b |r> |psi_r|^2
+              const double2 av = s_dv[ea], bv = s_dv[eb];
+              acc_re[k] = fma(w, av.x * bv.x - av.y * bv.y, acc_re[k]);
+              acc_im[k] = fma(w, av.x * bv.y + av.y * bv.x, acc_im[k]);
+              continue;
+            }
+            const int ca = na & (kDiagBit - 1), cb = nb & (kDiagBit - 1);
+            for (int ta = 0; ta < ca; ++ta) {
+              const int ia = ea * dm + ta;
+              const int ka = ket[ia];
+              const double2 av = amp[ia];
+              for (int tbi = 0; tbi < cb; ++tbi) {
+                const int ib = eb * dm + tbi;
+                const int kb = ket[ib];
+                const double2 bv = amp[ib];
+                double2 pc;
+                if (ka == ci && kb == cj) {
+                  pc = pr;  // both factors diagonal: the ket is this row
+                } else {
+                  // a padded local state (beyond the site's dimension) is no configuration
+                  const bool inside = (uint32_t)ka < s_ld[si[k]] && (uint32_t)kb < s_ld[sj[k]];
+                  const uint64_t q = key + ((uint64_t)ka - (uint64_t)ci) * __ldg(a.strides + si[k]) +
+                                     ((uint64_t)kb - (uint64_t)cj) * __ldg(a.strides + sj[k]);
+                  const int64_t col = inside ? edg::find_key(a.sec, q) : -1;
+                  if (col < 0) {
+                    atomicExch(a.err, 1);
+                    continue;
+                  }
+                  pc = load_psi<PT>(a.psi, col, a.psi_stride);
                 }
-                pc = load_psi<PT>(a.psi, col, a.psi_stride);
+                // acc += conj(pr) * (a * b) * pc
+                const double vr = av.x * bv.x - av.y * bv.y, vi = av.x * bv.y + av.y * bv.x;
+                const double tr = vr * pc.x - vi * pc.y, ti = vr * pc.y + vi * pc.x;
+                acc_re[k] = fma(pr.x, tr, fma(pr.y, ti, acc_re[k]));
+                acc_im[k] = fma(pr.x, ti, fma(-pr.y, tr, acc_im[k]));
               }
-              // acc += conj(pr) * (a * b) * pc
-              const double vr = av.x * bv.x - av.y * bv.y, vi = av.x * bv.y + av.y * bv.x;
-              const double tr = vr * pc.x - vi * pc.y, ti = vr * pc.y + vi * pc.x;
-              acc_re[k] = fma(pr.x, tr, fma(pr.y, ti, acc_re[k]));
-              acc_im[k] = fma(pr.x, ti, fma(-pr.y, tr, acc_im[k]));
             }
           }
         }
@@ -281,10 +345,10 @@ extern "C" int edg_twobody_expval(const edg_lookup_table* sector, const uint64_t
   e = cudaMemsetAsync(err, 0, sizeof(int32_t), stream);
   if (e != cudaSuccess) return edg::cuda_status(e, "edg_twobody_expval: flag");
   Args a{*sector, strides, loc_dims, t_count, t_ket, reinterpret_cast<const double2*>(t_amp), pair_i, pair_j, psi,
-         psi_stride, scratch, err, n_sites, dmax, n_pairs, 0};
-  const int64_t tbytes = table_bytes(n_sites, dmax);
-  a.tables_in_smem = tbytes <= kTableSmemCap;
-  const int64_t smem = (a.tables_in_smem ? ((tbytes + 15) / 16) * 16 : 0) + staging_bytes(n_sites) + kRedBytes;
+         psi_stride, scratch, err, n_sites, dmax, n_pairs, 0, 0};
+  a.tables_in_smem = table_bytes(n_sites, dmax) <= kTableSmemCap;
+  a.diag_in_smem = dmax * diag_pitch(n_sites) <= kDiagCap;
+  const int64_t smem = layout(n_sites, dmax, a.tables_in_smem, a.diag_in_smem).total;
   switch (psi_dtype) {
     case 0: e = launch<0>(a, smem, stream); break;
     case 1: e = launch<1>(a, smem, stream); break;

@@ -128,3 +128,34 @@ def test_twobody_missing_ket_is_an_error(dev):
     psi = torch.ones(len(model.sector), dtype=torch.float64, device=dev)
     with pytest.raises(EdgError, match="MISSING_KET"):
         model.twobody_expval(model.ops["Q_px_dag"], model.ops["N"], psi)
+
+
+@pytest.mark.parametrize("kind", ["real", "complex", "mixed"])
+def test_twobody_diagonal_operators(kind, dev):
+    """Diagonal operators take the per-row |psi_r|^2 a b paths (real: the
+    real-diagonal block path; complex or one off-diagonal factor: the
+    transition-table path); all against the oracle."""
+    import torch
+
+    from edgpu.models.quantum_model import twobody_corr_device
+
+    rng = np.random.default_rng(5)
+    loc_dims = np.array([4, 3, 5, 2, 4, 3, 2])
+    sector = _product_space(loc_dims, dev)
+    dmax = 5
+
+    def diag_ops(cplx):
+        ops = np.zeros((len(loc_dims), dmax, dmax), dtype=np.complex128)
+        for s, d in enumerate(loc_dims):
+            v = rng.normal(size=d) + (1j * rng.normal(size=d) if cplx else 0)
+            v[rng.random(d) < 0.3] = 0
+            ops[s, np.arange(d), np.arange(d)] = v
+        return ops
+
+    op_a = diag_ops(kind == "complex")
+    op_b = diag_ops(kind == "complex") if kind != "mixed" else _random_ops(rng, loc_dims, dmax)
+    psi = rng.normal(size=len(sector)) + 1j * rng.normal(size=len(sector))
+    psi /= np.linalg.norm(psi)
+    got = twobody_corr_device(sector, op_a, op_b, torch.from_numpy(psi).to(dev)).cpu().numpy()
+    ref = O.twobody_expval(psi, op_a, op_b, sector.configs, loc_dims)
+    assert np.max(np.abs(got - ref)) <= 1e-12 * max(1.0, np.max(np.abs(ref)))
