@@ -209,6 +209,17 @@ class ZnBasis(C.Structure):
     _fields_ = [("n_rows", I64), ("keys", P), ("orbit", P)]
 
 
+class PartSpec(C.Structure):
+    _fields_ = [
+        ("n_part", I32),
+        ("reserved", I32),
+        ("key_space", U64),
+        ("src_stride", U64 * MAX_SITES),
+        ("dim", U64 * MAX_SITES),
+        ("part_stride", U64 * MAX_SITES),
+    ]
+
+
 _SIGS = {
     "edg_get_last_error": (I32, [C.c_char_p, I32]),
     "edg_version": (I32, []),
@@ -238,6 +249,9 @@ _SIGS = {
     "edg_krylov_step": (I32, [C.POINTER(KrylovProblem), P, F64, P, I64, P, P]),
     "edg_twobody_scratch_elems": (I64, [I32]),
     "edg_twobody_expval": (I32, [C.POINTER(LookupTable), P, P, I32, P, P, P, I32, P, P, I32, P, I32, I64, P, P, I64, P]),
+    "edg_part_scratch_elems": (I64, [U64]),
+    "edg_part_map": (I32, [P, I64, C.POINTER(PartSpec), P, P, I64, C.POINTER(I64), P, I64, P]),
+    "edg_psi_matrix": (I32, [P, I32, I64, P, P, I64, I64, P, I32, P, P]),
     "edg_zn_bitmap_words": (I64, [C.POINTER(ZnLattice)]),
     "edg_zn_mark": (I32, [C.POINTER(ZnLattice), P, P, P]),
     "edg_zn_fill": (I32, [C.POINTER(ZnLattice), P, P, P, P]),

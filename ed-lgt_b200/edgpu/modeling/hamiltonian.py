@@ -47,6 +47,25 @@ class QMB_state:
     def get_norm(self):
         return float(np.sqrt(np.real(np.vdot(self.psi, self.psi))))
 
+    def _psi_for(self, keep_indices, partitions_dict):
+        from ..entanglement import _record
+
+        return self.device(_record(keep_indices, partitions_dict)["subsys_map_dev"].device)
+
+    def reduced_density_matrix(self, keep_indices, partitions_dict) -> np.ndarray:
+        """QMB_state.reduced_density_matrix (edlgt/modeling/qmb_state.py:211-243)
+        for a partition made by ``QuantumModel._get_partition``."""
+        from ..entanglement import reduced_density_matrix
+
+        return reduced_density_matrix(self._psi_for(keep_indices, partitions_dict), keep_indices, partitions_dict)
+
+    def entanglement_entropy(self, keep_indices, partitions_dict) -> float:
+        """QMB_state.entanglement_entropy (edlgt/modeling/qmb_state.py:245-291),
+        in bits, from the exact spectrum of the reduced density matrix."""
+        from ..entanglement import entanglement_entropy
+
+        return entanglement_entropy(self._psi_for(keep_indices, partitions_dict), keep_indices, partitions_dict)
+
 
 class QMB_hamiltonian:
     def __init__(self, lvals, size, sector=None, phase_weights=None):

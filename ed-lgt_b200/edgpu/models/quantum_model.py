@@ -130,6 +130,7 @@ class QuantumModel:
         self.phase_weights = None
         self.res = {}
         self.H = None
+        self._partition_cache = {}
 
     # ------------------------------------------------------------- sector
     @property
@@ -281,6 +282,19 @@ class QuantumModel:
         elif not isinstance(psi, torch.Tensor):
             psi = torch.from_numpy(np.asarray(psi)).to(self.device)
         return site_expval_device(self.sector, op, psi).cpu().numpy()
+
+    def _get_partition(self, keep_indices):
+        """QuantumModel._get_partition (edlgt/models/quantum_model.py:715-791):
+        subsystem/environment maps and unique configurations, built on the
+        device (``edg_part_map``) and cached per sorted site tuple."""
+        from ..entanglement import get_partition
+
+        key = tuple(sorted(int(i) for i in keep_indices))
+        if key not in self._partition_cache:
+            if self.sector is None:
+                raise ValueError("_get_partition needs a symmetry sector")
+            self._partition_cache[key] = get_partition(self.sector, self.n_sites, key)
+        return self._partition_cache[key]
 
     def twobody_expval(self, op_a, op_b, psi) -> np.ndarray:
         """Correlator matrix Re <psi| A_i B_j |psi>, i != j (TwoBodyTerm.get_expval)."""

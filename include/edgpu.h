@@ -413,6 +413,44 @@ int edg_twobody_expval(const edg_lookup_table* sector, const uint64_t* strides,
                        double* scratch, int64_t scratch_elems, cudaStream_t stream);
 
 /* ------------------------------------------------------------------------
+ * Bipartitions.  Replaces QuantumModel._get_partition with
+ * _unique_configs_with_inverse (edlgt/models/quantum_model.py:715-791,
+ * 73-117) and build_psi_matrix (edlgt/modeling/qmb_state.py:596-627).  A part
+ * (subsystem or environment) is a list of sites in ascending order; its key
+ * packs their local states mixed radix, last part site fastest, so ascending
+ * part keys are np.unique's order of the part configurations.
+ * ------------------------------------------------------------------------ */
+#define EDG_PART_MAX_KEY_SPACE (1ull << 34)
+
+typedef struct {
+  int32_t n_part;                       /* sites in the part, 0..EDG_MAX_SITES  */
+  int32_t reserved;
+  uint64_t key_space;                   /* product of the part's local dims     */
+  uint64_t src_stride[EDG_MAX_SITES];   /* each part site's stride in the key   */
+  uint64_t dim[EDG_MAX_SITES];          /* its local dimension                  */
+  uint64_t part_stride[EDG_MAX_SITES];  /* its stride in the part key           */
+} edg_part_spec;
+
+/* Scratch elements (8-byte) edg_part_map needs; -1 when key_space is 0 or
+ * above EDG_PART_MAX_KEY_SPACE. */
+int64_t edg_part_scratch_elems(uint64_t key_space);
+/* index[r] = position of row r's part configuration among the distinct part
+ * configurations of the sector (ascending keys); *n_unique (host) = their
+ * number; unique_keys (nullable, device, unique_cap entries) = those keys.
+ * Synchronizes the stream (one count read). */
+int edg_part_map(const uint64_t* keys, int64_t n, const edg_part_spec* spec, int64_t* index,
+                 uint64_t* unique_keys, int64_t unique_cap, int64_t* n_unique, uint64_t* scratch,
+                 int64_t scratch_elems, cudaStream_t stream);
+/* out[sub_index[r] * env_dim + env_index[r]] = psi[r], zero elsewhere: the
+ * dense (sub_dim, env_dim) state matrix.  psi_dtype 0 f64, 1 f32,
+ * 2 complex128, 3 complex64; out_dtype 0 f64 (real states only) or
+ * 2 complex128.  err_flag: one device int32.  An index out of range returns
+ * EDG_ERR_ARG.  Synchronizes the stream (one flag read). */
+int edg_psi_matrix(const void* psi, int32_t psi_dtype, int64_t n, const int64_t* sub_index,
+                   const int64_t* env_index, int64_t sub_dim, int64_t env_dim, void* out,
+                   int32_t out_dtype, int32_t* err_flag, cudaStream_t stream);
+
+/* ------------------------------------------------------------------------
  * Matrix-free Z_n lattice gauge theory with staggered fermions (periodic
  * Lx x Ly, Gauss law, zero charge, optional zero momentum).
  *

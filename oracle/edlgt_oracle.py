@@ -303,3 +303,49 @@ def twobody_expval(psi, op_a, op_b, cfg, loc_dims):
             e = np.sum(np.conj(psi[rows[ok]]) * vals[ok] * psi[cols[ok]])
             corr[i, j] = corr[j, i] = float(np.real(e))
     return corr
+
+
+def partition(cfg, loc_dims, keep):
+    """QuantumModel._get_partition with _unique_configs_with_inverse
+    (edlgt/models/quantum_model.py:715-791, 73-117): distinct subsystem and
+    environment rows (np.unique on their packed keys) and each row's index."""
+    n = cfg.shape[1]
+    keep = sorted(int(i) for i in keep)
+    env = [i for i in range(n) if i not in keep]
+    out = {"subsys_indices": np.array(keep), "env_indices": np.array(env)}
+    for tag, cols in (("subsys", keep), ("env", env)):
+        sub = cfg[:, cols]
+        if len(cols) == 0:
+            uniq, inv = np.empty((1, 0), dtype=cfg.dtype), np.zeros(cfg.shape[0], dtype=np.int64)
+        else:
+            k = keys_of(sub, np.asarray(loc_dims)[cols])
+            _, first, inv = np.unique(k, return_index=True, return_inverse=True)
+            uniq = sub[first]
+        out[f"unique_{tag}_configs"] = uniq
+        out[f"{tag}_map"] = inv.reshape(-1).astype(np.int64)
+        out[f"{tag}_dim"] = uniq.shape[0]
+    return out
+
+
+def psi_matrix(psi, part):
+    """build_psi_matrix (edlgt/modeling/qmb_state.py:596-627)."""
+    m = np.zeros((part["subsys_dim"], part["env_dim"]), dtype=np.complex128)
+    m[part["subsys_map"], part["env_map"]] = psi
+    return m
+
+
+def reduced_density_matrix(psi, part):
+    """QMB_state.reduced_density_matrix, sector case (qmb_state.py:211-243)."""
+    m = psi_matrix(psi, part)
+    return m @ m.conj().T
+
+
+def entanglement_entropy(psi, part):
+    """QMB_state.entanglement_entropy with the dense SVD branch
+    (qmb_state.py:245-291): -sum l log2 l over squared singular values > 1e-10."""
+    m = psi_matrix(psi, part)
+    if min(m.shape) == 1:
+        return 0.0
+    lam = np.linalg.svd(m, compute_uv=False) ** 2
+    lam = lam[lam > 1e-10]
+    return float(-np.sum(lam * np.log2(lam)))

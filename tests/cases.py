@@ -52,3 +52,10 @@ TWOBODY_CASES = {
     "qed2d_3x2_bg": [["N", "N"], ["E2_px", "E2_py"]],
     "su2_1d_L8_obc": [["N_tot", "N_tot"], ["N_pair", "T2_px"]],
 }
+
+# entanglement fixtures: case name -> subsystems measured on the ground state
+ENTROPY_CASES = {
+    "qed1d_L8_obc": [[0, 1, 2, 3], [1, 2, 5], [0, 1]],
+    "qed2d_3x2_bg": [[0, 1, 2], [0, 3], [4]],
+    "su2_1d_L8_obc": [[0, 1, 2, 3], [2, 3, 6], [0, 1]],
+}

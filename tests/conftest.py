@@ -51,3 +51,10 @@ def golden_twobody():
     import numpy as np
 
     return np.load(os.path.join(GOLDEN, "twobody_cases.npz"))
+
+
+@pytest.fixture(scope="session")
+def golden_entropy():
+    import numpy as np
+
+    return np.load(os.path.join(GOLDEN, "entropy_cases.npz"))

@@ -5,7 +5,7 @@ Run in a container that has the reference checkout (EDLGT_PATH, default
 
     python tests/golden/make_golden.py [group ...]
 
-Groups: small, pins, dynamics, big, twobody.  Output: .npz files next to
+Groups: small, pins, dynamics, big, twobody, entropy.  Output: .npz files next to
 this script.  Nothing here is imported by the library or by the GPU tests;
 the tests only read the .npz files.
 
@@ -313,8 +313,43 @@ def gen_twobody():
     np.savez_compressed(os.path.join(HERE, "twobody_cases.npz"), **out)
 
 
+ENTROPY_CASES = {
+    # name: (factory, kwargs, g, m, [subsystems])
+    "qed1d_L8_obc": (qed_model, QED_CASES["qed1d_L8_obc"][0], 1.0, 1.0, [[0, 1, 2, 3], [1, 2, 5], [0, 1]]),
+    "qed2d_3x2_bg": (qed_model, QED_CASES["qed2d_3x2_bg"][0], 1.0, 1.0, [[0, 1, 2], [0, 3], [4]]),
+    "su2_1d_L8_obc": (su2_model, SU2_CASES["su2_1d_L8_obc"][0], 1.0, 0.5, [[0, 1, 2, 3], [2, 3, 6], [0, 1]]),
+}
+
+
+def gen_entropy():
+    """Bipartition maps (_get_partition), reduced density matrices and
+    entanglement entropies of the reference's ground state."""
+    out = {}
+    for name, (factory, kw, g, mass, parts) in ENTROPY_CASES.items():
+        model = factory(kw)
+        model.build_Hamiltonian(g, mass)
+        model.diagonalize_Hamiltonian(1, "sparse")
+        st = model.H.Npsi[0]
+        out[f"{name}/keys"] = keys_of(model.sector_configs, model.loc_dims)
+        out[f"{name}/loc_dims"] = np.asarray(model.loc_dims, dtype=np.int64)
+        out[f"{name}/psi"] = np.asarray(st.psi, dtype=np.complex128)
+        for keep in parts:
+            tag = f"{name}/" + "-".join(str(i) for i in keep)
+            part = model._get_partition(keep)
+            for k in ("subsys_map", "env_map", "unique_subsys_configs", "unique_env_configs"):
+                out[f"{tag}/{k}"] = np.asarray(part[k])
+            out[f"{tag}/dims"] = np.array([part["subsys_dim"], part["env_dim"]], dtype=np.int64)
+            out[f"{tag}/entropy"] = np.float64(st.entanglement_entropy(keep, model._partition_cache))
+            if part["subsys_dim"] <= 64:
+                out[f"{tag}/rdm"] = np.asarray(st.reduced_density_matrix(keep, model._partition_cache))
+        print(name, len(model.sector_configs), flush=True)
+    np.savez_compressed(os.path.join(HERE, "entropy_cases.npz"), **out)
+
+
 if __name__ == "__main__":
-    groups = sys.argv[1:] or ["small", "pins", "dynamics", "big", "twobody"]
+    groups = sys.argv[1:] or ["small", "pins", "dynamics", "big", "twobody", "entropy"]
+    if "entropy" in groups:
+        gen_entropy()
     if "twobody" in groups:
         gen_twobody()
     if "small" in groups:

@@ -5,7 +5,7 @@ the package feed both, so these tests also pin the host model layer."""
 import numpy as np
 import pytest
 
-from cases import ALL_CASES, TWOBODY_CASES, build
+from cases import ALL_CASES, ENTROPY_CASES, TWOBODY_CASES, build
 from oracle import edlgt_oracle as O
 
 
@@ -102,3 +102,23 @@ def test_twobody_oracle(name, golden_twobody):
         corr = O.twobody_expval(psi, model.ops[a], model.ops[b], cfg, loc)
         ref = golden_twobody[f"{name}/{a}_{b}"]
         assert np.max(np.abs(corr - ref)) <= 1e-12 * max(1.0, np.max(np.abs(ref))), (a, b)
+
+
+@pytest.mark.parametrize("name", sorted(ENTROPY_CASES))
+def test_partition_and_entropy_oracle(name, golden_entropy):
+    """Bipartition maps bit-exact, entropies and reduced density matrices of
+    the reference's ground state to 1e-12, recomputed by the oracle."""
+    model, _, _ = build(name)
+    loc = golden_entropy[f"{name}/loc_dims"]
+    cfg = O.sector_configs(**model.sector_inputs)
+    assert np.array_equal(O.keys_of(cfg, loc), golden_entropy[f"{name}/keys"])
+    psi = golden_entropy[f"{name}/psi"]
+    for keep in ENTROPY_CASES[name]:
+        tag = f"{name}/" + "-".join(str(i) for i in keep)
+        part = O.partition(cfg, loc, keep)
+        for k in ("subsys_map", "env_map", "unique_subsys_configs", "unique_env_configs"):
+            assert np.array_equal(part[k], golden_entropy[f"{tag}/{k}"]), (keep, k)
+        assert [part["subsys_dim"], part["env_dim"]] == list(golden_entropy[f"{tag}/dims"])
+        assert abs(O.entanglement_entropy(psi, part) - float(golden_entropy[f"{tag}/entropy"])) <= 1e-12
+        if f"{tag}/rdm" in golden_entropy:
+            assert np.max(np.abs(O.reduced_density_matrix(psi, part) - golden_entropy[f"{tag}/rdm"])) <= 1e-13
