@@ -209,6 +209,16 @@ class ZnBasis(C.Structure):
     _fields_ = [("n_rows", I64), ("keys", P), ("orbit", P)]
 
 
+class MomentumGroup(C.Structure):
+    _fields_ = [
+        ("lattice_dim", I32),
+        ("n_shifts", I32),
+        ("shifts_per_dir", I32 * 4),
+        ("shift_strides", I32 * 4),
+        ("k_vals", I32 * 4),
+    ]
+
+
 class PartSpec(C.Structure):
     _fields_ = [
         ("n_part", I32),
@@ -249,6 +259,14 @@ _SIGS = {
     "edg_krylov_step": (I32, [C.POINTER(KrylovProblem), P, F64, P, I64, P, P]),
     "edg_twobody_scratch_elems": (I64, [I32]),
     "edg_twobody_expval": (I32, [C.POINTER(LookupTable), P, P, I32, P, P, P, I32, P, P, I32, P, I32, I64, P, P, I64, P]),
+    "edg_momentum_translations": (I32, [C.POINTER(LookupTable), P, P, I32, P, I32, P, P, P]),
+    "edg_momentum_scratch_elems": (I64, [I64]),
+    "edg_momentum_references": (I32, [P, I64, C.POINTER(MomentumGroup), P, P, C.POINTER(I64), P, I64, P]),
+    "edg_momentum_columns": (I32, [P, P, I64, P, C.POINTER(MomentumGroup), P, I32, I32, P, C.POINTER(I64), P, P, P,
+                                   I64, P]),
+    "edg_momentum_rowmap": (I32, [P, P, P, I64, I64, P, P, P, P]),
+    "edg_momentum_expand": (I32, [I64, P, P, P, P, P]),
+    "edg_momentum_reduce": (I32, [I64, P, P, P, P, P, P]),
     "edg_part_scratch_elems": (I64, [U64]),
     "edg_part_map": (I32, [P, I64, C.POINTER(PartSpec), P, P, I64, C.POINTER(I64), P, I64, P]),
     "edg_psi_matrix": (I32, [P, I32, I64, P, P, I64, I64, P, I32, P, P]),

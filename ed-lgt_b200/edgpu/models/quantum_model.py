@@ -258,12 +258,46 @@ class QuantumModel:
         return (xs[:, None] * n) % 4
 
     # ---------------------------------------------------------- solve
+    def set_momentum_sector(self, k_unit_cell_size, k_vals, TC_symmetry=False):
+        """QuantumModel.set_momentum_sector (edlgt/models/quantum_model.py:213-276):
+        the projector B of the momentum sector k_vals (labels in units of
+        2 pi / R_d, R_d = L_d / unit cell d), built on the device.  The
+        Hamiltonian is then diagonalised as B^dagger H B."""
+        from ..momentum import MomentumBasis
+
+        if self.sector is None:
+            raise ValueError("symmetry sector_configs not defined yet")
+        if self.has_obc[0]:
+            raise ValueError("Momentum is not conserved with OBC.")
+        if TC_symmetry:
+            raise NotImplementedError("the translation-charge (TC) momentum basis is not built on the device")
+        k_vals = np.atleast_1d(np.asarray(k_vals, dtype=np.int32))
+        if k_vals.size != self.dim:
+            raise ValueError(f"expected k_vals shape {self.dim}, got {k_vals.shape}")
+        self._momentum = MomentumBasis(self.sector, self.lvals, k_unit_cell_size, k_vals)
+        self.momentum_basis = self._momentum.host_arrays()
+
     def diagonalize_Hamiltonian(self, n_eigs, format="gpu", print_results=False, precision="fp64", tol=1e-12):
-        self.H.diagonalize(n_eigs, format, self.loc_dims, print_results, tol=tol, precision=precision)
+        mom = getattr(self, "_momentum", None)
+        if mom is not None:
+            if self.H.mat is None:
+                self.H.build(format)
+            mom.bind(self.H)
+            k = mom.n_cols if (isinstance(n_eigs, str) and n_eigs == "full") else int(n_eigs)
+            evals, vecs = mom.lowest(k, tol=tol)
+            self.H.n_eigs = k
+            self.H.Nenergies = np.asarray(evals) / self.n_sites
+            self.H.Npsi = [QMB_state(vecs[:, i].contiguous(), self.lvals, self.loc_dims) for i in range(k)]
+            self.H.GSenergy = self.H.Nenergies[0]
+            self.H.GSpsi = self.H.Npsi[0]
+        else:
+            self.H.diagonalize(n_eigs, format, self.loc_dims, print_results, tol=tol, precision=precision)
         self.n_eigs = self.H.n_eigs
         self.res["energy"] = self.H.Nenergies
 
     def time_evolution_Hamiltonian(self, initial_state, time_line, **kwargs):
+        if getattr(self, "_momentum", None) is not None:
+            raise NotImplementedError("time evolution inside a momentum sector is not built on the device")
         self.H.time_evolution(initial_state, time_line, self.loc_dims, **kwargs)
 
     def get_qmb_state_from_configs(self, configs):

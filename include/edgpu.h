@@ -413,6 +413,59 @@ int edg_twobody_expval(const edg_lookup_table* sector, const uint64_t* strides,
                        double* scratch, int64_t scratch_elems, cudaStream_t stream);
 
 /* ------------------------------------------------------------------------
+ * Momentum basis.  Replaces build_all_translations, select_references and
+ * momentum_basis_zero_k / momentum_basis_finite_k
+ * (edlgt/symmetries/translational_sym.py:567-949, get_momentum_basis
+ * :1307-1358) and the momentum-projected term builders
+ * (nbody_data_momentum*, :1394-1969): the projector B is built on the device
+ * (CSC, rows ascending, complex128 values) and H_k = B^dagger H B is applied
+ * matrix-free around the sector matvec (expand, matvec, reduce).
+ * ------------------------------------------------------------------------ */
+typedef struct {
+  int32_t lattice_dim;        /* 1..3                                         */
+  int32_t n_shifts;           /* prod(shifts_per_dir) <= EDG_MAX_SITES        */
+  int32_t shifts_per_dir[4];  /* R_d = L_d / unit cell d                      */
+  int32_t shift_strides[4];   /* row-major strides over the shifts            */
+  int32_t k_vals[4];          /* momentum labels                              */
+} edg_momentum_group;
+
+/* trans[r * n_shifts + t] = row of configuration r translated by shift t;
+ * source_sites [n_shifts][n_sites] (device): the site whose local state lands
+ * on each destination site.  A translated configuration outside the sector
+ * returns EDG_ERR_MISSING_KET.  Synchronizes the stream (one flag read). */
+int edg_momentum_translations(const edg_lookup_table* sector, const uint64_t* strides,
+                              const int32_t* loc_dims, int32_t n_sites, const int32_t* source_sites,
+                              int32_t n_shifts, int32_t* trans, int32_t* err_flag, cudaStream_t stream);
+/* Scratch elements (int64) edg_momentum_references needs. */
+int64_t edg_momentum_scratch_elems(int64_t n_rows);
+/* refs[c] = reference row of column c (the smallest row of each orbit whose
+ * axis periods are compatible with k_vals, ascending); pvec [n_rows][dim] =
+ * axis periods of every row; *n_cols (host).  Synchronizes the stream. */
+int edg_momentum_references(const int32_t* trans, int64_t n_rows, const edg_momentum_group* g,
+                            int32_t* pvec, int64_t* refs, int64_t* n_cols, int64_t* scratch,
+                            int64_t scratch_elems, cudaStream_t stream);
+/* Columns of B.  phase_table [dim][max_r] complex128 = exp(-2 pi i k_d t / R_d)
+ * by repeated products.  With row_idx == NULL (count pass): col_ptr [n_cols+1]
+ * = offsets, *nnz (host) = total, stream synchronized; scratch:
+ * edg_scan_scratch_elems(n_cols).  Otherwise (fill pass): row_idx [nnz],
+ * data [nnz] complex128. */
+int edg_momentum_columns(const int32_t* trans, const int64_t* refs, int64_t n_cols, const int32_t* pvec,
+                         const edg_momentum_group* g, const double* phase_table, int32_t max_r,
+                         int32_t zero_k, int64_t* col_ptr, int64_t* nnz, int32_t* row_idx, double* data,
+                         int64_t* scratch, int64_t scratch_elems, cudaStream_t stream);
+/* row_col[r] = column holding row r (-1 if none), row_val[r] its complex128
+ * value.  A row in two columns returns EDG_ERR_ARG.  Synchronizes. */
+int edg_momentum_rowmap(const int64_t* col_ptr, const int32_t* row_idx, const double* data, int64_t n_cols,
+                        int64_t n_rows, int64_t* row_col, double* row_val, int32_t* err_flag,
+                        cudaStream_t stream);
+/* v = B x (complex128, v [n_rows], x [n_cols]). */
+int edg_momentum_expand(int64_t n_rows, const int64_t* row_col, const double* row_val, const double* x,
+                        double* v, cudaStream_t stream);
+/* y = B^dagger w (complex128, w [n_rows], y [n_cols]), fixed summation order. */
+int edg_momentum_reduce(int64_t n_cols, const int64_t* col_ptr, const int32_t* row_idx, const double* data,
+                        const double* w, double* y, cudaStream_t stream);
+
+/* ------------------------------------------------------------------------
  * Bipartitions.  Replaces QuantumModel._get_partition with
  * _unique_configs_with_inverse (edlgt/models/quantum_model.py:715-791,
  * 73-117) and build_psi_matrix (edlgt/modeling/qmb_state.py:596-627).  A part

@@ -349,3 +349,76 @@ def entanglement_entropy(psi, part):
     lam = np.linalg.svd(m, compute_uv=False) ** 2
     lam = lam[lam > 1e-10]
     return float(-np.sum(lam * np.log2(lam)))
+
+
+def translation_sources(lvals, unit_cell):
+    """source[s, dest]: the site whose state lands on ``dest`` under block
+    shift s (row-major shifts and sites, as _prepare_translation_source_sites,
+    edlgt/symmetries/translational_sym.py:508-560)."""
+    lvals = np.asarray(lvals, dtype=np.int64)
+    ucs = np.asarray(unit_cell, dtype=np.int64)
+    R = lvals // ucs
+    n_sites = int(np.prod(lvals))
+    coords = np.array(np.unravel_index(np.arange(n_sites), tuple(lvals))).T  # row-major
+    shifts = np.array(np.unravel_index(np.arange(int(np.prod(R))), tuple(R))).T
+    src = np.empty((len(shifts), n_sites), dtype=np.int64)
+    for s, t in enumerate(shifts):
+        dest = np.ravel_multi_index(tuple(((coords + t * ucs) % lvals).T), tuple(lvals))
+        src[s, dest] = np.arange(n_sites)
+    return src, R
+
+
+def momentum_basis(cfg, loc_dims, lvals, unit_cell, k_vals):
+    """get_momentum_basis (translational_sym.py:1307-1358) for the zero-k and
+    finite-k projectors (:697-949): (col_ptr, row_idx, data complex128, n_cols).
+    Translations (build_all_translations :567-617) by key search; one
+    reference per orbit, its smallest row; axis periods and the k filter of
+    select_references (:620-694); Bloch sums over the period box with
+    duplicates summed, finite-k entries with |a| <= 1e-14 dropped, columns
+    normalised, rows ascending."""
+    src, R = translation_sources(lvals, unit_cell)
+    keys = keys_of(cfg, loc_dims)
+    n, n_shifts, D = len(cfg), len(src), len(R)
+    trans = np.empty((n, n_shifts), dtype=np.int64)
+    for s in range(n_shifts):
+        tk = keys_of(cfg[:, src[s]], loc_dims)
+        pos = np.searchsorted(keys, tk)
+        ok = (pos < n) & (keys[np.minimum(pos, n - 1)] == tk)
+        if not np.all(ok):
+            raise ValueError("the sector is not closed under these translations")
+        trans[:, s] = pos
+    strides = np.ones(D, dtype=np.int64)
+    for d in range(D - 2, -1, -1):
+        strides[d] = strides[d + 1] * R[d + 1]
+    k_vals = np.asarray(k_vals, dtype=np.int64)
+    zero_k = not np.any(k_vals != 0)
+    phase = [np.exp(-2j * np.pi * (k_vals[d] % R[d]) * np.arange(R[d]) / R[d]) for d in range(D)]
+    cols = []
+    for r in range(n):
+        if trans[r].min() < r:
+            continue
+        p = np.empty(D, dtype=np.int64)
+        for d in range(D):
+            p[d] = next((q for q in range(1, R[d] + 1) if trans[r, (q % R[d]) * strides[d]] == r), R[d])
+        if any((k_vals[d] * p[d]) % R[d] != 0 for d in range(D)):
+            continue
+        acc = {}
+        for t in np.ndindex(*p):
+            row = int(trans[r, int(np.dot(t, strides))])
+            ph = 1.0 + 0j if zero_k else np.prod([phase[d][t[d]] for d in range(D)])
+            acc[row] = acc.get(row, 0) + ph
+        rows = np.array(sorted(acc), dtype=np.int64)
+        vals = np.array([acc[x] for x in rows], dtype=np.complex128)
+        if not zero_k:
+            keep = np.abs(vals) > 1e-14
+            rows, vals = rows[keep], vals[keep]
+        nrm = np.sqrt(np.sum(np.abs(vals) ** 2))
+        if len(vals) == 0 or nrm ** 2 <= (0 if zero_k else 1e-30):
+            cols.append((rows[:0], vals[:0]))
+        else:
+            cols.append((rows, vals / nrm))
+    col_ptr = np.zeros(len(cols) + 1, dtype=np.int64)
+    col_ptr[1:] = np.cumsum([len(c[0]) for c in cols])
+    row_idx = np.concatenate([c[0] for c in cols]) if cols else np.zeros(0, dtype=np.int64)
+    data = np.concatenate([c[1] for c in cols]) if cols else np.zeros(0, dtype=np.complex128)
+    return col_ptr, row_idx, data, len(cols)

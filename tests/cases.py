@@ -59,3 +59,22 @@ ENTROPY_CASES = {
     "qed2d_3x2_bg": [[0, 1, 2], [0, 3], [4]],
     "su2_1d_L8_obc": [[0, 1, 2, 3], [2, 3, 6], [0, 1]],
 }
+
+# momentum fixtures: name -> (model kwargs, g, m, unit cell, k vectors)
+MOMENTUM_CASES = {
+    "su2_1d_L6_pbc": (dict(spin=0.5, pure_theory=False, lvals=[6], has_obc=[False], sectors=[6]), 1.0, 5.0, [1],
+                      [[0], [1], [3]]),
+    "su2_1d_L8_pbc_uc2": (dict(spin=0.5, pure_theory=False, lvals=[8], has_obc=[False], sectors=[8]), 1.0, 0.5, [2],
+                          [[0], [1], [2]]),
+    "qed1d_L6_pbc_uc2": (dict(spin=1, pure_theory=False, lvals=[6], has_obc=[False]), 1.0, 1.0, [2], [[0], [1]]),
+    "qed2d_2x2_pure_pbc": (dict(spin=1, pure_theory=True, lvals=[2, 2], has_obc=[False, False]), 1.3, None, [1, 1],
+                           [[0, 0], [1, 0], [1, 1]]),
+}
+
+
+def build_momentum_case(name, device="cpu"):
+    from edgpu.models import QED_Model, SU2_Model
+
+    kw, g, m, ucs, ks = MOMENTUM_CASES[name]
+    cls = QED_Model if name.startswith("qed") else SU2_Model
+    return cls(**kw, device=device), g, m, ucs, ks

@@ -58,3 +58,10 @@ def golden_entropy():
     import numpy as np
 
     return np.load(os.path.join(GOLDEN, "entropy_cases.npz"))
+
+
+@pytest.fixture(scope="session")
+def golden_momentum():
+    import numpy as np
+
+    return np.load(os.path.join(GOLDEN, "momentum_cases.npz"))

@@ -5,7 +5,7 @@ Run in a container that has the reference checkout (EDLGT_PATH, default
 
     python tests/golden/make_golden.py [group ...]
 
-Groups: small, pins, dynamics, big, twobody, entropy.  Output: .npz files next to
+Groups: small, pins, dynamics, big, twobody, entropy, momentum.  Output: .npz files next to
 this script.  Nothing here is imported by the library or by the GPU tests;
 the tests only read the .npz files.
 
@@ -346,8 +346,48 @@ def gen_entropy():
     np.savez_compressed(os.path.join(HERE, "entropy_cases.npz"), **out)
 
 
+MOMENTUM_CASES = {
+    # name: (factory, kwargs, g, m, unit cell, [k vectors]); the SU(2) L=6 k=3 case is the
+    # reference's own finite-momentum validation case
+    "su2_1d_L6_pbc": (su2_model, SU2_CASES["su2_1d_L6_pbc"][0], 1.0, 5.0, [1], [[0], [1], [3]]),
+    "su2_1d_L8_pbc_uc2": (su2_model, dict(spin=0.5, pure_theory=False, lvals=[8], has_obc=[False], sectors=[8]), 1.0,
+                          0.5, [2], [[0], [1], [2]]),
+    "qed1d_L6_pbc_uc2": (qed_model, dict(spin=1, pure_theory=False, lvals=[6], has_obc=[False]), 1.0, 1.0, [2],
+                         [[0], [1]]),
+    "qed2d_2x2_pure_pbc": (qed_model, QED_CASES["qed2d_2x2_pure_pbc"][0], 1.3, None, [1, 1],
+                           [[0, 0], [1, 0], [1, 1]]),
+}
+
+
+def gen_momentum():
+    """Momentum projectors (set_momentum_sector / get_momentum_basis) and the
+    two lowest energies of the projected Hamiltonian, from the reference."""
+    out = {}
+    for name, (factory, kw, g, mass, ucs, ks) in MOMENTUM_CASES.items():
+        for k in ks:
+            tag = f"{name}/k" + "_".join(str(x) for x in k)
+            model = factory(kw)
+            model.set_momentum_sector(ucs, k)
+            model.default_params()
+            if mass is None:
+                model.build_Hamiltonian(g)
+            else:
+                model.build_Hamiltonian(g, mass)
+            mb = model.momentum_basis
+            model.diagonalize_Hamiltonian(2, "sparse")
+            out[f"{tag}/L_col_ptr"] = np.asarray(mb["L_col_ptr"], dtype=np.int64)
+            out[f"{tag}/L_row_idx"] = np.asarray(mb["L_row_idx"], dtype=np.int64)
+            out[f"{tag}/L_data"] = np.asarray(mb["L_data"], dtype=np.complex128)
+            out[f"{tag}/energies"] = np.asarray(model.H.Nenergies)
+            out[f"{name}/keys"] = keys_of(model.sector_configs, model.loc_dims)
+            print(tag, len(model.sector_configs), mb["n_cols"], model.H.Nenergies, flush=True)
+    np.savez_compressed(os.path.join(HERE, "momentum_cases.npz"), **out)
+
+
 if __name__ == "__main__":
-    groups = sys.argv[1:] or ["small", "pins", "dynamics", "big", "twobody", "entropy"]
+    groups = sys.argv[1:] or ["small", "pins", "dynamics", "big", "twobody", "entropy", "momentum"]
+    if "momentum" in groups:
+        gen_momentum()
     if "entropy" in groups:
         gen_entropy()
     if "twobody" in groups:

@@ -62,10 +62,10 @@ def test_struct_layouts_match_header():
 #include <stdio.h>
 #include "edgpu.h"
 int main(void) {
-  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(edg_sector_tables), sizeof(edg_lookup_table),
+  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(edg_sector_tables), sizeof(edg_lookup_table),
          sizeof(edg_assembly), sizeof(edg_lanczos_problem), sizeof(edg_site_dims), sizeof(edg_krylov_problem),
          sizeof(edg_small_batch), sizeof(edg_zn_translation), sizeof(edg_zn_lattice), sizeof(edg_zn_basis),
-         sizeof(edg_part_spec));
+         sizeof(edg_part_spec), sizeof(edg_momentum_group));
   return 0;
 }
 '''
@@ -82,4 +82,4 @@ int main(void) {
                      ctypes.sizeof(_lib.LanczosProblem), ctypes.sizeof(_lib.SiteDims),
                      ctypes.sizeof(_lib.KrylovProblem), ctypes.sizeof(_lib.SmallBatch),
                      ctypes.sizeof(_lib.ZnTranslation), ctypes.sizeof(_lib.ZnLattice), ctypes.sizeof(_lib.ZnBasis),
-                     ctypes.sizeof(_lib.PartSpec)]
+                     ctypes.sizeof(_lib.PartSpec), ctypes.sizeof(_lib.MomentumGroup)]

@@ -5,7 +5,7 @@ the package feed both, so these tests also pin the host model layer."""
 import numpy as np
 import pytest
 
-from cases import ALL_CASES, ENTROPY_CASES, TWOBODY_CASES, build
+from cases import ALL_CASES, ENTROPY_CASES, MOMENTUM_CASES, TWOBODY_CASES, build, build_momentum_case
 from oracle import edlgt_oracle as O
 
 
@@ -122,3 +122,25 @@ def test_partition_and_entropy_oracle(name, golden_entropy):
         assert abs(O.entanglement_entropy(psi, part) - float(golden_entropy[f"{tag}/entropy"])) <= 1e-12
         if f"{tag}/rdm" in golden_entropy:
             assert np.max(np.abs(O.reduced_density_matrix(psi, part) - golden_entropy[f"{tag}/rdm"])) <= 1e-13
+
+
+@pytest.mark.parametrize("name", sorted(MOMENTUM_CASES))
+def test_momentum_basis_oracle(name, golden_momentum):
+    """Momentum projectors B (CSC pattern exact, values to 1e-13) and the two
+    lowest energies of B^dagger H B against the reference's
+    set_momentum_sector / build_Hamiltonian / diagonalize_Hamiltonian."""
+    model, g, m, ucs, ks = build_momentum_case(name)
+    cfg = O.sector_configs(**model.sector_inputs)
+    assert np.array_equal(O.keys_of(cfg, model.loc_dims), golden_momentum[f"{name}/keys"])
+    H = O.assemble(model.hamiltonian_blocks(g, m), cfg, model.loc_dims).toarray()
+    for k in ks:
+        tag = f"{name}/k" + "_".join(str(x) for x in k)
+        cp, ri, data, n_cols = O.momentum_basis(cfg, model.loc_dims, model.lvals, ucs, k)
+        assert np.array_equal(cp, golden_momentum[f"{tag}/L_col_ptr"])
+        assert np.array_equal(ri, golden_momentum[f"{tag}/L_row_idx"])
+        assert np.max(np.abs(data - golden_momentum[f"{tag}/L_data"]), initial=0.0) <= 1e-13
+        B = np.zeros((len(cfg), n_cols), dtype=np.complex128)
+        for c in range(n_cols):
+            B[ri[cp[c]:cp[c + 1]], c] = data[cp[c]:cp[c + 1]]
+        e = np.linalg.eigvalsh(B.conj().T @ H @ B)[:2] / model.n_sites
+        assert np.allclose(e, golden_momentum[f"{tag}/energies"], atol=1e-10, rtol=0), (k, e)
