@@ -743,6 +743,7 @@ def run_momentum(args, world, rank, local):
     ms = max_over_ranks(a0.elapsed_time(b0) / args.steps, world, dev)
     e_k0 = float(model.H.Nenergies[0])
     m_cols = model._momentum.n_cols
+    matvecs = model._momentum.last_matvecs
     # the full-sector ground state beside it (B has orthonormal columns: E_k0 >= E_full)
     model._momentum = None
     model.diagonalize_Hamiltonian(1, tol=1e-10)
@@ -766,7 +767,9 @@ def run_momentum(args, world, rank, local):
             "oracle_check": {"n_cols_match": int(n_cols_cpu) == int(m_cols)},
             "cpu_baseline": {"value": 1.0 / cpu_s, "unit": "bases/s", "cores": 1, "kind": "port",
                              "sample": "oracle momentum projector (translations, references, Bloch sums) only"},
-            "gpu_launches": None,
+            # per step: basis 14 (translations, references + scan + list, column count + scan + fill,
+            # row map), solve 3 per projected matvec (expand, sector matvec, reduce)
+            "gpu_launches": 14 + 3 * int(matvecs),
             "clocks": clocks,
         }), flush=True)
 

@@ -210,8 +210,11 @@ class MomentumBasis:
             h = self.dense()
             h = 0.5 * (h + h.conj().T)
             w, v = torch.linalg.eigh(h)
+            self.last_matvecs = m
             return w[:k].cpu().numpy(), v[:, :k]
-        return _lanczos(self.matvec, m, k, tol, max_iter or min(m, 400), self.device, seed)
+        w, v, its = _lanczos(self.matvec, m, k, tol, max_iter or min(m, 400), self.device, seed)
+        self.last_matvecs = its
+        return w, v
 
 
 def _lanczos(apply, m, k, tol, max_iter, device, seed):
@@ -243,4 +246,4 @@ def _lanczos(apply, m, k, tol, max_iter, device, seed):
         Q[j + 1] = w / b
     n_used = len(alpha)
     vecs = Q[:n_used].T @ torch.from_numpy(s.astype(np.complex128)).to(device)
-    return theta, vecs
+    return theta, vecs, n_used
