@@ -110,8 +110,8 @@ class QMB_hamiltonian:
     def build(self, format="gpu", force_complex=False):
         if self.sector is None:
             raise ValueError("the device Hamiltonian needs a symmetry sector")
-        if format not in ("gpu", "sparse", "linear"):
-            raise ValueError(f"format must be 'gpu' (or the aliases 'sparse'/'linear'), got {format}")
+        if format not in ("gpu", "sparse", "linear", "dense"):
+            raise ValueError(f"format must be 'gpu' (or the aliases 'sparse'/'linear'), or 'dense', got {format}")
         ed = self.extra_diag
         self.mat = assemble_blocks(self.sector, self.blocks, phase_weights=self.phase_weights,
                                    force_complex=force_complex, extra_diag=ed if ed != 0 else None)
@@ -166,6 +166,9 @@ class QMB_hamiltonian:
             raise ValueError(f"n_eigs must be int or 'full', not {n_eigs}.")
         self.loc_dims = loc_dims
         self.n_eigs = k
+        if format == "dense" or (isinstance(n_eigs, str) and n_eigs == "full"):
+            self._diagonalize_dense(k, loc_dims, print_results)
+            return
         if k > 16:
             raise NotImplementedError("the device Lanczos returns at most 16 eigenpairs")
         if max_iter is None:
@@ -187,11 +190,140 @@ class QMB_hamiltonian:
         self.GSenergy = self.Nenergies[0]
         self.GSpsi = self.Npsi[0]
 
+    # ------------------------------------------------------ full spectrum
+    DENSE_MAX = 32768
+
+    def _diagonalize_dense(self, k, loc_dims, print_results):
+        """All eigenpairs of the dense sector matrix (array_eigh after
+        convert_hamiltonian("dense"), qmb_hamiltonian.py:227-258, 300-302):
+        the matrix is densified on the device (``edg_csr_to_dense``) and
+        diagonalised by the library Hermitian solver."""
+        import ctypes  # noqa: F401
+
+        from .._lib import check, lib, ptr, stream_handle
+
+        n = self.shape[0]
+        if n > self.DENSE_MAX:
+            raise ValueError(f"dense diagonalisation limited to {self.DENSE_MAX} states, the sector has {n}")
+        mat = self.mat
+        dt = torch.complex128 if mat.is_complex else torch.float64
+        dense = torch.empty((n, n), dtype=dt, device=self.sector.device)
+        flag = torch.empty(1, dtype=torch.int32, device=self.sector.device)
+        check(lib.edg_csr_to_dense(2 if mat.is_complex else 0, n, ptr(mat.rowptr), ptr(mat.cols) if mat.nnz else None,
+                                   ptr(mat.vals) if mat.nnz else None, ptr(mat.diag), ptr(dense), ptr(flag),
+                                   stream_handle()), "edg_csr_to_dense")
+        w, v = torch.linalg.eigh(dense)
+        del dense
+        ph = self._row_phase()
+        if ph is not None:
+            v = ph[:, None] * v.to(torch.complex128)
+        self._evecs = v
+        self._evals_total = w.cpu().numpy()
+        n_sites = int(np.prod(self.lvals))
+        if print_results:
+            for e in self._evals_total[:k]:
+                logger.info(f"{e:.10f}  {e / n_sites:.10f}")
+        # as the reference's dense branch: every energy density, the first k states
+        self.Nenergies = self._evals_total / n_sites
+        self.Npsi = [QMB_state(v[:, i], self.lvals, loc_dims) for i in range(k)]
+        self.GSenergy = self.Nenergies[0]
+        self.GSpsi = self.Npsi[0]
+        self.Ham_type = "dense"
+
+    def _full(self):
+        return getattr(self, "_evecs", None) is not None and self.n_eigs == self.shape[0]
+
+    def energy_of(self, state):
+        """<state| H |state> (total energy) for a vector in the original basis."""
+        x = state if isinstance(state, torch.Tensor) else torch.from_numpy(np.asarray(state, dtype=np.complex128))
+        x = self.from_original_basis(x.to(self.sector.device))
+        hx = self._apply(x)
+        return float(torch.vdot(x.to(torch.complex128), hx.to(torch.complex128)).real)
+
+    def _apply(self, x):
+        if self.mat.is_complex or not x.is_complex():
+            return self.mat.matvec(x)
+        return torch.complex(self.mat.matvec(x.real.contiguous()), self.mat.matvec(x.imag.contiguous()))
+
+    def partition_function(self, beta):
+        """QMB_hamiltonian.partition_function (qmb_hamiltonian.py:428-452), on
+        the stored energy densities of the full spectrum."""
+        if not self._full():
+            raise NotImplementedError("the partition function needs the full spectrum (diagonalize 'full')")
+        Z = float(np.sum(np.exp(-beta * self.Nenergies)))
+        if Z <= 0:
+            raise ValueError(f"Z must be positive, not {Z}.")
+        return Z
+
+    def free_energy(self, beta):
+        return -1 / beta * np.log(self.partition_function(beta))
+
+    def thermal_average(self, beta):
+        Z = self.partition_function(beta)
+        return float(self.Nenergies.dot(np.exp(-beta * self.Nenergies)) / Z)
+
+    def F_prime(self, beta):
+        Z = self.partition_function(beta)
+        exph2 = np.square(self.Nenergies).dot(np.exp(-beta * self.Nenergies)) / Z
+        return float(-exph2 - self.thermal_average(beta) ** 2)
+
+    def get_beta(self, state, threshold=1e-10, max_iter=1000):
+        """Newton solve of QMB_hamiltonian.get_beta (qmb_hamiltonian.py:510-564),
+        full-spectrum branch: thermal average of the energy densities against
+        the state's total energy <state|H|state>."""
+        if not self._full():
+            raise NotImplementedError("get_beta needs the full spectrum (diagonalize 'full')")
+        e_state = self.energy_of(state)
+        beta, accuracy, it = 1e-7, 1.0, 0
+        E = self.Nenergies
+        while accuracy > threshold and it < max_iter:
+            it += 1
+            wgt = np.exp(-beta * E)
+            Z = np.sum(wgt)
+            Em = E.dot(wgt) / Z
+            F = Em - e_state
+            Fp = -np.square(E).dot(wgt) / Z - Em ** 2
+            prev = beta
+            beta = beta - F / Fp
+            accuracy = abs(beta - prev)
+        if it >= max_iter:
+            logger.warning("Maximum iterations reached without convergence.")
+        return beta
+
+    def get_r_value(self):
+        """Adjacent-gap ratios of the full spectrum and their bulk mean
+        (qmb_hamiltonian.py:566-601)."""
+        if self.Ham_type != "dense" or not hasattr(self, "Nenergies"):
+            raise ValueError("The Hamiltonian has to be fully diagonalized.")
+        dE = np.diff(np.sort(self.Nenergies))
+        r = np.minimum(dE[:-1], dE[1:]) / np.maximum(dE[:-1], dE[1:])
+        lo, hi = int(0.1 * len(r)), int(0.9 * len(r))
+        self.r_value = float(np.mean(r[lo:hi]))
+        return r
+
     # ------------------------------------------------------- time evolution
+    def _exact_time_evolution(self, initial_state, time_line, loc_dims):
+        """exact_time_evolution (qmb_hamiltonian.py:791-835) on the device:
+        psi(t) = V exp(-i E t) V^dagger psi0, all times as one product."""
+        dev = self.sector.device
+        v = self._evecs.to(torch.complex128)
+        psi0 = initial_state if isinstance(initial_state, torch.Tensor) else torch.from_numpy(
+            np.asarray(initial_state, dtype=np.complex128))
+        psi0 = psi0.to(dev).to(torch.complex128)
+        c = v.conj().T @ psi0
+        e = torch.from_numpy(self._evals_total.astype(np.float64)).to(dev)
+        t = torch.from_numpy(np.asarray(time_line, dtype=np.float64)).to(dev)
+        coeff = torch.exp(-1j * e[:, None] * t[None, :]) * c[:, None]
+        states = v @ coeff
+        self.loc_dims = loc_dims
+        self.psi_time = [QMB_state(states[:, j], self.lvals, loc_dims) for j in range(len(time_line))]
+
     def time_evolution(self, initial_state, time_line, loc_dims=None, m_krylov=30, precision="c128",
                        observables=None, reorth_passes=1):
         from ..dynamics import krylov_evolve
 
+        if self.Ham_type == "dense" and self._full():
+            return self._exact_time_evolution(initial_state, time_line, loc_dims)
         if self.mat is None:
             self.build()
         self.loc_dims = loc_dims

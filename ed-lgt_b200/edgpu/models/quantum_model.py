@@ -317,6 +317,118 @@ class QuantumModel:
             psi = torch.from_numpy(np.asarray(psi)).to(self.device)
         return site_expval_device(self.sector, op, psi).cpu().numpy()
 
+    # ------------------------------------------------- full-spectrum ensembles
+    def measure_fidelity(self, state, index, dynamics=False, print_value=False):
+        """|<ref|state>|^2 with ref = Npsi[index] or psi_time[index]
+        (edlgt/models/quantum_model.py:864-898)."""
+        state = np.asarray(state)
+        if len(state) != self.H.shape[0]:
+            raise ValueError(f"len(state) must be {self.H.shape[0]} not {len(state)}")
+        ref = self.H.Npsi[index].psi if not dynamics else self.H.psi_time[index].psi
+        fid = float(np.abs(state.conj().dot(ref)) ** 2)
+        if print_value:
+            logger.info(f"FIDELITY: {fid}")
+        return fid
+
+    def compute_expH(self, beta):
+        """exp(-beta H) (dense, host) from the full spectrum."""
+        v, e = self._full_spectrum()
+        w = torch.exp(-beta * torch.from_numpy(e).to(v.device))
+        return ((v * w[None, :]) @ v.conj().T).cpu().numpy()
+
+    def get_thermal_beta(self, state, threshold):
+        return self.H.get_beta(state, threshold)
+
+    def _full_spectrum(self):
+        if not self.H._full():
+            raise ValueError(f"Need all H eigvals {self.H.shape[0]}, not only {getattr(self, 'n_eigs', None)}")
+        return self.H._evecs, self.H._evals_total
+
+    def _eig_site_obs(self, name):
+        """(n_eigs, n_sites) array of <E_i| op_s |E_i> for a diagonal local
+        operator, for all eigenstates at once: |V|^2 (rows x states)
+        contracted with the per-row site values."""
+        v, _ = self._full_spectrum()
+        op = self.ops[name]
+        diag = torch.from_numpy(np.real(np.array([np.diagonal(op[s]) for s in range(op.shape[0])]))
+                                .astype(np.float64)).to(v.device)
+        cfg = torch.from_numpy(self.sector_configs.astype(np.int64)).to(v.device)
+        site = torch.arange(self.n_sites, device=v.device)[None, :]
+        d_rows = diag[site, cfg]
+        p = (v.conj() * v).real if v.is_complex() else v * v
+        return (p.T @ d_rows).cpu().numpy()
+
+    def _site_value(self, name, site_vals, special_norms, staggered_avgs):
+        if special_norms.get(name) is not None:
+            return float(np.dot(site_vals, special_norms[name]) / self.n_sites)
+        if staggered_avgs.get(name) is not None:
+            self.res[name] = site_vals
+            return self.stag_avg(name, staggered_avgs[name])
+        return float(np.mean(site_vals))
+
+    def canonical_avg(self, local_obs, beta):
+        """Tr(O exp(-beta H)) / (Z n_sites), O = sum_s op_s
+        (edlgt/models/quantum_model.py:911-938), from the full spectrum."""
+        _, e = self._full_spectrum()
+        w = np.exp(-beta * (e - e.min()))
+        obs = self._eig_site_obs(local_obs).sum(axis=1)
+        return float(np.dot(w, obs) / (np.sum(w) * self.n_sites))
+
+    def microcanonical_avg(self, local_obs_list, state, special_norms=None, staggered_avgs=None):
+        """Shell average over eigenstates with |e_i - e_q| < delta_e
+        (edlgt/models/quantum_model.py:940-1045)."""
+        special_norms = special_norms or {}
+        staggered_avgs = staggered_avgs or {}
+        v, _ = self._full_spectrum()
+        Eq = self.H.energy_of(state)
+        x = self.H.from_original_basis(torch.from_numpy(np.asarray(state, dtype=np.complex128)).to(v.device))
+        hx = self.H._apply(x)
+        E2q = float(torch.vdot(hx.to(torch.complex128), hx.to(torch.complex128)).real)
+        delta_e = np.sqrt(E2q - Eq ** 2) / self.n_sites
+        e_q = Eq / self.n_sites
+        shell = np.nonzero(np.abs(self.H.Nenergies - e_q) < delta_e)[0]
+        if len(shell) == 0:
+            raise ValueError(f"ME shell empty: no eigstate |e_i-e_q|<delta_e={delta_e}.")
+        idx = torch.from_numpy(shell).to(v.device)
+        psi_thermal = (v[:, idx].to(torch.complex128).sum(dim=1) / np.sqrt(len(shell))).cpu().numpy()
+        me = {}
+        for name in local_obs_list:
+            vals = self._eig_site_obs(name)[shell]
+            me[f"ME_{name}"] = float(np.mean([self._site_value(name, row, special_norms, staggered_avgs)
+                                              for row in vals]))
+        return psi_thermal, me
+
+    def diagonal_avg(self, local_obs_list, state, special_norms=None, staggered_avgs=None, tol_deg=1e-10):
+        """Diagonal-ensemble averages with degenerate blocks
+        (edlgt/models/quantum_model.py:1047-1156)."""
+        special_norms = special_norms or {}
+        staggered_avgs = staggered_avgs or {}
+        v, _ = self._full_spectrum()
+        E = np.real_if_close(np.asarray(self.H.Nenergies))
+        block = np.zeros(len(E), dtype=np.int64)
+        for kk in range(1, len(E)):
+            block[kk] = block[kk - 1] + (0 if abs(E[kk] - E[kk - 1]) < tol_deg else 1)
+        n_blocks = int(block[-1]) + 1
+        st = torch.from_numpy(np.asarray(state, dtype=np.complex128)).to(v.device)
+        coeffs = v.to(torch.complex128).conj().T @ st
+        de = {f"DE_{name}": 0.0 for name in local_obs_list}
+        if np.all(np.bincount(block, minlength=n_blocks) <= 1):
+            prob = (coeffs.abs() ** 2).cpu().numpy()
+            for name in local_obs_list:
+                vals = self._eig_site_obs(name)
+                de[f"DE_{name}"] = float(sum(prob[i] * self._site_value(name, vals[i], special_norms, staggered_avgs)
+                                             for i in range(len(prob))))
+            return de
+        for b in range(n_blocks):
+            idx = torch.from_numpy(np.nonzero(block == b)[0]).to(v.device)
+            psi_b = v[:, idx].to(torch.complex128) @ coeffs[idx]
+            if float(torch.vdot(psi_b, psi_b).real) < 1e-14:
+                continue
+            for name in local_obs_list:
+                site_vals = self.local_expval(self.ops[name], psi_b)
+                de[f"DE_{name}"] += self._site_value(name, site_vals, special_norms, staggered_avgs)
+        return de
+
     def _get_partition(self, keep_indices):
         """QuantumModel._get_partition (edlgt/models/quantum_model.py:715-791):
         subsystem/environment maps and unique configurations, built on the

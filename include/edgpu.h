@@ -412,6 +412,15 @@ int edg_twobody_expval(const edg_lookup_table* sector, const uint64_t* strides,
                        const void* psi, int32_t psi_dtype, int64_t psi_stride, double* corr,
                        double* scratch, int64_t scratch_elems, cudaStream_t stream);
 
+/* Dense row-major (n, n) form of a canonical sector matrix (off-diagonal CSR
+ * plus its diagonal), for full diagonalisation: QMB_hamiltonian.
+ * convert_hamiltonian("dense") (edlgt/modeling/qmb_hamiltonian.py:227-258).
+ * dtype 0 f64 or 2 complex128 (interleaved); err_flag: one device int32.
+ * Synchronizes the stream (one flag read). */
+int edg_csr_to_dense(int32_t dtype, int64_t n, const int64_t* rowptr, const int32_t* cols,
+                     const void* vals, const void* diag, void* out, int32_t* err_flag,
+                     cudaStream_t stream);
+
 /* ------------------------------------------------------------------------
  * Momentum basis.  Replaces build_all_translations, select_references and
  * momentum_basis_zero_k / momentum_basis_finite_k

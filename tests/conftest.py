@@ -65,3 +65,10 @@ def golden_momentum():
     import numpy as np
 
     return np.load(os.path.join(GOLDEN, "momentum_cases.npz"))
+
+
+@pytest.fixture(scope="session")
+def golden_full():
+    import numpy as np
+
+    return np.load(os.path.join(GOLDEN, "full_spectrum_cases.npz"))

@@ -5,7 +5,7 @@ Run in a container that has the reference checkout (EDLGT_PATH, default
 
     python tests/golden/make_golden.py [group ...]
 
-Groups: small, pins, dynamics, big, twobody, entropy, momentum.  Output: .npz files next to
+Groups: small, pins, dynamics, big, twobody, entropy, momentum, full.  Output: .npz files next to
 this script.  Nothing here is imported by the library or by the GPU tests;
 the tests only read the .npz files.
 
@@ -384,8 +384,56 @@ def gen_momentum():
     np.savez_compressed(os.path.join(HERE, "momentum_cases.npz"), **out)
 
 
+def gen_full():
+    """Full spectrum of SU(2) L=6 PBC (g=1, m=5, dim 282) through the
+    reference's dense path: energies, r value, thermal functions, thermal beta
+    and ensemble averages of the bare vacuum, exact time evolution."""
+    kw = SU2_CASES["su2_1d_L6_pbc"][0]
+    model = su2_model(kw)
+    model.build_Hamiltonian(1.0, 5.0)
+    model.diagonalize_Hamiltonian("full", "dense")
+    out = {"energies": np.asarray(model.H.Nenergies)}
+    out["r_array"] = np.asarray(model.H.get_r_value())
+    out["r_value"] = np.float64(model.H.r_value)
+    beta = 0.7
+    out["beta"] = np.float64(beta)
+    out["Z"] = np.float64(model.H.partition_function(beta))
+    out["F"] = np.float64(model.H.free_energy(beta))
+    out["E_thermal"] = np.float64(model.H.thermal_average(beta))
+    out["F_prime"] = np.float64(model.H.F_prime(beta))
+    config = model.overlap_QMB_state("V")
+    state = model.get_qmb_state_from_configs([config])
+    out["config"] = np.asarray(config, dtype=np.int64)
+    out["beta_state"] = np.float64(model.get_thermal_beta(state, 1e-10))
+    # canonical_avg itself hands the sector triplets of LocalTerm.get_Hamiltonian
+    # to csc_matrix, which scipy rejects; its formula is evaluated here with the
+    # reference's own pieces (compute_expH and the same triplets)
+    from edlgt.modeling import LocalTerm
+
+    rows, cols, vals = LocalTerm(model.ops["N_tot"], "N_tot", **model.def_params).get_Hamiltonian(1)
+    n = len(model.sector_configs)
+    op = coo_matrix((vals, (rows, cols)), shape=(n, n)).tocsc()
+    expm_matrix = model.compute_expH(beta)
+    Z = np.real(expm_matrix.trace())
+    out["canonical_N_tot"] = np.float64(np.real(op.dot(expm_matrix).trace()) / (Z * model.n_sites))
+    psi_th, me = model.microcanonical_avg(["N_tot", "T2_px"], state)
+    out["ME_psi"] = np.asarray(psi_th)
+    out["ME_N_tot"], out["ME_T2_px"] = np.float64(me["ME_N_tot"]), np.float64(me["ME_T2_px"])
+    de = model.diagonal_avg(["N_tot", "T2_px"], state)
+    out["DE_N_tot"], out["DE_T2_px"] = np.float64(de["DE_N_tot"]), np.float64(de["DE_T2_px"])
+    tline = np.array([0.0, 0.25, 0.5, 1.0, 2.0])
+    model.time_evolution_Hamiltonian(state, tline)
+    out["time"] = tline
+    out["psi_time"] = np.array([p.psi for p in model.H.psi_time])
+    out["keys"] = keys_of(model.sector_configs, model.loc_dims)
+    print("full", len(model.sector_configs), out["r_value"], out["beta_state"], me, de, flush=True)
+    np.savez_compressed(os.path.join(HERE, "full_spectrum_cases.npz"), **out)
+
+
 if __name__ == "__main__":
-    groups = sys.argv[1:] or ["small", "pins", "dynamics", "big", "twobody", "entropy", "momentum"]
+    groups = sys.argv[1:] or ["small", "pins", "dynamics", "big", "twobody", "entropy", "momentum", "full"]
+    if "full" in groups:
+        gen_full()
     if "momentum" in groups:
         gen_momentum()
     if "entropy" in groups:

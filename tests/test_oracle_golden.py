@@ -144,3 +144,42 @@ def test_momentum_basis_oracle(name, golden_momentum):
             B[ri[cp[c]:cp[c + 1]], c] = data[cp[c]:cp[c + 1]]
         e = np.linalg.eigvalsh(B.conj().T @ H @ B)[:2] / model.n_sites
         assert np.allclose(e, golden_momentum[f"{tag}/energies"], atol=1e-10, rtol=0), (k, e)
+
+
+def test_full_spectrum_oracle(golden_full):
+    """SU(2) L=6 PBC full spectrum and its thermal and ensemble quantities,
+    restated with numpy on the oracle's matrix, against the reference."""
+    g = golden_full
+    model, _, _ = build("su2_1d_L6_pbc")
+    cfg = O.sector_configs(**model.sector_inputs)
+    assert np.array_equal(O.keys_of(cfg, model.loc_dims), g["keys"])
+    H = O.assemble(model.hamiltonian_blocks(1.0, 5.0), cfg, model.loc_dims).toarray()
+    w, V = np.linalg.eigh(H)
+    n = model.n_sites
+    E = w / n
+    assert np.allclose(E, g["energies"], atol=1e-10, rtol=0)
+    beta = float(g["beta"])
+    Z = np.sum(np.exp(-beta * E))
+    assert np.isclose(Z, g["Z"], rtol=1e-10)
+    assert np.isclose(-np.log(Z) / beta, g["F"], rtol=1e-10)
+    assert np.isclose(E.dot(np.exp(-beta * E)) / Z, g["E_thermal"], rtol=1e-10)
+    idx = np.searchsorted(O.keys_of(cfg, model.loc_dims), O.keys_of(g["config"][None, :], model.loc_dims))
+    state = np.zeros(len(cfg), dtype=np.complex128)
+    state[idx] = 1.0
+    d_rows = lambda name: np.real(np.array([np.diagonal(model.ops[name][s]) for s in range(n)]))[  # noqa: E731
+        np.arange(n)[None, :], cfg.astype(np.int64)]
+    eig_obs = lambda name: (np.abs(V) ** 2).T @ d_rows(name)  # noqa: E731
+    wt = np.exp(-beta * (w - w.min()))
+    assert np.isclose(wt.dot(eig_obs("N_tot").sum(axis=1)) / (wt.sum() * n), g["canonical_N_tot"], rtol=1e-10)
+    c = V.conj().T @ state
+    block = np.concatenate([[0], np.cumsum(np.abs(np.diff(E)) >= 1e-10)])
+    for name in ("N_tot", "T2_px"):
+        de = 0.0
+        for b in range(block[-1] + 1):
+            psi_b = V[:, block == b] @ c[block == b]
+            if np.vdot(psi_b, psi_b).real >= 1e-14:
+                de += np.mean(np.abs(psi_b) ** 2 @ d_rows(name))
+        assert np.isclose(de, g[f"DE_{name}"], atol=1e-10), name
+    for j, t in enumerate(g["time"]):
+        psi_t = V @ (np.exp(-1j * w * t) * c)
+        assert np.max(np.abs(psi_t - g["psi_time"][j])) <= 1e-10
