@@ -22,7 +22,7 @@ import torch
 from .. import _lib
 from .._lib import check, lib, ptr, stream_handle
 from ..lattice import lattice_labels, link_site_pairs, neighbor_sites, staggered_mask, zig_zag
-from ..modeling import LocalTerm, PlaquetteTerm, QMB_hamiltonian, QMB_state, TwoBodyTerm
+from ..modeling import LocalTerm, NBodyTerm, PlaquetteTerm, QMB_hamiltonian, QMB_state, TwoBodyTerm
 from ..modeling.assembly import assemble_blocks
 from ..operators.common import project
 from ..symmetries import SectorSpec, enumerate_sector, get_symmetry_sector_generators
@@ -456,6 +456,10 @@ class QuantumModel:
         self.twobody_obs = [list(x) for x in twobody_obs]
         self.twobody_axes = twobody_axes
         self.plaquette_obs = [list(x) for x in plaquette_obs]
+        self.nbody_obs = [list(x) for x in nbody_obs]
+        self.nbody_dist = [[tuple(d) for d in dl] for dl in nbody_dist]
+        if len(self.nbody_dist) != len(self.nbody_obs):
+            raise ValueError("nbody_dist needs one list of distances per n-body observable")
         self.obs_list = {}
         self._plaq_mats = {}
         for names in self.plaquette_obs:
@@ -475,6 +479,33 @@ class QuantumModel:
         for names in self.plaquette_obs:
             key = "_".join(names)
             self.res[key] = self.plaquette_avg(names, st)
+        for names, dist in zip(self.nbody_obs, self.nbody_dist):
+            self.res["_".join(names)] = self.nbody_expval(names, dist, st)
+
+    def nbody_expval(self, names, distances, st, component="real"):
+        """NBodyTerm.get_expval (edlgt/modeling/nbody_term.py:164-257): for every
+        starting site whose pattern stays on the lattice, <psi| prod_j op_j |psi>
+        (real or imaginary part), each instance assembled once on the device."""
+        cache = self.__dict__.setdefault("_nb_mats", {})
+        key = (tuple(names), tuple(tuple(d) for d in distances))
+        if key not in cache:
+            term = NBodyTerm([self.ops[o] for o in names], list(names), [list(d) for d in distances],
+                             **self.def_params)
+            mats = []
+            for inst in term.get_Hamiltonian(1.0).sites:
+                blk = term.get_Hamiltonian(1.0)
+                blk.sites = np.array([inst])
+                mats.append(assemble_blocks(self.sector, [blk], phase_weights=self.phase_weights, force_complex=True))
+            cache[key] = mats
+        psi = st.device(self.device) if isinstance(st, QMB_state) else st
+        if not isinstance(psi, torch.Tensor):
+            psi = torch.from_numpy(np.asarray(psi)).to(self.device)
+        psi_c = psi.to(torch.complex128)
+        vals = []
+        for m in cache[key]:
+            z = torch.vdot(psi_c, m.matvec(psi_c)).item()
+            vals.append(z.real if component == "real" else z.imag)
+        return np.array(vals)
 
     def plaquette_avg(self, names, st, component="real"):
         """Average over plaquettes of <Re P> (PlaquetteTerm.get_expval)."""

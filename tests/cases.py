@@ -78,3 +78,34 @@ def build_momentum_case(name, device="cpu"):
     kw, g, m, ucs, ks = MOMENTUM_CASES[name]
     cls = QED_Model if name.startswith("qed") else SU2_Model
     return cls(**kw, device=device), g, m, ucs, ks
+
+# n-body correlator fixtures: name -> ([operator lists], [distance lists])
+NBODY_CASES = {
+    "su2_1d_L8_obc": ([["N_tot", "N_tot", "N_tot"], ["N_pair", "T2_px"]], [[[1], [2]], [[3]]]),
+    "qed1d_L8_obc": ([["Q_px_dag", "Q_mx"], ["N", "E2_px", "N"]], [[[1]], [[1], [2]]]),
+    "qed2d_3x2_bg": ([["N", "N"]], [[[1, 1]]]),
+}
+
+
+def nbody_instances(lvals, has_obc, distances):
+    """Site lists of an n-body pattern from every starting site (PBC wraps, a
+    pattern leaving an open lattice is dropped), zig-zag site order."""
+    from edgpu.lattice import inverse_zig_zag, zig_zag
+
+    n = 1
+    for L in lvals:
+        n *= L
+    out = []
+    for ii in range(n):
+        c0 = zig_zag(lvals, ii)
+        sites = [ii]
+        for d in distances:
+            c = [c0[k] + d[k] for k in range(len(lvals))]
+            c = [c[k] % lvals[k] if not has_obc[k] else c[k] for k in range(len(lvals))]
+            if not all(0 <= c[k] < lvals[k] for k in range(len(lvals))):
+                sites = None
+                break
+            sites.append(inverse_zig_zag(lvals, tuple(c)))
+        if sites is not None:
+            out.append(sites)
+    return out

@@ -72,3 +72,10 @@ def golden_full():
     import numpy as np
 
     return np.load(os.path.join(GOLDEN, "full_spectrum_cases.npz"))
+
+
+@pytest.fixture(scope="session")
+def golden_nbody():
+    import numpy as np
+
+    return np.load(os.path.join(GOLDEN, "nbody_cases.npz"))

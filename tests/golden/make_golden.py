@@ -5,7 +5,8 @@ Run in a container that has the reference checkout (EDLGT_PATH, default
 
     python tests/golden/make_golden.py [group ...]
 
-Groups: small, pins, dynamics, big, twobody, entropy, momentum, full.  Output: .npz files next to
+Groups: small, pins, dynamics, big, twobody, entropy, momentum, full,
+nbody.  Output: .npz files next to
 this script.  Nothing here is imported by the library or by the GPU tests;
 the tests only read the .npz files.
 
@@ -384,6 +385,34 @@ def gen_momentum():
     np.savez_compressed(os.path.join(HERE, "momentum_cases.npz"), **out)
 
 
+NBODY_CASES = {
+    # name: (factory, kwargs, g, m, [operator lists], [distance lists])
+    "su2_1d_L8_obc": (su2_model, SU2_CASES["su2_1d_L8_obc"][0], 1.0, 0.5,
+                      [["N_tot", "N_tot", "N_tot"], ["N_pair", "T2_px"]], [[[1], [2]], [[3]]]),
+    "qed1d_L8_obc": (qed_model, QED_CASES["qed1d_L8_obc"][0], 1.0, 1.0, [["Q_px_dag", "Q_mx"], ["N", "E2_px", "N"]],
+                     [[[1]], [[1], [2]]]),
+    "qed2d_3x2_bg": (qed_model, QED_CASES["qed2d_3x2_bg"][0], 1.0, 1.0, [["N", "N"]], [[[1, 1]]]),
+}
+
+
+def gen_nbody():
+    """N-body correlators (NBodyTerm.get_expval through get_observables /
+    measure_observables) of the reference's ground state."""
+    out = {}
+    for name, (factory, kw, g, mass, ops, dists) in NBODY_CASES.items():
+        model = factory(kw)
+        model.build_Hamiltonian(g, mass)
+        model.diagonalize_Hamiltonian(1, "sparse")
+        model.get_observables([], [], [], nbody_obs=ops, nbody_dist=dists)
+        model.measure_observables(0)
+        out[f"{name}/psi"] = np.asarray(model.H.Npsi[0].psi, dtype=np.complex128)
+        out[f"{name}/keys"] = keys_of(model.sector_configs, model.loc_dims)
+        for names in ops:
+            out[f"{name}/{'_'.join(names)}"] = np.asarray(model.res["_".join(names)], dtype=np.float64)
+        print(name, {"_".join(n): model.res["_".join(n)] for n in ops}, flush=True)
+    np.savez_compressed(os.path.join(HERE, "nbody_cases.npz"), **out)
+
+
 def gen_full():
     """Full spectrum of SU(2) L=6 PBC (g=1, m=5, dim 282) through the
     reference's dense path: energies, r value, thermal functions, thermal beta
@@ -431,7 +460,9 @@ def gen_full():
 
 
 if __name__ == "__main__":
-    groups = sys.argv[1:] or ["small", "pins", "dynamics", "big", "twobody", "entropy", "momentum", "full"]
+    groups = sys.argv[1:] or ["small", "pins", "dynamics", "big", "twobody", "entropy", "momentum", "full", "nbody"]
+    if "nbody" in groups:
+        gen_nbody()
     if "full" in groups:
         gen_full()
     if "momentum" in groups:

@@ -5,7 +5,8 @@ the package feed both, so these tests also pin the host model layer."""
 import numpy as np
 import pytest
 
-from cases import ALL_CASES, ENTROPY_CASES, MOMENTUM_CASES, TWOBODY_CASES, build, build_momentum_case
+from cases import (ALL_CASES, ENTROPY_CASES, MOMENTUM_CASES, NBODY_CASES, TWOBODY_CASES, build, build_momentum_case,
+                   nbody_instances)
 from oracle import edlgt_oracle as O
 
 
@@ -183,3 +184,20 @@ def test_full_spectrum_oracle(golden_full):
     for j, t in enumerate(g["time"]):
         psi_t = V @ (np.exp(-1j * w * t) * c)
         assert np.max(np.abs(psi_t - g["psi_time"][j])) <= 1e-10
+
+
+@pytest.mark.parametrize("name", sorted(NBODY_CASES))
+def test_nbody_oracle(name, golden_nbody):
+    """NBodyTerm.get_expval of the reference's ground state, recomputed from
+    the oracle's n-site triplets (real part, 1e-12)."""
+    model, _, _ = build(name)
+    cfg = O.sector_configs(**model.sector_inputs)
+    assert np.array_equal(O.keys_of(cfg, model.loc_dims), golden_nbody[f"{name}/keys"])
+    psi = golden_nbody[f"{name}/psi"]
+    for names, dist in zip(*NBODY_CASES[name]):
+        vals = []
+        for sites in nbody_instances(model.lvals, model.has_obc, dist):
+            rows, cols, v = O.nbody_triplets([model.ops[o] for o in names], sites, cfg, model.loc_dims)
+            vals.append(np.real(np.sum(np.conj(psi[rows]) * v * psi[cols])))
+        ref = golden_nbody[f"{name}/{'_'.join(names)}"]
+        assert len(vals) == len(ref) and np.max(np.abs(np.array(vals) - ref)) <= 1e-12, names
