@@ -296,8 +296,21 @@ class QuantumModel:
         self.res["energy"] = self.H.Nenergies
 
     def time_evolution_Hamiltonian(self, initial_state, time_line, **kwargs):
-        if getattr(self, "_momentum", None) is not None:
-            raise NotImplementedError("time evolution inside a momentum sector is not built on the device")
+        mom = getattr(self, "_momentum", None)
+        if mom is not None:
+            from ..momentum import krylov_evolve
+
+            if self.H.mat is None:
+                self.H.build()
+            mom.bind(self.H)
+            psi0 = initial_state if isinstance(initial_state, torch.Tensor) else torch.from_numpy(
+                np.asarray(initial_state, dtype=np.complex128))
+            if psi0.shape[0] != mom.n_cols:
+                raise ValueError(f"the initial state must live in the momentum sector ({mom.n_cols} states)")
+            states = krylov_evolve(mom.matvec, psi0.to(self.device), np.asarray(time_line, dtype=np.float64),
+                                   m_krylov=kwargs.get("m_krylov", 40), tol=kwargs.get("tol", 1e-12))
+            self.H.psi_time = [QMB_state(x, self.lvals, self.loc_dims) for x in states]
+            return
         self.H.time_evolution(initial_state, time_line, self.loc_dims, **kwargs)
 
     def get_qmb_state_from_configs(self, configs):

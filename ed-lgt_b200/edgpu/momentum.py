@@ -23,7 +23,7 @@ import torch
 from . import _lib
 from ._lib import check, lib, ptr, stream_handle
 
-__all__ = ["MomentumBasis", "translation_sources", "DENSE_MAX"]
+__all__ = ["MomentumBasis", "translation_sources", "krylov_evolve", "DENSE_MAX"]
 
 DENSE_MAX = 4096
 
@@ -215,6 +215,61 @@ class MomentumBasis:
         w, v, its = _lanczos(self.matvec, m, k, tol, max_iter or min(m, 400), self.device, seed)
         self.last_matvecs = its
         return w, v
+
+
+def krylov_evolve(apply, psi0, time_line, m_krylov=40, tol=1e-12):
+    """psi(t) = exp(-i H t) psi0 at every (absolute) time of ``time_line``, the
+    role of expm_multiply in QMB_hamiltonian.time_evolution
+    (edlgt/modeling/qmb_hamiltonian.py:370-384): each interval is covered by
+    Lanczos-exponential steps whose size halves until the a-posteriori error
+    estimate beta_m |[exp(-i T dt)]_{m-1,0}| is at most ``tol``."""
+    from scipy.linalg import expm
+
+    time_line = np.asarray(time_line, dtype=np.float64)
+    if len(time_line) == 0 or time_line[0] < 0 or np.any(np.diff(time_line) < 0):
+        raise ValueError("time_line must be ascending and start at t >= 0")
+    psi = psi0.to(torch.complex128).clone()
+    n = psi.shape[0]
+    m_k = max(1, min(m_krylov, n))
+    out = []
+    t_prev = 0.0  # expm_multiply returns exp(-i H t) psi0 at the absolute times
+    dt_try = None
+    for t in time_line:
+        remaining = float(t) - t_prev
+        while remaining > 0:
+            nrm = float(torch.linalg.vector_norm(psi))
+            if nrm == 0.0:
+                break
+            V = torch.empty((m_k + 1, n), dtype=torch.complex128, device=psi.device)
+            V[0] = psi / nrm
+            a, b = [], []
+            j_used = m_k
+            for j in range(m_k):
+                w = apply(V[j])
+                a.append(float(torch.vdot(V[j], w).real))
+                for _ in range(2):
+                    w = w - V[: j + 1].T @ (V[: j + 1].conj() @ w)
+                bj = float(torch.linalg.vector_norm(w))
+                b.append(bj)
+                if bj <= 1e-14 * max(1.0, abs(a[-1])):
+                    j_used = j + 1
+                    break
+                V[j + 1] = w / bj
+            T = np.diag(a[:j_used]) + np.diag(b[: j_used - 1], 1) + np.diag(b[: j_used - 1], -1)
+            dt = remaining if dt_try is None else min(remaining, dt_try)
+            while True:
+                E = expm(-1j * dt * T)
+                err = (b[j_used - 1] if j_used == m_k else 0.0) * abs(E[j_used - 1, 0]) * nrm
+                if err <= tol or dt < 1e-12:
+                    break
+                dt *= 0.5
+            coef = torch.from_numpy(np.ascontiguousarray(E[:, 0] * nrm)).to(psi.device)
+            psi = V[:j_used].T @ coef
+            remaining -= dt
+            dt_try = 2 * dt
+        t_prev = float(t)
+        out.append(psi.clone())
+    return out
 
 
 def _lanczos(apply, m, k, tol, max_iter, device, seed):

@@ -111,3 +111,29 @@ def test_sector_not_closed_under_translation_is_an_error(dev):
     obc.has_obc = [True]
     with pytest.raises(ValueError):
         obc.set_momentum_sector([1], [0])
+
+
+def test_time_evolution_in_momentum_sector(dev):
+    """Krylov evolution with the projected matvec against the dense
+    exp(-i H_k t) of the oracle's B^dagger H B (1e-9), at absolute times."""
+    import torch
+    from scipy.linalg import expm
+
+    model, g, m, ucs, _ = build_momentum_case("su2_1d_L6_pbc", device=dev)
+    model.build_Hamiltonian(g, m)
+    cfg = model.sector_configs
+    H = O.assemble(model.hamiltonian_blocks(g, m), cfg, model.loc_dims).toarray()
+    model.set_momentum_sector(ucs, [1])
+    cp, ri, data, n_cols = O.momentum_basis(cfg, model.loc_dims, model.lvals, ucs, [1])
+    Bd = np.zeros((len(cfg), n_cols), dtype=np.complex128)
+    for c in range(n_cols):
+        Bd[ri[cp[c]:cp[c + 1]], c] = data[cp[c]:cp[c + 1]]
+    Hk = Bd.conj().T @ H @ Bd
+    rng = np.random.default_rng(9)
+    psi0 = rng.normal(size=n_cols) + 1j * rng.normal(size=n_cols)
+    psi0 /= np.linalg.norm(psi0)
+    times = np.array([0.0, 0.1, 0.5, 1.5])
+    model.time_evolution_Hamiltonian(torch.from_numpy(psi0).to(dev), times)
+    for j, t in enumerate(times):
+        ref = expm(-1j * t * Hk) @ psi0
+        assert np.max(np.abs(model.H.psi_time[j].psi - ref)) <= 1e-9, t
