@@ -25,8 +25,10 @@ constexpr int kMaxShifts = EDG_MAX_SITES;
 
 __global__ void translations_k(const edg_lookup_table sec, const uint64_t* __restrict__ strides,
                                const int32_t* __restrict__ loc_dims, int n_sites,
-                               const int32_t* __restrict__ source_sites, int n_shifts, int32_t* __restrict__ trans,
-                               int32_t* __restrict__ err) {
+                               const int32_t* __restrict__ source_sites, int n_shifts,
+                               const int32_t* __restrict__ local_map, int map_dim,
+                               const double* __restrict__ label_sign, double* __restrict__ row_sign,
+                               int32_t* __restrict__ trans, int32_t* __restrict__ err) {
   uint8_t dig[EDG_MAX_SITES];
   for (int64_t r = (int64_t)blockIdx.x * kThreads + threadIdx.x; r < sec.n; r += (int64_t)gridDim.x * kThreads) {
     uint64_t x = __ldg(sec.keys + r);
@@ -36,13 +38,21 @@ __global__ void translations_k(const edg_lookup_table sec, const uint64_t* __res
       dig[s] = (uint8_t)(x - q * d);
       x = q;
     }
+    if (row_sign != nullptr) {  // product of the local labels' signs
+      double sg = 1.0;
+      for (int s = 0; s < n_sites; ++s) sg *= dig[s] < map_dim ? __ldg(label_sign + dig[s]) : 1.0;
+      row_sign[r] = sg;
+    }
     for (int t = 0; t < n_shifts; ++t) {
       uint64_t key = 0;
       const int32_t* src = source_sites + (int64_t)t * n_sites;
       bool ok = true;
       for (int s = 0; s < n_sites; ++s) {
         const int from = __ldg(src + s);
-        const uint32_t c = dig[from];
+        uint32_t c = dig[from];
+        if (local_map != nullptr) {  // the local map applied once per unit shift
+          for (int k = 0; k < t; ++k) c = c < (uint32_t)map_dim ? (uint32_t)__ldg(local_map + c) : 0xFFFFu;
+        }
         ok = ok && c < (uint32_t)__ldg(loc_dims + s);  // a local state the destination site cannot hold
         key += (uint64_t)c * __ldg(strides + s);
       }
@@ -88,7 +98,7 @@ __global__ void list_refs_k(const int64_t* __restrict__ offsets, int64_t n, int6
 // Returns the entry count; vals are not yet normalised.
 __device__ int column_entries(const int32_t* __restrict__ row, const int32_t* __restrict__ p,
                               const edg_momentum_group& g, const double2* __restrict__ phase_table, int max_r,
-                              int zero_k, int32_t* rows, double2* vals) {
+                              int zero_k, double odd_sign, int32_t* rows, double2* vals) {
   int t_local[4] = {0, 0, 0, 0};
   int full = 0, len = 0;
   for (;;) {
@@ -99,6 +109,7 @@ __device__ int column_entries(const int32_t* __restrict__ row, const int32_t* __
         ph = make_double2(ph.x * f.x - ph.y * f.y, ph.x * f.y + ph.y * f.x);
       }
     }
+    if (full & 1) ph = make_double2(ph.x * odd_sign, ph.y * odd_sign);
     const int32_t rr = row[full];
     int u = 0;
     while (u < len && rows[u] != rr) ++u;
@@ -149,24 +160,28 @@ __device__ int column_entries(const int32_t* __restrict__ row, const int32_t* __
 
 __global__ void columns_k(const int32_t* __restrict__ trans, int n_shifts, const int64_t* __restrict__ refs,
                           int64_t n_cols, const int32_t* __restrict__ pvec, const edg_momentum_group g,
-                          const double2* __restrict__ phase_table, int max_r, int zero_k, int64_t* __restrict__ counts,
+                          const double2* __restrict__ phase_table, int max_r, int zero_k,
+                          const double* __restrict__ row_sign, int64_t* __restrict__ counts,
                           const int64_t* __restrict__ col_ptr, int32_t* __restrict__ row_idx,
                           double2* __restrict__ data) {
   int32_t rows[kMaxShifts];
   double2 vals[kMaxShifts];
   for (int64_t c = (int64_t)blockIdx.x * kThreads + threadIdx.x; c < n_cols; c += (int64_t)gridDim.x * kThreads) {
     const int64_t ref = refs[c];
+    const double odd_sign = row_sign != nullptr ? row_sign[ref] : 1.0;
     const int len = column_entries(trans + ref * n_shifts, pvec + ref * g.lattice_dim, g, phase_table, max_r, zero_k,
-                                   rows, vals);
+                                   odd_sign, rows, vals);
     double norm2 = 0.0;
     for (int u = 0; u < len; ++u) norm2 += vals[u].x * vals[u].x + vals[u].y * vals[u].y;
-    const bool empty = zero_k ? false : (norm2 <= 1e-30 || len == 0);
+    // zero k keeps every image (a sign-twisted orbit may still cancel: its
+    // column is then written as zeros); finite k drops cancelled images
+    const bool empty = zero_k ? norm2 <= 1e-8 : (norm2 <= 1e-30 || len == 0);
     if (counts != nullptr) {
       counts[c] = len;  // the count pass keeps what survived the pruning
       continue;
     }
-    if (empty) continue;
-    const double inv = 1.0 / sqrt(norm2);
+    if (empty && !zero_k) continue;
+    const double inv = empty ? 0.0 : 1.0 / sqrt(norm2);
     int64_t w = col_ptr[c];
     for (int u = 0; u < len; ++u, ++w) {
       row_idx[w] = rows[u];
@@ -243,18 +258,24 @@ int check_group(const edg_momentum_group* g) {
 
 extern "C" int edg_momentum_translations(const edg_lookup_table* sector, const uint64_t* strides,
                                          const int32_t* loc_dims, int32_t n_sites, const int32_t* source_sites,
-                                         int32_t n_shifts, int32_t* trans, int32_t* err_flag, cudaStream_t stream) {
+                                         int32_t n_shifts, const int32_t* local_map, int32_t map_dim,
+                                         const double* label_sign, double* row_sign, int32_t* trans,
+                                         int32_t* err_flag, cudaStream_t stream) {
   EDG_REQUIRE(sector != nullptr && strides != nullptr && loc_dims != nullptr && source_sites != nullptr &&
                   trans != nullptr && err_flag != nullptr,
               "edg_momentum_translations: null argument");
   EDG_REQUIRE(n_sites >= 1 && n_sites <= EDG_MAX_SITES && n_shifts >= 1 && n_shifts <= kMaxShifts,
               "edg_momentum_translations: bad sizes");
   EDG_REQUIRE(sector->n < (int64_t)INT32_MAX, "edg_momentum_translations: sector above 2^31 rows");
+  EDG_REQUIRE((local_map == nullptr && row_sign == nullptr) || (map_dim >= 1 && map_dim <= 256),
+              "edg_momentum_translations: map_dim must be 1..256");
+  EDG_REQUIRE((row_sign == nullptr) == (label_sign == nullptr), "edg_momentum_translations: label_sign and row_sign go together");
   cudaError_t e = cudaMemsetAsync(err_flag, 0, sizeof(int32_t), stream);
   if (e != cudaSuccess) return edg::cuda_status(e, "edg_momentum_translations: flag");
   if (sector->n == 0) return EDG_OK;
   translations_k<<<edg::grid_for(sector->n, kThreads), kThreads, 0, stream>>>(*sector, strides, loc_dims, n_sites,
-                                                                             source_sites, n_shifts, trans, err_flag);
+                                                                             source_sites, n_shifts, local_map, map_dim,
+                                                                             label_sign, row_sign, trans, err_flag);
   EDG_CHECK_LAUNCH("edg_momentum_translations");
   int32_t h = 0;
   e = cudaMemcpyAsync(&h, err_flag, sizeof(int32_t), cudaMemcpyDeviceToHost, stream);
@@ -298,8 +319,9 @@ extern "C" int edg_momentum_references(const int32_t* trans, int64_t n_rows, con
 
 extern "C" int edg_momentum_columns(const int32_t* trans, const int64_t* refs, int64_t n_cols, const int32_t* pvec,
                                     const edg_momentum_group* g, const double* phase_table, int32_t max_r,
-                                    int32_t zero_k, int64_t* col_ptr, int64_t* nnz, int32_t* row_idx, double* data,
-                                    int64_t* scratch, int64_t scratch_elems, cudaStream_t stream) {
+                                    int32_t zero_k, const double* row_sign, int64_t* col_ptr, int64_t* nnz,
+                                    int32_t* row_idx, double* data, int64_t* scratch, int64_t scratch_elems,
+                                    cudaStream_t stream) {
   if (check_group(g) != EDG_OK) return EDG_ERR_ARG;
   EDG_REQUIRE(col_ptr != nullptr && nnz != nullptr && scratch != nullptr && phase_table != nullptr && n_cols >= 0 &&
                   (n_cols == 0 || (trans != nullptr && refs != nullptr && pvec != nullptr)),
@@ -317,8 +339,8 @@ extern "C" int edg_momentum_columns(const int32_t* trans, const int64_t* refs, i
       return e == cudaSuccess ? EDG_OK : edg::cuda_status(e, "edg_momentum_columns");
     }
     columns_k<<<edg::grid_for(n_cols, kThreads), kThreads, 0, stream>>>(trans, g->n_shifts, refs, n_cols, pvec, *g, ph,
-                                                                        max_r, zero_k, col_ptr, nullptr, nullptr,
-                                                                        nullptr);
+                                                                        max_r, zero_k, row_sign, col_ptr, nullptr,
+                                                                        nullptr, nullptr);
     EDG_CHECK_LAUNCH("edg_momentum_columns: count");
     int st = edg_scan_i64(col_ptr, col_ptr, n_cols, scratch, stream);
     if (st != EDG_OK) return st;
@@ -329,8 +351,8 @@ extern "C" int edg_momentum_columns(const int32_t* trans, const int64_t* refs, i
   EDG_REQUIRE(data != nullptr, "edg_momentum_columns: data is null");
   if (n_cols == 0) return EDG_OK;
   columns_k<<<edg::grid_for(n_cols, kThreads), kThreads, 0, stream>>>(trans, g->n_shifts, refs, n_cols, pvec, *g, ph,
-                                                                      max_r, zero_k, nullptr, col_ptr, row_idx,
-                                                                      reinterpret_cast<double2*>(data));
+                                                                      max_r, zero_k, row_sign, nullptr, col_ptr,
+                                                                      row_idx, reinterpret_cast<double2*>(data));
   EDG_CHECK_LAUNCH("edg_momentum_columns: fill");
   return EDG_OK;
 }

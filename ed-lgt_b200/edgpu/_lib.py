@@ -260,11 +260,11 @@ _SIGS = {
     "edg_twobody_scratch_elems": (I64, [I32]),
     "edg_twobody_expval": (I32, [C.POINTER(LookupTable), P, P, I32, P, P, P, I32, P, P, I32, P, I32, I64, P, P, I64, P]),
     "edg_csr_to_dense": (I32, [I32, I64, P, P, P, P, P, P, P]),
-    "edg_momentum_translations": (I32, [C.POINTER(LookupTable), P, P, I32, P, I32, P, P, P]),
+    "edg_momentum_translations": (I32, [C.POINTER(LookupTable), P, P, I32, P, I32, P, I32, P, P, P, P, P]),
     "edg_momentum_scratch_elems": (I64, [I64]),
     "edg_momentum_references": (I32, [P, I64, C.POINTER(MomentumGroup), P, P, C.POINTER(I64), P, I64, P]),
-    "edg_momentum_columns": (I32, [P, P, I64, P, C.POINTER(MomentumGroup), P, I32, I32, P, C.POINTER(I64), P, P, P,
-                                   I64, P]),
+    "edg_momentum_columns": (I32, [P, P, I64, P, C.POINTER(MomentumGroup), P, I32, I32, P, P, C.POINTER(I64), P, P,
+                                   P, I64, P]),
     "edg_momentum_rowmap": (I32, [P, P, P, I64, I64, P, P, P, P]),
     "edg_momentum_expand": (I32, [I64, P, P, P, P, P]),
     "edg_momentum_reduce": (I32, [I64, P, P, P, P, P, P]),

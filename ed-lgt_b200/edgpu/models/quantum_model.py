@@ -269,12 +269,21 @@ class QuantumModel:
             raise ValueError("symmetry sector_configs not defined yet")
         if self.has_obc[0]:
             raise ValueError("Momentum is not conserved with OBC.")
-        if TC_symmetry:
-            raise NotImplementedError("the translation-charge (TC) momentum basis is not built on the device")
         k_vals = np.atleast_1d(np.asarray(k_vals, dtype=np.int32))
         if k_vals.size != self.dim:
             raise ValueError(f"expected k_vals shape {self.dim}, got {k_vals.shape}")
-        self._momentum = MomentumBasis(self.sector, self.lvals, k_unit_cell_size, k_vals)
+        tc = {}
+        if TC_symmetry:
+            # translation combined with the charge-conjugation map of the
+            # six-state SU(2) j=1/2 dressed site and its state signs, the
+            # fixed tables of momentum_basis_zero_k_TC / _finite_k_TC
+            # (edlgt/symmetries/translational_sym.py:995-997, 1161-1163)
+            if self.dim != 1 or np.any(np.asarray(self.loc_dims) != 6):
+                raise ValueError("the TC momentum basis is defined for 1D chains of six-state dressed sites")
+            tc = dict(local_map=np.array([4, 5, 2, 3, 0, 1], dtype=np.int32),
+                      label_sign=np.array([1.0, 1.0, 1.0, -1.0, 1.0, 1.0]))
+            k_unit_cell_size = [1]
+        self._momentum = MomentumBasis(self.sector, self.lvals, k_unit_cell_size, k_vals, **tc)
         self.momentum_basis = self._momentum.host_arrays()
 
     def diagonalize_Hamiltonian(self, n_eigs, format="gpu", print_results=False, precision="fp64", tol=1e-12):

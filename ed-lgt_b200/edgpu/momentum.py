@@ -67,12 +67,18 @@ def _phase_table(k_vals, R):
 class MomentumBasis:
     """The projector B of one momentum sector, on the device."""
 
-    def __init__(self, sector, lvals, unit_cell, k_vals):
+    def __init__(self, sector, lvals, unit_cell, k_vals, local_map=None, label_sign=None):
+        """``local_map`` / ``label_sign``: the translation-charge variant (1D,
+        unit cell 1): the local map applied with every unit shift and the
+        per-state signs whose product twists the odd shifts."""
         dev = sector.device
         self.sector = sector
         self.device = dev
         n = len(sector)
         src, R = translation_sources(lvals, unit_cell)
+        tc = local_map is not None
+        if tc and (len(R) != 1 or src.shape[0] != src.shape[1]):
+            raise ValueError("the translation-charge basis is defined on a 1D ring with a one-site unit cell")
         k_vals = np.asarray(k_vals, dtype=np.int64).reshape(-1)
         if len(k_vals) != len(R):
             raise ValueError(f"expected {len(R)} momentum labels, got {len(k_vals)}")
@@ -97,9 +103,18 @@ class MomentumBasis:
         loc = up(sector.loc_dims.astype(np.int32))
         flag = torch.zeros(1, dtype=torch.int32, device=dev)
         trans = torch.empty((max(n, 1), n_shifts), dtype=torch.int32, device=dev)
+        if tc:
+            cmap = up(np.asarray(local_map, dtype=np.int32))
+            lsign = up(np.asarray(label_sign, dtype=np.float64))
+            row_sign = torch.empty(max(n, 1), dtype=torch.float64, device=dev)
+            map_args = (ptr(cmap), int(cmap.shape[0]), ptr(lsign), ptr(row_sign))
+        else:
+            row_sign = None
+            map_args = (None, 0, None, None)
         check(lib.edg_momentum_translations(sector.lookup_table(), ptr(strides), ptr(loc), int(sector.n_sites),
-                                            ptr(src_d), n_shifts, ptr(trans), ptr(flag), stream_handle()),
+                                            ptr(src_d), n_shifts, *map_args, ptr(trans), ptr(flag), stream_handle()),
               "edg_momentum_translations")
+        rs = ptr(row_sign) if tc else None
         ns = lib.edg_momentum_scratch_elems(n)
         scratch = torch.empty(max(ns, 1), dtype=torch.int64, device=dev)
         pvec = torch.empty((max(n, 1), len(R)), dtype=torch.int32, device=dev)
@@ -116,14 +131,14 @@ class MomentumBasis:
         cscratch = torch.empty(max(cs, 1), dtype=torch.int64, device=dev)
         zk = 1 if self.zero_k else 0
         check(lib.edg_momentum_columns(ptr(trans), ptr(refs), m, ptr(pvec), ctypes.byref(g), ptr(tab), tab.shape[1],
-                                       zk, ptr(col_ptr), ctypes.byref(nnz), None, None, ptr(cscratch), cs,
+                                       zk, rs, ptr(col_ptr), ctypes.byref(nnz), None, None, ptr(cscratch), cs,
                                        stream_handle()), "edg_momentum_columns")
         self.nnz = int(nnz.value)
         row_idx = torch.empty(max(self.nnz, 1), dtype=torch.int32, device=dev)
         data = torch.empty(max(self.nnz, 1), dtype=torch.complex128, device=dev)
         check(lib.edg_momentum_columns(ptr(trans), ptr(refs), m, ptr(pvec), ctypes.byref(g), ptr(tab), tab.shape[1],
-                                       zk, ptr(col_ptr), ctypes.byref(nnz), ptr(row_idx), ptr(data), ptr(cscratch),
-                                       cs, stream_handle()), "edg_momentum_columns")
+                                       zk, rs, ptr(col_ptr), ctypes.byref(nnz), ptr(row_idx), ptr(data),
+                                       ptr(cscratch), cs, stream_handle()), "edg_momentum_columns")
         row_col = torch.empty(max(n, 1), dtype=torch.int64, device=dev)
         row_val = torch.empty(max(n, 1), dtype=torch.complex128, device=dev)
         check(lib.edg_momentum_rowmap(ptr(col_ptr), ptr(row_idx), ptr(data), m, n, ptr(row_col), ptr(row_val),

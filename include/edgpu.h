@@ -440,11 +440,19 @@ typedef struct {
 
 /* trans[r * n_shifts + t] = row of configuration r translated by shift t;
  * source_sites [n_shifts][n_sites] (device): the site whose local state lands
- * on each destination site.  A translated configuration outside the sector
- * returns EDG_ERR_MISSING_KET.  Synchronizes the stream (one flag read). */
+ * on each destination site.  local_map (nullable, device [map_dim]): a local
+ * state map applied t times along with shift t, the translation-charge
+ * generator of build_TC_translations (translational_sym.py:455-505; 1D, unit
+ * cell 1); label_sign / row_sign (nullable together, device [map_dim] /
+ * [n_rows]): row_sign[r] = prod_s label_sign[c_s(r)]
+ * (precompute_C_sign_per_config, :108-128).  A translated configuration
+ * outside the sector returns EDG_ERR_MISSING_KET.  Synchronizes the stream
+ * (one flag read). */
 int edg_momentum_translations(const edg_lookup_table* sector, const uint64_t* strides,
                               const int32_t* loc_dims, int32_t n_sites, const int32_t* source_sites,
-                              int32_t n_shifts, int32_t* trans, int32_t* err_flag, cudaStream_t stream);
+                              int32_t n_shifts, const int32_t* local_map, int32_t map_dim,
+                              const double* label_sign, double* row_sign, int32_t* trans,
+                              int32_t* err_flag, cudaStream_t stream);
 /* Scratch elements (int64) edg_momentum_references needs. */
 int64_t edg_momentum_scratch_elems(int64_t n_rows);
 /* refs[c] = reference row of column c (the smallest row of each orbit whose
@@ -454,14 +462,17 @@ int edg_momentum_references(const int32_t* trans, int64_t n_rows, const edg_mome
                             int32_t* pvec, int64_t* refs, int64_t* n_cols, int64_t* scratch,
                             int64_t scratch_elems, cudaStream_t stream);
 /* Columns of B.  phase_table [dim][max_r] complex128 = exp(-2 pi i k_d t / R_d)
- * by repeated products.  With row_idx == NULL (count pass): col_ptr [n_cols+1]
+ * by repeated products.  row_sign (nullable, [n_rows]): images at odd flat
+ * shifts take the reference row's sign (the TC bases, :952-1303).  With
+ * row_idx == NULL (count pass): col_ptr [n_cols+1]
  * = offsets, *nnz (host) = total, stream synchronized; scratch:
  * edg_scan_scratch_elems(n_cols).  Otherwise (fill pass): row_idx [nnz],
  * data [nnz] complex128. */
 int edg_momentum_columns(const int32_t* trans, const int64_t* refs, int64_t n_cols, const int32_t* pvec,
                          const edg_momentum_group* g, const double* phase_table, int32_t max_r,
-                         int32_t zero_k, int64_t* col_ptr, int64_t* nnz, int32_t* row_idx, double* data,
-                         int64_t* scratch, int64_t scratch_elems, cudaStream_t stream);
+                         int32_t zero_k, const double* row_sign, int64_t* col_ptr, int64_t* nnz,
+                         int32_t* row_idx, double* data, int64_t* scratch, int64_t scratch_elems,
+                         cudaStream_t stream);
 /* row_col[r] = column holding row r (-1 if none), row_val[r] its complex128
  * value.  A row in two columns returns EDG_ERR_ARG.  Synchronizes. */
 int edg_momentum_rowmap(const int64_t* col_ptr, const int32_t* row_idx, const double* data, int64_t n_cols,

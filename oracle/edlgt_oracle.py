@@ -368,20 +368,26 @@ def translation_sources(lvals, unit_cell):
     return src, R
 
 
-def momentum_basis(cfg, loc_dims, lvals, unit_cell, k_vals):
+def momentum_basis(cfg, loc_dims, lvals, unit_cell, k_vals, local_map=None, label_sign=None):
     """get_momentum_basis (translational_sym.py:1307-1358) for the zero-k and
     finite-k projectors (:697-949): (col_ptr, row_idx, data complex128, n_cols).
     Translations (build_all_translations :567-617) by key search; one
     reference per orbit, its smallest row; axis periods and the k filter of
     select_references (:620-694); Bloch sums over the period box with
     duplicates summed, finite-k entries with |a| <= 1e-14 dropped, columns
-    normalised, rows ascending."""
+    normalised, rows ascending.  ``local_map`` / ``label_sign``: the TC
+    variant (:455-505, 952-1303): the map applied once per unit shift, and
+    odd shifts weighted by the reference's product of label signs."""
     src, R = translation_sources(lvals, unit_cell)
     keys = keys_of(cfg, loc_dims)
     n, n_shifts, D = len(cfg), len(src), len(R)
     trans = np.empty((n, n_shifts), dtype=np.int64)
     for s in range(n_shifts):
-        tk = keys_of(cfg[:, src[s]], loc_dims)
+        moved = cfg[:, src[s]].astype(np.int64)
+        if local_map is not None:
+            for _ in range(s):
+                moved = np.asarray(local_map, dtype=np.int64)[moved]
+        tk = keys_of(moved, loc_dims)
         pos = np.searchsorted(keys, tk)
         ok = (pos < n) & (keys[np.minimum(pos, n - 1)] == tk)
         if not np.all(ok):
@@ -402,10 +408,14 @@ def momentum_basis(cfg, loc_dims, lvals, unit_cell, k_vals):
             p[d] = next((q for q in range(1, R[d] + 1) if trans[r, (q % R[d]) * strides[d]] == r), R[d])
         if any((k_vals[d] * p[d]) % R[d] != 0 for d in range(D)):
             continue
+        sign = 1.0 if label_sign is None else float(np.prod(np.asarray(label_sign)[cfg[r].astype(np.int64)]))
         acc = {}
         for t in np.ndindex(*p):
-            row = int(trans[r, int(np.dot(t, strides))])
+            full = int(np.dot(t, strides))
+            row = int(trans[r, full])
             ph = 1.0 + 0j if zero_k else np.prod([phase[d][t[d]] for d in range(D)])
+            if full & 1:
+                ph = ph * sign
             acc[row] = acc.get(row, 0) + ph
         rows = np.array(sorted(acc), dtype=np.int64)
         vals = np.array([acc[x] for x in rows], dtype=np.complex128)
@@ -413,7 +423,9 @@ def momentum_basis(cfg, loc_dims, lvals, unit_cell, k_vals):
             keep = np.abs(vals) > 1e-14
             rows, vals = rows[keep], vals[keep]
         nrm = np.sqrt(np.sum(np.abs(vals) ** 2))
-        if len(vals) == 0 or nrm ** 2 <= (0 if zero_k else 1e-30):
+        if zero_k and nrm ** 2 <= 1e-8:
+            cols.append((rows, np.zeros_like(vals)))  # a cancelled sign-twisted orbit
+        elif len(vals) == 0 or nrm ** 2 <= (0 if zero_k else 1e-30):
             cols.append((rows[:0], vals[:0]))
         else:
             cols.append((rows, vals / nrm))

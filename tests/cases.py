@@ -69,7 +69,14 @@ MOMENTUM_CASES = {
     "qed1d_L6_pbc_uc2": (dict(spin=1, pure_theory=False, lvals=[6], has_obc=[False]), 1.0, 1.0, [2], [[0], [1]]),
     "qed2d_2x2_pure_pbc": (dict(spin=1, pure_theory=True, lvals=[2, 2], has_obc=[False, False]), 1.3, None, [1, 1],
                            [[0, 0], [1, 0], [1, 1]]),
+    "su2_1d_L6_pbc_tc": (dict(spin=0.5, pure_theory=False, lvals=[6], has_obc=[False], sectors=[6]), 1.0, 5.0, [1],
+                         [[0], [1], [3]]),
+    "su2_1d_L8_pbc_tc": (dict(spin=0.5, pure_theory=False, lvals=[8], has_obc=[False], sectors=[8]), 1.0, 0.5, [1],
+                         [[0], [2], [5]]),
 }
+# the TC variant's fixed tables (six-state SU(2) j=1/2 dressed site)
+TC_MAP = [4, 5, 2, 3, 0, 1]
+TC_SIGN = [1.0, 1.0, 1.0, -1.0, 1.0, 1.0]
 
 
 def build_momentum_case(name, device="cpu"):

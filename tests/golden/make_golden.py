@@ -357,6 +357,10 @@ MOMENTUM_CASES = {
                          [[0], [1]]),
     "qed2d_2x2_pure_pbc": (qed_model, QED_CASES["qed2d_2x2_pure_pbc"][0], 1.3, None, [1, 1],
                            [[0, 0], [1, 0], [1, 1]]),
+    # translation combined with charge conjugation (TC_symmetry=True)
+    "su2_1d_L6_pbc_tc": (su2_model, SU2_CASES["su2_1d_L6_pbc"][0], 1.0, 5.0, [1], [[0], [1], [3]]),
+    "su2_1d_L8_pbc_tc": (su2_model, dict(spin=0.5, pure_theory=False, lvals=[8], has_obc=[False], sectors=[8]), 1.0,
+                         0.5, [1], [[0], [2], [5]]),
 }
 
 
@@ -368,7 +372,7 @@ def gen_momentum():
         for k in ks:
             tag = f"{name}/k" + "_".join(str(x) for x in k)
             model = factory(kw)
-            model.set_momentum_sector(ucs, k)
+            model.set_momentum_sector(ucs, k, name.endswith("_tc"))
             model.default_params()
             if mass is None:
                 model.build_Hamiltonian(g)

@@ -32,7 +32,7 @@ def test_projector_and_spectrum_match_reference(name, golden_momentum, dev):
     model.build_Hamiltonian(g, m)
     for k in ks:
         tag = _tag(name, k)
-        model.set_momentum_sector(ucs, k)
+        model.set_momentum_sector(ucs, k, TC_symmetry=name.endswith("_tc"))
         mb = model.momentum_basis
         cp, ri, dv = (golden_momentum[f"{tag}/{x}"] for x in ("L_col_ptr", "L_row_idx", "L_data"))
         assert mb["n_cols"] == len(cp) - 1

@@ -5,8 +5,8 @@ the package feed both, so these tests also pin the host model layer."""
 import numpy as np
 import pytest
 
-from cases import (ALL_CASES, ENTROPY_CASES, MOMENTUM_CASES, NBODY_CASES, TWOBODY_CASES, build, build_momentum_case,
-                   nbody_instances)
+from cases import (ALL_CASES, ENTROPY_CASES, MOMENTUM_CASES, NBODY_CASES, TC_MAP, TC_SIGN, TWOBODY_CASES, build,
+                   build_momentum_case, nbody_instances)
 from oracle import edlgt_oracle as O
 
 
@@ -136,7 +136,8 @@ def test_momentum_basis_oracle(name, golden_momentum):
     H = O.assemble(model.hamiltonian_blocks(g, m), cfg, model.loc_dims).toarray()
     for k in ks:
         tag = f"{name}/k" + "_".join(str(x) for x in k)
-        cp, ri, data, n_cols = O.momentum_basis(cfg, model.loc_dims, model.lvals, ucs, k)
+        tc = dict(local_map=TC_MAP, label_sign=TC_SIGN) if name.endswith("_tc") else {}
+        cp, ri, data, n_cols = O.momentum_basis(cfg, model.loc_dims, model.lvals, ucs, k, **tc)
         assert np.array_equal(cp, golden_momentum[f"{tag}/L_col_ptr"])
         assert np.array_equal(ri, golden_momentum[f"{tag}/L_row_idx"])
         assert np.max(np.abs(data - golden_momentum[f"{tag}/L_data"]), initial=0.0) <= 1e-13
