@@ -198,8 +198,6 @@ class QMB_hamiltonian:
         convert_hamiltonian("dense"), qmb_hamiltonian.py:227-258, 300-302):
         the matrix is densified on the device (``edg_csr_to_dense``) and
         diagonalised by the library Hermitian solver."""
-        import ctypes  # noqa: F401
-
         from .._lib import check, lib, ptr, stream_handle
 
         n = self.shape[0]
