@@ -1,0 +1,68 @@
+"""Host-side pieces of the momentum, n-body and partition paths (CPU only):
+the translation tables and phase tables the device kernels receive, and the
+n-body pattern instances, against the oracle's restatements."""
+
+import numpy as np
+import pytest
+
+from cases import nbody_instances
+from oracle import edlgt_oracle as O
+
+
+@pytest.mark.parametrize("lvals,ucs", [([6], [1]), ([8], [2]), ([4, 2], [1, 1]), ([4, 4], [2, 1]),
+                                       ([2, 2, 2], [1, 1, 1])])
+def test_translation_sources_match_oracle(lvals, ucs):
+    from edgpu.momentum import translation_sources
+
+    src, R = translation_sources(lvals, ucs)
+    ref, R_ref = O.translation_sources(lvals, ucs)
+    assert np.array_equal(src, ref) and np.array_equal(R, R_ref)
+    n = int(np.prod(lvals))
+    assert np.array_equal(src[0], np.arange(n))  # shift 0 is the identity
+    for s in range(src.shape[0]):
+        assert np.array_equal(np.sort(src[s]), np.arange(n))  # every shift permutes the sites
+
+
+def test_translation_sources_reject_bad_cells():
+    from edgpu.momentum import translation_sources
+
+    with pytest.raises(ValueError):
+        translation_sources([6], [4])
+    with pytest.raises(ValueError):
+        translation_sources([4, 2], [1])
+
+
+def test_phase_table_is_the_bloch_phase():
+    from edgpu.momentum import _phase_table
+
+    R = np.array([6, 4], dtype=np.int32)
+    tab = _phase_table(np.array([5, -1]), R)
+    for d in range(2):
+        k = [5, -1][d] % R[d]
+        want = np.exp(-2j * np.pi * k * np.arange(R[d]) / R[d])
+        assert np.max(np.abs(tab[d, : R[d]] - want)) <= 1e-14
+
+
+@pytest.mark.parametrize("lvals,obc,dist", [([8], [True], [[1], [2]]), ([8], [False], [[3]]),
+                                            ([3, 2], [True, True], [[1, 1]]), ([4, 3], [False, True], [[1, 0], [0, 1]])])
+def test_nbody_instances_match_the_term(lvals, obc, dist):
+    from edgpu.modeling import NBodyTerm
+
+    ops = [np.zeros((int(np.prod(lvals)), 2, 2))] * (len(dist) + 1)
+    term = NBodyTerm(ops, ["a"] * len(ops), dist, lvals=lvals, has_obc=obc)
+    got = term.get_Hamiltonian(1.0).sites.tolist()
+    assert got == nbody_instances(lvals, obc, dist)
+
+
+def test_oracle_partition_edges():
+    """Empty subsystem and empty environment give one unique configuration on
+    the empty side (the reference's _unique_configs_with_inverse)."""
+    cfg = np.array([[0, 1, 2], [1, 0, 2], [1, 1, 0]], dtype=np.uint16)
+    loc = np.array([2, 2, 3])
+    p = O.partition(cfg, loc, [])
+    assert p["subsys_dim"] == 1 and p["unique_subsys_configs"].shape == (1, 0)
+    assert np.array_equal(p["subsys_map"], [0, 0, 0]) and p["env_dim"] == 3
+    p = O.partition(cfg, loc, [0, 1, 2])
+    assert p["env_dim"] == 1 and np.array_equal(p["subsys_map"], [0, 1, 2])
+    p = O.partition(cfg, loc, [0])
+    assert np.array_equal(p["subsys_map"], [0, 1, 1]) and p["subsys_dim"] == 2
