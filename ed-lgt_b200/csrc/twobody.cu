@@ -17,8 +17,6 @@
 // conj(psi_row) * a * b * psi_ket in f64 registers.  Blocks reduce their warps
 // per pair in shared memory; a second kernel sums the block partials in a
 // fixed order, so results do not depend on scheduling.
-#include <vector>
-
 #include "internal.cuh"
 #include "lookup.cuh"
 
@@ -30,9 +28,6 @@ constexpr int kPairsPerLane = 4;
 constexpr int kTilePairs = 32 * kPairsPerLane;
 constexpr int kBlocks = edg::kSmCount * 3;
 constexpr int kTableSmemCap = 24 * 1024;  // transition tables larger than this stay in global memory
-constexpr int kGramRows = 64;    // rows per staged tile of the 16-site product path
-constexpr int kGramPitch = 18;   // doubles per staged row: 16-byte aligned rows, banks spread
-constexpr int64_t kGramBytes = 2LL * kGramRows * kGramPitch * 8;
 
 template <int PT>
 __device__ __forceinline__ double2 load_psi(const void* psi, int64_t r, int64_t stride) {
@@ -96,126 +91,6 @@ __host__ __device__ inline Layout layout(int ns, int dm, int tables_in_smem, int
   off += (int64_t)kWarps * kTilePairs * 16;
   l.total = off;
   return l;
-}
-
-// Real-diagonal operators on at most 16 sites: the correlators of one operator
-// pair form the 16 x 16 product C = A^T B over the rows, A[r][i] =
-// |psi_r|^2 a_i(c_i(r)) and B[r][j] = b_j(c_j(r)).  A tile of kGramRows rows
-// is staged in shared memory (one decoding thread per row), then every
-// 16-lane group accumulates a 4 x 4 block of C over its rows of the tile in
-// registers: two 16-byte reads of A and of B feed 16 FMAs.  Blocks reduce
-// their groups in a fixed order and write one partial per listed pair.
-__host__ __device__ inline int64_t gram_smem_bytes(int n_sites, int dmax) {
-  return (int64_t)dmax * diag_pitch(n_sites) * 8 + round16((int64_t)n_sites * 12) + kGramBytes;
-}
-
-// Launched only when every table entry of both operators is zero or a real
-// self-transition (checked on the host) and n_sites <= 16.
-template <int PT>
-__global__ void __launch_bounds__(kThreads, 3) twobody_gram_k(const Args a) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  const int ns = a.n_sites, dm = a.dmax;
-  const int pitch = diag_pitch(ns);
-  double* s_dre = reinterpret_cast<double*>(smem);
-  uint64_t* s_magic = reinterpret_cast<uint64_t*>(smem + (int64_t)dm * pitch * 8);
-  uint32_t* s_ld = reinterpret_cast<uint32_t*>(s_magic + ns);
-  double* sA = reinterpret_cast<double*>(smem + (int64_t)dm * pitch * 8 + round16((int64_t)ns * 12));
-  double* sB = sA + kGramRows * kGramPitch;
-  for (int s = threadIdx.x; s < ns; s += kThreads) {
-    uint32_t d = (uint32_t)a.loc_dims[s];
-    if (d < 1) {
-      atomicExch(a.err, 1);
-      d = 1;
-    }
-    s_ld[s] = d;
-    s_magic[s] = d > 1 ? ~0ull / d + 1 : 0;
-  }
-  for (int k = threadIdx.x; k < 2 * ns * dm; k += kThreads) {
-    const double v = a.count[k] > 0 ? a.amp[k * dm].x : 0.0;
-    s_dre[(k % dm) * pitch + k / dm] = v;
-  }
-  __syncthreads();
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int grp = tid >> 4, l16 = tid & 15, bi = l16 >> 2, bj = l16 & 3;
-  double acc[4][4];
-#pragma unroll
-  for (int u = 0; u < 4; ++u)
-#pragma unroll
-    for (int v = 0; v < 4; ++v) acc[u][v] = 0.0;
-  const int64_t n = a.sec.n;
-  const int64_t n_tiles = (n + kGramRows - 1) / kGramRows;
-  for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
-    if (tid < kGramRows) {
-      double* Ar = sA + tid * kGramPitch;
-      double* Br = sB + tid * kGramPitch;
-      const int64_t r = tile * kGramRows + tid;
-      int s0 = 0;
-      if (r < n) {
-        uint64_t x = __ldg(a.sec.keys + r);
-        const double2 pr = load_psi<PT>(a.psi, r, a.psi_stride);
-        const double w = fma(pr.x, pr.x, pr.y * pr.y);
-        for (int s = ns - 1; s >= 0; --s) {  // last site fastest
-          const uint32_t d = s_ld[s];
-          const uint64_t q = (x >> 32) ? x / d : (d > 1 ? __umul64hi(s_magic[s], x) : x);
-          uint32_t c = (uint32_t)(x - q * d);
-          if (c >= (uint32_t)dm) {  // a local state beyond the operators' dimension
-            atomicExch(a.err, 1);
-            c = 0;
-          }
-          x = q;
-          Ar[s] = s_dre[c * pitch + s] * w;
-          Br[s] = s_dre[c * pitch + ns + s];
-        }
-        s0 = ns;
-      }
-      for (int s = s0; s < 16; ++s) {
-        Ar[s] = 0.0;
-        Br[s] = 0.0;
-      }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < kGramRows / 16; ++k) {
-      const int t = grp * (kGramRows / 16) + k;
-      const double2* Ap = reinterpret_cast<const double2*>(sA + t * kGramPitch + 4 * bi);
-      const double2* Bp = reinterpret_cast<const double2*>(sB + t * kGramPitch + 4 * bj);
-      const double2 a01 = Ap[0], a23 = Ap[1], b01 = Bp[0], b23 = Bp[1];
-      const double av[4] = {a01.x, a01.y, a23.x, a23.y};
-      const double bv[4] = {b01.x, b01.y, b23.x, b23.y};
-#pragma unroll
-      for (int u = 0; u < 4; ++u)
-#pragma unroll
-        for (int v = 0; v < 4; ++v) acc[u][v] = fma(av[u], bv[v], acc[u][v]);
-    }
-    __syncthreads();
-  }
-  // the two groups of a warp hold the same block; then the 8 warps in order
-#pragma unroll
-  for (int u = 0; u < 4; ++u)
-#pragma unroll
-    for (int v = 0; v < 4; ++v) acc[u][v] += __shfl_down_sync(0xffffffffu, acc[u][v], 16);
-  double* red = sA;          // [8 warps][256], over the staged tiles
-  double* C = red + 8 * 256;  // [16][16]
-  if (lane < 16) {
-#pragma unroll
-    for (int u = 0; u < 4; ++u)
-#pragma unroll
-      for (int v = 0; v < 4; ++v) red[warp * 256 + (4 * bi + u) * 16 + 4 * bj + v] = acc[u][v];
-  }
-  __syncthreads();
-  for (int q = tid; q < 256; q += kThreads) {
-    double sum = 0.0;
-    for (int w = 0; w < kWarps; ++w) sum += red[w * 256 + q];
-    C[q] = sum;
-  }
-  __syncthreads();
-  for (int p = tid; p < a.n_pairs; p += kThreads) {
-    const int i = a.pair_i[p], j = a.pair_j[p];
-    const bool ok = i >= 0 && j >= 0 && i < ns && j < ns && i != j;
-    if (!ok && blockIdx.x == 0) atomicExch(a.err, 2);
-    a.partial[((int64_t)blockIdx.x * a.n_pairs + p) * 2] = ok ? C[i * 16 + j] : 0.0;
-    a.partial[((int64_t)blockIdx.x * a.n_pairs + p) * 2 + 1] = 0.0;
-  }
 }
 
 template <int PT>
@@ -471,44 +346,14 @@ extern "C" int edg_twobody_expval(const edg_lookup_table* sector, const uint64_t
   if (e != cudaSuccess) return edg::cuda_status(e, "edg_twobody_expval: flag");
   Args a{*sector, strides, loc_dims, t_count, t_ket, reinterpret_cast<const double2*>(t_amp), pair_i, pair_j, psi,
          psi_stride, scratch, err, n_sites, dmax, n_pairs, 0, 0};
-  // real diagonal operators on at most 16 sites take the tiled product kernel:
-  // read back the one entry per (operator, site, bra state) that decides it
-  bool gram = false;
-  if (n_sites <= 16 && (int64_t)dmax * diag_pitch(n_sites) <= kDiagCap) {
-    const int ne = 2 * n_sites * dmax;
-    std::vector<int32_t> hc(ne);
-    std::vector<uint8_t> hk(ne);
-    std::vector<double2> ha(ne);
-    e = cudaMemcpyAsync(hc.data(), t_count, sizeof(int32_t) * ne, cudaMemcpyDeviceToHost, stream);
-    if (e == cudaSuccess)
-      e = cudaMemcpy2DAsync(hk.data(), 1, t_ket, (size_t)dmax, 1, (size_t)ne, cudaMemcpyDeviceToHost, stream);
-    if (e == cudaSuccess)
-      e = cudaMemcpy2DAsync(ha.data(), 16, t_amp, (size_t)dmax * 16, 16, (size_t)ne, cudaMemcpyDeviceToHost, stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
-    if (e != cudaSuccess) return edg::cuda_status(e, "edg_twobody_expval: table read");
-    gram = true;
-    for (int k = 0; k < ne && gram; ++k)
-      gram = hc[k] == 0 || (hc[k] == 1 && hk[k] == k % dmax && ha[k].y == 0.0);
-  }
   a.tables_in_smem = table_bytes(n_sites, dmax) <= kTableSmemCap;
   a.diag_in_smem = dmax * diag_pitch(n_sites) <= kDiagCap;
   const int64_t smem = layout(n_sites, dmax, a.tables_in_smem, a.diag_in_smem).total;
-  if (gram) {
-    const size_t gs = (size_t)gram_smem_bytes(n_sites, dmax);
-    switch (psi_dtype) {
-      case 0: twobody_gram_k<0><<<kBlocks, kThreads, gs, stream>>>(a); break;
-      case 1: twobody_gram_k<1><<<kBlocks, kThreads, gs, stream>>>(a); break;
-      case 2: twobody_gram_k<2><<<kBlocks, kThreads, gs, stream>>>(a); break;
-      default: twobody_gram_k<3><<<kBlocks, kThreads, gs, stream>>>(a); break;
-    }
-    e = cudaGetLastError();
-  } else {
-    switch (psi_dtype) {
-      case 0: e = launch<0>(a, smem, stream); break;
-      case 1: e = launch<1>(a, smem, stream); break;
-      case 2: e = launch<2>(a, smem, stream); break;
-      default: e = launch<3>(a, smem, stream); break;
-    }
+  switch (psi_dtype) {
+    case 0: e = launch<0>(a, smem, stream); break;
+    case 1: e = launch<1>(a, smem, stream); break;
+    case 2: e = launch<2>(a, smem, stream); break;
+    default: e = launch<3>(a, smem, stream); break;
   }
   if (e != cudaSuccess) return edg::cuda_status(e, "edg_twobody_expval");
   twobody_reduce_k<<<(n_pairs + 7) / 8, 256, 0, stream>>>(scratch, kBlocks, n_pairs, pair_i, pair_j, n_sites, corr);
