@@ -20,6 +20,12 @@ Arms.
   C/OpenMP triplet builder and CSR matvec, SciPy ARPACK), one coupling per
   step (bounded sample), on all host cores.
 
+Other workloads (``--workload``), each printing its own JSON line: ``batch``
+(QED 3x2 instance batch), ``quench`` (SU(2) L=16 Krylov dynamics), ``z3``
+(Z3 4x3 zero-momentum matrix-free batch), ``corr`` (two-body correlator
+matrices, SU(2) L=16), ``entropy`` (half-chain entanglement, SU(2) L=14) and
+``momentum`` (zero-momentum ground state, SU(2) L=14 PBC).
+
 Multi-GPU: one process per GPU (torchrun); every rank solves its own replica
 of the sweep (independent instances, no data exchange: weak scaling);
 timings are the max over ranks.

@@ -131,6 +131,7 @@ class QuantumModel:
         self.res = {}
         self.H = None
         self._partition_cache = {}
+        self._momentum = None
 
     # ------------------------------------------------------------- sector
     @property
