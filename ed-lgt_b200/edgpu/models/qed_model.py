@@ -108,6 +108,32 @@ class QED_Model(QuantumModel):
             }
         self.coeffs = coeffs
 
+    def overlap_QMB_state(self, name):
+        """Named benchmark configurations of 1D QED with matter and the
+        truncated spin-1 basis (QED_Model.overlap_QMB_state,
+        edlgt/models/QED_model.py:778-849): ``V`` (alias ``PV``) the vacuum,
+        states 1 / 3 on even / odd sites (0 and 1 at the open edges), and
+        ``meson_center``, states 4 / 1 on the central (even, odd) pair.  The
+        integrated basis and the 3D string states are not built."""
+        key = name.strip().lower().replace(" ", "_")
+        key = "v" if key == "pv" else key
+        if self.dim != 1 or self.pure_theory or key not in ("v", "meson_center"):
+            raise NotImplementedError("named states are built for 1D QED with matter ('V', 'meson_center')")
+        if not (np.isscalar(self.spin) and int(self.spin) == 1):
+            raise NotImplementedError("named 1D states need the truncated spin=1 basis")
+        n = self.n_sites
+        cfg = np.array([1 if ii % 2 == 0 else 3 for ii in range(n)], dtype=np.int32)
+        if all(self.has_obc):
+            cfg[0] = 0
+            if n >= 2:
+                cfg[-1] = 1
+        if key == "meson_center":
+            even = n // 2
+            even -= even % 2
+            even = max(0, min(even, n - 2))
+            cfg[even], cfg[even + 1] = 4, 1
+        return cfg
+
     def build_Hamiltonian(self, g, m=None, theta=0.0, dtype_mode="auto"):
         return self.build_truncated_Hamiltonian(g, m, theta, dtype_mode)
 

@@ -88,6 +88,45 @@ class SU2_Model(QuantumModel):
                 "m_even": m,
             }
 
+    # named benchmark configurations of the j = 1/2 dressed-site basis
+    # (SU2_Model.overlap_QMB_state, edlgt/models/SU2_model.py:486-553): 1D
+    # labels give (even-site state, odd-site state, left edge, right edge)
+    _OVERLAP_1D = {"V": (0, 4, 0, 2), "PV": (1, 5, 1, 1), "T": (6, 12, 1, 1), "M": (2, 3, 1, 1),
+                   "B": (7, 11, 1, 1)}
+    _OVERLAP_2D_OBC = {"V": [0, 9, 0, 4, 4, 0, 9, 0], "PV1": [1, 12, 3, 5, 5, 2, 11, 1],
+                       "PV2": [1, 11, 1, 5, 5, 3, 10, 1]}
+
+    def overlap_QMB_state(self, name):
+        """Configuration (local-state index per site) of a named benchmark state:
+        V bare vacuum, PV polarized vacuum, T, M, B, and the domain walls DW /
+        DW2 in 1D; V, PV1, PV2 on the 2x2 lattice with matter; V of the pure
+        theory.  Unknown 1D labels give the all-zero configuration, as in the
+        reference."""
+        n = self.n_sites
+        if len(self.lvals) == 1:
+            if name == "DW":
+                cfg = [0 if ii < n // 2 else 4 for ii in range(n)]
+                edges = (0, 2)
+            elif name == "DW2":
+                cfg = [0 if (ii // 2) % 2 == 0 else 4 for ii in range(n)]
+                edges = (0, 2)
+            else:
+                even, odd, left, right = self._OVERLAP_1D.get(name, (0, 0, 0, 0))
+                cfg = [even if ii % 2 == 0 else odd for ii in range(n)]
+                edges = (left, right)
+            if self.has_obc[0]:
+                cfg[0], cfg[-1] = edges
+            return np.array(cfg)
+        if self.pure_theory:
+            if name != "V":
+                raise ValueError(f"unknown pure-theory state {name}")
+            return np.zeros(n, dtype=np.int64)
+        if not self.has_obc[0]:
+            return np.array([0, 9, 0, 9, 9, 0, 9, 0])
+        if name not in self._OVERLAP_2D_OBC:
+            raise ValueError(f"unknown 2D state {name}")
+        return np.array(self._OVERLAP_2D_OBC[name])
+
     def build_Hamiltonian(self, g, m=None, theta=0.0, lambda_noise=0.0, dtype_mode="auto"):
         self.build_base_Hamiltonian(g, m, theta, lambda_noise, dtype_mode)
 

@@ -79,3 +79,10 @@ def golden_nbody():
     import numpy as np
 
     return np.load(os.path.join(GOLDEN, "nbody_cases.npz"))
+
+
+@pytest.fixture(scope="session")
+def golden_overlap():
+    import numpy as np
+
+    return np.load(os.path.join(GOLDEN, "overlap_cases.npz"))

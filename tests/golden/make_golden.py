@@ -6,7 +6,7 @@ Run in a container that has the reference checkout (EDLGT_PATH, default
     python tests/golden/make_golden.py [group ...]
 
 Groups: small, pins, dynamics, big, twobody, entropy, momentum, full,
-nbody.  Output: .npz files next to
+nbody, overlap.  Output: .npz files next to
 this script.  Nothing here is imported by the library or by the GPU tests;
 the tests only read the .npz files.
 
@@ -417,6 +417,30 @@ def gen_nbody():
     np.savez_compressed(os.path.join(HERE, "nbody_cases.npz"), **out)
 
 
+OVERLAP_CASES = {
+    # name: (factory, kwargs, labels)
+    "su2_1d_L6_pbc": (SU2_Model, SU2_CASES["su2_1d_L6_pbc"][0], ["V", "PV", "T", "M", "B", "DW", "DW2", "X"]),
+    "su2_1d_L8_obc": (SU2_Model, SU2_CASES["su2_1d_L8_obc"][0], ["V", "PV", "T", "M", "B", "DW", "DW2", "X"]),
+    "su2_2d_2x2_obc": (SU2_Model, SU2_CASES["su2_2d_2x2_obc"][0], ["V", "PV1", "PV2"]),
+    "su2_2d_2x2_pbc": (SU2_Model, dict(spin=0.5, pure_theory=False, lvals=[2, 2], has_obc=[False, False],
+                                       sectors=[4]), ["V"]),
+    "su2_2d_2x2_pure_pbc": (SU2_Model, SU2_CASES["su2_2d_2x2_pure_pbc"][0], ["V"]),
+    "qed1d_L8_obc": (QED_Model, QED_CASES["qed1d_L8_obc"][0], ["V", "PV", "meson_center", "Meson Center"]),
+    "qed1d_L6_pbc": (QED_Model, dict(spin=1, pure_theory=False, lvals=[6], has_obc=[False]), ["V", "meson_center"]),
+}
+
+
+def gen_overlap():
+    """Named benchmark configurations (overlap_QMB_state) of the reference."""
+    out = {}
+    for name, (cls, kw, labels) in OVERLAP_CASES.items():
+        model = cls(**kw)
+        for lab in labels:
+            out[f"{name}/{lab}"] = np.asarray(model.overlap_QMB_state(lab), dtype=np.int64)
+        print(name, {lab: out[f"{name}/{lab}"].tolist() for lab in labels}, flush=True)
+    np.savez_compressed(os.path.join(HERE, "overlap_cases.npz"), **out)
+
+
 def gen_full():
     """Full spectrum of SU(2) L=6 PBC (g=1, m=5, dim 282) through the
     reference's dense path: energies, r value, thermal functions, thermal beta
@@ -464,7 +488,10 @@ def gen_full():
 
 
 if __name__ == "__main__":
-    groups = sys.argv[1:] or ["small", "pins", "dynamics", "big", "twobody", "entropy", "momentum", "full", "nbody"]
+    groups = sys.argv[1:] or ["small", "pins", "dynamics", "big", "twobody", "entropy", "momentum", "full", "nbody",
+                             "overlap"]
+    if "overlap" in groups:
+        gen_overlap()
     if "nbody" in groups:
         gen_nbody()
     if "full" in groups:

@@ -66,3 +66,27 @@ def test_oracle_partition_edges():
     assert p["env_dim"] == 1 and np.array_equal(p["subsys_map"], [0, 1, 2])
     p = O.partition(cfg, loc, [0])
     assert np.array_equal(p["subsys_map"], [0, 1, 1]) and p["subsys_dim"] == 2
+
+
+OVERLAP_MODELS = {
+    "su2_1d_L6_pbc": ("SU2", dict(spin=0.5, pure_theory=False, lvals=[6], has_obc=[False], sectors=[6])),
+    "su2_1d_L8_obc": ("SU2", dict(spin=0.5, pure_theory=False, lvals=[8], has_obc=[True], sectors=[8])),
+    "su2_2d_2x2_obc": ("SU2", dict(spin=0.5, pure_theory=False, lvals=[2, 2], has_obc=[True, True], sectors=[4])),
+    "su2_2d_2x2_pbc": ("SU2", dict(spin=0.5, pure_theory=False, lvals=[2, 2], has_obc=[False, False], sectors=[4])),
+    "su2_2d_2x2_pure_pbc": ("SU2", dict(spin=0.5, pure_theory=True, lvals=[2, 2], has_obc=[False, False])),
+    "qed1d_L8_obc": ("QED", dict(spin=1, pure_theory=False, lvals=[8], has_obc=[True])),
+    "qed1d_L6_pbc": ("QED", dict(spin=1, pure_theory=False, lvals=[6], has_obc=[False])),
+}
+
+
+@pytest.mark.parametrize("name", sorted(OVERLAP_MODELS))
+def test_named_states_match_reference(name, golden_overlap):
+    """overlap_QMB_state configurations against the reference's tables."""
+    from edgpu.models import QED_Model, SU2_Model
+
+    kind, kw = OVERLAP_MODELS[name]
+    model = (SU2_Model if kind == "SU2" else QED_Model)(**kw, device="cpu")
+    labels = [k.split("/", 1)[1] for k in golden_overlap.files if k.startswith(name + "/")]
+    assert labels
+    for lab in labels:
+        assert np.array_equal(model.overlap_QMB_state(lab), golden_overlap[f"{name}/{lab}"]), lab
