@@ -47,6 +47,68 @@ class QMB_state:
     def get_norm(self):
         return float(np.sqrt(np.real(np.vdot(self.psi, self.psi))))
 
+    def expectation_value(self, operator, component="real"):
+        """<psi| O |psi> for O given as (rows, cols, values) triplets or as a
+        dense / scipy sparse matrix, real or imaginary part
+        (QMB_state.expectation_value, edlgt/modeling/qmb_state.py:112-157)."""
+        from scipy.sparse import csr_matrix, isspmatrix
+
+        psi = self.psi
+        if isinstance(operator, tuple) and len(operator) == 3:
+            rows, cols, vals = (np.asarray(x) for x in operator)
+            ev = np.sum(np.conj(psi[rows]) * vals * psi[cols])
+        elif isinstance(operator, np.ndarray) or isspmatrix(operator):
+            if operator.shape[0] != psi.shape[0]:
+                raise ValueError(f"quantum state dim {psi.shape[0]} is NOT the operator dim {operator.shape[0]}")
+            op = csr_matrix(operator) if isinstance(operator, np.ndarray) else operator
+            ev = np.vdot(psi, op.dot(psi))
+        else:
+            raise TypeError("Operator must be provided as a tuple (row_list, col_list, value_list), "
+                            "a dense matrix (np.ndarray), or a sparse matrix (scipy sparse matrix).")
+        if component == "real":
+            return float(np.real(ev))
+        if component == "imag":
+            return float(np.imag(ev))
+        raise ValueError(f"Unknown component='{component}'")
+
+    def get_state_configurations(self, threshold=1e-2, sector_configs=None, return_configs=False):
+        """Configurations with |psi|^2 above ``threshold`` (relaxed tenfold until
+        one qualifies), largest first (qmb_state.py:293-354)."""
+        psi = self.psi
+        prob = np.abs(psi) ** 2
+        thr = float(threshold)
+        idx = np.nonzero(prob > thr)[0]
+        while idx.size == 0:
+            thr /= 10
+            idx = np.nonzero(prob > thr)[0]
+        vals = psi[idx]
+        order = np.argsort(-np.abs(vals))
+        idx, vals = idx[order], vals[order]
+        if sector_configs is not None:
+            cfgs = np.asarray(sector_configs)[idx, :]
+        else:
+            if self.loc_dims is None:
+                raise ValueError("sector_configs or loc_dims are needed to decode the configurations")
+            dims = np.asarray(self.loc_dims, dtype=np.int64)
+            cfgs = np.empty((len(idx), len(dims)), dtype=np.uint8)
+            rem = idx.astype(np.int64)
+            for s in range(len(dims) - 1, -1, -1):
+                cfgs[:, s] = rem % dims[s]
+                rem //= dims[s]
+        for config, amp in zip(cfgs, vals):
+            coords = " ".join(f"{c:>3d}" for c in config)
+            logger.info(f"[{coords}] |psi|^2={abs(amp) ** 2:6f} ({amp:6f})")
+        if return_configs:
+            return cfgs, vals
+
+    def participation_renyi_entropy(self, alpha=2):
+        """PE_alpha = log(sum_r |psi_r|^(2 alpha) + 1e-16) / (1 - alpha)
+        (qmb_state.py:356-391)."""
+        if alpha <= 0 or alpha == 1:
+            raise ValueError(f"alpha must be > 0 and != 1. Got alpha={alpha}.")
+        prob = np.abs(self.psi) ** 2
+        return float(1.0 / (1.0 - float(alpha)) * np.log(np.sum(prob ** alpha) + 1e-16))
+
     def _psi_for(self, keep_indices, partitions_dict):
         from ..entanglement import _record
 

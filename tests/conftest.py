@@ -86,3 +86,10 @@ def golden_overlap():
     import numpy as np
 
     return np.load(os.path.join(GOLDEN, "overlap_cases.npz"))
+
+
+@pytest.fixture(scope="session")
+def golden_state():
+    import numpy as np
+
+    return np.load(os.path.join(GOLDEN, "state_cases.npz"))

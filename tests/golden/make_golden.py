@@ -6,7 +6,7 @@ Run in a container that has the reference checkout (EDLGT_PATH, default
     python tests/golden/make_golden.py [group ...]
 
 Groups: small, pins, dynamics, big, twobody, entropy, momentum, full,
-nbody, overlap.  Output: .npz files next to
+nbody, overlap, state.  Output: .npz files next to
 this script.  Nothing here is imported by the library or by the GPU tests;
 the tests only read the .npz files.
 
@@ -441,6 +441,36 @@ def gen_overlap():
     np.savez_compressed(os.path.join(HERE, "overlap_cases.npz"), **out)
 
 
+def gen_state():
+    """QMB_state post-processing of the reference on the SU(2) L=8 OBC ground
+    state: participation entropies, large-amplitude configurations and the
+    expectation value of a seeded dense Hermitian matrix."""
+    from edlgt.modeling.qmb_state import QMB_state
+
+    kw = SU2_CASES["su2_1d_L8_obc"][0]
+    model = su2_model(kw)
+    model.build_Hamiltonian(1.0, 0.5)
+    model.diagonalize_Hamiltonian(1, "sparse")
+    psi = np.asarray(model.H.Npsi[0].psi, dtype=np.complex128)
+    st = QMB_state(psi, model.lvals, model.loc_dims)
+    out = {"psi": psi, "keys": keys_of(model.sector_configs, model.loc_dims)}
+    for a in (0.5, 2, 3):
+        out[f"PE_{a}"] = np.float64(st.participation_renyi_entropy(a))
+    cfgs, vals = st.get_state_configurations(1e-2, model.sector_configs, return_configs=True)
+    out["cfgs"], out["vals"] = np.asarray(cfgs, dtype=np.int64), np.asarray(vals)
+    cfgs, vals = st.get_state_configurations(0.9, model.sector_configs, return_configs=True)
+    out["cfgs_relaxed"], out["vals_relaxed"] = np.asarray(cfgs, dtype=np.int64), np.asarray(vals)
+    rng = np.random.default_rng(21)
+    n = len(psi)
+    m = rng.normal(size=(n, n)) + 1j * rng.normal(size=(n, n))
+    m = m + m.conj().T
+    out["ev_dense_real"] = np.float64(st.expectation_value(m, "real"))
+    out["ev_dense_imag"] = np.float64(st.expectation_value(1j * m, "imag"))
+    np.savez_compressed(os.path.join(HERE, "state_cases.npz"), **out)
+    print("state", {k: out[k] for k in out if k.startswith("PE") or k.startswith("ev")}, len(out["cfgs"]),
+          len(out["cfgs_relaxed"]), flush=True)
+
+
 def gen_full():
     """Full spectrum of SU(2) L=6 PBC (g=1, m=5, dim 282) through the
     reference's dense path: energies, r value, thermal functions, thermal beta
@@ -489,7 +519,9 @@ def gen_full():
 
 if __name__ == "__main__":
     groups = sys.argv[1:] or ["small", "pins", "dynamics", "big", "twobody", "entropy", "momentum", "full", "nbody",
-                             "overlap"]
+                             "overlap", "state"]
+    if "state" in groups:
+        gen_state()
     if "overlap" in groups:
         gen_overlap()
     if "nbody" in groups:

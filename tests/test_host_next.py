@@ -90,3 +90,35 @@ def test_named_states_match_reference(name, golden_overlap):
     assert labels
     for lab in labels:
         assert np.array_equal(model.overlap_QMB_state(lab), golden_overlap[f"{name}/{lab}"]), lab
+
+
+def test_state_post_processing_matches_reference(golden_state):
+    """QMB_state participation entropies, large-amplitude configurations
+    (with the threshold relaxation) and dense expectation values on the
+    reference's SU(2) L=8 ground state."""
+    from cases import build
+    from edgpu.modeling import QMB_state
+
+    g = golden_state
+    model, _, _ = build("su2_1d_L8_obc")
+    cfg = O.sector_configs(**model.sector_inputs)
+    assert np.array_equal(O.keys_of(cfg, model.loc_dims), g["keys"])
+    st = QMB_state(g["psi"], model.lvals, model.loc_dims)
+    for a in (0.5, 2, 3):
+        assert abs(st.participation_renyi_entropy(a) - float(g[f"PE_{a}"])) <= 1e-12
+    with pytest.raises(ValueError):
+        st.participation_renyi_entropy(1)
+    cfgs, vals = st.get_state_configurations(1e-2, cfg, return_configs=True)
+    assert np.array_equal(cfgs, g["cfgs"]) and np.array_equal(vals, g["vals"])
+    cfgs, vals = st.get_state_configurations(0.9, cfg, return_configs=True)
+    assert np.array_equal(cfgs, g["cfgs_relaxed"]) and np.array_equal(vals, g["vals_relaxed"])
+    rng = np.random.default_rng(21)
+    n = len(g["psi"])
+    m = rng.normal(size=(n, n)) + 1j * rng.normal(size=(n, n))
+    m = m + m.conj().T
+    assert abs(st.expectation_value(m, "real") - float(g["ev_dense_real"])) <= 1e-10
+    assert abs(st.expectation_value(1j * m, "imag") - float(g["ev_dense_imag"])) <= 1e-10
+    from scipy.sparse import coo_matrix
+
+    mc = coo_matrix(m)
+    assert abs(st.expectation_value((mc.row, mc.col, mc.data)) - float(g["ev_dense_real"])) <= 1e-10
