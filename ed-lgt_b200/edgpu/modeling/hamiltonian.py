@@ -47,6 +47,24 @@ class QMB_state:
     def get_norm(self):
         return float(np.sqrt(np.real(np.vdot(self.psi, self.psi))))
 
+    def normalize(self, threshold=1e-14):
+        """Divide by the norm when it differs from 1 by more than threshold;
+        returns the norm (QMB_state.normalize, qmb_state.py:79-95)."""
+        nrm = self.get_norm()
+        if abs(nrm - 1) > threshold:
+            if self._psi_dev is not None:
+                self._psi_dev = self._psi_dev / nrm
+                self._psi = None
+            else:
+                self._psi = self._psi / nrm
+        return nrm
+
+    def truncate(self, threshold=1e-14):
+        """The amplitudes with |psi_r| > threshold, zero elsewhere (a copy;
+        QMB_state.truncate, qmb_state.py:97-110)."""
+        psi = self.psi
+        return np.where(np.abs(psi) > threshold, psi, 0)
+
     def expectation_value(self, operator, component="real"):
         """<psi| O |psi> for O given as (rows, cols, values) triplets or as a
         dense / scipy sparse matrix, real or imaginary part
@@ -251,6 +269,29 @@ class QMB_hamiltonian:
         self.Npsi = [QMB_state(self.to_original_basis(vecs[:, i]), self.lvals, loc_dims) for i in range(k)]
         self.GSenergy = self.Nenergies[0]
         self.GSpsi = self.Npsi[0]
+
+    def convert_hamiltonian(self, format):
+        """Select the representation used by diagonalize / time_evolution:
+        "dense" (full diagonalisation, exact evolution) or the device sparse
+        matrix ("gpu", alias "sparse" / "linear") (qmb_hamiltonian.py:227-258)."""
+        if format not in ("gpu", "sparse", "linear", "dense"):
+            raise ValueError(f"Invalid format: {format}. Use 'dense', 'sparse', 'linear' or 'gpu'.")
+        if self.mat is None:
+            self.build(format)
+        self.Ham_type = "dense" if format == "dense" else "gpu"
+
+    def get_sparsity(self):
+        """Stored entries over shape[0]^2 (qmb_hamiltonian.py:614-618)."""
+        if self.mat is None:
+            self.build()
+        pres = int(self.mat.diag_present.sum().item()) if self.mat.diag_present is not None else self.shape[0]
+        sparsity = (self.mat.nnz + pres) / float(self.shape[0]) ** 2
+        logger.info(f"SPARSITY: {round(sparsity, 16)}")
+        return sparsity
+
+    def print_energy(self, en_state):
+        logger.info("====================================================")
+        logger.info(f"{en_state} ENERGY: {round(float(self.Nenergies[en_state]), 16)}")
 
     # ------------------------------------------------------ full spectrum
     DENSE_MAX = 32768

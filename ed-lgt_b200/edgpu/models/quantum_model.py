@@ -287,6 +287,105 @@ class QuantumModel:
         self._momentum = MomentumBasis(self.sector, self.lvals, k_unit_cell_size, k_vals, **tc)
         self.momentum_basis = self._momentum.host_arrays()
 
+    def set_momentum_pair(self, k_left, k_right, k_unit_cell_size, TC_symmetry=False):
+        """Two momentum sectors at once (QuantumModel.set_momentum_pair,
+        edlgt/models/quantum_model.py:278-348): the CSC arrays of B_left and the
+        CSR arrays of B_right, for operators projected as B_left^dagger O
+        B_right."""
+        self.set_momentum_sector(k_unit_cell_size, k_left, TC_symmetry)
+        left = self.momentum_basis
+        self.set_momentum_sector(k_unit_cell_size, k_right, TC_symmetry)
+        right = self.momentum_basis
+        self._momentum = None  # pair mode projects operators, it has no single sector to diagonalise
+        self.momentum_basis = {
+            "pair_mode": True, "n_rows_full": len(self.sector), "n_cols_L": left["n_cols"],
+            "n_cols_R": int(right["R_col_idx"].max()) + 1 if len(right["R_col_idx"]) else 0,
+            "L_col_ptr": left["L_col_ptr"], "L_row_idx": left["L_row_idx"], "L_data": left["L_data"],
+            "R_row_ptr": right["R_row_ptr"], "R_col_idx": right["R_col_idx"], "R_data": right["R_data"],
+            "k_left": np.asarray(k_left, dtype=np.int32), "k_right": np.asarray(k_right, dtype=np.int32)}
+
+    def _momentum_matrices(self):
+        from scipy.sparse import csc_matrix, csr_matrix
+
+        mb = self.momentum_basis
+        if mb is None:
+            raise ValueError("Basis projector B is not set.")
+        if mb.get("pair_mode"):
+            n = mb["n_rows_full"]
+            left = csc_matrix((mb["L_data"], mb["L_row_idx"], mb["L_col_ptr"]), shape=(n, mb["n_cols_L"]))
+            right = csr_matrix((mb["R_data"], mb["R_col_idx"], mb["R_row_ptr"]), shape=(n, mb["n_cols_R"]))
+            return left, right
+        b = csr_matrix((mb["R_data"], mb["R_col_idx"], mb["R_row_ptr"]), shape=(mb["n_rows"], mb["n_cols"]))
+        return b, b
+
+    def check_momentum_pair(self):
+        """Frobenius norms of B_L^dagger B_L - 1, B_R^dagger B_R - 1 and
+        B_L^dagger B_R (quantum_model.py:350-398)."""
+        from scipy.sparse import identity
+        from scipy.sparse.linalg import norm
+
+        left, right = self._momentum_matrices()
+        out = (float(norm(left.conj().T @ left - identity(left.shape[1]))),
+               float(norm(right.conj().T @ right - identity(right.shape[1]))),
+               float(norm(left.conj().T @ right)))
+        logger.info(f"norms: {out}")
+        return out
+
+    def _original_basis_scipy(self):
+        """The sector Hamiltonian as a host scipy matrix in the reference basis."""
+        h = self.H.to_scipy()
+        ph = self.H._row_phase()
+        if ph is None:
+            return h
+        from scipy.sparse import diags
+
+        p = diags(ph.cpu().numpy())
+        return (p @ h @ p.conj()).tocsr()
+
+    def momentum_basis_projection(self, operator):
+        """B^dagger A B (B_L^dagger A B_R in pair mode) for a dense or sparse
+        sector operator, or for "H", stored in ``H.Ham``
+        (quantum_model.py:680-713)."""
+        from scipy.sparse import csr_matrix, isspmatrix
+
+        left, right = self._momentum_matrices()
+        a = self._original_basis_scipy() if isinstance(operator, str) and operator == "H" else operator
+        if not isspmatrix(a):
+            a = csr_matrix(a)
+        proj = (left.conj().T @ (a.tocsr() @ right)).tocsr()
+        if isinstance(operator, str) and operator == "H":
+            self.H.Ham = proj
+            return None
+        return proj
+
+    def _project_state_with_basis(self, state_realspace):
+        """psi_k = B^dagger psi (quantum_model.py:654-678), on the device
+        (``edg_momentum_reduce``) when a single momentum sector is set."""
+        mom = self._momentum
+        if self.momentum_basis is None:
+            return np.asarray(state_realspace).astype(np.complex128, copy=False)
+        if mom is None:
+            left, _ = self._momentum_matrices()
+            return left.conj().T @ np.asarray(state_realspace, dtype=np.complex128)
+        x = torch.from_numpy(np.ascontiguousarray(state_realspace, dtype=np.complex128)).to(self.device)
+        y = torch.empty(mom.n_cols, dtype=torch.complex128, device=self.device)
+        check(lib.edg_momentum_reduce(mom.n_cols, ptr(mom.col_ptr), ptr(mom.row_idx), ptr(mom.data), ptr(x), ptr(y),
+                                      stream_handle()), "edg_momentum_reduce")
+        return y.cpu().numpy()
+
+    def build_projector_from_sector_to_fullspace(self, indices):
+        """Sparse (prod loc_dims[indices], subsys_dim) map from the subsystem's
+        sector configurations to the product basis (quantum_model.py:793-824)."""
+        from scipy.sparse import csc_matrix
+
+        cfg = self._get_partition(indices)["unique_subsys_configs"]
+        dims = np.asarray(self.loc_dims)[sorted(int(i) for i in indices)].astype(np.int64)
+        rows = np.zeros(cfg.shape[0], dtype=np.int64)
+        for k, d in enumerate(dims):
+            rows = rows * d + cfg[:, k].astype(np.int64)
+        return csc_matrix((np.ones(cfg.shape[0]), (rows, np.arange(cfg.shape[0]))),
+                          shape=(int(np.prod(dims)), cfg.shape[0]))
+
     def diagonalize_Hamiltonian(self, n_eigs, format="gpu", print_results=False, precision="fp64", tol=1e-12):
         mom = getattr(self, "_momentum", None)
         if mom is not None:

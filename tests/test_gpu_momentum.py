@@ -137,3 +137,51 @@ def test_time_evolution_in_momentum_sector(dev):
     for j, t in enumerate(times):
         ref = expm(-1j * t * Hk) @ psi0
         assert np.max(np.abs(model.H.psi_time[j].psi - ref)) <= 1e-9, t
+
+
+def test_pair_mode_projection_and_state_projection(golden_momentum, dev):
+    """set_momentum_pair arrays against the single-sector fixtures, the
+    check_momentum_pair norms, momentum_basis_projection of H (spectrum of the
+    reference) and of a state (B^dagger psi)."""
+    from scipy.sparse import csc_matrix
+
+    model, g, m, ucs, _ = build_momentum_case("su2_1d_L6_pbc", device=dev)
+    model.build_Hamiltonian(g, m)
+    model.set_momentum_pair([0], [1], ucs, False)
+    mb = model.momentum_basis
+    assert mb["pair_mode"]
+    assert np.array_equal(mb["L_col_ptr"], golden_momentum["su2_1d_L6_pbc/k0/L_col_ptr"])
+    right = csc_matrix((golden_momentum["su2_1d_L6_pbc/k1/L_data"], golden_momentum["su2_1d_L6_pbc/k1/L_row_idx"],
+                        golden_momentum["su2_1d_L6_pbc/k1/L_col_ptr"]), shape=(mb["n_rows_full"], mb["n_cols_R"]))
+    right = right.tocsr()
+    right.sort_indices()
+    assert np.array_equal(mb["R_row_ptr"], right.indptr) and np.array_equal(mb["R_col_idx"], right.indices)
+    nl, nr, mix = model.check_momentum_pair()
+    assert nl <= 1e-10 and nr <= 1e-10 and mix <= 1e-10
+    model.set_momentum_sector(ucs, [3])
+    model.momentum_basis_projection("H")
+    e = np.linalg.eigvalsh(model.H.Ham.toarray())[:2] / model.n_sites
+    assert np.allclose(e, golden_momentum["su2_1d_L6_pbc/k3/energies"], atol=1e-10, rtol=0)
+    rng = np.random.default_rng(2)
+    psi = rng.normal(size=len(model.sector)) + 1j * rng.normal(size=len(model.sector))
+    cp = golden_momentum["su2_1d_L6_pbc/k3/L_col_ptr"]
+    B = csc_matrix((golden_momentum["su2_1d_L6_pbc/k3/L_data"], golden_momentum["su2_1d_L6_pbc/k3/L_row_idx"], cp),
+                   shape=(len(psi), len(cp) - 1))
+    assert np.max(np.abs(model._project_state_with_basis(psi) - B.conj().T @ psi)) <= 1e-12
+
+
+def test_hamiltonian_utilities_and_fullspace_projector(dev):
+    from cases import build
+
+    model, g, m = build("qed1d_L8_obc", device=dev)
+    model.build_Hamiltonian(g, m)
+    sp = model.H.get_sparsity()
+    mat = model.H.to_scipy()
+    assert abs(sp - mat.nnz / mat.shape[0] ** 2) <= 1e-15
+    model.H.convert_hamiltonian("dense")
+    assert model.H.Ham_type == "dense"
+    P = model.build_projector_from_sector_to_fullspace([0, 1])
+    ref = O.partition(model.sector_configs, model.loc_dims, [0, 1])["unique_subsys_configs"].astype(np.int64)
+    dims = np.asarray(model.loc_dims)[[0, 1]]
+    assert P.shape == (int(np.prod(dims)), len(ref))
+    assert np.array_equal(P.tocsc().indices, ref[:, 0] * dims[1] + ref[:, 1])

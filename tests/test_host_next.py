@@ -122,3 +122,13 @@ def test_state_post_processing_matches_reference(golden_state):
 
     mc = coo_matrix(m)
     assert abs(st.expectation_value((mc.row, mc.col, mc.data)) - float(g["ev_dense_real"])) <= 1e-10
+
+
+def test_state_normalize_and_truncate():
+    from edgpu.modeling import QMB_state
+
+    st = QMB_state(np.array([3.0, 4.0j, 1e-15]))
+    assert np.array_equal(st.truncate(1e-14), np.array([3.0, 4.0j, 0]))
+    assert st.normalize() == 5.0
+    assert abs(st.get_norm() - 1.0) <= 1e-15
+    assert st.normalize() == pytest.approx(1.0)
