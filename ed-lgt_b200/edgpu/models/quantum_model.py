@@ -132,6 +132,7 @@ class QuantumModel:
         self.H = None
         self._partition_cache = {}
         self._momentum = None
+        self.dtype_mode = "auto"
 
     # ------------------------------------------------------------- sector
     @property
@@ -286,6 +287,39 @@ class QuantumModel:
             k_unit_cell_size = [1]
         self._momentum = MomentumBasis(self.sector, self.lvals, k_unit_cell_size, k_vals, **tc)
         self.momentum_basis = self._momentum.host_arrays()
+
+    @staticmethod
+    def _normalize_dtype_mode(dtype_mode, allow_auto=True):
+        """bool / None / "real" / "complex" / "auto" -> a mode string
+        (QuantumModel._normalize_dtype_mode, quantum_model.py:1342-1371)."""
+        if isinstance(dtype_mode, (bool, np.bool_)):
+            return "complex" if bool(dtype_mode) else "real"
+        if dtype_mode is None:
+            if allow_auto:
+                return "auto"
+            raise ValueError("dtype_mode cannot be None in this context")
+        if not isinstance(dtype_mode, str):
+            raise TypeError(f"dtype_mode must be bool/str/None, got {type(dtype_mode)}")
+        mode = dtype_mode.strip().lower()
+        valid = {"real", "complex", "auto"} if allow_auto else {"real", "complex"}
+        if mode not in valid:
+            raise ValueError(f"dtype_mode must be one of {sorted(valid)}, got {dtype_mode!r}")
+        return mode
+
+    def configure_dtype_mode(self, dtype_mode="auto", auto_mode="complex"):
+        """The model's value type for later builds (quantum_model.py:1373-1408).
+        On the device a matrix whose phases can be gauged away is stored in
+        real form whatever the mode (its spectrum and the states mapped back
+        are those of the complex matrix); "complex" stores it complex."""
+        mode = self._normalize_dtype_mode(dtype_mode, allow_auto=True)
+        if mode == "auto":
+            mode = self._normalize_dtype_mode(auto_mode, allow_auto=False)
+        self.dtype_mode = mode
+        return mode
+
+    def _resolve_dtype_mode(self, dtype_mode):
+        mode = self._normalize_dtype_mode(dtype_mode, allow_auto=True)
+        return self.dtype_mode if mode == "auto" else mode
 
     def set_momentum_pair(self, k_left, k_right, k_unit_cell_size, TC_symmetry=False):
         """Two momentum sectors at once (QuantumModel.set_momentum_pair,

@@ -167,4 +167,4 @@ class SU2_Model(QuantumModel):
         self.default_params()
         for b in self.hamiltonian_blocks(g, m, theta, lambda_noise):
             self.H.add_term(b)
-        self.H.build(self.ham_format, force_complex=(dtype_mode == "complex"))
+        self.H.build(self.ham_format, force_complex=(self._resolve_dtype_mode(dtype_mode) == "complex"))

@@ -132,3 +132,20 @@ def test_state_normalize_and_truncate():
     assert st.normalize() == 5.0
     assert abs(st.get_norm() - 1.0) <= 1e-15
     assert st.normalize() == pytest.approx(1.0)
+
+
+def test_dtype_mode_normalisation():
+    from edgpu.models.quantum_model import QuantumModel
+
+    n = QuantumModel._normalize_dtype_mode
+    assert n(True) == "complex" and n(False) == "real" and n(None) == "auto" and n(" Real ") == "real"
+    with pytest.raises(ValueError):
+        n(None, allow_auto=False)
+    with pytest.raises(ValueError):
+        n("half")
+    with pytest.raises(TypeError):
+        n(3)
+    m = QuantumModel([4], [True], device="cpu")
+    assert m.configure_dtype_mode() == "complex" and m._resolve_dtype_mode("auto") == "complex"
+    assert m._resolve_dtype_mode("real") == "real"
+    assert m.configure_dtype_mode("real") == "real" and m._resolve_dtype_mode(None) == "real"
