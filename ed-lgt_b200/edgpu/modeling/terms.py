@@ -11,6 +11,7 @@ assembler turns all blocks of a Hamiltonian into one canonical matrix.
 
 from __future__ import annotations
 
+import logging
 from math import prod
 
 import numpy as np
@@ -18,6 +19,8 @@ import numpy as np
 from ..lattice import neighbor_sites, plaquette_sites, zig_zag
 
 __all__ = ["TermBlock", "LocalTerm", "TwoBodyTerm", "PlaquetteTerm", "NBodyTerm"]
+
+logger = logging.getLogger(__name__)
 
 
 class TermBlock:
@@ -46,7 +49,7 @@ class TermBlock:
 class QMBTerm:
     def __init__(self, lvals, has_obc, operator=None, op_name=None, op_list=None, op_names_list=None,
                  sector_configs=None, loc_dims=None, staggered_basis=False, gauge_basis=None, momentum_basis=None,
-                 **_):
+                 sector=None, phase_weights=None, **_):
         self.lvals = list(lvals)
         self.dimensions = "xyz"[: len(lvals)]
         self.has_obc = list(has_obc)
@@ -58,13 +61,60 @@ class QMBTerm:
         self.op_list = op_list
         self.op_names_list = op_names_list
         self.sector_configs = sector_configs
+        # a momentum sector is applied to the assembled sector matrix when the
+        # Hamiltonian is diagonalised, so the terms themselves stay in the sector
         self.momentum_basis = momentum_basis
-        if momentum_basis is not None:
-            raise NotImplementedError("momentum-projected terms are not part of the device engine yet")
+        self.sector = sector
+        self.phase_weights = phase_weights
         self.n_sites = prod(self.lvals)
 
     def _mask_ok(self, coords, mask):
         return mask is None or bool(np.asarray(mask)[tuple(coords)])
+
+    def get_staggered_conditions(self, coords, stag_label):
+        """even / odd sublattice selection by (-1)^sum(coords) (qmb_term.py:105-127)."""
+        stag = (-1) ** int(sum(coords))
+        return stag_label is None or (stag_label == "even" and stag > 0) or (stag_label == "odd" and stag < 0)
+
+    def get_mask_conditions(self, coords, mask):
+        return self._mask_ok(coords, mask)
+
+    def _device_psi(self, psi):
+        import torch
+
+        from .hamiltonian import QMB_state
+
+        if self.sector is None:
+            raise ValueError("expectation values need the model's symmetry sector (build the term from def_params)")
+        if not isinstance(psi, QMB_state):
+            raise TypeError(f"psi must be instance of class:QMB_state not {type(psi)}")
+        x = psi.device(self.sector.device)
+        if x.shape[0] != len(self.sector):
+            raise ValueError("the state does not live in the sector basis (momentum-basis states are not supported)")
+        return x if isinstance(x, torch.Tensor) else torch.from_numpy(np.asarray(x)).to(self.sector.device)
+
+    def _instances_expval(self, blocks, psi, component):
+        """<psi| O_inst |psi> for each single-instance block, assembled once."""
+        import torch
+
+        from .assembly import assemble_blocks
+
+        if not hasattr(self, "_inst_mats"):
+            self._inst_mats = [assemble_blocks(self.sector, [b], phase_weights=self.phase_weights, force_complex=True)
+                               for b in blocks]
+        x = self._device_psi(psi).to(torch.complex128)
+        vals = []
+        for m in self._inst_mats:
+            z = torch.vdot(x, m.matvec(x)).item()
+            vals.append(z.real if component == "real" else z.imag)
+        return np.array(vals)
+
+    def _split_instances(self, block):
+        out = []
+        for inst in block.sites:
+            b = TermBlock(block.ops, np.array([inst]), 1.0, add_dagger=False, diagonal=block.diagonal, name=block.name)
+            out.append(b)
+        return out
 
 
 class LocalTerm(QMBTerm):
@@ -78,6 +128,23 @@ class LocalTerm(QMBTerm):
             raise TypeError(f"strength must be SCALAR not a {type(strength)}")
         sites = [ii for ii in range(self.n_sites) if self._mask_ok(zig_zag(self.lvals, ii), mask)]
         return TermBlock([self.op], np.array(sites).reshape(-1, 1), strength, diagonal=True, name=self.op_name)
+
+    def get_expval(self, psi, stag_label=None, print_values=True, get_variance=False):
+        """Per-site <psi| op_s |psi> in ``self.obs`` and their average over the
+        selected sublattice in ``self.avg`` (LocalTerm.get_expval,
+        edlgt/modeling/local_term.py:119-237), one device reduction."""
+        from ..models.quantum_model import site_expval_device
+
+        x = self._device_psi(psi)
+        self.obs = site_expval_device(self.sector, self.op, x).cpu().numpy()
+        if get_variance:
+            op2 = np.array([np.asarray(self.op[s]) @ np.asarray(self.op[s]) for s in range(self.op.shape[0])])
+            self.var = site_expval_device(self.sector, op2, x).cpu().numpy() - self.obs ** 2
+        sel = [ii for ii in range(self.n_sites) if self.get_staggered_conditions(zig_zag(self.lvals, ii), stag_label)]
+        self.avg = float(np.mean(self.obs[sel]))
+        self.std = float(np.sqrt(np.abs(np.sum(self.var[sel])) / len(sel))) if get_variance else 0.0
+        if print_values:
+            logger.info(f"{self.op_name} {self.avg:.16f}")
 
 
 class TwoBodyTerm(QMBTerm):
@@ -102,6 +169,14 @@ class TwoBodyTerm(QMBTerm):
         return TermBlock(self.op_list, np.array(inst).reshape(-1, 2), strength, add_dagger=add_dagger,
                          name="-".join(self.op_names_list or []))
 
+    def get_expval(self, psi):
+        """Correlator matrix Re <psi| A_i B_j |psi> over all pairs i < j in
+        ``self.corr`` (TwoBodyTerm.get_expval, twobody_term.py:160-209)."""
+        from ..models.quantum_model import twobody_corr_device
+
+        self.corr = twobody_corr_device(self.sector, self.op_list[0], self.op_list[1],
+                                        self._device_psi(psi)).cpu().numpy()
+
 
 class PlaquetteTerm(QMBTerm):
     """Four-site plaquette product ``op0[o] op1[o+a] op2[o+b] op3[o+a+b]``."""
@@ -123,6 +198,19 @@ class PlaquetteTerm(QMBTerm):
             inst.append(sl)
         return TermBlock(self.op_list, np.array(inst).reshape(-1, 4), strength, add_dagger=add_dagger,
                          name="-".join(self.op_names_list or []))
+
+    def get_expval(self, psi, component="real", stag_label=None):
+        """Per-plaquette <psi| P |psi> (real or imaginary part) in ``self.obs``,
+        their mean in ``self.avg`` (PlaquetteTerm.get_expval,
+        plaquette_term.py:165-263), plaquettes of the selected sublattice."""
+        if component not in ("real", "imag"):
+            raise ValueError(f"component must be 'real' or 'imag': got {component}")
+        block = self.get_Hamiltonian(1.0)
+        keep = [k for k, inst in enumerate(block.sites)
+                if self.get_staggered_conditions(zig_zag(self.lvals, int(inst[0])), stag_label)]
+        block.sites = block.sites[keep]
+        self.obs = self._instances_expval(self._split_instances(block), psi, component)
+        self.avg = float(np.mean(self.obs))
 
 
 class NBodyTerm(QMBTerm):
@@ -165,3 +253,8 @@ class NBodyTerm(QMBTerm):
                 inst.append(sites)
         return TermBlock(self.op_list, np.array(inst).reshape(-1, len(self.op_list)), strength,
                          add_dagger=add_dagger, name="-".join(self.op_names_list or []))
+
+    def get_expval(self, psi, component="real"):
+        """<psi| prod_j op_j |psi> for every starting site whose pattern stays on
+        the lattice, in ``self.obs`` (NBodyTerm.get_expval, nbody_term.py:164-220)."""
+        self.obs = self._instances_expval(self._split_instances(self.get_Hamiltonian(1.0)), psi, component)

@@ -246,6 +246,8 @@ class QuantumModel:
             "gauge_basis": self.gauge_basis,
             "sector_configs": None,
             "momentum_basis": self.momentum_basis,
+            "sector": self.sector,
+            "phase_weights": self.phase_weights,
         }
         if self.sector is not None:
             self.H = QMB_hamiltonian(self.lvals, len(self.sector), sector=self.sector,

@@ -1,0 +1,62 @@
+"""Term-level expectation values (LocalTerm / TwoBodyTerm / PlaquetteTerm /
+NBodyTerm .get_expval) and the reference's momentum workflow order
+(set_momentum_sector, default_params, build_Hamiltonian, diagonalize) on the
+device, against the reference's fixtures."""
+
+import numpy as np
+import pytest
+
+from cases import NBODY_CASES, TWOBODY_CASES, build, build_momentum_case
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def dev():
+    import torch
+
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    return "cuda"
+
+
+def test_term_expvals_match_reference(golden_twobody, golden_nbody, golden_pins, dev):
+    import torch
+
+    from edgpu.modeling import LocalTerm, NBodyTerm, PlaquetteTerm, QMB_state, TwoBodyTerm
+
+    name = "su2_1d_L8_obc"
+    model, _, _ = build(name, device=dev)
+    st = QMB_state(torch.from_numpy(golden_twobody[f"{name}/psi"]).to(dev))
+    a, b = TWOBODY_CASES[name][0]
+    t = TwoBodyTerm("x", [model.ops[a], model.ops[b]], [a, b], **model.def_params)
+    t.get_expval(st)
+    assert np.max(np.abs(t.corr - golden_twobody[f"{name}/{a}_{b}"])) <= 1e-12
+    lt = LocalTerm(model.ops["N_tot"], "N_tot", **model.def_params)
+    lt.get_expval(st, get_variance=True)
+    assert np.allclose(lt.obs, model.local_expval(model.ops["N_tot"], st), atol=1e-14)
+    assert abs(lt.avg - np.mean(lt.obs)) <= 1e-15 and lt.std >= 0
+    lt.get_expval(st, stag_label="even")
+    assert abs(lt.avg - np.mean(lt.obs[0::2])) <= 1e-15
+    ops, dists = NBODY_CASES[name]
+    st_nb = QMB_state(torch.from_numpy(golden_nbody[f"{name}/psi"]).to(dev))
+    nt = NBodyTerm([model.ops[o] for o in ops[0]], ops[0], dists[0], **model.def_params)
+    nt.get_expval(st_nb)
+    assert np.max(np.abs(nt.obs - golden_nbody[f"{name}/{'_'.join(ops[0])}"])) <= 1e-12
+    model, g, m = build("qed2d_3x2_bg", device=dev)
+    model.build_Hamiltonian(g, m)
+    model.diagonalize_Hamiltonian(1)
+    names = ["C_px,py", "C_py,mx", "C_my,px", "C_mx,my"]
+    pt = PlaquetteTerm(["x", "y"], [model.ops[o] for o in names], names, **model.def_params)
+    pt.get_expval(model.H.GSpsi)
+    assert abs(pt.avg - golden_pins["qed2d_3x2_bg/plaq"]) < 1e-10
+
+
+def test_momentum_in_reference_workflow_order(golden_momentum, dev):
+    """set_momentum_sector before default_params and build_Hamiltonian, as the
+    reference's workflows call them."""
+    model, g, m, ucs, _ = build_momentum_case("su2_1d_L6_pbc", device=dev)
+    model.set_momentum_sector(ucs, [3])
+    model.default_params()
+    model.build_Hamiltonian(g, m)
+    model.diagonalize_Hamiltonian(2)
+    assert np.allclose(model.H.Nenergies, golden_momentum["su2_1d_L6_pbc/k3/energies"], atol=1e-10, rtol=0)
