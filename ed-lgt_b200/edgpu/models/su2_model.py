@@ -14,7 +14,7 @@ import logging
 import numpy as np
 
 from ..lattice import origin_surfaces, staggered_mask
-from ..modeling import LocalTerm, PlaquetteTerm, TwoBodyTerm
+from ..modeling import LocalTerm, PlaquetteTerm, QMB_hamiltonian, TwoBodyTerm
 from ..operators import su2_dressed_site_operators, su2_gauge_invariant_states
 from .quantum_model import QuantumModel
 
@@ -126,6 +126,35 @@ class SU2_Model(QuantumModel):
         if name not in self._OVERLAP_2D_OBC:
             raise ValueError(f"unknown 2D state {name}")
         return np.array(self._OVERLAP_2D_OBC[name])
+
+    def get_mask(self, sites_list):
+        """Boolean lattice mask selecting the given sites (SU2_model.py:701-706)."""
+        mask = np.zeros(self.lvals, dtype=bool)
+        for site in sites_list:
+            mask[site] = True
+        return mask
+
+    def build_local_Hamiltonian(self, g, m, R0):
+        """``self.Hlocal``: the 1D Hamiltonian density around site R0 (electric
+        and mass terms at R0, half of the hoppings on the bonds (R0-1, R0) and
+        (R0, R0+1) with their conjugates), SU2_Model.build_local_Hamiltonian
+        (edlgt/models/SU2_model.py:626-699), assembled on the device."""
+        if self.dim > 1:
+            raise ValueError(f"Local Hamiltonian valid only for D=1, got {self.dim}")
+        self.SU2_Hamiltonian_couplings(g, m)
+        dp = self.def_params
+        c = self.coeffs
+        self.Hlocal = QMB_hamiltonian(self.lvals, len(self.sector), sector=self.sector,
+                                      phase_weights=self.phase_weights)
+        here, left = self.get_mask([R0]), self.get_mask([(R0 - 1) % self.n_sites])
+        self.Hlocal.add_term(LocalTerm(self.ops["E_square"], "E_square", **dp).get_Hamiltonian(c["E"], here))
+        self.Hlocal.add_term(LocalTerm(self.ops["N-1"], "N-1", **dp).get_Hamiltonian(((-1) ** R0) * c["m"], here))
+        hop = TwoBodyTerm("x", [self.ops["Qpx_dag"], self.ops["Qmx"]], ["Qpx_dag", "Qmx"], **dp)
+        hop_dag = TwoBodyTerm("x", [self.ops["Qpx"], self.ops["Qmx_dag"]], ["Qpx", "Qmx_dag"], **dp)
+        half = 0.5 * c["tx_even"]
+        for term, sign in ((hop, 1.0), (hop_dag, -1.0)):
+            self.Hlocal.add_term(term.get_Hamiltonian(sign * half, mask=here))
+            self.Hlocal.add_term(term.get_Hamiltonian(sign * half, mask=left))
 
     def build_Hamiltonian(self, g, m=None, theta=0.0, lambda_noise=0.0, dtype_mode="auto"):
         self.build_base_Hamiltonian(g, m, theta, lambda_noise, dtype_mode)

@@ -93,3 +93,10 @@ def golden_state():
     import numpy as np
 
     return np.load(os.path.join(GOLDEN, "state_cases.npz"))
+
+
+@pytest.fixture(scope="session")
+def golden_local():
+    import numpy as np
+
+    return np.load(os.path.join(GOLDEN, "local_hamiltonian_cases.npz"))

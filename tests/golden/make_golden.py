@@ -6,7 +6,7 @@ Run in a container that has the reference checkout (EDLGT_PATH, default
     python tests/golden/make_golden.py [group ...]
 
 Groups: small, pins, dynamics, big, twobody, entropy, momentum, full,
-nbody, overlap, state.  Output: .npz files next to
+nbody, overlap, state, local.  Output: .npz files next to
 this script.  Nothing here is imported by the library or by the GPU tests;
 the tests only read the .npz files.
 
@@ -471,6 +471,28 @@ def gen_state():
           len(out["cfgs_relaxed"]), flush=True)
 
 
+def gen_local():
+    """SU2_Model.build_local_Hamiltonian of the reference (SU(2) L=8 OBC,
+    g^2 = 1, m = 0.5) around the interior sites 3 and 6, as canonical CSR (an
+    open-chain edge site makes the reference concatenate an empty bond list)."""
+    out = {}
+    kw = SU2_CASES["su2_1d_L8_obc"][0]
+    for R0 in (3, 6):
+        model = su2_model(kw)
+        model.build_local_Hamiltonian(1.0, 0.5, R0)
+        H = model.Hlocal
+        H._materialize_triplets()
+        n = len(model.sector_configs)
+        m = coo_matrix((H.value_list, (H.row_list.astype(np.int64), H.col_list.astype(np.int64))),
+                       shape=(n, n)).tocsr()
+        m.sum_duplicates()
+        m.sort_indices()
+        out[f"R{R0}/indptr"], out[f"R{R0}/indices"] = m.indptr.astype(np.int64), m.indices.astype(np.int64)
+        out[f"R{R0}/data"] = np.asarray(m.data, dtype=np.complex128)
+        print("local", R0, n, m.nnz, flush=True)
+    np.savez_compressed(os.path.join(HERE, "local_hamiltonian_cases.npz"), **out)
+
+
 def gen_full():
     """Full spectrum of SU(2) L=6 PBC (g=1, m=5, dim 282) through the
     reference's dense path: energies, r value, thermal functions, thermal beta
@@ -519,7 +541,9 @@ def gen_full():
 
 if __name__ == "__main__":
     groups = sys.argv[1:] or ["small", "pins", "dynamics", "big", "twobody", "entropy", "momentum", "full", "nbody",
-                             "overlap", "state"]
+                             "overlap", "state", "local"]
+    if "local" in groups:
+        gen_local()
     if "state" in groups:
         gen_state()
     if "overlap" in groups:

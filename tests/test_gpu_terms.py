@@ -60,3 +60,23 @@ def test_momentum_in_reference_workflow_order(golden_momentum, dev):
     model.build_Hamiltonian(g, m)
     model.diagonalize_Hamiltonian(2)
     assert np.allclose(model.H.Nenergies, golden_momentum["su2_1d_L6_pbc/k3/energies"], atol=1e-10, rtol=0)
+
+
+@pytest.mark.parametrize("R0", [3, 6])
+def test_local_hamiltonian_matches_reference(R0, golden_local, dev):
+    """SU2_Model.build_local_Hamiltonian against the reference's matrix (in
+    the reference basis, 1e-13)."""
+    from scipy.sparse import csr_matrix, diags
+
+    model, _, _ = build("su2_1d_L8_obc", device=dev)
+    model.build_local_Hamiltonian(1.0, 0.5, R0)
+    model.Hlocal.build()
+    h = model.Hlocal.to_scipy()
+    ph = model.Hlocal._row_phase()
+    if ph is not None:
+        p = diags(ph.cpu().numpy())
+        h = p @ h @ p.conj()
+    n = h.shape[0]
+    ref = csr_matrix((golden_local[f"R{R0}/data"], golden_local[f"R{R0}/indices"], golden_local[f"R{R0}/indptr"]),
+                     shape=(n, n))
+    assert abs(h - ref).max() <= 1e-13
