@@ -28,7 +28,8 @@ class QED_Model(QuantumModel):
                  charge=0, **kwargs):
         super().__init__(**kwargs)
         if isinstance(spin, str):
-            raise NotImplementedError("the integrated-gauge QED model is not part of the device engine yet")
+            self._init_integrated(spin, pure_theory, bg_list)
+            return
         if plaq_basis:
             raise NotImplementedError("the plaquette basis is not part of the device engine yet")
         if bg_list is not None:
@@ -83,6 +84,97 @@ class QED_Model(QuantumModel):
             self.phase_weights = self._matter_phase_weights(self.ops["N"])
         self.default_params()
 
+    def _init_integrated(self, spin, pure_theory, bg_list):
+        """Gauge fields integrated out through Gauss's law (1D with matter):
+        one two-state matter site per lattice site, Pauli operators with
+        basis index 0 occupied (N = (Sz + 1) / 2), sector N = n_sites / 2
+        (QED_Model.__init__, edlgt/models/QED_model.py:49-64, 120-125, and
+        QED_gauge_integrated_operators, edlgt/operators/QED_operators.py:541-545)."""
+        if spin != "integrated":
+            raise ValueError(f"spin must be integer or 'integrated': got {spin}")
+        if pure_theory or self.dim != 1:
+            raise ValueError("QED with integrated gauge fields is only in 1D with matter")
+        if bg_list is not None:
+            bg = np.asarray(bg_list, dtype=float)
+            if bg.shape != (self.n_sites,):
+                raise ValueError(f"len(bg_list) must match n_sites = {self.n_sites}: got {bg.shape}")
+            self.bg_list = bg.tolist()
+        else:
+            self.bg_list = None
+        self.spin = spin
+        self.pure_theory = False
+        self.plaq_basis = False
+        self.link_symmetries = False
+        self.staggered_basis = False
+        self.background = 0
+        self.gauge_basis = self.gauge_states = None
+        eye = np.eye(2)
+        sz = np.diag([1.0, -1.0])
+        sp = np.array([[0.0, 1.0], [0.0, 0.0]])
+        ops = {"I": eye, "Sz": sz, "Sp": sp, "Sm": sp.T.copy(), "Sx": sp + sp.T, "Sy": -1j * (sp - sp.T)}
+        ops["N"] = 0.5 * (sz + eye)
+        ops["N_zero"] = eye - ops["N"]
+        self.project_operators(ops)
+        self.get_abelian_symmetry_sector(global_ops=[self.ops["N"]], global_sectors=[int(self.n_sites / 2)])
+        self.phase_weights = self._matter_phase_weights(self.ops["N"])
+        self.default_params()
+
+    def _integrated_static_charges(self):
+        return np.zeros(self.n_sites) if self.bg_list is None else np.asarray(self.bg_list, dtype=float)
+
+    def integrated_blocks(self, g, m):
+        """(term blocks, constant) of the integrated Hamiltonian
+        (build_integrated_Hamiltonian, edlgt/models/QED_model.py:396-492):
+        staggered mass, hopping t Sp_i Sm_{i+1} + h.c., and the electric energy
+        sum over links of [sum_{k<=n} (q_k + (Sz_k + (-1)^k) / 2)]^2 expanded
+        into Sz fields, Sz_i Sz_j couplings J_ij = E (L - 1 - j) / 2 and a
+        constant."""
+        from ..modeling import NBodyTerm
+
+        self.QED_Hamiltonian_couplings(g, m)
+        c, dp, n = self.coeffs, self.def_params, self.n_sites
+        n_links = n - 1
+        blocks = []
+        for lab in ("even", "odd"):
+            blocks.append(LocalTerm(self.ops["N"], "N", **dp).get_Hamiltonian(c[f"m_{lab}"],
+                                                                               staggered_mask(self.lvals, lab)))
+        hop = TwoBodyTerm("x", [self.ops["Sp"], self.ops["Sm"]], ["Sp", "Sm"], **dp)
+        blocks.append(hop.get_Hamiltonian(strength=c["t"], add_dagger=True))
+        stagger = np.array([1.0 if ii % 2 == 0 else -1.0 for ii in range(n)])
+        prefix = np.cumsum(self._integrated_static_charges() + 0.5 * stagger)
+        site_mask = [self._single_site_mask(ii) for ii in range(n)]
+        sz = LocalTerm(self.ops["Sz"], "Sz", **dp)
+        for kk in range(n_links):
+            h = c["E"] * np.sum(prefix[kk:n_links])
+            if abs(h) >= 1e-14:
+                blocks.append(sz.get_Hamiltonian(strength=h, mask=site_mask[kk]))
+        for jj in range(1, n_links):
+            w = 0.5 * c["E"] * (n - 1 - jj)
+            if abs(w) > 1e-14:
+                for ii in range(jj):
+                    term = NBodyTerm([self.ops["Sz"], self.ops["Sz"]], ["Sz", "Sz"], [(jj - ii,)], **dp)
+                    blocks.append(term.get_Hamiltonian(strength=w, mask=site_mask[ii]))
+        const = 0.0
+        if n_links > 0:
+            const = c["E"] * (np.sum(prefix[:n_links] ** 2) + 0.25 * 0.5 * n_links * (n_links + 1))
+        return blocks, float(const)
+
+    def _single_site_mask(self, site_index):
+        mask = np.zeros(tuple(self.lvals), dtype=bool)
+        mask[(site_index,)] = True
+        return mask
+
+    def build_integrated_Hamiltonian(self, g, m, theta=0.0, dtype_mode="auto"):
+        from scipy.sparse import identity
+
+        self.default_params()
+        blocks, const = self.integrated_blocks(g, m)
+        for b in blocks:
+            self.H.add_term(b)
+        if abs(const) > 1e-14:
+            self.H.add_term(const * identity(self.H.shape[0], format="csc"))
+        self.H.build(self.ham_format, force_complex=(self._resolve_dtype_mode(dtype_mode) == "complex"))
+
     def _bg_values(self, states):
         return np.asarray(states, dtype=float)[:, 0]
 
@@ -135,6 +227,8 @@ class QED_Model(QuantumModel):
         return cfg
 
     def build_Hamiltonian(self, g, m=None, theta=0.0, dtype_mode="auto"):
+        if self.spin == "integrated":
+            return self.build_integrated_Hamiltonian(g, m, theta, dtype_mode)
         return self.build_truncated_Hamiltonian(g, m, theta, dtype_mode)
 
     def hamiltonian_blocks(self, g, m=None, theta=0.0):

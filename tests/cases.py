@@ -116,3 +116,10 @@ def nbody_instances(lvals, has_obc, distances):
         if sites is not None:
             out.append(sites)
     return out
+
+# integrated-gauge 1D QED fixtures: name -> (lvals, bg_list, g, m)
+INTEGRATED_CASES = {
+    "qedint_L4": ([4], None, 1.4, 0.7),
+    "qedint_L8_bg": ([8], [1, 0, 0, 0, 0, 0, 0, -1], 1.0, 0.5),
+    "qedint_L10": ([10], None, 0.8, 1.2),
+}

@@ -100,3 +100,10 @@ def golden_local():
     import numpy as np
 
     return np.load(os.path.join(GOLDEN, "local_hamiltonian_cases.npz"))
+
+
+@pytest.fixture(scope="session")
+def golden_integrated():
+    import numpy as np
+
+    return np.load(os.path.join(GOLDEN, "integrated_cases.npz"))

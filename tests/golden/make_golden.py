@@ -6,7 +6,7 @@ Run in a container that has the reference checkout (EDLGT_PATH, default
     python tests/golden/make_golden.py [group ...]
 
 Groups: small, pins, dynamics, big, twobody, entropy, momentum, full,
-nbody, overlap, state, local.  Output: .npz files next to
+nbody, overlap, state, local, integrated.  Output: .npz files next to
 this script.  Nothing here is imported by the library or by the GPU tests;
 the tests only read the .npz files.
 
@@ -493,6 +493,29 @@ def gen_local():
     np.savez_compressed(os.path.join(HERE, "local_hamiltonian_cases.npz"), **out)
 
 
+INTEGRATED_CASES = {
+    # name: (lvals, bg_list, g, m)
+    "qedint_L4": ([4], None, 1.4, 0.7),
+    "qedint_L8_bg": ([8], [1, 0, 0, 0, 0, 0, 0, -1], 1.0, 0.5),
+    "qedint_L10": ([10], None, 0.8, 1.2),
+}
+
+
+def gen_integrated():
+    """Integrated-gauge 1D QED (spin="integrated") through the reference's
+    build_Hamiltonian: sector keys, canonical matrix and two lowest energies."""
+    out = {}
+    for name, (lvals, bg, g, mass) in INTEGRATED_CASES.items():
+        model = QED_Model(spin="integrated", pure_theory=False, lvals=lvals, has_obc=[True], bg_list=bg)
+        model.build_Hamiltonian(g, mass)
+        out |= sector_record(model, f"{name}/", True)
+        out |= matrix_record(canonical(model), f"{name}/H_", True)
+        model.diagonalize_Hamiltonian(2, "sparse")
+        out[f"{name}/energies"] = np.asarray(model.H.Nenergies)
+        print(name, len(model.sector_configs), model.H.Nenergies, flush=True)
+    np.savez_compressed(os.path.join(HERE, "integrated_cases.npz"), **out)
+
+
 def gen_full():
     """Full spectrum of SU(2) L=6 PBC (g=1, m=5, dim 282) through the
     reference's dense path: energies, r value, thermal functions, thermal beta
@@ -541,7 +564,9 @@ def gen_full():
 
 if __name__ == "__main__":
     groups = sys.argv[1:] or ["small", "pins", "dynamics", "big", "twobody", "entropy", "momentum", "full", "nbody",
-                             "overlap", "state", "local"]
+                             "overlap", "state", "local", "integrated"]
+    if "integrated" in groups:
+        gen_integrated()
     if "local" in groups:
         gen_local()
     if "state" in groups:

@@ -80,3 +80,29 @@ def test_local_hamiltonian_matches_reference(R0, golden_local, dev):
     ref = csr_matrix((golden_local[f"R{R0}/data"], golden_local[f"R{R0}/indices"], golden_local[f"R{R0}/indptr"]),
                      shape=(n, n))
     assert abs(h - ref).max() <= 1e-13
+
+
+@pytest.mark.parametrize("name", ["qedint_L4", "qedint_L8_bg", "qedint_L10"])
+def test_integrated_qed_on_device(name, golden_integrated, dev):
+    """Integrated-gauge 1D QED built on the device: sector keys bit-exact, the
+    matrix in the reference basis to 1e-12, energies to 1e-10."""
+    from scipy.sparse import csr_matrix, diags
+
+    from cases import INTEGRATED_CASES
+    from edgpu.models import QED_Model
+
+    lvals, bg, g, m = INTEGRATED_CASES[name]
+    model = QED_Model(spin="integrated", pure_theory=False, lvals=lvals, has_obc=[True], bg_list=bg, device=dev)
+    assert np.array_equal(model.sector.host_keys(), golden_integrated[f"{name}/keys"])
+    model.build_Hamiltonian(g, m)
+    h = model.H.to_scipy()
+    ph = model.H._row_phase()
+    if ph is not None:
+        p = diags(ph.cpu().numpy())
+        h = p @ h @ p.conj()
+    n = h.shape[0]
+    ref = csr_matrix((golden_integrated[f"{name}/H_data"], golden_integrated[f"{name}/H_indices"],
+                      golden_integrated[f"{name}/H_indptr"]), shape=(n, n))
+    assert abs(h - ref).max() <= 1e-12
+    model.diagonalize_Hamiltonian(2)
+    assert np.allclose(model.H.Nenergies, golden_integrated[f"{name}/energies"], atol=1e-10, rtol=0)

@@ -202,3 +202,26 @@ def test_nbody_oracle(name, golden_nbody):
             vals.append(np.real(np.sum(np.conj(psi[rows]) * v * psi[cols])))
         ref = golden_nbody[f"{name}/{'_'.join(names)}"]
         assert len(vals) == len(ref) and np.max(np.abs(np.array(vals) - ref)) <= 1e-12, names
+
+
+@pytest.mark.parametrize("name", ["qedint_L4", "qedint_L8_bg", "qedint_L10"])
+def test_integrated_qed_oracle(name, golden_integrated):
+    """Integrated-gauge 1D QED: sector keys bit-exact, the matrix of the
+    package's term list (oracle assembly plus the constant) against the
+    reference's to 1e-12, energies to 1e-10."""
+    from cases import INTEGRATED_CASES
+    from edgpu.models import QED_Model
+    from scipy.sparse import csr_matrix
+
+    lvals, bg, g, m = INTEGRATED_CASES[name]
+    model = QED_Model(spin="integrated", pure_theory=False, lvals=lvals, has_obc=[True], bg_list=bg, device="cpu")
+    cfg = O.sector_configs(**model.sector_inputs)
+    assert np.array_equal(O.keys_of(cfg, model.loc_dims), golden_integrated[f"{name}/keys"])
+    blocks, const = model.integrated_blocks(g, m)
+    H = O.assemble(blocks, cfg, model.loc_dims).toarray() + const * np.eye(len(cfg))
+    n = len(cfg)
+    ref = csr_matrix((golden_integrated[f"{name}/H_data"], golden_integrated[f"{name}/H_indices"],
+                      golden_integrated[f"{name}/H_indptr"]), shape=(n, n)).toarray()
+    assert np.max(np.abs(H - ref)) <= 1e-12
+    e = np.linalg.eigvalsh(H)[:2] / model.n_sites
+    assert np.allclose(e, golden_integrated[f"{name}/energies"], atol=1e-10, rtol=0)
