@@ -159,6 +159,57 @@ class QED_Model(QuantumModel):
             const = c["E"] * (np.sum(prefix[:n_links] ** 2) + 0.25 * 0.5 * n_links * (n_links + 1))
         return blocks, float(const)
 
+    def reconstruct_integrated_E2_from_N(self, density_obs_name="N", density_corr_obs_name="N_N", state_index=None,
+                                         dynamics=False, compute_density_corr=True, print_values=True):
+        """<E_n^2> per link of the integrated model from the measured densities
+        <N_k> and correlators <N_k N_l> (E_n = sum_{k<=n} (q_k + ((-1)^k - 1)/2
+        + N_k)), QED_Model.reconstruct_integrated_E2_from_N
+        (edlgt/models/QED_model.py:505-665).  A missing correlator is measured
+        on the device on the chosen eigenstate or time step."""
+        if self.spin != "integrated" or self.dim != 1 or self.pure_theory:
+            raise ValueError("Integrated E2 reconstruction is defined only for 1D QED with matter")
+        if density_obs_name not in self.res:
+            raise KeyError(f"Missing '{density_obs_name}' in self.res. Measure local density first.")
+        dens = np.asarray(self.res[density_obs_name], dtype=float)
+        if dens.shape != (self.n_sites,):
+            raise ValueError(f"Expected {density_obs_name}.shape=({self.n_sites},) got {dens.shape}.")
+        n_links = self.n_sites - 1
+        if n_links <= 0:
+            self.res["E2"], self.res["E2_avg"] = np.zeros(0), 0.0
+            return self.res["E2"]
+        if density_corr_obs_name in self.res:
+            corr = np.asarray(self.res[density_corr_obs_name], dtype=float)
+        else:
+            if not compute_density_corr:
+                raise KeyError(f"Missing '{density_corr_obs_name}' in self.res. "
+                               "Measure ['N','N_N'] or set compute_density_corr=True.")
+            states = self.H.psi_time if dynamics else self.H.Npsi
+            if state_index is None:
+                if len(states) != 1:
+                    raise ValueError("state_index is required when several states are available")
+                state_index = 0
+            term = TwoBodyTerm("x", [self.ops["N"], self.ops["N"]], ["N", "N"], **self.def_params)
+            term.get_expval(states[state_index])
+            corr = np.asarray(term.corr, dtype=float)
+            self.res[density_corr_obs_name] = corr
+        if corr.shape != (self.n_sites, self.n_sites):
+            raise ValueError(f"Expected '{density_corr_obs_name}' shape ({self.n_sites}, {self.n_sites}), "
+                             f"got {corr.shape}.")
+        corr = np.array(corr, dtype=float, copy=True)
+        np.fill_diagonal(corr, dens)  # N_k^2 = N_k
+        k = np.arange(self.n_sites, dtype=float)
+        prefix_charge = np.cumsum(self._integrated_static_charges() + 0.5 * ((-1.0) ** k - 1.0))
+        prefix_dens = np.cumsum(dens)
+        prefix_corr = np.diag(corr.cumsum(axis=0).cumsum(axis=1))
+        e2 = prefix_charge[:n_links] ** 2 + 2.0 * prefix_charge[:n_links] * prefix_dens[:n_links] + \
+            prefix_corr[:n_links]
+        self.res["E2"] = e2
+        self.res["E2_avg"] = float(np.mean(e2))
+        if print_values:
+            for ii in range(n_links):
+                logger.info(f"E2[{ii}] = {e2[ii]:.12f}")
+        return e2
+
     def _single_site_mask(self, site_index):
         mask = np.zeros(tuple(self.lvals), dtype=bool)
         mask[(site_index,)] = True

@@ -225,3 +225,28 @@ def test_integrated_qed_oracle(name, golden_integrated):
     assert np.max(np.abs(H - ref)) <= 1e-12
     e = np.linalg.eigvalsh(H)[:2] / model.n_sites
     assert np.allclose(e, golden_integrated[f"{name}/energies"], atol=1e-10, rtol=0)
+
+
+def test_integrated_e2_reconstruction():
+    """reconstruct_integrated_E2_from_N from oracle-measured <N_k>, <N_k N_l>
+    of the integrated ground state against <E_n^2> evaluated directly in the
+    sector basis (the electric field is diagonal there)."""
+    from cases import INTEGRATED_CASES
+    from edgpu.models import QED_Model
+
+    lvals, bg, g, m = INTEGRATED_CASES["qedint_L8_bg"]
+    model = QED_Model(spin="integrated", pure_theory=False, lvals=lvals, has_obc=[True], bg_list=bg, device="cpu")
+    cfg = O.sector_configs(**model.sector_inputs)
+    blocks, const = model.integrated_blocks(g, m)
+    H = O.assemble(blocks, cfg, model.loc_dims).toarray() + const * np.eye(len(cfg))
+    w, V = np.linalg.eigh(H)
+    p = np.abs(V[:, 0]) ** 2
+    n_site = (cfg == 0).astype(float)  # basis index 0 is the occupied state
+    model.res["N"] = p @ n_site
+    model.res["N_N"] = (n_site * p[:, None]).T @ n_site
+    e2 = model.reconstruct_integrated_E2_from_N(print_values=False)
+    q = np.asarray(bg, dtype=float)
+    k = np.arange(model.n_sites)
+    field = np.cumsum(q + 0.5 * ((-1.0) ** k - 1.0) + n_site, axis=1)[:, :-1]
+    assert np.allclose(e2, p @ field ** 2, atol=1e-12)
+    assert abs(model.res["E2_avg"] - np.mean(e2)) <= 1e-15
