@@ -38,6 +38,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -104,7 +105,7 @@ class ClockSampler:
     def __init__(self, gpu_index):
         self.gpu = gpu_index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{gpu_index}.csv")
+        self.path = os.path.join(tempfile.gettempdir(), f"edgpu_clocks_rank{gpu_index}_{os.getpid()}.csv")
 
     def start(self):
         try:

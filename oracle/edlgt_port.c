@@ -1,5 +1,5 @@
 /*
- * CPU port of ed-lgt's hot loops -- TEST / BASELINE INFRASTRUCTURE ONLY.
+ * CPU port of ed-lgt's hot loops -- TEST AND CPU-BASELINE INFRASTRUCTURE ONLY.
  *
  * Multithreaded (OpenMP) C restatement of:
  *   - nbody_data / nbody_data_2sites / nbody_data_4sites

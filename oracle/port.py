@@ -1,4 +1,4 @@
-"""Python side of the multithreaded C port (edlgt_port.c) -- TEST / BASELINE
+"""Python side of the multithreaded C port (edlgt_port.c) -- TEST AND CPU-BASELINE
 INFRASTRUCTURE ONLY.
 
 ``assemble_port`` builds the reference's triplets term instance by term
