@@ -1,8 +1,8 @@
 #!/usr/bin/env python
 """Benchmark: Lanczos ground-state time-to-solution and matvec bandwidth,
 mixed-precision batched vs plain FP64 on the GPU, for the SU(2) coupling
-sweep workload (1D SU(2) Yang-Mills + staggered matter, j_max = 1/2, open
-chain L = 14, N_tot = 14 sector of dimension 616,227, g^2 in {0.5, 1, 2},
+sweep workload (1D SU(2) Yang-Mills + staggered matter, j_max = 1/2, periodic
+chain L = 14, N_tot = 14 sector of dimension 1,232,454, g^2 in {0.5, 1, 2},
 m = 0.5).  One step solves the three ground states.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl edgpu|reference]
@@ -15,10 +15,14 @@ Arms.
   second with the matrix resident in HBM; ``e2e`` = the same through the
   public model API from host inputs (sector enumeration, assembly, solve,
   eigenvectors copied back to the host) every step.  The plain FP64 path
-  (three sequential f64 Lanczos solves) is timed beside it.
-* reference: the CPU restatement of ed-lgt's path (numpy sector enumeration,
-  C/OpenMP triplet builder and CSR matvec, SciPy ARPACK), one coupling per
-  step (bounded sample), on all host cores.
+  (three sequential f64 Lanczos solves) is timed beside it, and the sector
+  enumeration and assembly phases are timed on their own.
+* reference: the unmodified ed-lgt (``baseline/_ref``) through its own model
+  API -- ``SU2_Model(...)`` (sector), ``build_Hamiltonian`` (assembly),
+  ``diagonalize_Hamiltonian(1, fmt)`` (ARPACK on the faster of its "linear"
+  Numba CSR and "sparse" SciPy formats) -- one coupling per step, on all host
+  cores, in a child process that never loads this engine
+  (``oracle/stock_ref.py``).  Under torchrun only rank 0 runs it.
 
 Other workloads (``--workload``), each printing its own JSON line: ``batch``
 (QED 3x2 instance batch), ``quench`` (SU(2) L=16 Krylov dynamics), ``z3``
@@ -49,16 +53,36 @@ for _p in (os.path.join(ROOT, "ed-lgt_b200"), ROOT):
         sys.path.insert(0, _p)
 
 L = 14
+PBC = True
 SWEEP = (0.5, 1.0, 2.0)
 MASS = 0.5
 METRIC = "Lanczos GS time-to-solution & matvec GB/s: mixed/batched vs plain FP64 GPU at 1e-9 rel."
 UNIT = "ground_states/s"
-WORKLOAD = (f"SU(2) 1D Yang-Mills + staggered matter, j_max=1/2, open chain L={L}, N_tot={L} sector; "
-            f"ground states for g^2 in {list(SWEEP)}, m={MASS}")
+WORKLOAD = (f"SU(2) 1D Yang-Mills + staggered matter, j_max=1/2, {'periodic' if PBC else 'open'} chain L={L}, "
+            f"N_tot={L} sector; ground states for g^2 in {list(SWEEP)}, m={MASS}")
 
 
 def model_kwargs():
-    return dict(spin=0.5, pure_theory=False, lvals=[L], has_obc=[True], sectors=[L])
+    return dict(spin=0.5, pure_theory=False, lvals=[L], has_obc=[not PBC], sectors=[L])
+
+
+def stock_reference(steps, warmup, fmt="auto", couplings=SWEEP, timeout=3000):
+    """Run the unmodified ed-lgt through its model API in a child process
+    (oracle/stock_ref.py, which never loads this engine); returns its JSON."""
+    cmd = [sys.executable, os.path.join(ROOT, "oracle", "stock_ref.py"), "--L", str(L), "--m", str(MASS),
+           "--steps", str(steps), "--warmup", str(warmup), "--format", fmt, "--g", *[str(g) for g in couplings]]
+    if PBC:
+        cmd.append("--pbc")
+    env = dict(os.environ)
+    for k in ("RANK", "LOCAL_RANK", "WORLD_SIZE", "LOCAL_WORLD_SIZE", "MASTER_ADDR", "MASTER_PORT"):
+        env.pop(k, None)
+    out = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=timeout)
+    if out.returncode != 0:
+        raise RuntimeError(f"stock reference failed (rc {out.returncode}): {out.stderr[-2000:]}")
+    res = json.loads(out.stdout.strip().splitlines()[-1])
+    if res["engine_loaded"]:
+        raise RuntimeError("the reference process mapped libedgpu.so")
+    return res
 
 
 def dist_setup(n_gpus):
@@ -103,7 +127,15 @@ class ClockSampler:
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, gpu_index):
-        self.gpu = gpu_index
+        # nvidia-smi numbers GPUs by PCI order, not by CUDA_VISIBLE_DEVICES:
+        # name the device by its UUID so the samples describe this process's GPU
+        self.gpu = str(gpu_index)
+        try:
+            import torch
+
+            self.gpu = "GPU-" + str(torch.cuda.get_device_properties(gpu_index).uuid)
+        except Exception:
+            pass
         self.proc = None
         self.path = os.path.join(tempfile.gettempdir(), f"edgpu_clocks_rank{gpu_index}_{os.getpid()}.csv")
 
@@ -111,7 +143,7 @@ class ClockSampler:
         try:
             os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.f = open(self.path, "w")
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", self.gpu, f"--query-gpu={self.FIELDS}",
                                           "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
                                          stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
@@ -151,44 +183,84 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def cpu_pipeline_one(g):
-    """ed-lgt's CPU path (restated) for one coupling: sector, assembly, eigsh."""
-    from edgpu.models import SU2_Model
-    from oracle import edlgt_oracle as O
-    from oracle import port as PT
-
-    t0 = time.perf_counter()
-    model = SU2_Model(**model_kwargs(), device="cpu")
-    cfg = O.sector_configs(**model.sector_inputs)
-    keys = O.keys_of(cfg, model.loc_dims)
-    H = PT.assemble_port(model.hamiltonian_blocks(g, MASS), keys, model.loc_dims)
-    w, _ = PT.lowest_eigs_port(H, 1)
-    return time.perf_counter() - t0, float(w[0])
-
-
-def run_reference(args, world, rank):
-    if rank != 0:
+def run_reference(args):
+    """The reference arm: stock ed-lgt on the host cores, rank 0 only (no
+    process group is created, so other ranks exit at once)."""
+    if int(os.environ.get("RANK", "0")) != 0:
         return
-    from oracle import port as PT
-
-    for i in range(args.warmup):
-        cpu_pipeline_one(SWEEP[i % 3])
-    times = []
-    for i in range(args.steps):
-        t, _ = cpu_pipeline_one(SWEEP[i % 3])
-        times.append(t)
-    ms = 1e3 * float(np.mean(times))
+    res = stock_reference(args.steps, args.warmup)
+    steps = res["steps"]
+    ms = 1e3 * float(np.mean([st["total_s"] for st in steps]))
     value = 1e3 / ms
+    phases = {k: 1e3 * float(np.mean([st[k] for st in steps])) for k in ("sector_s", "assembly_s", "solve_s")}
+    sample = (f"one coupling per step (cycling g^2 over {list(SWEEP)}): SU2_Model(...) sector, build_Hamiltonian, "
+              f"diagonalize_Hamiltonian(1, '{res['format']}') = ARPACK eigsh")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "complex128", "data": "synthetic (model Hamiltonian; no dataset)",
-        "config": {"workload": WORKLOAD, "instances_per_step": 1, "sample": "one coupling per step, cycling the sweep"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": PT.threads(), "kind": "port",
-                         "sample": "full CPU pipeline (sector, triplets, ARPACK eigsh) for one coupling"},
+        "config": {"workload": WORKLOAD, "sector_dim": steps[0]["dim"] if steps else None, "instances_per_step": 1,
+                   "sample": sample},
+        "phases_ms_per_step": {"sector": phases["sector_s"], "assembly": phases["assembly_s"],
+                               "solve": phases["solve_s"]},
+        "format_trial_solve_s": res["format_trial_solve_s"],
+        "energies_per_site": [st["energy_density"] for st in steps[:3]],
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": res["threads"], "kind": "reference",
+                         "cpu_model": res.get("cpu_model"), "sample": sample,
+                         "reference": "edlgt 0.2.3, unmodified, from baseline/_ref; Numba/SciPy/ARPACK threads = "
+                                      "host cores; warm JIT; engine library not loaded"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def setup_phases(dev, reps=3):
+    """Sector enumeration and assembly on the device, each timed on its own
+    (host clock around synchronised calls: the enumeration reads each level's
+    size back to the host).  Returns timings and the compulsory bytes."""
+    import torch
+
+    from edgpu.models import SU2_Model
+
+    def once():
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        m = SU2_Model(**model_kwargs(), device=dev)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        m.build_Hamiltonian(SWEEP[1], MASS)
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        return m, t1 - t0, t2 - t1
+
+    once()  # warm-up: host caches, kernel loads
+    ts_sec, ts_asm = [], []
+    for _ in range(reps):
+        m, a, b = once()
+        ts_sec.append(a)
+        ts_asm.append(b)
+    sec = m.sector
+    ng = getattr(sec, "n_glob", 1)
+    rec = 8 + 4 * max(ng, 1)  # a prefix: its key and its running global sums
+    parents = [1] + list(sec.level_sizes[:-1])
+    # every level reads its parents twice (count, fill) and writes its survivors
+    enum_bytes = sum(2 * p * rec + c * rec for p, c in zip(parents, sec.level_sizes))
+    mat = m.H.mat
+    n, nnz = mat.n, mat.nnz
+    # compulsory assembly bytes: sector keys in; canonical CSR (rowptr, cols,
+    # f64 values), f64 diagonal and the diagonal-present bytes out
+    asm_bytes = 8 * n + 8 * (n + 1) + nnz * (4 + 8) + 8 * n + n
+    sec_ms, asm_ms = 1e3 * float(np.median(ts_sec)), 1e3 * float(np.median(ts_asm))
+    return {
+        "sector_enumeration": {"ms": sec_ms, "levels": len(sec.level_sizes), "algorithmic_bytes": int(enum_bytes),
+                               "GBps": enum_bytes / (sec_ms * 1e-3) / 1e9,
+                               "includes": "model construction (operator tables) + level-by-level enumeration, "
+                                           "one host read of each level's size"},
+        "assembly": {"ms": asm_ms, "raw_entries": int(getattr(mat, "raw_entries", 0)), "nnz": nnz,
+                     "algorithmic_bytes": int(asm_bytes), "GBps": asm_bytes / (asm_ms * 1e-3) / 1e9,
+                     "includes": "build_Hamiltonian(g^2=1): term tables, count, scan, fill (key search per "
+                                 "transition), per-row merge, compaction"},
+    }
 
 
 def run_edgpu(args, world, rank, local):
@@ -200,6 +272,8 @@ def run_edgpu(args, world, rank, local):
 
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
+    # ---------------- setup phases, timed on their own -----------------------
+    phases_setup = setup_phases(dev)
     # ---------------- setup (untimed): sector, assembly, f32 copies ----------
     model = SU2_Model(**model_kwargs(), device=dev)
     diags = []
@@ -217,9 +291,9 @@ def run_edgpu(args, world, rank, local):
     def ev():
         return torch.cuda.Event(enable_timing=True)
 
-    from edgpu.solvers import tune_spmv_group as _tune
+    from edgpu.solvers import tune_spmv_group
 
-    g64s = args.spmv_group or _tune(mat, 1, 0, vals=mat.vals)
+    g64s = args.spmv_group or tune_spmv_group(mat, 1, 0, vals=mat.vals)
     # ---------------- plain FP64 GPU path: three sequential solves -----------
     e64 = []
     t64 = []
@@ -244,8 +318,6 @@ def run_edgpu(args, world, rank, local):
     fp64_ms = float(np.sum(t64))
 
     # ---------------- mixed batched: warm-up + timed steps --------------------
-    from edgpu.solvers import tune_spmv_group
-
     # matvec threads-per-row: the autotuner's choice (or --spmv-group), fixed
     # before the timed region
     g32 = args.spmv_group or tune_spmv_group(mat, 3, 1, vals=vals32)
@@ -309,7 +381,7 @@ def run_edgpu(args, world, rank, local):
     # ---------------- e2e through the public API with host inputs ------------
     e2e_ms = []
     d2h = h2d = 0
-    for it in range(min(args.steps, 2) + 1):
+    for it in range(args.steps + 1):
         barrier(world)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -318,11 +390,11 @@ def run_edgpu(args, world, rank, local):
         for g in SWEEP:
             m2.build_Hamiltonian(g, MASS)
             dg.append(m2.H.mat.diag.clone())
-        r64, _ = lanczos_mixed(m2.H.mat, diags=dg)
-        gs_host = torch.empty(r64.evecs[0].shape, dtype=r64.evecs[0].dtype, pin_memory=True)
-        gs_host.copy_(r64.evecs[0])  # ground states to pinned host memory
+        r64e, _ = lanczos_mixed(m2.H.mat, diags=dg)
+        gs_host = torch.empty(r64e.evecs[0].shape, dtype=r64e.evecs[0].dtype, pin_memory=True)
+        gs_host.copy_(r64e.evecs[0])  # ground states to pinned host memory
         gs = gs_host.numpy()
-        energies = r64.evals[:, 0] / L
+        energies = r64e.evals[:, 0] / L
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
         if it > 0:  # first iteration warms the host-side caches
@@ -339,14 +411,17 @@ def run_edgpu(args, world, rank, local):
     # ---------------- CPU baseline (rank 0, bounded sample) ------------------
     cpu = None
     if rank == 0 and not args.no_cpu:
-        from oracle import port as PT
-
-        cpu_pipeline_one(1.0)  # warm caches
-        t, e_cpu = cpu_pipeline_one(1.0)
-        cpu = {"value": 1.0 / t, "unit": UNIT, "cores": PT.threads(), "kind": "port",
-               "sample": "full CPU pipeline (sector, triplets, ARPACK eigsh with a multithreaded CSR matvec) "
-                         "for the g^2=1 coupling only",
-               "seconds": t, "energy_matches_gpu": bool(abs(e_cpu - e64[1]) < 1e-8 * abs(e64[1]))}
+        # the format trial of the stock runner: one full pipeline per matvec
+        # format; the faster one is the sample
+        res = stock_reference(0, 1, fmt="auto", couplings=(1.0,))
+        st0 = min(res["format_trials"], key=lambda t: t["total_s"])
+        cpu = {"value": 1.0 / st0["total_s"], "unit": UNIT, "cores": res["threads"], "kind": "reference",
+               "cpu_model": res.get("cpu_model"),
+               "sample": "one ground state (g^2=1) through the unmodified ed-lgt model API: SU2_Model(...) sector, "
+                         f"build_Hamiltonian, diagonalize_Hamiltonian(1, '{st0['format']}') (the faster of its "
+                         "'linear' and 'sparse' formats, both run)",
+               "phases_s": {k: st0[k] for k in ("sector_s", "assembly_s", "solve_s")},
+               "energy_matches_gpu": bool(abs(st0["energy_density"] * L - e64[1]) < 1e-8 * abs(e64[1]))}
     if rank != 0:
         return
     launches = int(agg32[3] + agg64[3]) // max(args.steps, 1) + 1  # + the f32->f64 start-vector conversion
@@ -369,11 +444,14 @@ def run_edgpu(args, world, rank, local):
         "fp64_gpu": {"ms_per_sweep": fp64_ms, "speedup_mixed_vs_fp64": fp64_ms / ms,
                      "steps_total": int(stats_fp64[4]), "spmv_ms": fp64_spmv_ms,
                      "spmv_GBps": fp64_spmv_bytes / (fp64_spmv_ms * 1e-3) / 1e9},
-        "accuracy": {"max_rel_dE_vs_fp64": rel, "f32_lanczos_steps": iters32, "target": 1e-9, "energies_per_site": [float(x) / L for x in emix]},
+        "accuracy": {"max_rel_dE_vs_fp64": rel, "f32_lanczos_steps": iters32, "target": 1e-9,
+                     "energies_per_site": [float(x) / L for x in emix]},
         "phases_ms_per_step": {"f32_matvec": agg32[0] / args.steps, "f32_reorth": agg32[2] / args.steps,
-                               "f32_checks": agg32[5] / args.steps, "f64_refine_total": 0.0,
-                               "f32_steps": agg32[4] / args.steps, "f64_matvec": agg64[0] / args.steps,
-                               "f64_reorth": agg64[2] / args.steps},
+                               "f32_checks": agg32[5] / args.steps, "f32_steps": agg32[4] / args.steps,
+                               "f64_refine_total": (agg64[0] + agg64[2] + agg64[5]) / args.steps,
+                               "f64_matvec": agg64[0] / args.steps, "f64_reorth": agg64[2] / args.steps,
+                               "f64_checks": agg64[5] / args.steps, "f64_steps": agg64[4] / args.steps},
+        "setup_phases": phases_setup,
         "roofline": {"kernel": "f32 delayed Gram-Schmidt reorthogonalisation (dots2_k<float,3> + "
                                "dcgs_update_k<float,3> + scale_store_k, two reads of the basis per Lanczos step)",
                      "bound": "hbm",
@@ -385,7 +463,7 @@ def run_edgpu(args, world, rank, local):
                             "frac": spmv_achieved / hbm, "peak_source": peak_kind,
                             "algorithmic_bytes_per_launch": spmv_bytes, "avg_launch_ms": spmv_ms, "traffic": None},
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-                "ms_per_step": float(np.mean(e2e_ms))},
+                "ms_per_step": float(np.mean(e2e_ms)), "steps": len(e2e_ms)},
         "gpu_launches": launches,
         "clocks": clk,
         "cpu_baseline": cpu,
@@ -913,11 +991,12 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+        return
     world, rank, local = dist_setup(args.gpus)
     try:
-        if args.impl == "reference":
-            run_reference(args, world, rank)
-        elif args.workload == "batch":
+        if args.workload == "batch":
             run_batch(args, world, rank, local)
         elif args.workload == "quench":
             run_quench(args, world, rank, local)

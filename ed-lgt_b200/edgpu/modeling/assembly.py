@@ -312,4 +312,5 @@ def assemble_blocks(sector, blocks, phase_weights=None, force_complex=False, ext
     mat = DeviceMatrix(n, rowptr, cols[:nnz], vals[: nnz * w], diag, present[:n], is_complex,
                        phase_weights if (use_real and phase_weights is not None) else None)
     mat._keep = keep
+    mat.raw_entries = total  # generated entries before the per-row merge
     return mat

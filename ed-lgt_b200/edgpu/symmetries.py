@@ -393,6 +393,7 @@ def enumerate_sector(spec: SectorSpec, device=None) -> Sector:
     prev_keys = torch.zeros(1, dtype=torch.int64, device=device)
     prev_sums = torch.zeros(max(ng, 1), dtype=torch.int32, device=device)
     n_prev = 1
+    level_sizes = []
     for depth in range(spec.n_sites):
         n_cand = n_prev * int(spec.loc_dims[depth])
         nb = lib.edg_sector_level_blocks(n_cand)
@@ -407,10 +408,14 @@ def enumerate_sector(spec: SectorSpec, device=None) -> Sector:
             check(lib.edg_sector_level_fill(C_ref(tables.struct), depth, ptr(prev_keys), ptr(prev_sums), n_prev,
                                             ptr(offsets), ptr(next_keys), ptr(next_sums), st), "edg_sector_level_fill")
         prev_keys, prev_sums, n_prev = next_keys, next_sums, total
+        level_sizes.append(total)
         if total == 0:
             break
     keys = prev_keys[:n_prev].clone()
-    return Sector(keys, spec.loc_dims, device)
+    sector = Sector(keys, spec.loc_dims, device)
+    sector.level_sizes = level_sizes  # surviving prefixes per depth
+    sector.n_glob = ng
+    return sector
 
 
 def C_ref(struct):

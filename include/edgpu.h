@@ -297,7 +297,10 @@ int edg_tridiag_lowest(const double* alpha, const double* beta, int32_t m,
  * looks up the array's device address (with that device current); make that
  * first call before any stream capture.  All calls share the one array:
  * calls that overlap on the GPU race, so serialise them (one stream, or
- * events).  Inputs and outputs are caller-owned device pointers. */
+ * events).  Inputs and outputs are caller-owned device pointers.  The
+ * address is cached per device for the life of the process: a device reset
+ * (cudaDeviceReset, or destroying the primary context) between calls is not
+ * supported. */
 int edg_tridiag_lowest_noalloc(const double* alpha, const double* beta,
                                int32_t m, int32_t k, double* evals,
                                double* evecs, cudaStream_t stream);

@@ -3,7 +3,7 @@
 Used only by make_golden.py to produce fixtures.  It stubs the modules the
 reference imports but that are absent here (matplotlib and two edlgt.tools
 submodules that are not in the snapshot), without touching the reference
-tree.  Set EDLGT_PATH to the reference checkout (default /root/reference).
+tree.  Set EDLGT_PATH to the reference checkout (required).
 """
 
 import os
@@ -38,4 +38,6 @@ for _n in ("edlgt.tools.wannier", "edlgt.tools.tensor_networks"):
     _m = types.ModuleType(_n)
     _m.__all__ = []
     sys.modules[_n] = _m
-sys.path.insert(0, os.environ.get("EDLGT_PATH", "/root/reference"))
+if "EDLGT_PATH" not in os.environ:
+    raise SystemExit("set EDLGT_PATH to an ed-lgt checkout (the directory that holds the edlgt package)")
+sys.path.insert(0, os.environ["EDLGT_PATH"])

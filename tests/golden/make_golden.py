@@ -1,7 +1,7 @@
 """Generate golden fixtures by running ed-lgt (the reference) itself.
 
-Run in a container that has the reference checkout (EDLGT_PATH, default
-/root/reference) and numba/scipy/sympy:
+Run in a container that has the reference checkout (EDLGT_PATH, required)
+and numba/scipy/sympy:
 
     python tests/golden/make_golden.py [group ...]
 
