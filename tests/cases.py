@@ -123,3 +123,20 @@ INTEGRATED_CASES = {
     "qedint_L8_bg": ([8], [1, 0, 0, 0, 0, 0, 0, -1], 1.0, 0.5),
     "qedint_L10": ([10], None, 0.8, 1.2),
 }
+
+
+# ---------------------------------------------------------------------------
+# string (site-resolved) constraint cases, stored with every input of the
+# reference's symmetry_sector_configs call (tests/golden/string_cases.npz)
+def string_case_names(golden):
+    return sorted({k.split("/")[0] for k in golden.files})
+
+
+def string_case_inputs(golden, name):
+    """Keyword inputs of a string case, in the reference's argument names."""
+    pairs = [golden[f"{name}/pairs{d}"] for d in range(int(golden[f"{name}/n_dirs"]))]
+    return dict(loc_dims=golden[f"{name}/loc_dims"], glob_op_diags=golden[f"{name}/glob_diags"],
+                glob_sectors=golden[f"{name}/glob_sectors"], sym_type_flag="U",
+                link_op_diags=golden[f"{name}/link_diags"], link_sectors=golden[f"{name}/link_sectors"],
+                pair_list=pairs, string_op_diags=golden[f"{name}/string_diags"],
+                string_sectors=golden[f"{name}/string_sectors"])

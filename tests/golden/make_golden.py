@@ -6,7 +6,7 @@ and numba/scipy/sympy:
     python tests/golden/make_golden.py [group ...]
 
 Groups: small, pins, dynamics, big, twobody, entropy, momentum, full,
-nbody, overlap, state, local, integrated.  Output: .npz files next to
+nbody, overlap, state, local, integrated, string.  Output: .npz files next to
 this script.  Nothing here is imported by the library or by the GPU tests;
 the tests only read the .npz files.
 
@@ -562,9 +562,94 @@ def gen_full():
     np.savez_compressed(os.path.join(HERE, "full_spectrum_cases.npz"), **out)
 
 
+def _parity_string(s, k):
+    return float(s % 2)
+
+
+def _dyadic_string(s, k):
+    return 0.25 * ((s + k) % 3)
+
+
+def gen_string():
+    """String (site-resolved background) constraints: the reference's
+    symmetry_sector_configs with string_op_diags/string_sectors, which
+    dispatches to iterative_sitebased_sym_sector_configs1
+    (edlgt/symmetries/symmetry_sector.py:68-145, 970-1164).  Every input of
+    the call is stored with the resulting sorted keys, so the test pins the
+    builder directly.  String diagonals are model operators or synthetic
+    per-site functions of the local state (any real diagonal is a valid
+    input); targets are read off a configuration of the sector without
+    strings, so the sector contains it.  One case has an infeasible target
+    and an empty result."""
+    from edlgt.modeling.lattice_geometry import get_lattice_link_site_pairs
+    from edlgt.symmetries import get_symmetry_sector_generators, symmetry_sector_configs
+
+    qed1 = (QED_Model, dict(spin=1, pure_theory=False, lvals=[8], has_obc=[True]), "N", 4, "E")
+    qed32 = (QED_Model, dict(spin=1, pure_theory=False, lvals=[3, 2], has_obc=[True, True]), "N", 3, "E")
+    qed42 = (QED_Model, dict(spin=1, pure_theory=False, lvals=[4, 2], has_obc=[True, True]), "N", 4, "E")
+    su8p = (SU2_Model, dict(spin=0.5, pure_theory=False, lvals=[8], has_obc=[False], sectors=[8]), "N_tot", 8, "T2")
+    su10 = (SU2_Model, dict(spin=0.5, pure_theory=False, lvals=[10], has_obc=[True], sectors=[10]), "N_tot", 10, "T2")
+    su12 = (SU2_Model, dict(spin=0.5, pure_theory=False, lvals=[12], has_obc=[True], sectors=[12]), "N_tot", 12, "T2")
+    cases = {
+        "qed1d_L8_N_E2": (qed1, ["N", "E2_px"], 0.61),
+        "qed2d_3x2_N": (qed32, ["N"], 0.5),
+        "qed2d_4x2_N": (qed42, ["N"], 0.5),
+        "qed2d_4x2_dyadic": (qed42, [_dyadic_string], 0.4),
+        "su2_L8_pbc_Ntot_T2": (su8p, ["N_tot", "T2_px"], 0.7),
+        "su2_L10_Npair": (su10, ["N_pair"], 0.45),
+        "su2_L12_parity": (su12, [_parity_string], 0.4),
+        "qed1d_L8_empty": (qed1, ["N"], None),
+    }
+    out = {}
+    for name, ((cls, kw, gop, gsec, lname), sops, frac) in cases.items():
+        m = cls(**kw)
+        link_ops = [[m.ops[f"{lname}_p{d}"], -m.ops[f"{lname}_m{d}"]] for d in m.directions]
+        gd = get_symmetry_sector_generators([m.ops[gop]], action="global")
+        ld = get_symmetry_sector_generators(link_ops, action="link")
+        pairs = get_lattice_link_site_pairs(m.lvals, m.has_obc)
+        gs = np.array([gsec], dtype=float)
+        lsec = [0 for _ in m.directions]
+        base = symmetry_sector_configs(loc_dims=m.loc_dims, glob_op_diags=gd, glob_sectors=gs, sym_type_flag="U",
+                                       link_op_diags=ld, link_sectors=lsec, pair_list=pairs)
+        n_sites, dmax = gd.shape[1], gd.shape[2]
+        rows = []
+        for o in sops:
+            if isinstance(o, str):
+                rows.append(get_symmetry_sector_generators([m.ops[o]], action="global")[0])
+            else:
+                rows.append(np.array([[o(st, k) for st in range(dmax)] for k in range(n_sites)], dtype=float))
+        sd = np.stack(rows)
+        if frac is None:
+            # every site occupied: infeasible with the global sector
+            targets = np.ones((len(sops), n_sites))
+        else:
+            c = np.asarray(base[int(frac * (len(base) - 1))], dtype=np.int64)
+            targets = np.array([[sd[k, s, c[s]] for s in range(n_sites)] for k in range(len(sops))])
+        cfg = symmetry_sector_configs(loc_dims=m.loc_dims, glob_op_diags=gd, glob_sectors=gs, sym_type_flag="U",
+                                      link_op_diags=ld, link_sectors=lsec, pair_list=pairs, string_op_diags=sd,
+                                      string_sectors=targets)
+        cfg = np.zeros((0, n_sites), dtype=np.uint16) if cfg is None else np.asarray(cfg)
+        out[f"{name}/loc_dims"] = np.asarray(m.loc_dims, dtype=np.int64)
+        out[f"{name}/glob_diags"] = np.asarray(gd)
+        out[f"{name}/glob_sectors"] = gs
+        out[f"{name}/link_diags"] = np.asarray(ld)
+        out[f"{name}/link_sectors"] = np.asarray(lsec, dtype=float)
+        out[f"{name}/n_dirs"] = np.int64(len(pairs))
+        for d, pl in enumerate(pairs):
+            out[f"{name}/pairs{d}"] = np.asarray(pl, dtype=np.int64)
+        out[f"{name}/string_diags"] = sd
+        out[f"{name}/string_sectors"] = targets
+        out[f"{name}/keys"] = keys_of(cfg, m.loc_dims) if len(cfg) else np.zeros(0, dtype=np.uint64)
+        out[f"{name}/base_dim"] = np.int64(len(base))
+        print(name, len(base), "->", len(cfg), flush=True)
+    np.savez_compressed(os.path.join(HERE, "string_cases.npz"), **out)
+
+
 if __name__ == "__main__":
     groups = sys.argv[1:] or ["small", "pins", "dynamics", "big", "twobody", "entropy", "momentum", "full", "nbody",
-                             "overlap", "state", "local", "integrated"]
+                             "overlap", "state", "local", "integrated", "string"]
+    if "string" in groups:
+        gen_string()
     if "integrated" in groups:
         gen_integrated()
     if "local" in groups:

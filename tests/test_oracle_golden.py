@@ -250,3 +250,20 @@ def test_integrated_e2_reconstruction():
     field = np.cumsum(q + 0.5 * ((-1.0) ** k - 1.0) + n_site, axis=1)[:, :-1]
     assert np.allclose(e2, p @ field ** 2, atol=1e-12)
     assert abs(model.res["E2_avg"] - np.mean(e2)) <= 1e-15
+
+
+def test_string_constraint_sectors_oracle(golden_string):
+    """Site-resolved string constraints (the reference's
+    iterative_sitebased_sym_sector_configs1): the oracle reproduces the
+    reference's keys from the same inputs, including the empty sector."""
+    from cases import string_case_inputs, string_case_names
+
+    names = string_case_names(golden_string)
+    assert len(names) >= 8
+    for name in names:
+        a = string_case_inputs(golden_string, name)
+        cfg = O.sector_configs(a["loc_dims"], a["glob_op_diags"], a["glob_sectors"], "U", a["link_op_diags"],
+                               a["link_sectors"], a["pair_list"], a["string_op_diags"], a["string_sectors"])
+        keys = O.keys_of(cfg, a["loc_dims"]) if len(cfg) else np.zeros(0, dtype=np.uint64)
+        assert np.array_equal(keys, golden_string[f"{name}/keys"]), name
+        assert len(keys) <= int(golden_string[f"{name}/base_dim"])
