@@ -8,7 +8,8 @@ build_Hamiltonian -> diagonalize / time_evolution).
 """
 
 from . import _lib  # noqa: F401  (loads libedgpu.so; fails loudly if it is missing)
+from .context import Context, default_context
 from .models import QED_Model, QuantumModel, SU2_Model
 
-__all__ = ["QED_Model", "SU2_Model", "QuantumModel"]
+__all__ = ["QED_Model", "SU2_Model", "QuantumModel", "Context", "default_context"]
 __version__ = "0.1.0"

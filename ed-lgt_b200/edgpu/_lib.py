@@ -29,6 +29,7 @@ STATUS_NAMES = {
     -4: "EDG_ERR_MISSING_KET",
     -5: "EDG_ERR_NOT_CONVERGED",
     -6: "EDG_ERR_BREAKDOWN",
+    -7: "EDG_ERR_TIMEOUT",
 }
 
 
@@ -174,6 +175,35 @@ class SmallBatch(C.Structure):
     ]
 
 
+class TiledBatch(C.Structure):
+    _fields_ = [
+        ("dtype", I32),
+        ("n_inst", I32),
+        ("n_items", I32),
+        ("tile_rows", I32),
+        ("lanes", I32),
+        ("k", I32),
+        ("max_iter", I32),
+        ("reserved", I32),
+        ("tol", F64),
+        ("seed", U64),
+        ("inst", P),
+        ("item_inst", P),
+        ("check_at", P),
+        ("rowptr", P),
+        ("cols", P),
+        ("vals", P),
+        ("diag", P),
+        ("v0", P),
+        ("workspace", P),
+        ("evals", P),
+        ("resid", P),
+        ("iters", P),
+        ("evecs", P),
+        ("status", P),
+    ]
+
+
 class ZnTranslation(C.Structure):
     _fields_ = [
         ("sf", I32), ("sx", I32), ("sm", I32), ("smx", I32),
@@ -255,6 +285,14 @@ _SIGS = {
     "edg_local_expval": (I32, [P, I64, C.POINTER(SiteDims), I32, P, I32, I64, P, I32, P, P]),
     "edg_small_batch_work_elems": (I64, [I64, I32, I32]),
     "edg_lanczos_small_batched": (I32, [C.POINTER(SmallBatch), P, P]),
+    "edg_ctx_create": (P, []),
+    "edg_ctx_destroy": (None, [P]),
+    "edg_ctx_put": (I32, [P, U64, P, I32]),
+    "edg_ctx_get": (I32, [P, U64, P, I32]),
+    "edg_ctx_size": (I64, [P]),
+    "edg_tiled_batch_plan": (I32, [I32, P, I32, I32, I32, I32, I32, P, P, P, P, P]),
+    "edg_tiled_batch_header_bytes": (I32, [I32]),
+    "edg_lanczos_tiled_batch": (I32, [C.POINTER(TiledBatch), P]),
     "edg_krylov_workspace_bytes": (I64, [C.POINTER(KrylovProblem)]),
     "edg_krylov_step": (I32, [C.POINTER(KrylovProblem), P, F64, P, I64, P, P]),
     "edg_twobody_scratch_elems": (I64, [I32]),

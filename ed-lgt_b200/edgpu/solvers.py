@@ -25,30 +25,33 @@ from ._lib import check, lib, ptr, stream_handle
 __all__ = ["LanczosResult", "lanczos", "lanczos_mixed", "stack_diagonals", "tune_spmv_group"]
 
 SPMV_GROUPS = (2, 4, 8, 16, 32)
-_TUNED_BY_SHAPE = {}  # (n, nnz, dtype, nvec, device) -> threads per row
 
 
-def tune_spmv_group(mat, nvec=1, dtype=0, reps=5, vals=None, diag=None):
+def _spmv_key(n, nnz, dtype, nvec):
+    h = 1469598103934665603
+    for x in (0x5350, n, nnz, dtype, nvec):  # 0x5350: the matvec tuner's tag
+        h = ((h ^ (int(x) & 0xFFFFFFFFFFFFFFFF)) * 1099511628211) & 0xFFFFFFFFFFFFFFFF
+    return h
+
+
+def tune_spmv_group(mat, nvec=1, dtype=0, reps=5, vals=None, diag=None, ctx=None):
     """Autotuner: threads per matvec row that is fastest on this matrix.
 
     Times ``edg_spmv_group`` for every group size with CUDA events (after one
     warm-up launch each) on the real matrix and the requested precision and
-    batch width; the choice is cached on the matrix object and, for the rest
-    of the process, for every matrix of the same shape (a performance choice
-    only: every group size gives the same result).
+    batch width.  The choice is kept in the tuning context ``ctx`` (an
+    :class:`edgpu.Context`; the device's default context when None) under the
+    matrix shape (n, nnz), precision and batch width, so later matrices of the
+    same shape reuse it (a performance choice only: every group size gives the
+    same result).
     """
-    key = (dtype, nvec)
-    cache = getattr(mat, "_tuned_groups", None)
-    if cache is None:
-        cache = mat._tuned_groups = {}
-    if key in cache:
-        return cache[key]
-    # a matrix of the same shape (n, nnz) was tuned before in this process:
-    # the choice depends on the sparsity structure only, reuse it
-    shape_key = (mat.n, mat.nnz, dtype, nvec, mat.rowptr.device.index)
-    if shape_key in _TUNED_BY_SHAPE:
-        cache[key] = _TUNED_BY_SHAPE[shape_key]
-        return cache[key]
+    from .context import default_context
+
+    ctx = ctx if ctx is not None else default_context(mat.rowptr.device)
+    key = _spmv_key(mat.n, mat.nnz, dtype, nvec)
+    got = ctx.get(key, 1)
+    if got is not None:
+        return got[0]
     dev = mat.rowptr.device
     tdt = {0: torch.float64, 1: torch.float32}[dtype]
     if vals is None:
@@ -73,8 +76,7 @@ def tune_spmv_group(mat, nvec=1, dtype=0, reps=5, vals=None, diag=None):
         t = a.elapsed_time(b) / reps
         if t < best_t:
             best, best_t = g, t
-    cache[key] = best
-    _TUNED_BY_SHAPE[shape_key] = best
+    ctx.put(key, (best,))
     return best
 
 

@@ -34,6 +34,8 @@ extern "C" {
 #define EDG_ERR_MISSING_KET -4  /* an operator maps a sector state outside it */
 #define EDG_ERR_NOT_CONVERGED -5
 #define EDG_ERR_BREAKDOWN -6    /* Krylov space exhausted before convergence  */
+#define EDG_ERR_TIMEOUT -7      /* a grid-wide wait of a persistent kernel    */
+                                /* ran out (the launch returned early)        */
 
 #define EDG_MAX_OPS 4           /* max operator factors of one term instance  */
 #define EDG_MAX_SITES 64        /* max lattice sites of one configuration     */
@@ -46,6 +48,28 @@ extern "C" {
 int edg_get_last_error(char* buf, int len);
 /* ABI version (major * 100 + minor). */
 int edg_version(void);
+
+/* ------------------------------------------------------------------------ */
+/* Tuning context (no counterpart in the reference, which has no autotuner). */
+/* Autotuners store their launch-shape choices here, keyed by a hash of the  */
+/* problem shape; the caller creates, passes and destroys the context, so    */
+/* the library holds no global tuning state.  Thread-safe.                   */
+/* ------------------------------------------------------------------------ */
+
+#define EDG_CTX_MAX_PARAMS 8
+typedef struct edg_ctx edg_ctx;
+
+/* NULL when out of host memory. */
+edg_ctx* edg_ctx_create(void);
+void edg_ctx_destroy(edg_ctx* ctx);
+/* Stores n_params (1..EDG_CTX_MAX_PARAMS) int32 values under key. */
+int edg_ctx_put(edg_ctx* ctx, uint64_t key, const int32_t* params,
+                int32_t n_params);
+/* Copies up to n_params values stored under key; returns how many (0 when
+ * the key is absent) or a negative status. */
+int edg_ctx_get(edg_ctx* ctx, uint64_t key, int32_t* params, int32_t n_params);
+/* Number of stored keys (-1 for a null context). */
+int64_t edg_ctx_size(edg_ctx* ctx);
 
 /* ------------------------------------------------------------------------ */
 /* Exclusive prefix sum of int64 counts (the two-pass count/scan/fill idiom  */
@@ -304,6 +328,70 @@ int edg_tridiag_lowest(const double* alpha, const double* beta, int32_t m,
 int edg_tridiag_lowest_noalloc(const double* alpha, const double* beta,
                                int32_t m, int32_t k, double* evals,
                                double* evecs, cudaStream_t stream);
+
+/* ------------------------------------------------------------------------ */
+/* Batched Lanczos over an (instance, row-tile) work queue: instances of any */
+/* dimension (charge sectors, coupling sweeps, lattice sizes) in one         */
+/* persistent cooperative launch.  Every phase of a Lanczos step (matvec,    */
+/* dots, coefficients, update, convergence check) walks the list of          */
+/* (instance, tile of tile_rows rows) items; phases are separated by         */
+/* grid-wide barriers, so one instance spreads over many CTAs and small      */
+/* instances share the grid.  Replaces the sequential loop of eigsh calls of */
+/* QMB_hamiltonian.diagonalize (edlgt/modeling/qmb_hamiltonian.py:260-332)   */
+/* over a sweep of instances.  dtype 1 keeps the Krylov basis and matvec     */
+/* operands in f32 (dots, recurrence, reorthogonalisation coefficients and   */
+/* the tridiagonal eigen-solve in f64); dtype 0 is f64 throughout.  The      */
+/* launch does no host synchronisation and no allocation, so a whole solve   */
+/* can be recorded in a CUDA graph.                                          */
+/* ------------------------------------------------------------------------ */
+
+#define EDG_TB_FIELDS 8  /* int64 fields per instance in the plan table   */
+
+typedef struct {
+  int32_t dtype;              /* 0: f64 vectors and matvec; 1: f32          */
+  int32_t n_inst;
+  int32_t n_items;            /* from edg_tiled_batch_plan                  */
+  int32_t tile_rows;          /* rows per work item (multiple of 4)         */
+  int32_t lanes;              /* threads per matrix row: 2, 4, 8, 16, 32    */
+  int32_t k;                  /* lowest eigenpairs per instance (1..8)      */
+  int32_t max_iter;           /* Krylov steps at most (<= 2000)             */
+  int32_t reserved;
+  double tol;                 /* |beta_m s_q(m)| <= tol * max(1, |theta_q|) */
+  uint64_t seed;              /* random start vectors when v0 is NULL       */
+  const int64_t* inst;        /* [n_inst][EDG_TB_FIELDS] plan table         */
+  const int32_t* item_inst;   /* [n_items] instance of each item            */
+  const uint8_t* check_at;    /* [max_iter] 1 = check after that step       */
+  const int64_t* rowptr;      /* per-instance rowptr blocks, concatenated;  */
+                              /* entries index the concatenated cols/vals   */
+  const int32_t* cols;        /* instance-local columns                     */
+  const void* vals;           /* off-diagonal values, f64 or f32 (dtype)    */
+  const void* diag;           /* diagonals concatenated [sum dims] (dtype)  */
+  const double* v0;           /* start vectors concatenated (f64) or NULL   */
+  void* workspace;            /* plan's byte count, 256-byte aligned        */
+  double* evals;              /* [n_inst][k] (NaN where never checked)      */
+  double* resid;              /* [n_inst][k] residual bounds                */
+  int32_t* iters;             /* [n_inst] Krylov dimension used             */
+  double* evecs;              /* ground-state vectors concatenated (f64,    */
+                              /* normalised) or NULL                        */
+  int32_t* status;            /* device word: EDG_OK or EDG_ERR_TIMEOUT     */
+} edg_tiled_batch;
+
+/* Host-side plan: per-instance table (dims in rows), the item list, the
+ * convergence-check schedule (every check_every steps, the last step, and
+ * each instance's Krylov cap min(dim, max_iter)), the item count and the
+ * workspace size.  inst_out / item_inst_out / check_at_out may be NULL
+ * (query).  All pointers are host memory. */
+int edg_tiled_batch_plan(int32_t n_inst, const int64_t* dims, int32_t dtype,
+                         int32_t max_iter, int32_t k, int32_t tile_rows,
+                         int32_t check_every, int64_t* inst_out,
+                         int32_t* item_inst_out, uint8_t* check_at_out,
+                         int32_t* n_items_out, int64_t* workspace_bytes_out);
+/* Bytes at the start of the workspace that every launch resets. */
+int edg_tiled_batch_header_bytes(int32_t n_inst);
+/* One solve: resets the workspace header, one cooperative launch, copies the
+ * launch status to b->status.  Asynchronous; converged instances leave the
+ * queue, an unconverged one stops at its cap with its residual reported. */
+int edg_lanczos_tiled_batch(const edg_tiled_batch* b, cudaStream_t stream);
 
 /* ------------------------------------------------------------------------ */
 /* Batched Lanczos for many small instances (charge sectors, coupling        */

@@ -62,10 +62,10 @@ def test_struct_layouts_match_header():
 #include <stdio.h>
 #include "edgpu.h"
 int main(void) {
-  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(edg_sector_tables), sizeof(edg_lookup_table),
+  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(edg_sector_tables), sizeof(edg_lookup_table),
          sizeof(edg_assembly), sizeof(edg_lanczos_problem), sizeof(edg_site_dims), sizeof(edg_krylov_problem),
          sizeof(edg_small_batch), sizeof(edg_zn_translation), sizeof(edg_zn_lattice), sizeof(edg_zn_basis),
-         sizeof(edg_part_spec), sizeof(edg_momentum_group));
+         sizeof(edg_part_spec), sizeof(edg_momentum_group), sizeof(edg_tiled_batch));
   return 0;
 }
 '''
@@ -82,4 +82,62 @@ int main(void) {
                      ctypes.sizeof(_lib.LanczosProblem), ctypes.sizeof(_lib.SiteDims),
                      ctypes.sizeof(_lib.KrylovProblem), ctypes.sizeof(_lib.SmallBatch),
                      ctypes.sizeof(_lib.ZnTranslation), ctypes.sizeof(_lib.ZnLattice), ctypes.sizeof(_lib.ZnBasis),
-                     ctypes.sizeof(_lib.PartSpec), ctypes.sizeof(_lib.MomentumGroup)]
+                     ctypes.sizeof(_lib.PartSpec), ctypes.sizeof(_lib.MomentumGroup),
+                     ctypes.sizeof(_lib.TiledBatch)]
+
+
+def test_tuning_context_roundtrip():
+    """edg_ctx: an explicit, caller-owned store of tuning choices."""
+    from edgpu.context import Context
+
+    a, b = Context(), Context()
+    assert len(a) == 0 and a.get(7, 2) is None
+    a.put(7, (512, 8))
+    a.put(2**64 - 1, (3,))
+    assert a.get(7, 2) == (512, 8)
+    assert a.get(7, 1) == (512,)
+    assert a.get(2**64 - 1, 4) == (3,)
+    assert len(a) == 2 and len(b) == 0  # no shared state between contexts
+    from edgpu import _lib
+
+    assert _lib.lib.edg_ctx_put(a.handle, 1, None, 0) == -1
+    assert _lib.lib.edg_ctx_size(None) == -1
+
+
+def test_tiled_batch_plan():
+    """Host-side plan of the (instance, row-tile) batched solver: tiles,
+    items, Krylov caps, check schedule and workspace size."""
+    import numpy as np
+
+    from edgpu import _lib
+
+    dims = np.array([26, 90, 5, 1000, 4096], dtype=np.int64)
+    n_items, wb = ctypes.c_int32(0), ctypes.c_int64(0)
+    inst = np.zeros((5, 8), dtype=np.int64)
+    items = np.zeros(64, dtype=np.int32)
+    chk = np.zeros(120, dtype=np.uint8)
+    st = _lib.lib.edg_tiled_batch_plan(5, dims.ctypes.data, 1, 120, 1, 256, 8, inst.ctypes.data, items.ctypes.data,
+                                       chk.ctypes.data, ctypes.byref(n_items), ctypes.byref(wb))
+    assert st == 0
+    pad = (dims + 3) // 4 * 4
+    tiles = (pad + 255) // 256
+    assert np.array_equal(inst[:, 0], dims)                                   # dim
+    assert np.array_equal(inst[:, 1], np.concatenate([[0], np.cumsum(dims)[:-1]]))          # row offset
+    assert np.array_equal(inst[:, 2], np.concatenate([[0], np.cumsum(dims + 1)[:-1]]))      # rowptr offset
+    assert np.array_equal(inst[:, 5], tiles)
+    assert np.array_equal(inst[:, 6], np.concatenate([[0], np.cumsum(tiles)[:-1]]))
+    assert np.array_equal(inst[:, 7], np.minimum(dims, 120))                  # Krylov cap
+    assert n_items.value == tiles.sum()
+    assert np.array_equal(items[: n_items.value], np.repeat(np.arange(5), tiles))
+    # arenas are 256-byte aligned and disjoint; the V arena of the last
+    # instance ends inside the workspace
+    assert np.all(inst[:, 3] % 256 == 0) and np.all(inst[:, 4] % 256 == 0)
+    assert inst[-1, 3] + (inst[-1, 7] + 1) * pad[-1] * 4 <= wb.value
+    # checks every 8 steps, at the last step and at every instance's cap
+    want = {j for j in range(120) if (j + 1) % 8 == 0} | {119} | {int(c) - 1 for c in inst[:, 7]}
+    assert set(np.nonzero(chk)[0].tolist()) == want
+    # invalid arguments
+    assert _lib.lib.edg_tiled_batch_plan(5, dims.ctypes.data, 1, 120, 1, 250, 8, None, None, None,
+                                         ctypes.byref(n_items), ctypes.byref(wb)) == -1
+    assert _lib.lib.edg_tiled_batch_plan(5, dims.ctypes.data, 1, 120, 9, 256, 8, None, None, None,
+                                         ctypes.byref(n_items), ctypes.byref(wb)) == -1
