@@ -365,13 +365,12 @@ def run_edgpu(args, world, rank, local):
     spmv_bytes = nnz * (4 + 4) + 8 * (n + 1) + n * nv * 4 + n * nv * 8 + n * nv * 4
     spmv_ms = agg32[0] / max(agg32[1], 1)
     spmv_achieved = spmv_bytes / (spmv_ms * 1e-3) / 1e9
-    # reorthogonalisation of step j (delayed Gram-Schmidt), per row of all
-    # problems: dots read V[0..j] (f32) plus u (f32) and w (f64) once per tile
-    # of 8; the update reads V[0..j) and reads and writes u and w; the
-    # normalisation reads w and writes V[j+1] and the matvec input (f32)
+    # reorthogonalisation of step j (delayed Gram-Schmidt), per row of every
+    # problem: the dots read V[0..j] (f32, the candidate u = V[j] among them)
+    # and w (f64) once; the update reads V[0..j) and u, w and writes q_j = V[j]
+    # and w; the normalisation reads w and writes V[j+1] and the matvec input
     steps = int(round(agg32[4] / max(args.steps, 1)))
-    reorth_bytes = sum(n_pad * nv * (4 * (2 * j + 1) + 12 * ((j + 8) // 8) + 2 * 4 + 2 * 8 + 8 + 4 + 4)
-                       for j in range(steps))
+    reorth_bytes = sum(n_pad * nv * (4 * (j + 1) + 8 + 4 * j + 4 + 8 + 4 + 8 + 8 + 4 + 4) for j in range(steps))
     reorth_ms_step = agg32[2] / args.steps
     reorth_achieved = reorth_bytes / (reorth_ms_step * 1e-3) / 1e9
     reorth_ms = agg32[2] / max(agg32[4], 1)
@@ -452,8 +451,8 @@ def run_edgpu(args, world, rank, local):
                                "f64_matvec": agg64[0] / args.steps, "f64_reorth": agg64[2] / args.steps,
                                "f64_checks": agg64[5] / args.steps, "f64_steps": agg64[4] / args.steps},
         "setup_phases": phases_setup,
-        "roofline": {"kernel": "f32 delayed Gram-Schmidt reorthogonalisation (dots2_k<float,3> + "
-                               "dcgs_update_k<float,3> + scale_store_k, two reads of the basis per Lanczos step)",
+        "roofline": {"kernel": "f32 delayed Gram-Schmidt reorthogonalisation (dots_rows_k<float,3> + "
+                               "update_rows_k<float,3> + scale_store_k, two reads of the basis per Lanczos step)",
                      "bound": "hbm",
                      "achieved": reorth_achieved, "peak": hbm, "unit": "GB/s", "frac": reorth_achieved / hbm,
                      "peak_source": peak_kind, "algorithmic_bytes_per_solve": reorth_bytes,

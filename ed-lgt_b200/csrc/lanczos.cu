@@ -53,6 +53,9 @@ __device__ __forceinline__ void ld4(const double* p, double* out) {
   double2 b = *reinterpret_cast<const double2*>(p + 2);
   out[0] = a.x; out[1] = a.y; out[2] = b.x; out[3] = b.y;
 }
+__device__ __forceinline__ void st4(float* p, const double* v) {
+  *reinterpret_cast<float4*>(p) = make_float4((float)v[0], (float)v[1], (float)v[2], (float)v[3]);
+}
 __device__ __forceinline__ void st4(double* p, const double* v) {
   *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
   *reinterpret_cast<double2*>(p + 2) = make_double2(v[2], v[3]);
@@ -149,40 +152,53 @@ __global__ void scale_store_k(const double* __restrict__ w, int64_t n, int64_t n
   }
 }
 
-// partial[bx][i][r][v] over the Krylov tile i in [blockIdx.y*kItile, ...]
-// (i <= j) and the problem v = blockIdx.z: dots of V[i] with the candidate
-// u = V[j] (r = 0) and with w (r = 1).
+// Rows of one work item of the reorthogonalisation kernels: 256 threads x two
+// row quads (8 rows per thread), the quads of a thread 256 apart so that a warp
+// reads contiguous 16-byte segments.
+constexpr int kSubRows = kThreads * 8;
+
+// partial[s][i][r][v] for the row chunk s (kSubRows rows) of problem v (one
+// CTA per (s, v)): dots of V[0..j] with the candidate u = V[j] (r = 0) and
+// with w (r = 1).  u and w of the chunk stay in registers while all j+1
+// Krylov vectors stream through once, eight at a time (16 loads of 16 bytes
+// in flight per thread).
 template <typename T, int NV>
-__global__ void __launch_bounds__(kThreads, 2) dots2_k(const T* __restrict__ V, int64_t n_pad, int j,
-                                                    const double* __restrict__ w, double* __restrict__ partial,
-                                                    int ld_i, int64_t stride_i) {
+__global__ void __launch_bounds__(kThreads, 2) dots_rows_k(const T* __restrict__ V, int64_t n_pad, int j,
+                                                        const double* __restrict__ w, double* __restrict__ partial,
+                                                        int ld_i, int64_t stride_i, int64_t n_sub) {
   __shared__ double red[(kThreads / 32) * kItile * 2];
-  const int i0 = blockIdx.y * kItile;
-  const int nt = min(kItile, j + 1 - i0);
+  const int64_t s = blockIdx.x % n_sub;
+  const int v = (int)(blockIdx.x / n_sub);
   const int64_t nq = n_pad / 4;
-  const int64_t cq = (nq + gridDim.x - 1) / gridDim.x;
-  const int64_t q0 = blockIdx.x * cq, q1 = min(nq, q0 + cq);
+  const int64_t qa = s * (kSubRows / 4) + threadIdx.x, qb = qa + kThreads;
+  const bool ha = qa < nq, hb = qb < nq;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  {
-    const int v = blockIdx.z;  // one problem per CTA: grid (row chunks, Krylov tiles, problems)
+  const double* wv = w + (int64_t)v * n_pad;
+  const T* Vv = V + (int64_t)v * n_pad;
+  double ua[4] = {0, 0, 0, 0}, ub[4] = {0, 0, 0, 0}, wa[4] = {0, 0, 0, 0}, wb[4] = {0, 0, 0, 0};
+  if (ha) {
+    ld4(Vv + (int64_t)j * stride_i + 4 * qa, ua);
+    ld4(wv + 4 * qa, wa);
+  }
+  if (hb) {
+    ld4(Vv + (int64_t)j * stride_i + 4 * qb, ub);
+    ld4(wv + 4 * qb, wb);
+  }
+  for (int i0 = 0; i0 <= j; i0 += kItile) {
+    const int nt = min(kItile, j + 1 - i0);
     double au[kItile], aw[kItile];
 #pragma unroll
-    for (int t = 0; t < kItile; ++t) au[t] = aw[t] = 0.0;
-    const double* wv = w + (int64_t)v * n_pad;
-    const T* U = V + (int64_t)j * stride_i + (int64_t)v * n_pad;
-    const T* Vv = V + (int64_t)i0 * stride_i + (int64_t)v * n_pad;
-#pragma unroll 1
-    for (int64_t q = q0 + threadIdx.x; q < q1; q += kThreads) {
-      double w4[4], u4[4];
-      ld4(wv + 4 * q, w4);
-      ld4(U + 4 * q, u4);
+    for (int t = 0; t < kItile; ++t) {
+      au[t] = aw[t] = 0.0;
+      if (t < nt) {
+        double xa[4] = {0, 0, 0, 0}, xb[4] = {0, 0, 0, 0};
+        const T* Vi = Vv + (int64_t)(i0 + t) * stride_i;
+        if (ha) ld4(Vi + 4 * qa, xa);
+        if (hb) ld4(Vi + 4 * qb, xb);
 #pragma unroll
-      for (int t = 0; t < kItile; ++t) {
-        if (t < nt) {
-          double x4[4];
-          ld4(Vv + (int64_t)t * stride_i + 4 * q, x4);
-          au[t] = fma(x4[0], u4[0], fma(x4[1], u4[1], fma(x4[2], u4[2], fma(x4[3], u4[3], au[t]))));
-          aw[t] = fma(x4[0], w4[0], fma(x4[1], w4[1], fma(x4[2], w4[2], fma(x4[3], w4[3], aw[t]))));
+        for (int e = 0; e < 4; ++e) {
+          au[t] = fma(xa[e], ua[e], fma(xb[e], ub[e], au[t]));
+          aw[t] = fma(xa[e], wa[e], fma(xb[e], wb[e], aw[t]));
         }
       }
     }
@@ -204,7 +220,7 @@ __global__ void __launch_bounds__(kThreads, 2) dots2_k(const T* __restrict__ V, 
       const int t = threadIdx.x / 2, r = threadIdx.x % 2;
       double a = 0.0;
       for (int wi = 0; wi < kThreads / 32; ++wi) a += red[(wi * kItile + t) * 2 + r];
-      partial[(((int64_t)blockIdx.x * ld_i + i0 + t) * 2 + r) * NV + v] = a;
+      partial[((s * ld_i + i0 + t) * 2 + r) * NV + v] = a;
     }
     __syncthreads();
   }
@@ -279,66 +295,112 @@ __global__ void __launch_bounds__(kThreads) reduce2_coef_k(const double* __restr
   if (threadIdx.x == 0) *counter = 0;
 }
 
-// One read of V[0..j): V[j] <- (u_j - sum_i V[i] s_i) / r, w <- w - sum_i V[i] z_i
-// - V[j] c, with block partials of |w_v|^2 (planar layouts, row quads).
+// One read of V[0..j) for the row chunk s of problem v (one CTA per (s, v),
+// two row quads per thread): V[j] <- (u_j - sum_i V[i] s_i) / r,
+// w <- w - sum_i V[i] z_i - V[j] c, and the chunk's partial of |w_v|^2.  The
+// basis loop is unrolled by four (eight 16-byte loads in flight per thread).
+// The last CTA to finish (ticket counter) forms |w_v| and beta_{j+1}.
 template <typename T, int NV>
-__global__ void __launch_bounds__(kThreads) dcgs_update_k(T* __restrict__ V, int64_t n_pad, int j,
+__global__ void __launch_bounds__(kThreads) update_rows_k(T* __restrict__ V, int64_t n_pad, int j,
                                                           const double* __restrict__ hu,
                                                           const double* __restrict__ hw,
                                                           const double* __restrict__ rc, double* __restrict__ w,
                                                           double* __restrict__ norm_partial, int64_t stride_i,
                                                           double* __restrict__ wnorm, double* __restrict__ beta,
-                                                          int ldb, int* __restrict__ counter) {
-  extern __shared__ double sz[];  // s [j][NV] | z [j][NV]
+                                                          int ldb, int* __restrict__ counter, int64_t n_sub) {
+  extern __shared__ double sz[];  // s [j] | z [j] of this problem
   __shared__ double red[(kThreads / 32) * NV];
-  for (int t = threadIdx.x; t < j * NV; t += kThreads) {
-    sz[t] = hu[t];
-    sz[j * NV + t] = hw[t];
+  const int64_t s = blockIdx.x % n_sub;
+  const int v = (int)(blockIdx.x / n_sub);
+  for (int t = threadIdx.x; t < j; t += kThreads) {
+    sz[t] = hu[t * NV + v];
+    sz[j + t] = hw[t * NV + v];
   }
   __syncthreads();
-  double nrm[NV];
-#pragma unroll
-  for (int v = 0; v < NV; ++v) nrm[v] = 0.0;
   const int64_t nq = n_pad / 4;
-  for (int64_t g = blockIdx.x * (int64_t)kThreads + threadIdx.x; g < nq * NV; g += (int64_t)gridDim.x * kThreads) {
-    const int v = (int)(g / nq);
-    const int64_t q = g - v * nq;
-    const T* Vp = V + (int64_t)v * n_pad + 4 * q;
-    T* Up = V + (int64_t)j * stride_i + (int64_t)v * n_pad + 4 * q;
-    double u4[4], w4[4];
-    ld4(Up, u4);
-    double* wp = w + (int64_t)v * n_pad + 4 * q;
-    ld4(wp, w4);
-    for (int i = 0; i < j; ++i) {
-      double a4[4];
-      ld4(Vp + (int64_t)i * stride_i, a4);
-      const double si = sz[i * NV + v], zi = sz[(j + i) * NV + v];
+  const int64_t qa = s * (kSubRows / 4) + threadIdx.x, qb = qa + kThreads;
+  const bool ha = qa < nq, hb = qb < nq;
+  T* Vv = V + (int64_t)v * n_pad;
+  double* wv = w + (int64_t)v * n_pad;
+  double ua[4] = {0, 0, 0, 0}, ub[4] = {0, 0, 0, 0}, wa[4] = {0, 0, 0, 0}, wb[4] = {0, 0, 0, 0};
+  T* U = Vv + (int64_t)j * stride_i;
+  if (ha) {
+    ld4(U + 4 * qa, ua);
+    ld4(wv + 4 * qa, wa);
+  }
+  if (hb) {
+    ld4(U + 4 * qb, ub);
+    ld4(wv + 4 * qb, wb);
+  }
+  int i = 0;
+  for (; i + 4 <= j; i += 4) {
+    double xa[4][4], xb[4][4];
 #pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        u4[k] = fma(-a4[k], si, u4[k]);
-        w4[k] = fma(-a4[k], zi, w4[k]);
+    for (int c = 0; c < 4; ++c) {
+      const T* Vi = Vv + (int64_t)(i + c) * stride_i;
+#pragma unroll
+      for (int e = 0; e < 4; ++e) xa[c][e] = xb[c][e] = 0.0;
+      if (ha) ld4(Vi + 4 * qa, xa[c]);
+      if (hb) ld4(Vi + 4 * qb, xb[c]);
+    }
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const double si = sz[i + c], zi = sz[j + i + c];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        ua[e] = fma(-xa[c][e], si, ua[e]);
+        ub[e] = fma(-xb[c][e], si, ub[e]);
+        wa[e] = fma(-xa[c][e], zi, wa[e]);
+        wb[e] = fma(-xb[c][e], zi, wb[e]);
       }
     }
-    const double ri = rc[v], c = rc[NV + v];
-    double sq = 0.0;
+  }
+  for (; i < j; ++i) {
+    double xa[4] = {0, 0, 0, 0}, xb[4] = {0, 0, 0, 0};
+    const T* Vi = Vv + (int64_t)i * stride_i;
+    if (ha) ld4(Vi + 4 * qa, xa);
+    if (hb) ld4(Vi + 4 * qb, xb);
+    const double si = sz[i], zi = sz[j + i];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const T qk = (T)(u4[k] * ri);
-      Up[k] = qk;
-      w4[k] = fma(-(double)qk, c, w4[k]);
-      sq = fma(w4[k], w4[k], sq);
+    for (int e = 0; e < 4; ++e) {
+      ua[e] = fma(-xa[e], si, ua[e]);
+      ub[e] = fma(-xb[e], si, ub[e]);
+      wa[e] = fma(-xa[e], zi, wa[e]);
+      wb[e] = fma(-xb[e], zi, wb[e]);
     }
-    st4(wp, w4);
+  }
+  const double ri = rc[v], c = rc[NV + v];
+  double sq = 0.0;
+  if (ha) {
+    double q4[4];
 #pragma unroll
-    for (int vv = 0; vv < NV; ++vv)
-      if (vv == v) nrm[vv] += sq;
+    for (int e = 0; e < 4; ++e) {
+      const T qe = (T)(ua[e] * ri);
+      q4[e] = (double)qe;
+      wa[e] = fma(-q4[e], c, wa[e]);
+      sq = fma(wa[e], wa[e], sq);
+    }
+    st4(U + 4 * qa, q4);
+    st4(wv + 4 * qa, wa);
   }
-  block_sum<NV>(nrm, red);
-  if (threadIdx.x < NV) {
-    norm_partial[blockIdx.x * NV + threadIdx.x] = nrm[threadIdx.x];
-    __threadfence();  // the writers publish before the ticket
+  if (hb) {
+    double q4[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const T qe = (T)(ub[e] * ri);
+      q4[e] = (double)qe;
+      wb[e] = fma(-q4[e], c, wb[e]);
+      sq = fma(wb[e], wb[e], sq);
+    }
+    st4(U + 4 * qb, q4);
+    st4(wv + 4 * qb, wb);
   }
-  // the last CTA: |w_v| (fixed-order sum of the block partials) and
+  block_sum<1>(&sq, red);  // this CTA works on problem v alone
+  if (threadIdx.x == 0) {
+    norm_partial[s * NV + v] = sq;
+    __threadfence();  // the writer publishes before the ticket
+  }
+  // the last CTA: |w_v| (fixed-order sum of the chunk partials) and
   // beta[v][j+1] = |w_v| / r_v, the coupling to the next candidate
   __shared__ int last;
   __syncthreads();
@@ -348,10 +410,10 @@ __global__ void __launch_bounds__(kThreads) dcgs_update_k(T* __restrict__ V, int
   __threadfence();
   double tot[NV];
 #pragma unroll
-  for (int v = 0; v < NV; ++v) tot[v] = 0.0;
-  for (int b = threadIdx.x; b < (int)gridDim.x; b += kThreads)
+  for (int vv = 0; vv < NV; ++vv) tot[vv] = 0.0;
+  for (int64_t b = threadIdx.x; b < n_sub; b += kThreads)
 #pragma unroll
-    for (int v = 0; v < NV; ++v) tot[v] += __ldcg(norm_partial + b * NV + v);
+    for (int vv = 0; vv < NV; ++vv) tot[vv] += __ldcg(norm_partial + b * NV + vv);
   block_sum<NV>(tot, red);
   if (threadIdx.x < NV) {
     const double nv = sqrt(tot[threadIdx.x]);
@@ -404,8 +466,11 @@ Layout make_layout(const edg_lanczos_problem* p) {
   L.n_pad = (n + 3) & ~int64_t(3);
   L.m_max = p->max_iter;
   L.ld_h = L.m_max + 1;
-  L.nblk_dot = edg::kSmCount * 8;  // upper bound of the row-chunk grid of dots_k
-  L.nblk_upd = edg::kSmCount * 8;
+  // row chunks of the reorthogonalisation kernels (kSubRows rows each); the
+  // norm kernels use at least kSmCount * 8 CTAs
+  const int64_t n_sub = (L.n_pad + kSubRows - 1) / kSubRows;
+  L.nblk_dot = (int)(n_sub > edg::kSmCount * 8 ? n_sub : edg::kSmCount * 8);
+  L.nblk_upd = L.nblk_dot;
   int64_t off = 0;
   L.V = off; off = align256(off + (int64_t)(L.m_max + 1) * L.n_pad * nv * esz);
   L.X = off; off = align256(off + n * nv * esz);
@@ -488,9 +553,9 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
   if ((e = cudaMemsetAsync(tickets, 0, 2 * sizeof(int), s)) != cudaSuccess)
     return edg::cuda_status(e, "edg_lanczos: tickets");
   if ((e = cudaGetLastError()) != cudaSuccess) return edg::cuda_status(e, "edg_lanczos: start");
-  const size_t upd_smem = (size_t)2 * (L.m_max + 1) * NV * sizeof(double);
+  const size_t upd_smem = (size_t)2 * (L.m_max + 1) * sizeof(double);
   if (upd_smem > 40 * 1024) {
-    e = cudaFuncSetAttribute(dcgs_update_k<T, NV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)upd_smem);
+    e = cudaFuncSetAttribute(update_rows_k<T, NV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)upd_smem);
     if (e != cudaSuccess) return edg::cuda_status(e, "edg_lanczos: smem attribute");
   }
   std::vector<double> hb((size_t)NV * ld_b), ha((size_t)NV * ld_a), hev((size_t)NV * kMaxK),
@@ -549,24 +614,15 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
     if (st) return st;
     if (timing) cudaEventRecord(event_at(3 * j + 1), s);
     launches += 5;
-    // one delayed Gram-Schmidt step: two reads of V[0..j]; the row-chunk grid
-    // of the dots shrinks as the Krylov tiles grow (about 8 CTAs per SM)
-    // every thread of the dots handles at least 4 row quads per problem (the
-    // per-CTA reduction is then amortised), at most 8 CTAs per SM overall
-    // grid (row chunks, Krylov tiles, problems): about four CTAs per SM in
-    // all, each thread at least two row quads, at most L.nblk_dot row chunks
-    const int tiles = (j + kItile) / kItile;
-    int nx = (4 * edg::kSmCount + tiles * NV - 1) / (tiles * NV);
-    const int64_t most = (n_pad / 4 + 2 * kThreads - 1) / (2 * kThreads);
-    if (nx > most) nx = (int)most;
-    if (nx > L.nblk_dot) nx = L.nblk_dot;
-    if (nx < 1) nx = 1;
-    const dim3 gd(nx, tiles, NV);
-    dots2_k<T, NV><<<gd, kThreads, 0, s>>>(V, n_pad, j, w, partial, ld_a, stride_i);
-    reduce2_coef_k<NV><<<2 * (j + 1), kThreads, 0, s>>>(partial, nx, ld_a, j, hu, hw, alpha, ld_a, beta, ld_b, rc,
-                                                         tickets);
-    dcgs_update_k<T, NV><<<L.nblk_upd, kThreads, upd_smem, s>>>(V, n_pad, j, hu, hw, rc, w, normp, stride_i, wnorm,
-                                                                beta, ld_b, tickets + 1);
+    // one delayed Gram-Schmidt step: two reads of V[0..j], one CTA per
+    // (row chunk, problem) in each
+    const int64_t n_sub = (n_pad + kSubRows - 1) / kSubRows;
+    const unsigned g_rows = (unsigned)(n_sub * NV);
+    dots_rows_k<T, NV><<<g_rows, kThreads, 0, s>>>(V, n_pad, j, w, partial, ld_a, stride_i, n_sub);
+    reduce2_coef_k<NV><<<2 * (j + 1), kThreads, 0, s>>>(partial, (int)n_sub, ld_a, j, hu, hw, alpha, ld_a, beta, ld_b,
+                                                         rc, tickets);
+    update_rows_k<T, NV><<<g_rows, kThreads, upd_smem, s>>>(V, n_pad, j, hu, hw, rc, w, normp, stride_i, wnorm, beta,
+                                                            ld_b, tickets + 1, n_sub);
     scale_store_k<T, NV><<<g_vec, 256, 0, s>>>(w, n, n_pad, wnorm, V + (int64_t)(j + 1) * stride_i, X);
     if (timing) cudaEventRecord(event_at(3 * j + 2), s);
     if ((e = cudaGetLastError()) != cudaSuccess) return edg::cuda_status(e, "edg_lanczos: step");

@@ -74,16 +74,19 @@ def test_tiled_mixed_matches_reference(golden_small, golden_big, dev):
     for i, (name, ns, ref) in enumerate(meta):
         rel = abs(e[i] / ns - ref[0]) / abs(ref[0])
         assert rel <= 1e-9, (name, e[i] / ns, ref[0], rel)
-    # ground-state vectors: normalised and H x = E x
+    # ground-state vectors: normalised, Rayleigh quotient = E (to the energy
+    # tolerance) and a small residual (the short f64 refinement converges the
+    # eigenvalue quadratically faster than the vector)
     ev = tb.evecs.cpu().numpy()
     off = 0
     for i, mat in enumerate(mats):
         x = ev[off: off + mat.n]
         off += mat.n
         assert abs(np.linalg.norm(x) - 1.0) < 1e-10
-        if mat.n <= 20000:
-            H = mat.to_scipy()
-            assert np.linalg.norm(H @ x - e[i] * x) < 1e-6 * max(1.0, abs(e[i])), meta[i][0]
+        H = mat.to_scipy()
+        hx = H @ x
+        assert abs(float(x @ hx) - e[i]) <= 1e-9 * abs(e[i]), meta[i][0]
+        assert np.linalg.norm(hx - e[i] * x) < 1e-4 * max(1.0, abs(e[i])), meta[i][0]
 
 
 def _c3_instances(dev):
