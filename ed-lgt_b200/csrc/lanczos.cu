@@ -19,6 +19,7 @@
 // Every check_every steps the k lowest Ritz pairs of the tridiagonal matrix are
 // computed on the device (multisection + inverse iteration) and the residual
 // bound |beta_{j+1} s_{j}| is compared with tol * max(1, |theta|).
+#include "reorth_bulk.cuh"
 #include "spmv.cuh"
 #include "tridiag.cuh"
 
@@ -152,78 +153,47 @@ __global__ void scale_store_k(const double* __restrict__ w, int64_t n, int64_t n
   }
 }
 
-// Rows of one work item of the reorthogonalisation kernels: 256 threads x two
-// row quads (8 rows per thread), the quads of a thread 256 apart so that a warp
-// reads contiguous 16-byte segments.
-constexpr int kSubRows = kThreads * 8;
-
-// partial[s][i][r][v] for the row chunk s (kSubRows rows) of problem v (one
-// CTA per (s, v)): dots of V[0..j] with the candidate u = V[j] (r = 0) and
-// with w (r = 1).  u and w of the chunk stay in registers while all j+1
-// Krylov vectors stream through once, eight at a time (16 loads of 16 bytes
-// in flight per thread).
-template <typename T, int NV>
-__global__ void __launch_bounds__(kThreads, 2) dots_rows_k(const T* __restrict__ V, int64_t n_pad, int j,
-                                                        const double* __restrict__ w, double* __restrict__ partial,
-                                                        int ld_i, int64_t stride_i, int64_t n_sub) {
-  __shared__ double red[(kThreads / 32) * kItile * 2];
-  const int64_t s = blockIdx.x % n_sub;
-  const int v = (int)(blockIdx.x / n_sub);
-  const int64_t nq = n_pad / 4;
-  const int64_t qa = s * (kSubRows / 4) + threadIdx.x, qb = qa + kThreads;
-  const bool ha = qa < nq, hb = qb < nq;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const double* wv = w + (int64_t)v * n_pad;
-  const T* Vv = V + (int64_t)v * n_pad;
-  double ua[4] = {0, 0, 0, 0}, ub[4] = {0, 0, 0, 0}, wa[4] = {0, 0, 0, 0}, wb[4] = {0, 0, 0, 0};
-  if (ha) {
-    ld4(Vv + (int64_t)j * stride_i + 4 * qa, ua);
-    ld4(wv + 4 * qa, wa);
-  }
-  if (hb) {
-    ld4(Vv + (int64_t)j * stride_i + 4 * qb, ub);
-    ld4(wv + 4 * qb, wb);
-  }
-  for (int i0 = 0; i0 <= j; i0 += kItile) {
-    const int nt = min(kItile, j + 1 - i0);
-    double au[kItile], aw[kItile];
+// Sums of 16 per-lane values over a warp, scattered: afterwards lanes L and
+// L^1 hold the total of value index ((L>>4)&1)*8 + ((L>>3)&1)*4 + ((L>>2)&1)*2
+// + ((L>>1)&1).  Recursive halving: 8 + 4 + 2 + 1 + 1 shuffles instead of
+// 16 x 5 for separate butterflies.
+__device__ __forceinline__ double warp_reduce_scatter16(const double* v16) {
+  const int lane = threadIdx.x & 31;
+  double a[8];
+  {
+    const bool hi = lane & 16;
 #pragma unroll
-    for (int t = 0; t < kItile; ++t) {
-      au[t] = aw[t] = 0.0;
-      if (t < nt) {
-        double xa[4] = {0, 0, 0, 0}, xb[4] = {0, 0, 0, 0};
-        const T* Vi = Vv + (int64_t)(i0 + t) * stride_i;
-        if (ha) ld4(Vi + 4 * qa, xa);
-        if (hb) ld4(Vi + 4 * qb, xb);
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          au[t] = fma(xa[e], ua[e], fma(xb[e], ub[e], au[t]));
-          aw[t] = fma(xa[e], wa[e], fma(xb[e], wb[e], aw[t]));
-        }
-      }
+    for (int k = 0; k < 8; ++k) {
+      const double send = hi ? v16[k] : v16[k + 8];
+      const double keep = hi ? v16[k + 8] : v16[k];
+      a[k] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
     }
-#pragma unroll
-    for (int t = 0; t < kItile; ++t) {
-      double a = au[t], b = aw[t];
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        a += __shfl_down_sync(0xffffffffu, a, o);
-        b += __shfl_down_sync(0xffffffffu, b, o);
-      }
-      if (lane == 0) {
-        red[(warp * kItile + t) * 2 + 0] = a;
-        red[(warp * kItile + t) * 2 + 1] = b;
-      }
-    }
-    __syncthreads();
-    if (threadIdx.x < 2 * nt) {
-      const int t = threadIdx.x / 2, r = threadIdx.x % 2;
-      double a = 0.0;
-      for (int wi = 0; wi < kThreads / 32; ++wi) a += red[(wi * kItile + t) * 2 + r];
-      partial[((s * ld_i + i0 + t) * 2 + r) * NV + v] = a;
-    }
-    __syncthreads();
   }
+  {
+    const bool hi = lane & 8;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const double send = hi ? a[k] : a[k + 4];
+      const double keep = hi ? a[k + 4] : a[k];
+      a[k] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+    }
+  }
+  {
+    const bool hi = lane & 4;
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const double send = hi ? a[k] : a[k + 2];
+      const double keep = hi ? a[k + 2] : a[k];
+      a[k] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+    }
+  }
+  {
+    const bool hi = lane & 2;
+    const double send = hi ? a[0] : a[1];
+    const double keep = hi ? a[1] : a[0];
+    a[0] = keep + __shfl_xor_sync(0xffffffffu, send, 2);
+  }
+  return a[0] + __shfl_xor_sync(0xffffffffu, a[0], 1);
 }
 
 // hu[i][v] (r = 0), hw[i][v] (r = 1) = sum over row chunks (one CTA per (i, r),
@@ -231,7 +201,8 @@ __global__ void __launch_bounds__(kThreads, 2) dots_rows_k(const T* __restrict__
 // computes, one warp per problem, r and c of the delayed step and the new
 // tridiagonal entries alpha_j, beta_j from hu, hw and the previous alpha, beta.
 template <int NV>
-__global__ void __launch_bounds__(kThreads) reduce2_coef_k(const double* __restrict__ partial, int nblocks, int ld_i,
+__global__ void __launch_bounds__(kThreads) reduce2_coef_k(const double* __restrict__ partial, int nblocks,
+                                                           int64_t ld_p,
                                                            int j, double* __restrict__ hu, double* __restrict__ hw,
                                                            double* __restrict__ alpha, int lda,
                                                            double* __restrict__ beta, int ldb,
@@ -244,7 +215,7 @@ __global__ void __launch_bounds__(kThreads) reduce2_coef_k(const double* __restr
   for (int v = 0; v < NV; ++v) a[v] = 0.0;
   for (int b = threadIdx.x; b < nblocks; b += kThreads)
 #pragma unroll
-    for (int v = 0; v < NV; ++v) a[v] += partial[(((int64_t)b * ld_i + i) * 2 + r) * NV + v];
+    for (int v = 0; v < NV; ++v) a[v] += partial[(((int64_t)i * 2 + r) * NV + v) * ld_p + b];
   block_sum<NV>(a, red);
   if (threadIdx.x < NV) {
     (r == 0 ? hu : hw)[i * NV + threadIdx.x] = a[threadIdx.x];
@@ -295,132 +266,184 @@ __global__ void __launch_bounds__(kThreads) reduce2_coef_k(const double* __restr
   if (threadIdx.x == 0) *counter = 0;
 }
 
-// One read of V[0..j) for the row chunk s of problem v (one CTA per (s, v),
-// two row quads per thread): V[j] <- (u_j - sum_i V[i] s_i) / r,
-// w <- w - sum_i V[i] z_i - V[j] c, and the chunk's partial of |w_v|^2.  The
-// basis loop is unrolled by four (eight 16-byte loads in flight per thread).
-// The last CTA to finish (ticket counter) forms |w_v| and beta_{j+1}.
+// ---------------------------------------------------------------------------
+// Reorthogonalisation passes streamed through shared memory (reorth_bulk.cuh)
+// ---------------------------------------------------------------------------
+
+// Dots pass: partial[i][r][v][g] for the 1024-row segment g of problem v:
+// V[i] . u (r = 0) and V[i] . w (r = 1) for i <= j, u = V[j].  Consumers
+// reduce each tile of 8 vectors with a warp reduce-scatter and one sum over
+// the 8 warps.
 template <typename T, int NV>
-__global__ void __launch_bounds__(kThreads) update_rows_k(T* __restrict__ V, int64_t n_pad, int j,
-                                                          const double* __restrict__ hu,
-                                                          const double* __restrict__ hw,
-                                                          const double* __restrict__ rc, double* __restrict__ w,
-                                                          double* __restrict__ norm_partial, int64_t stride_i,
-                                                          double* __restrict__ wnorm, double* __restrict__ beta,
-                                                          int ldb, int* __restrict__ counter, int64_t n_sub) {
-  extern __shared__ double sz[];  // s [j] | z [j] of this problem
-  __shared__ double red[(kThreads / 32) * NV];
-  const int64_t s = blockIdx.x % n_sub;
-  const int v = (int)(blockIdx.x / n_sub);
-  for (int t = threadIdx.x; t < j; t += kThreads) {
-    sz[t] = hu[t * NV + v];
-    sz[j + t] = hw[t * NV + v];
-  }
-  __syncthreads();
-  const int64_t nq = n_pad / 4;
-  const int64_t qa = s * (kSubRows / 4) + threadIdx.x, qb = qa + kThreads;
-  const bool ha = qa < nq, hb = qb < nq;
-  T* Vv = V + (int64_t)v * n_pad;
-  double* wv = w + (int64_t)v * n_pad;
-  double ua[4] = {0, 0, 0, 0}, ub[4] = {0, 0, 0, 0}, wa[4] = {0, 0, 0, 0}, wb[4] = {0, 0, 0, 0};
-  T* U = Vv + (int64_t)j * stride_i;
-  if (ha) {
-    ld4(U + 4 * qa, ua);
-    ld4(wv + 4 * qa, wa);
-  }
-  if (hb) {
-    ld4(U + 4 * qb, ub);
-    ld4(wv + 4 * qb, wb);
-  }
-  int i = 0;
-  for (; i + 4 <= j; i += 4) {
-    double xa[4][4], xb[4][4];
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      const T* Vi = Vv + (int64_t)(i + c) * stride_i;
-#pragma unroll
-      for (int e = 0; e < 4; ++e) xa[c][e] = xb[c][e] = 0.0;
-      if (ha) ld4(Vi + 4 * qa, xa[c]);
-      if (hb) ld4(Vi + 4 * qb, xb[c]);
+__global__ void __launch_bounds__(edg::bulk::kThreadsAll) dots_bulk_k(const T* __restrict__ V, int64_t n_pad, int j,
+                                                                       const double* __restrict__ w,
+                                                                       double* __restrict__ partial, int64_t stride_i,
+                                                                       int64_t n_seg, int* __restrict__ err_out) {
+  using namespace edg::bulk;
+  extern __shared__ __align__(128) unsigned char smraw[];
+  Smem<T>& sm = *reinterpret_cast<Smem<T>*>(smraw);
+  init_barriers(sm);
+  const Run run = run_of((int64_t)NV * n_seg);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int n_vec = j + 1;
+  if (warp == kConsumers / 32) {
+    if (lane == 0) {
+      produce(sm, V, n_pad, stride_i, n_seg, n_vec, run);
+      if (sm.err) atomicExch(err_out, EDG_ERR_TIMEOUT);
     }
+    return;
+  }
+  const int tid = threadIdx.x;
+  const int64_t nq = n_pad / 4;
+  const int idx = ((lane >> 4) & 1) * 8 + ((lane >> 3) & 1) * 4 + ((lane >> 2) & 1) * 2 + ((lane >> 1) & 1);
+  int64_t k = 0;
+  for (int64_t item = run.first; item < run.last; ++item) {
+    const int64_t v = item / n_seg, g = item - v * n_seg;
+    const int64_t q = g * kSegQuads + tid;
+    const bool has = q < nq;
+    double u4[4] = {0, 0, 0, 0}, w4[4] = {0, 0, 0, 0};
+    if (has) {
+      ld4(V + (int64_t)j * stride_i + v * n_pad + 4 * q, u4);
+      ld4(w + v * n_pad + 4 * q, w4);
+    }
+    for (int i0 = 0; i0 < n_vec; i0 += kItile) {
+      const int nt = min(kItile, n_vec - i0);
+      double acc[2 * kItile];
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      const double si = sz[i + c], zi = sz[j + i + c];
+      for (int t = 0; t < 2 * kItile; ++t) acc[t] = 0.0;
+#pragma unroll
+      for (int t = 0; t < kItile; ++t) {
+        if (t < nt) {
+          const bool ok = acquire(sm, k);
+          if (ok && has) {
+            double x4[4];
+            lds4(&sm.ring[k % Smem<T>::S][4 * tid], x4);
+            acc[2 * t] = fma(x4[0], u4[0], fma(x4[1], u4[1], fma(x4[2], u4[2], fma(x4[3], u4[3], acc[2 * t]))));
+            acc[2 * t + 1] =
+                fma(x4[0], w4[0], fma(x4[1], w4[1], fma(x4[2], w4[2], fma(x4[3], w4[3], acc[2 * t + 1]))));
+          }
+          release(sm, k);
+          ++k;
+        }
+      }
+      const double tot = warp_reduce_scatter16(acc);
+      if ((lane & 1) == 0) sm.red[warp][idx] = tot;
+      edg::bulk::consumers_sync();
+      if (tid < 2 * nt) {
+        double a = 0.0;
+        for (int wi = 0; wi < kConsumers / 32; ++wi) a += sm.red[wi][tid];
+        const int t = tid >> 1, r = tid & 1;
+        partial[(((int64_t)(i0 + t) * 2 + r) * NV + v) * n_seg + g] = a;
+      }
+      edg::bulk::consumers_sync();
+    }
+  }
+}
+
+// Update pass: for every row of the CTA's segments, V[j] <- (u - sum_{i<j}
+// V[i] s_i) / r, w <- w - sum_{i<j} V[i] z_i - V[j] c; per-CTA partials of
+// |w_v|^2, and the last CTA (ticket) forms |w_v| and beta_{j+1}.  The s, z
+// coefficients of every problem sit after the ring in shared memory.
+template <typename T, int NV>
+__global__ void __launch_bounds__(edg::bulk::kThreadsAll) update_bulk_k(
+    T* __restrict__ V, int64_t n_pad, int j, const double* __restrict__ hu, const double* __restrict__ hw,
+    const double* __restrict__ rc, double* __restrict__ w, double* __restrict__ norm_partial, int64_t stride_i,
+    double* __restrict__ wnorm, double* __restrict__ beta, int ldb, int* __restrict__ counter, int64_t n_seg,
+    int* __restrict__ err_out) {
+  using namespace edg::bulk;
+  extern __shared__ __align__(128) unsigned char smraw[];
+  Smem<T>& sm = *reinterpret_cast<Smem<T>*>(smraw);
+  double* sz = reinterpret_cast<double*>(smraw + sizeof(Smem<T>));  // s [j][NV] | z [j][NV]
+  for (int t = threadIdx.x; t < j * NV; t += kThreadsAll) {
+    sz[t] = hu[t];
+    sz[j * NV + t] = hw[t];
+  }
+  init_barriers(sm);  // includes __syncthreads: sz is visible after it
+  const Run run = run_of((int64_t)NV * n_seg);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (warp == kConsumers / 32) {
+    if (lane == 0) {
+      produce(sm, (const T*)V, n_pad, stride_i, n_seg, j, run);
+      if (sm.err) atomicExch(err_out, EDG_ERR_TIMEOUT);
+    }
+    return;
+  }
+  const int tid = threadIdx.x;
+  const int64_t nq = n_pad / 4;
+  double nrm[NV];
+#pragma unroll
+  for (int vv = 0; vv < NV; ++vv) nrm[vv] = 0.0;
+  int64_t k = 0;
+  for (int64_t item = run.first; item < run.last; ++item) {
+    const int v = (int)(item / n_seg);
+    const int64_t g = item - (int64_t)v * n_seg;
+    const int64_t q = g * kSegQuads + tid;
+    const bool has = q < nq;
+    T* U = V + (int64_t)j * stride_i + (int64_t)v * n_pad + 4 * q;
+    double* wp = w + (int64_t)v * n_pad + 4 * q;
+    double u4[4] = {0, 0, 0, 0}, w4[4] = {0, 0, 0, 0};
+    if (has) {
+      ld4(U, u4);
+      ld4(wp, w4);
+    }
+    for (int i = 0; i < j; ++i, ++k) {
+      const bool ok = acquire(sm, k);
+      if (ok && has) {
+        double x4[4];
+        lds4(&sm.ring[k % Smem<T>::S][4 * tid], x4);
+        const double si = sz[i * NV + v], zi = sz[(j + i) * NV + v];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          u4[e] = fma(-x4[e], si, u4[e]);
+          w4[e] = fma(-x4[e], zi, w4[e]);
+        }
+      }
+      release(sm, k);
+    }
+    if (has && !sm.err) {
+      const double ri = rc[v], c = rc[NV + v];
+      double q4[4], sq = 0.0;
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
-        ua[e] = fma(-xa[c][e], si, ua[e]);
-        ub[e] = fma(-xb[c][e], si, ub[e]);
-        wa[e] = fma(-xa[c][e], zi, wa[e]);
-        wb[e] = fma(-xb[c][e], zi, wb[e]);
+        q4[e] = (double)(T)(u4[e] * ri);
+        w4[e] = fma(-q4[e], c, w4[e]);
+        sq = fma(w4[e], w4[e], sq);
       }
-    }
-  }
-  for (; i < j; ++i) {
-    double xa[4] = {0, 0, 0, 0}, xb[4] = {0, 0, 0, 0};
-    const T* Vi = Vv + (int64_t)i * stride_i;
-    if (ha) ld4(Vi + 4 * qa, xa);
-    if (hb) ld4(Vi + 4 * qb, xb);
-    const double si = sz[i], zi = sz[j + i];
+      st4(U, q4);
+      st4(wp, w4);
 #pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      ua[e] = fma(-xa[e], si, ua[e]);
-      ub[e] = fma(-xb[e], si, ub[e]);
-      wa[e] = fma(-xa[e], zi, wa[e]);
-      wb[e] = fma(-xb[e], zi, wb[e]);
+      for (int vv = 0; vv < NV; ++vv)
+        if (vv == v) nrm[vv] += sq;
     }
   }
-  const double ri = rc[v], c = rc[NV + v];
-  double sq = 0.0;
-  if (ha) {
-    double q4[4];
+  // CTA partials of |w_v|^2 (consumer threads only: the producer warp has left)
 #pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      const T qe = (T)(ua[e] * ri);
-      q4[e] = (double)qe;
-      wa[e] = fma(-q4[e], c, wa[e]);
-      sq = fma(wa[e], wa[e], sq);
-    }
-    st4(U + 4 * qa, q4);
-    st4(wv + 4 * qa, wa);
-  }
-  if (hb) {
-    double q4[4];
+  for (int vv = 0; vv < NV; ++vv) {
+    double a = nrm[vv];
 #pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      const T qe = (T)(ub[e] * ri);
-      q4[e] = (double)qe;
-      wb[e] = fma(-q4[e], c, wb[e]);
-      sq = fma(wb[e], wb[e], sq);
-    }
-    st4(U + 4 * qb, q4);
-    st4(wv + 4 * qb, wb);
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+    if (lane == 0) sm.red[warp][vv] = a;
   }
-  block_sum<1>(&sq, red);  // this CTA works on problem v alone
-  if (threadIdx.x == 0) {
-    norm_partial[s * NV + v] = sq;
-    __threadfence();  // the writer publishes before the ticket
+  edg::bulk::consumers_sync();
+  if (tid < NV) {
+    double a = 0.0;
+    for (int wi = 0; wi < kConsumers / 32; ++wi) a += sm.red[wi][tid];
+    norm_partial[(int64_t)blockIdx.x * NV + tid] = a;
+    __threadfence();
   }
-  // the last CTA: |w_v| (fixed-order sum of the chunk partials) and
-  // beta[v][j+1] = |w_v| / r_v, the coupling to the next candidate
-  __shared__ int last;
-  __syncthreads();
-  if (threadIdx.x == 0) last = atomicAdd(counter, 1) == (int)gridDim.x - 1;
-  __syncthreads();
-  if (!last) return;
+  edg::bulk::consumers_sync();
+  if (tid == 0) sm.last = atomicAdd(counter, 1) == (int)gridDim.x - 1;
+  edg::bulk::consumers_sync();
+  if (!sm.last) return;
   __threadfence();
-  double tot[NV];
-#pragma unroll
-  for (int vv = 0; vv < NV; ++vv) tot[vv] = 0.0;
-  for (int64_t b = threadIdx.x; b < n_sub; b += kThreads)
-#pragma unroll
-    for (int vv = 0; vv < NV; ++vv) tot[vv] += __ldcg(norm_partial + b * NV + vv);
-  block_sum<NV>(tot, red);
-  if (threadIdx.x < NV) {
-    const double nv = sqrt(tot[threadIdx.x]);
-    wnorm[threadIdx.x] = nv;
-    beta[(int64_t)threadIdx.x * ldb + j + 1] = nv * rc[threadIdx.x];
+  if (tid < NV) {
+    double a = 0.0;
+    for (int b = 0; b < (int)gridDim.x; ++b) a += __ldcg(norm_partial + (int64_t)b * NV + tid);
+    const double nv = sqrt(a);
+    wnorm[tid] = nv;
+    beta[(int64_t)tid * ldb + j + 1] = nv * rc[tid];
   }
-  if (threadIdx.x == 0) *counter = 0;
+  if (tid == 0) *counter = 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -466,11 +489,13 @@ Layout make_layout(const edg_lanczos_problem* p) {
   L.n_pad = (n + 3) & ~int64_t(3);
   L.m_max = p->max_iter;
   L.ld_h = L.m_max + 1;
-  // row chunks of the reorthogonalisation kernels (kSubRows rows each); the
-  // norm kernels use at least kSmCount * 8 CTAs
-  const int64_t n_sub = (L.n_pad + kSubRows - 1) / kSubRows;
-  L.nblk_dot = (int)(n_sub > edg::kSmCount * 8 ? n_sub : edg::kSmCount * 8);
-  L.nblk_upd = L.nblk_dot;
+  // partial slots: one per warp row block of the dots kernel, one per CTA of
+  // the update kernel; the norm kernels use at least kSmCount * 8 CTAs
+  // dot partials: one slot per 1024-row segment of a problem; norm partials:
+  // one per CTA of the update pass (at most kSmCount * 8)
+  const int64_t n_seg = (L.n_pad / 4 + edg::bulk::kSegQuads - 1) / edg::bulk::kSegQuads;
+  L.nblk_dot = (int)(n_seg > edg::kSmCount * 8 ? n_seg : edg::kSmCount * 8);
+  L.nblk_upd = edg::kSmCount * 8;
   int64_t off = 0;
   L.V = off; off = align256(off + (int64_t)(L.m_max + 1) * L.n_pad * nv * esz);
   L.X = off; off = align256(off + n * nv * esz);
@@ -483,7 +508,7 @@ Layout make_layout(const edg_lanczos_problem* p) {
   L.tri_eval = off; off = align256(off + (int64_t)nv * kMaxK * 8);
   L.tri_vec = off; off = align256(off + (int64_t)nv * kMaxK * (L.m_max + 1) * 8);
   L.tri_work = off; off = align256(off + (int64_t)nv * 6 * (L.m_max + 1) * 8);
-  L.sync = off; off = align256(off + 2 * (int64_t)sizeof(int));  // last-CTA tickets
+  L.sync = off; off = align256(off + 4 * (int64_t)sizeof(int));  // last-CTA tickets | error word
   L.total = off;
   return L;
 }
@@ -540,6 +565,7 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
   double* rc = hw + (int64_t)(L.m_max + 1) * NV;     // [2][NV]: 1/r, c of the current step
   double* wnorm = rc + 2 * NV;                        // [NV]: |w| of the next candidate
   int* tickets = (int*)(ws + L.sync);                  // [2] last-CTA counters (left at 0)
+  int* err_word = tickets + 2;                          // EDG_ERR_TIMEOUT when a ring wait ran out
   const unsigned g_vec = edg::grid_for(n_pad, 256);
   cudaError_t e;
   // padding rows (r >= n) of w are zero from start_k on, so every Krylov plane
@@ -550,14 +576,37 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
   scale_store_k<T, NV><<<g_vec, 256, 0, s>>>(w, n, n_pad, h, V, X);
   zero_k<NV><<<(NV * ld_b + 255) / 256, 256, 0, s>>>(beta, NV * ld_b);
   zero_k<NV><<<(NV * ld_a + 255) / 256, 256, 0, s>>>(alpha, NV * ld_a);
-  if ((e = cudaMemsetAsync(tickets, 0, 2 * sizeof(int), s)) != cudaSuccess)
+  if ((e = cudaMemsetAsync(tickets, 0, 4 * sizeof(int), s)) != cudaSuccess)
     return edg::cuda_status(e, "edg_lanczos: tickets");
   if ((e = cudaGetLastError()) != cudaSuccess) return edg::cuda_status(e, "edg_lanczos: start");
-  const size_t upd_smem = (size_t)2 * (L.m_max + 1) * sizeof(double);
-  if (upd_smem > 40 * 1024) {
-    e = cudaFuncSetAttribute(update_rows_k<T, NV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)upd_smem);
-    if (e != cudaSuccess) return edg::cuda_status(e, "edg_lanczos: smem attribute");
+  // the reorthogonalisation passes: persistent grids of the bulk-copy kernels
+  const size_t dot_smem = sizeof(edg::bulk::Smem<T>);
+  const size_t upd_smem = sizeof(edg::bulk::Smem<T>) + (size_t)2 * (L.m_max + 1) * NV * sizeof(double);
+  const int64_t n_seg = (n_pad / 4 + edg::bulk::kSegQuads - 1) / edg::bulk::kSegQuads;
+  int occ_dot = 0, occ_upd = 0, n_sm = 0, dev = 0;
+  e = cudaFuncSetAttribute(dots_bulk_k<T, NV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dot_smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(update_bulk_k<T, NV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)upd_smem);
+  if (e == cudaSuccess) e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_dot, dots_bulk_k<T, NV>, edg::bulk::kThreadsAll, dot_smem);
+  if (e == cudaSuccess)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_upd, update_bulk_k<T, NV>, edg::bulk::kThreadsAll,
+                                                      upd_smem);
+  if (e != cudaSuccess) return edg::cuda_status(e, "edg_lanczos: reorthogonalisation set-up");
+  if (occ_dot < 1 || occ_upd < 1) {
+    edg::set_error("edg_lanczos: max_iter %d needs too much shared memory for the update pass", L.m_max);
+    return EDG_ERR_ARG;
   }
+  const int64_t items = n_seg * NV;
+  auto grid_of = [&](int occ) {
+    int64_t g = (int64_t)n_sm * (occ < 2 ? occ : 2);
+    if (g > items) g = items;
+    if (g > edg::kSmCount * 8) g = edg::kSmCount * 8;
+    return (unsigned)(g < 1 ? 1 : g);
+  };
+  const unsigned g_dot = grid_of(occ_dot), g_upd = grid_of(occ_upd);
   std::vector<double> hb((size_t)NV * ld_b), ha((size_t)NV * ld_a), hev((size_t)NV * kMaxK),
       hs((size_t)NV * kMaxK * ld_s), res((size_t)NV * k, 0.0);
   std::vector<int> m_conv(NV, 0), m_use(NV, 0);
@@ -616,13 +665,13 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
     launches += 5;
     // one delayed Gram-Schmidt step: two reads of V[0..j], one CTA per
     // (row chunk, problem) in each
-    const int64_t n_sub = (n_pad + kSubRows - 1) / kSubRows;
-    const unsigned g_rows = (unsigned)(n_sub * NV);
-    dots_rows_k<T, NV><<<g_rows, kThreads, 0, s>>>(V, n_pad, j, w, partial, ld_a, stride_i, n_sub);
-    reduce2_coef_k<NV><<<2 * (j + 1), kThreads, 0, s>>>(partial, (int)n_sub, ld_a, j, hu, hw, alpha, ld_a, beta, ld_b,
+    dots_bulk_k<T, NV><<<g_dot, edg::bulk::kThreadsAll, dot_smem, s>>>(V, n_pad, j, w, partial, stride_i, n_seg,
+                                                                         err_word);
+    reduce2_coef_k<NV><<<2 * (j + 1), kThreads, 0, s>>>(partial, (int)n_seg, n_seg, j, hu, hw, alpha, ld_a, beta, ld_b,
                                                          rc, tickets);
-    update_rows_k<T, NV><<<g_rows, kThreads, upd_smem, s>>>(V, n_pad, j, hu, hw, rc, w, normp, stride_i, wnorm, beta,
-                                                            ld_b, tickets + 1, n_sub);
+    update_bulk_k<T, NV><<<g_upd, edg::bulk::kThreadsAll, upd_smem, s>>>(V, n_pad, j, hu, hw, rc, w, normp, stride_i,
+                                                                           wnorm, beta, ld_b, tickets + 1, n_seg,
+                                                                           err_word);
     scale_store_k<T, NV><<<g_vec, 256, 0, s>>>(w, n, n_pad, wnorm, V + (int64_t)(j + 1) * stride_i, X);
     if (timing) cudaEventRecord(event_at(3 * j + 2), s);
     if ((e = cudaGetLastError()) != cudaSuccess) return edg::cuda_status(e, "edg_lanczos: step");
@@ -728,8 +777,14 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
     }
     if ((e = cudaGetLastError()) != cudaSuccess) return edg::cuda_status(e, "edg_lanczos: ritz vectors");
   }
-  e = cudaStreamSynchronize(s);
+  int h_err = 0;
+  e = cudaMemcpyAsync(&h_err, err_word, sizeof(int), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return edg::cuda_status(e, "edg_lanczos: finish");
+  if (h_err != 0) {
+    edg::set_error("edg_lanczos: a shared-memory ring wait of the reorthogonalisation ran out");
+    return EDG_ERR_TIMEOUT;
+  }
   if (timing) {
     accumulate(j);
     launches += 2 + (evecs ? 4 * k : 0);

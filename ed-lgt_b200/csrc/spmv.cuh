@@ -17,21 +17,27 @@ struct Store;
 template <>
 struct Store<double> {
   using acc = double;
+  using acc_t = double;
   static constexpr bool cplx = false;
+  __device__ static double zero() { return 0.0; }
   __device__ static double ld(const double* p, int64_t i) { return __ldg(p + i); }
   __device__ static void st(double* p, int64_t i, double v) { p[i] = v; }
 };
 template <>
 struct Store<float> {
   using acc = double;
+  using acc_t = double;
   static constexpr bool cplx = false;
+  __device__ static double zero() { return 0.0; }
   __device__ static double ld(const float* p, int64_t i) { return (double)__ldg(p + i); }
   __device__ static void st(float* p, int64_t i, double v) { p[i] = (float)v; }
 };
 template <>
 struct Store<double2> {
   using acc = cd;
+  using acc_t = cd;
   static constexpr bool cplx = true;
+  __device__ static cd zero() { return {0.0, 0.0}; }
   __device__ static cd ld(const double2* p, int64_t i) {
     double2 v = __ldg(p + i);
     return {v.x, v.y};
@@ -41,7 +47,9 @@ struct Store<double2> {
 template <>
 struct Store<float2> {
   using acc = cd;
+  using acc_t = cd;
   static constexpr bool cplx = true;
+  __device__ static cd zero() { return {0.0, 0.0}; }
   __device__ static cd ld(const float2* p, int64_t i) {
     float2 v = __ldg(p + i);
     return {(double)v.x, (double)v.y};
@@ -108,11 +116,25 @@ __global__ void __launch_bounds__(256) spmv_k(int64_t n, const int64_t* __restri
     for (int v = 0; v < NV; ++v) zero_acc(acc[v]);
     if (r < n) {
       const int64_t beg = __ldg(rowptr + r), end = __ldg(rowptr + r + 1);
-      for (int64_t p = beg + lane; p < end; p += G) {
-        const int64_t c = __ldg(cols + p);
-        const auto a = Store<SV>::ld(vals, p);
+      // four entries of the lane at a time: their columns and values are
+      // loaded first, then all gathers of x are in flight together (the
+      // accumulation order is the entry order, as in a one-at-a-time loop)
+      constexpr int U = 4;
+      for (int64_t p0 = beg + lane; p0 < end; p0 += U * G) {
+        int64_t c[U];
+        typename Store<SV>::acc_t a[U];
 #pragma unroll
-        for (int v = 0; v < NV; ++v) fma_acc(acc[v], a, Store<SX>::ld(x, c * NV + v));
+        for (int k = 0; k < U; ++k) {
+          const int64_t p = p0 + (int64_t)k * G;
+          c[k] = p < end ? (int64_t)__ldg(cols + p) : r;
+          a[k] = p < end ? Store<SV>::ld(vals, p) : Store<SV>::zero();
+        }
+#pragma unroll
+        for (int k = 0; k < U; ++k)
+          if (p0 + (int64_t)k * G < end) {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) fma_acc(acc[v], a[k], Store<SX>::ld(x, c[k] * NV + v));
+          }
       }
     }
 #pragma unroll
