@@ -32,6 +32,7 @@ namespace {
 using edg::tridiag_body;
 constexpr int kThreads = 256;
 constexpr int kItile = 8;  // Krylov vectors per reduction tile
+static_assert(kItile == edg::bulk::kVecs, "a ring stage of the dots pass is one reduction tile");
 constexpr int kMaxK = 16;
 
 __device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
@@ -306,26 +307,26 @@ __global__ void __launch_bounds__(edg::bulk::kThreadsAll) dots_bulk_k(const T* _
       ld4(V + (int64_t)j * stride_i + v * n_pad + 4 * q, u4);
       ld4(w + v * n_pad + 4 * q, w4);
     }
-    for (int i0 = 0; i0 < n_vec; i0 += kItile) {
+    for (int i0 = 0; i0 < n_vec; i0 += kItile, ++k) {
       const int nt = min(kItile, n_vec - i0);
       double acc[2 * kItile];
 #pragma unroll
       for (int t = 0; t < 2 * kItile; ++t) acc[t] = 0.0;
+      const bool ok = acquire(sm, k);
+      if (ok && has) {
+        const T* st = &sm.ring[k % Smem<T>::S][0][4 * tid];
 #pragma unroll
-      for (int t = 0; t < kItile; ++t) {
-        if (t < nt) {
-          const bool ok = acquire(sm, k);
-          if (ok && has) {
+        for (int t = 0; t < kItile; ++t) {
+          if (t < nt) {
             double x4[4];
-            lds4(&sm.ring[k % Smem<T>::S][4 * tid], x4);
+            lds4(st + t * kSegRows, x4);
             acc[2 * t] = fma(x4[0], u4[0], fma(x4[1], u4[1], fma(x4[2], u4[2], fma(x4[3], u4[3], acc[2 * t]))));
             acc[2 * t + 1] =
                 fma(x4[0], w4[0], fma(x4[1], w4[1], fma(x4[2], w4[2], fma(x4[3], w4[3], acc[2 * t + 1]))));
           }
-          release(sm, k);
-          ++k;
         }
       }
+      release(sm, k);
       const double tot = warp_reduce_scatter16(acc);
       if ((lane & 1) == 0) sm.red[warp][idx] = tot;
       edg::bulk::consumers_sync();
@@ -342,8 +343,7 @@ __global__ void __launch_bounds__(edg::bulk::kThreadsAll) dots_bulk_k(const T* _
 
 // Update pass: for every row of the CTA's segments, V[j] <- (u - sum_{i<j}
 // V[i] s_i) / r, w <- w - sum_{i<j} V[i] z_i - V[j] c; per-CTA partials of
-// |w_v|^2, and the last CTA (ticket) forms |w_v| and beta_{j+1}.  The s, z
-// coefficients of every problem sit after the ring in shared memory.
+// |w_v|^2, and the last CTA (ticket) forms |w_v| and beta_{j+1}.
 template <typename T, int NV>
 __global__ void __launch_bounds__(edg::bulk::kThreadsAll) update_bulk_k(
     T* __restrict__ V, int64_t n_pad, int j, const double* __restrict__ hu, const double* __restrict__ hw,
@@ -353,12 +353,7 @@ __global__ void __launch_bounds__(edg::bulk::kThreadsAll) update_bulk_k(
   using namespace edg::bulk;
   extern __shared__ __align__(128) unsigned char smraw[];
   Smem<T>& sm = *reinterpret_cast<Smem<T>*>(smraw);
-  double* sz = reinterpret_cast<double*>(smraw + sizeof(Smem<T>));  // s [j][NV] | z [j][NV]
-  for (int t = threadIdx.x; t < j * NV; t += kThreadsAll) {
-    sz[t] = hu[t];
-    sz[j * NV + t] = hw[t];
-  }
-  init_barriers(sm);  // includes __syncthreads: sz is visible after it
+  init_barriers(sm);
   const Run run = run_of((int64_t)NV * n_seg);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (warp == kConsumers / 32) {
@@ -386,16 +381,24 @@ __global__ void __launch_bounds__(edg::bulk::kThreadsAll) update_bulk_k(
       ld4(U, u4);
       ld4(wp, w4);
     }
-    for (int i = 0; i < j; ++i, ++k) {
+    for (int i0 = 0; i0 < j; i0 += kVecs, ++k) {
+      const int nt = min(kVecs, j - i0);
       const bool ok = acquire(sm, k);
       if (ok && has) {
-        double x4[4];
-        lds4(&sm.ring[k % Smem<T>::S][4 * tid], x4);
-        const double si = sz[i * NV + v], zi = sz[(j + i) * NV + v];
+        const T* st = &sm.ring[k % Smem<T>::S][0][4 * tid];
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          u4[e] = fma(-x4[e], si, u4[e]);
-          w4[e] = fma(-x4[e], zi, w4[e]);
+        for (int t = 0; t < kVecs; ++t) {
+          if (t < nt) {
+            double x4[4];
+            lds4(st + t * kSegRows, x4);
+            // s_i, z_i: the same address in every lane (one L1 broadcast)
+            const double si = __ldg(hu + (i0 + t) * NV + v), zi = __ldg(hw + (i0 + t) * NV + v);
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              u4[e] = fma(-x4[e], si, u4[e]);
+              w4[e] = fma(-x4[e], zi, w4[e]);
+            }
+          }
         }
       }
       release(sm, k);
@@ -581,7 +584,7 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
   if ((e = cudaGetLastError()) != cudaSuccess) return edg::cuda_status(e, "edg_lanczos: start");
   // the reorthogonalisation passes: persistent grids of the bulk-copy kernels
   const size_t dot_smem = sizeof(edg::bulk::Smem<T>);
-  const size_t upd_smem = sizeof(edg::bulk::Smem<T>) + (size_t)2 * (L.m_max + 1) * NV * sizeof(double);
+  const size_t upd_smem = sizeof(edg::bulk::Smem<T>);
   const int64_t n_seg = (n_pad / 4 + edg::bulk::kSegQuads - 1) / edg::bulk::kSegQuads;
   int occ_dot = 0, occ_upd = 0, n_sm = 0, dev = 0;
   e = cudaFuncSetAttribute(dots_bulk_k<T, NV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dot_smem);

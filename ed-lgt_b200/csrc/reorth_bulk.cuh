@@ -27,10 +27,11 @@ constexpr int kConsumers = 256;               // 8 consumer warps
 constexpr int kThreadsAll = kConsumers + 32;  // + producer warp
 constexpr int kSegQuads = kConsumers;         // one quad per consumer thread
 constexpr int kSegRows = 4 * kSegQuads;       // 1024 rows per segment
-// ring stages: 64 KB of copies in flight per CTA (16 f32 / 8 f64 segments)
+constexpr int kVecs = 8;                    // Krylov vectors per ring stage (one tile)
+// ring stages: 96 KB (f32, 3 stages) or 128 KB (f64, 2 stages) in flight
 template <typename T>
 struct Ring {
-  static constexpr int kStages = 64 * 1024 / (kSegRows * (int)sizeof(T));
+  static constexpr int kStages = sizeof(T) == 4 ? 3 : 2;
 };
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
@@ -104,7 +105,7 @@ __device__ __forceinline__ Run run_of(int64_t n_items) {
 template <typename T>
 struct Smem {
   static constexpr int S = Ring<T>::kStages;
-  alignas(128) T ring[S][kSegRows];
+  alignas(128) T ring[S][kVecs][kSegRows];
   alignas(8) uint64_t full[S];
   alignas(8) uint64_t empty[S];
   int err;
@@ -113,9 +114,10 @@ struct Smem {
 };
 
 // Producer lane: streams n_vec vectors (V + i * stride_i) of every item of the
-// CTA's run, segment by segment, through the ring.  Stops issuing when the
-// error word is set; before returning it waits (1 s at most, error or not)
-// until the copies it issued into every stage have landed, so none is in
+// CTA's run, one tile of up to kVecs vectors per ring stage (one bulk copy per
+// vector segment, all counted on the stage's full barrier).  Stops issuing when
+// the error word is set; before returning it waits (1 s at most, error or
+// not) until the copies it issued into every stage have landed, so none is in
 // flight at exit.
 template <typename T>
 __device__ void produce(Smem<T>& sm, const T* V, int64_t n_pad, int64_t stride_i, int64_t n_seg, int n_vec,
@@ -126,18 +128,23 @@ __device__ void produce(Smem<T>& sm, const T* V, int64_t n_pad, int64_t stride_i
   for (int s = 0; s < S; ++s) issued[s] = 0;
   const int64_t nq = n_pad / 4;
   int64_t k = 0;
-  for (int64_t item = run.first; item < run.last && !sm.err; ++item) {
+  bool stop = false;
+  for (int64_t item = run.first; item < run.last && !stop; ++item) {
     const int64_t v = item / n_seg, g = item - v * n_seg;
     const int64_t q0 = g * kSegQuads;
     const int64_t nqs = nq - q0 < kSegQuads ? nq - q0 : kSegQuads;
     const unsigned bytes = (unsigned)(nqs * 4 * sizeof(T));
     const T* src = V + v * n_pad + 4 * q0;
-    for (int i = 0; i < n_vec; ++i, ++k) {
+    for (int i0 = 0; i0 < n_vec; i0 += kVecs, ++k) {
+      const int nt = n_vec - i0 < kVecs ? n_vec - i0 : kVecs;
       const int s = (int)(k % S);
       const int64_t round = k / S;
-      if (round > 0 && !wait_bounded(&sm.empty[s], (unsigned)((round - 1) & 1), &sm.err)) break;
-      mbar_expect_tx(&sm.full[s], bytes);
-      bulk_g2s(sm.ring[s], src + (int64_t)i * stride_i, bytes, &sm.full[s]);
+      if (round > 0 && !wait_bounded(&sm.empty[s], (unsigned)((round - 1) & 1), &sm.err)) {
+        stop = true;
+        break;
+      }
+      mbar_expect_tx(&sm.full[s], bytes * (unsigned)nt);
+      for (int t = 0; t < nt; ++t) bulk_g2s(sm.ring[s][t], src + (int64_t)(i0 + t) * stride_i, bytes, &sm.full[s]);
       issued[s] = round + 1;
     }
   }
@@ -151,8 +158,9 @@ __device__ void produce(Smem<T>& sm, const T* V, int64_t n_pad, int64_t stride_i
   }
 }
 
-// Consumer side of one ring stage: wait for stage k, return whether the data
-// may be used; release() hands the stage back (one arrival per warp).
+// Consumer side of ring stage k (one tile of vectors): wait for it, return
+// whether the data may be used; release() hands the stage back (one arrival
+// per warp).
 template <typename T>
 __device__ __forceinline__ bool acquire(Smem<T>& sm, int64_t k) {
   constexpr int S = Smem<T>::S;
