@@ -383,6 +383,14 @@ __global__ void __launch_bounds__(edg::bulk::kThreadsAll) update_bulk_k(
     }
     for (int i0 = 0; i0 < j; i0 += kVecs, ++k) {
       const int nt = min(kVecs, j - i0);
+      // the tile's coefficients (the same addresses in every lane: L1
+      // broadcasts), loaded before the stage wait so they overlap it
+      double si[kVecs], zi[kVecs];
+#pragma unroll
+      for (int t = 0; t < kVecs; ++t) {
+        si[t] = t < nt ? __ldg(hu + (i0 + t) * NV + v) : 0.0;
+        zi[t] = t < nt ? __ldg(hw + (i0 + t) * NV + v) : 0.0;
+      }
       const bool ok = acquire(sm, k);
       if (ok && has) {
         const T* st = &sm.ring[k % Smem<T>::S][0][4 * tid];
@@ -391,12 +399,10 @@ __global__ void __launch_bounds__(edg::bulk::kThreadsAll) update_bulk_k(
           if (t < nt) {
             double x4[4];
             lds4(st + t * kSegRows, x4);
-            // s_i, z_i: the same address in every lane (one L1 broadcast)
-            const double si = __ldg(hu + (i0 + t) * NV + v), zi = __ldg(hw + (i0 + t) * NV + v);
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
-              u4[e] = fma(-x4[e], si, u4[e]);
-              w4[e] = fma(-x4[e], zi, w4[e]);
+              u4[e] = fma(-x4[e], si[t], u4[e]);
+              w4[e] = fma(-x4[e], zi[t], w4[e]);
             }
           }
         }
