@@ -23,8 +23,10 @@
 #include "spmv.cuh"
 #include "tridiag.cuh"
 
+#include <chrono>
 #include <cmath>
 #include <mutex>
+#include <thread>
 #include <vector>
 
 namespace {
@@ -34,6 +36,24 @@ constexpr int kThreads = 256;
 constexpr int kItile = 8;  // Krylov vectors per reduction tile
 static_assert(kItile == edg::bulk::kVecs, "a ring stage of the dots pass is one reduction tile");
 constexpr int kMaxK = 16;
+
+// State of a device-driven solve (in the workspace).  The step kernels read
+// j, the update pass advances it, the check kernel decides and schedules.
+struct DevState {
+  int j;           // Krylov vectors finished; the candidate is V[j]
+  int done;        // every problem converged, or the Krylov limit reached
+  int next_check;  // Krylov dimension of the next convergence check
+  int checks;      // checks made
+  int status;      // EDG_OK or EDG_ERR_NOT_CONVERGED
+  int prev_m;      // dimension of the previous check
+  int m_conv[4];   // per problem: dimension at convergence, 0 while running
+  int m_use[4];    // per problem: dimension of its last tridiagonal solve
+  int ticket;      // last-CTA counter of the check kernel
+  int pad;
+  double prev_worst;
+  double worst[4];       // worst relative residual of an unconverged problem
+  double resid[4][kMaxK];
+};
 
 __device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
   x += 0x9E3779B97F4A7C15ull;
@@ -154,6 +174,26 @@ __global__ void scale_store_k(const double* __restrict__ w, int64_t n, int64_t n
   }
 }
 
+// The next candidate: V[j] = w / |w| (j = the state's step, advanced by the
+// update pass) and the interleaved matvec input X; nothing once done.
+template <typename T, int NV>
+__global__ void scale_next_k(const double* __restrict__ w, int64_t n, int64_t n_pad, const double* __restrict__ wnorm,
+                             T* __restrict__ V, int64_t stride_i, T* __restrict__ X, const DevState* __restrict__ st) {
+  if (st->done) return;
+  T* plane = V + (int64_t)st->j * stride_i;
+  double inv[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) inv[v] = wnorm[v] > 0.0 ? 1.0 / wnorm[v] : 0.0;
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n_pad; r += (int64_t)gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      const T x = (T)(w[(int64_t)v * n_pad + r] * inv[v]);
+      plane[(int64_t)v * n_pad + r] = x;
+      if (r < n) X[r * NV + v] = x;
+    }
+  }
+}
+
 // Sums of 16 per-lane values over a warp, scattered: afterwards lanes L and
 // L^1 hold the total of value index ((L>>4)&1)*8 + ((L>>3)&1)*4 + ((L>>2)&1)*2
 // + ((L>>1)&1).  Recursive halving: 8 + 4 + 2 + 1 + 1 shuffles instead of
@@ -197,31 +237,34 @@ __device__ __forceinline__ double warp_reduce_scatter16(const double* v16) {
   return a[0] + __shfl_xor_sync(0xffffffffu, a[0], 1);
 }
 
-// hu[i][v] (r = 0), hw[i][v] (r = 1) = sum over row chunks (one CTA per (i, r),
-// fixed order).  The last CTA to finish (ticket counter, reset by it) then
-// computes, one warp per problem, r and c of the delayed step and the new
-// tridiagonal entries alpha_j, beta_j from hu, hw and the previous alpha, beta.
+// hu[i][v] (r = 0), hw[i][v] (r = 1) = sum over the segment partials (fixed
+// order), for i <= j strided over the CTA pairs of a fixed grid.  The last
+// CTA to finish (ticket counter, reset by it) then computes, one warp per
+// problem, r and c of the delayed step and the new tridiagonal entries
+// alpha_j, beta_j from hu, hw and the previous alpha, beta.
 template <int NV>
 __global__ void __launch_bounds__(kThreads) reduce2_coef_k(const double* __restrict__ partial, int nblocks,
-                                                           int64_t ld_p,
-                                                           int j, double* __restrict__ hu, double* __restrict__ hw,
+                                                           int64_t ld_p, const DevState* __restrict__ st,
+                                                           double* __restrict__ hu, double* __restrict__ hw,
                                                            double* __restrict__ alpha, int lda,
                                                            double* __restrict__ beta, int ldb,
                                                            double* __restrict__ rc, int* __restrict__ counter) {
   __shared__ double red[(kThreads / 32) * NV];
   __shared__ int last;
-  const int i = blockIdx.x / 2, r = blockIdx.x % 2;
-  double a[NV];
+  if (st->done) return;
+  const int j = st->j;
+  const int r = blockIdx.x % 2;
+  for (int i = blockIdx.x / 2; i <= j; i += gridDim.x / 2) {
+    double a[NV];
 #pragma unroll
-  for (int v = 0; v < NV; ++v) a[v] = 0.0;
-  for (int b = threadIdx.x; b < nblocks; b += kThreads)
+    for (int v = 0; v < NV; ++v) a[v] = 0.0;
+    for (int b = threadIdx.x; b < nblocks; b += kThreads)
 #pragma unroll
-    for (int v = 0; v < NV; ++v) a[v] += partial[(((int64_t)i * 2 + r) * NV + v) * ld_p + b];
-  block_sum<NV>(a, red);
-  if (threadIdx.x < NV) {
-    (r == 0 ? hu : hw)[i * NV + threadIdx.x] = a[threadIdx.x];
-    __threadfence();  // the writers publish before the ticket
+      for (int v = 0; v < NV; ++v) a[v] += partial[(((int64_t)i * 2 + r) * NV + v) * ld_p + b];
+    block_sum<NV>(a, red);
+    if (threadIdx.x < NV) (r == 0 ? hu : hw)[i * NV + threadIdx.x] = a[threadIdx.x];
   }
+  if (threadIdx.x < NV) __threadfence();  // the writers publish before the ticket
   __syncthreads();
   if (threadIdx.x == 0) last = atomicAdd(counter, 1) == (int)gridDim.x - 1;
   __syncthreads();
@@ -276,11 +319,14 @@ __global__ void __launch_bounds__(kThreads) reduce2_coef_k(const double* __restr
 // reduce each tile of 8 vectors with a warp reduce-scatter and one sum over
 // the 8 warps.
 template <typename T, int NV>
-__global__ void __launch_bounds__(edg::bulk::kThreadsAll) dots_bulk_k(const T* __restrict__ V, int64_t n_pad, int j,
+__global__ void __launch_bounds__(edg::bulk::kThreadsAll) dots_bulk_k(const T* __restrict__ V, int64_t n_pad,
+                                                                       const DevState* __restrict__ st,
                                                                        const double* __restrict__ w,
                                                                        double* __restrict__ partial, int64_t stride_i,
                                                                        int64_t n_seg, int* __restrict__ err_out) {
   using namespace edg::bulk;
+  if (st->done) return;
+  const int j = st->j;
   extern __shared__ __align__(128) unsigned char smraw[];
   Smem<T>& sm = *reinterpret_cast<Smem<T>*>(smraw);
   init_barriers(sm);
@@ -346,11 +392,13 @@ __global__ void __launch_bounds__(edg::bulk::kThreadsAll) dots_bulk_k(const T* _
 // |w_v|^2, and the last CTA (ticket) forms |w_v| and beta_{j+1}.
 template <typename T, int NV>
 __global__ void __launch_bounds__(edg::bulk::kThreadsAll) update_bulk_k(
-    T* __restrict__ V, int64_t n_pad, int j, const double* __restrict__ hu, const double* __restrict__ hw,
-    const double* __restrict__ rc, double* __restrict__ w, double* __restrict__ norm_partial, int64_t stride_i,
-    double* __restrict__ wnorm, double* __restrict__ beta, int ldb, int* __restrict__ counter, int64_t n_seg,
-    int* __restrict__ err_out) {
+    T* __restrict__ V, int64_t n_pad, DevState* __restrict__ st, const double* __restrict__ hu,
+    const double* __restrict__ hw, const double* __restrict__ rc, double* __restrict__ w,
+    double* __restrict__ norm_partial, int64_t stride_i, double* __restrict__ wnorm, double* __restrict__ beta,
+    int ldb, int* __restrict__ counter, int64_t n_seg, int* __restrict__ err_out) {
   using namespace edg::bulk;
+  if (st->done) return;
+  const int j = st->j;
   extern __shared__ __align__(128) unsigned char smraw[];
   Smem<T>& sm = *reinterpret_cast<Smem<T>*>(smraw);
   init_barriers(sm);
@@ -452,7 +500,129 @@ __global__ void __launch_bounds__(edg::bulk::kThreadsAll) update_bulk_k(
     wnorm[tid] = nv;
     beta[(int64_t)tid * ldb + j + 1] = nv * rc[tid];
   }
-  if (tid == 0) *counter = 0;
+  if (tid == 0) {
+    *counter = 0;
+    st->j = j + 1;  // every CTA read j before arriving at the ticket
+  }
+}
+
+// Convergence check after a step, launched after every step (one CTA per
+// problem).  It works only when the state's schedule says a check is due:
+// then each CTA of an unconverged problem finds the invariant-subspace
+// dimension, solves its tridiagonal matrix and tests the residual bounds;
+// the last CTA sets the done flag, schedules the next check from the
+// contraction of the worst residual (never sooner than check_every steps,
+// never later than 4 * check_every) and writes the progress words to the
+// host.  Otherwise block 0 only publishes the step count.
+template <int NV>
+__global__ void __launch_bounds__(kThreads) check_k(DevState* __restrict__ st, const double* __restrict__ alpha,
+                                                    int lda, const double* __restrict__ beta, int ldb, int m_max,
+                                                    int64_t n, int k, double tol, int check_every,
+                                                    double* __restrict__ tri_eval, double* __restrict__ tri_vec,
+                                                    int ld_s, double* __restrict__ tri_work,
+                                                    int32_t* __restrict__ host_progress) {
+  __shared__ int mv_s, exact_s, last_s;
+  volatile DevState* vst = st;
+  if (vst->done) return;
+  const int m = vst->j;
+  const bool due = m >= vst->next_check || m >= m_max || (int64_t)m >= n;
+  if (!due) {
+    if (blockIdx.x == 0 && threadIdx.x == 0 && host_progress) {
+      volatile int32_t* hp = host_progress;
+      hp[0] = m;
+    }
+    return;
+  }
+  const int v = blockIdx.x;
+  if (vst->m_conv[v] == 0) {
+    const double* al = alpha + (int64_t)v * lda;
+    const double* be = beta + (int64_t)v * ldb;
+    if (threadIdx.x == 0) {
+      double scale = 0.0;
+      for (int i = 0; i < m; ++i) scale = fmax(scale, fabs(al[i]) + fabs(be[i]));
+      const double thr = 1e-12 * fmax(scale, 1e-300);
+      int mv = m;
+      for (int i = 1; i <= m; ++i)
+        if (fabs(be[i]) <= thr) {
+          mv = i;
+          break;
+        }
+      mv_s = mv;
+      exact_s = mv < m || (mv == m && fabs(be[m]) <= thr) || (int64_t)m == n;
+    }
+    __syncthreads();
+    const int mv = mv_s, kk = k < mv ? k : mv;
+    double* S = tri_vec + (int64_t)v * kMaxK * ld_s;
+    for (int e = threadIdx.x; e < kMaxK * ld_s; e += kThreads) S[e] = 0.0;
+    __syncthreads();
+    tridiag_body(al, be, mv, kk, tri_eval + (int64_t)v * kMaxK, S, ld_s, tri_work + (int64_t)v * 6 * ld_s);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const bool exact = exact_s != 0;
+      bool ok = kk == k || exact;
+      double worst = 0.0;
+      for (int q = 0; q < kk; ++q) {
+        const double theta = tri_eval[(int64_t)v * kMaxK + q];
+        const double last = S[(int64_t)q * ld_s + (mv - 1)];
+        const double r = exact ? 0.0 : fabs(be[mv] * last);
+        vst->resid[v][q] = r;
+        if (r > tol * fmax(1.0, fabs(theta))) ok = false;
+        worst = fmax(worst, r / fmax(1.0, fabs(theta)));
+      }
+      vst->m_use[v] = mv;
+      vst->worst[v] = ok ? 0.0 : worst;
+      if (ok) vst->m_conv[v] = mv;
+      __threadfence();
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) last_s = atomicAdd(&st->ticket, 1) == (int)gridDim.x - 1;
+  __syncthreads();
+  if (!last_s || threadIdx.x != 0) return;
+  __threadfence();
+  vst->ticket = 0;
+  bool all = true;
+  double worst = 0.0;
+  for (int vv = 0; vv < NV; ++vv)
+    if (vst->m_conv[vv] == 0) {
+      all = false;
+      worst = fmax(worst, vst->worst[vv]);
+    }
+  int done = all ? 1 : 0;
+  if (!all && (m >= m_max || (int64_t)m >= n)) {
+    done = 1;
+    vst->status = EDG_ERR_NOT_CONVERGED;
+  }
+  if (!done) {
+    int step = check_every;
+    const double pw = vst->prev_worst;
+    if (pw > 0.0 && worst > 0.0 && worst < pw && m > vst->prev_m) {
+      const double rate = log(worst / pw) / (double)(m - vst->prev_m);  // < 0
+      const double need = log(tol / worst) / rate;                       // steps to reach tol
+      const int predicted = (int)floor(need * 0.8);
+      if (predicted > step) step = predicted < 4 * check_every ? predicted : 4 * check_every;
+    }
+    vst->prev_worst = worst;
+    vst->prev_m = m;
+    vst->next_check = m + step;
+  }
+  vst->checks = vst->checks + 1;
+  vst->done = done;
+  __threadfence();
+  if (host_progress) {
+    volatile int32_t* hp = host_progress;
+    hp[1] = done;
+    __threadfence_system();
+    hp[0] = m;
+  }
+}
+
+__global__ void state_init_k(DevState* st, int first_check) {
+  if (threadIdx.x != 0) return;
+  DevState s{};
+  s.next_check = first_check;
+  s.prev_worst = -1.0;
+  *st = s;
 }
 
 // ---------------------------------------------------------------------------
@@ -484,7 +654,7 @@ __global__ void ritz_k(const T* __restrict__ V, int64_t n_pad, int m, const doub
 // Workspace layout
 // ---------------------------------------------------------------------------
 struct Layout {
-  int64_t V, X, w, h, partial, normp, alpha, beta, tri_eval, tri_vec, tri_work, sync, total;
+  int64_t V, X, w, h, partial, normp, alpha, beta, tri_eval, tri_vec, tri_work, sync, state, total;
   int nblk_dot, nblk_upd, m_max, ld_h;
   int64_t n_pad;
 };
@@ -518,6 +688,7 @@ Layout make_layout(const edg_lanczos_problem* p) {
   L.tri_vec = off; off = align256(off + (int64_t)nv * kMaxK * (L.m_max + 1) * 8);
   L.tri_work = off; off = align256(off + (int64_t)nv * 6 * (L.m_max + 1) * 8);
   L.sync = off; off = align256(off + 4 * (int64_t)sizeof(int));  // last-CTA tickets | error word
+  L.state = off; off = align256(off + (int64_t)sizeof(DevState));
   L.total = off;
   return L;
 }
@@ -526,28 +697,6 @@ template <int NV>
 __global__ void zero_k(double* p, int n) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t < n) p[t] = 0.0;
-}
-
-// per-problem Krylov dimension of a batched tridiagonal solve
-struct Dims4 {
-  int m[4];
-  int k[4];
-};
-
-__global__ void __launch_bounds__(kThreads) tridiag_batch_k(const double* __restrict__ alpha, int lda,
-                                                            const double* __restrict__ beta, int ldb, Dims4 dims,
-                                                            double* __restrict__ evals, int ld_eval,
-                                                            double* __restrict__ evecs, int ldk, int lds,
-                                                            double* __restrict__ work, int ldw);
-
-__global__ void __launch_bounds__(kThreads) tridiag_batch_k(const double* __restrict__ alpha, int lda,
-                                                            const double* __restrict__ beta, int ldb, Dims4 dims,
-                                                            double* __restrict__ evals, int ld_eval,
-                                                            double* __restrict__ evecs, int ldk, int lds,
-                                                            double* __restrict__ work, int ldw) {
-  const int prob = blockIdx.x;
-  tridiag_body(alpha + (int64_t)prob * lda, beta + (int64_t)prob * ldb, dims.m[prob], dims.k[prob],
-               evals + (int64_t)prob * ld_eval, evecs + (int64_t)prob * ldk * lds, lds, work + (int64_t)prob * ldw);
 }
 
 template <typename T, int NV>
@@ -567,6 +716,7 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
   double* tri_eval = (double*)(ws + L.tri_eval);
   double* tri_vec = (double*)(ws + L.tri_vec);  // [NV][kMaxK][m_max+1]
   double* tri_work = (double*)(ws + L.tri_work);
+  DevState* st = (DevState*)(ws + L.state);
   const int ld_a = L.m_max + 1, ld_b = L.m_max + 2, ld_s = L.m_max + 1;
   const int64_t stride_i = n_pad * NV;  // entries per Krylov vector (all problems)
   double* hu = h;                                   // [m_max+1][NV] dots with the candidate
@@ -576,7 +726,21 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
   int* tickets = (int*)(ws + L.sync);                  // [2] last-CTA counters (left at 0)
   int* err_word = tickets + 2;                          // EDG_ERR_TIMEOUT when a ring wait ran out
   const unsigned g_vec = edg::grid_for(n_pad, 256);
+  const int first_check = p->check_every > 8 ? p->check_every : 8;
   cudaError_t e;
+  // device address of the caller's pinned progress words (NULL: host syncs)
+  int32_t* progress_dev = nullptr;
+  volatile int32_t* progress = p->host_progress;
+  if (progress) {
+    if (cudaHostGetDevicePointer((void**)&progress_dev, (void*)p->host_progress, 0) != cudaSuccess) {
+      cudaGetLastError();  // not pinned and mapped: fall back to synchronising
+      progress = nullptr;
+      progress_dev = nullptr;
+    } else {
+      progress[0] = 0;
+      progress[1] = 0;
+    }
+  }
   // padding rows (r >= n) of w are zero from start_k on, so every Krylov plane
   // written from w has zero padding and no reset of V is needed
   start_k<T, NV><<<edg::grid_for(n_pad * NV, 256), 256, 0, s>>>(n, n_pad, p->seed, (const T*)p->v0, w);
@@ -585,6 +749,7 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
   scale_store_k<T, NV><<<g_vec, 256, 0, s>>>(w, n, n_pad, h, V, X);
   zero_k<NV><<<(NV * ld_b + 255) / 256, 256, 0, s>>>(beta, NV * ld_b);
   zero_k<NV><<<(NV * ld_a + 255) / 256, 256, 0, s>>>(alpha, NV * ld_a);
+  state_init_k<<<1, 32, 0, s>>>(st, first_check);
   if ((e = cudaMemsetAsync(tickets, 0, 4 * sizeof(int), s)) != cudaSuccess)
     return edg::cuda_status(e, "edg_lanczos: tickets");
   if ((e = cudaGetLastError()) != cudaSuccess) return edg::cuda_status(e, "edg_lanczos: start");
@@ -605,7 +770,7 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
                                                       upd_smem);
   if (e != cudaSuccess) return edg::cuda_status(e, "edg_lanczos: reorthogonalisation set-up");
   if (occ_dot < 1 || occ_upd < 1) {
-    edg::set_error("edg_lanczos: max_iter %d needs too much shared memory for the update pass", L.m_max);
+    edg::set_error("edg_lanczos: the reorthogonalisation kernels do not fit on an SM");
     return EDG_ERR_ARG;
   }
   const int64_t items = n_seg * NV;
@@ -616,164 +781,156 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
     return (unsigned)(g < 1 ? 1 : g);
   };
   const unsigned g_dot = grid_of(occ_dot), g_upd = grid_of(occ_upd);
-  std::vector<double> hb((size_t)NV * ld_b), ha((size_t)NV * ld_a), hev((size_t)NV * kMaxK),
-      hs((size_t)NV * kMaxK * ld_s), res((size_t)NV * k, 0.0);
-  std::vector<int> m_conv(NV, 0), m_use(NV, 0);
-  auto tridiag_all = [&](const std::vector<int>& mv) -> int {
-    cudaError_t err = cudaMemsetAsync(tri_vec, 0, sizeof(double) * NV * kMaxK * ld_s, s);
-    if (err != cudaSuccess) return edg::cuda_status(err, "edg_lanczos: tridiag reset");
-    Dims4 d{};
-    for (int v = 0; v < NV; ++v) {
-      d.m[v] = mv[v];
-      d.k[v] = k < mv[v] ? k : mv[v];
-    }
-    tridiag_batch_k<<<NV, kThreads, 0, s>>>(alpha, ld_a, beta, ld_b, d, tri_eval, kMaxK, tri_vec, kMaxK, ld_s,
-                                            tri_work, 6 * ld_s);
-    err = cudaGetLastError();
-    if (err != cudaSuccess) return edg::cuda_status(err, "edg_lanczos: tridiag");
+  const unsigned g_red = 2u * (unsigned)(L.m_max + 1 < 2 * edg::kSmCount ? L.m_max + 1 : 2 * edg::kSmCount);
+  // one Lanczos step and its check; every kernel reads the step index and the
+  // done flag from the device state
+  auto enqueue_step = [&](cudaStream_t cs) -> int {
+    int st_ = edg::launch_spmv<T, T, double>(NV, n, p->nnz, p->rowptr, p->cols, (const T*)p->vals,
+                                             (const T*)p->diag, X, w, cs, n_pad, p->spmv_group, &st->done);
+    if (st_) return st_;
+    dots_bulk_k<T, NV><<<g_dot, edg::bulk::kThreadsAll, dot_smem, cs>>>(V, n_pad, st, w, partial, stride_i, n_seg,
+                                                                          err_word);
+    reduce2_coef_k<NV><<<g_red, kThreads, 0, cs>>>(partial, (int)n_seg, n_seg, st, hu, hw, alpha, ld_a, beta, ld_b, rc,
+                                                   tickets);
+    update_bulk_k<T, NV><<<g_upd, edg::bulk::kThreadsAll, upd_smem, cs>>>(V, n_pad, st, hu, hw, rc, w, normp, stride_i,
+                                                                            wnorm, beta, ld_b, tickets + 1, n_seg,
+                                                                            err_word);
+    scale_next_k<T, NV><<<g_vec, 256, 0, cs>>>(w, n, n_pad, wnorm, V, stride_i, X, st);
     return EDG_OK;
   };
-  // optional phase timing with CUDA events on the launch stream
-  const bool timing = p->stats != nullptr;
-  std::vector<cudaEvent_t> ev;
-  int ev_done = 0;
-  double t_spmv = 0.0, t_reorth = 0.0, t_check = 0.0;
-  int64_t launches = 8;
-  auto event_at = [&](int idx) -> cudaEvent_t {
-    while ((int)ev.size() <= idx) {
-      cudaEvent_t e2;
-      cudaEventCreate(&e2);
-      ev.push_back(e2);
-    }
-    return ev[idx];
+  auto enqueue_check = [&](cudaStream_t cs) {
+    check_k<NV><<<NV, kThreads, 0, cs>>>(st, alpha, ld_a, beta, ld_b, L.m_max, n, k, p->tol, p->check_every,
+                                         tri_eval, tri_vec, ld_s, tri_work, progress_dev);
   };
-  auto accumulate = [&](int upto) {
-    for (; ev_done < upto; ++ev_done) {
-      float a = 0.f, b = 0.f;
-      cudaEventElapsedTime(&a, ev[3 * ev_done], ev[3 * ev_done + 1]);
-      cudaEventElapsedTime(&b, ev[3 * ev_done + 1], ev[3 * ev_done + 2]);
+  // wait until `target` steps are done or the solve has finished
+  auto wait_progress = [&](int target) -> int {
+    if (!progress) {
+      cudaError_t err = cudaStreamSynchronize(s);
+      return err == cudaSuccess ? EDG_OK : edg::cuda_status(err, "edg_lanczos: step");
+    }
+    const auto t0 = std::chrono::steady_clock::now();
+    for (unsigned it = 0; progress[0] < target && progress[1] == 0; ++it) {
+      if ((it & 255u) == 255u) {
+        cudaError_t q = cudaStreamQuery(s);
+        if (q == cudaSuccess) break;  // nothing more will come
+        if (q != cudaErrorNotReady) return edg::cuda_status(q, "edg_lanczos: step");
+        if (std::chrono::steady_clock::now() - t0 > std::chrono::seconds(120)) {
+          edg::set_error("edg_lanczos: no progress from the device for 120 s");
+          return EDG_ERR_TIMEOUT;
+        }
+        std::this_thread::yield();
+      }
+    }
+    return EDG_OK;
+  };
+  auto read_state = [&](DevState* hs) -> int {
+    cudaError_t err = cudaMemcpyAsync(hs, st, sizeof(DevState), cudaMemcpyDeviceToHost, s);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+    return err == cudaSuccess ? EDG_OK : edg::cuda_status(err, "edg_lanczos: state");
+  };
+  const bool timing = p->stats != nullptr;
+  double t_spmv = 0.0, t_reorth = 0.0, t_check = 0.0;
+  int64_t launches = 9;
+  DevState hs{};
+  int rc_ = EDG_OK;
+  if (timing) {
+    // instrumented: steps launched one by one with events around each phase
+    cudaEvent_t ev[4];
+    for (auto& x : ev) cudaEventCreate(&x);
+    for (int j = 0; j < L.m_max; ++j) {
+      cudaEventRecord(ev[0], s);
+      int st_ = edg::launch_spmv<T, T, double>(NV, n, p->nnz, p->rowptr, p->cols, (const T*)p->vals,
+                                               (const T*)p->diag, X, w, s, n_pad, p->spmv_group, &st->done);
+      if (st_) return st_;
+      cudaEventRecord(ev[1], s);
+      dots_bulk_k<T, NV><<<g_dot, edg::bulk::kThreadsAll, dot_smem, s>>>(V, n_pad, st, w, partial, stride_i, n_seg,
+                                                                           err_word);
+      reduce2_coef_k<NV><<<g_red, kThreads, 0, s>>>(partial, (int)n_seg, n_seg, st, hu, hw, alpha, ld_a, beta, ld_b,
+                                                    rc, tickets);
+      update_bulk_k<T, NV><<<g_upd, edg::bulk::kThreadsAll, upd_smem, s>>>(V, n_pad, st, hu, hw, rc, w, normp,
+                                                                             stride_i, wnorm, beta, ld_b, tickets + 1,
+                                                                             n_seg, err_word);
+      scale_next_k<T, NV><<<g_vec, 256, 0, s>>>(w, n, n_pad, wnorm, V, stride_i, X, st);
+      cudaEventRecord(ev[2], s);
+      enqueue_check(s);
+      cudaEventRecord(ev[3], s);
+      if ((e = cudaGetLastError()) != cudaSuccess) return edg::cuda_status(e, "edg_lanczos: step");
+      if ((rc_ = read_state(&hs))) return rc_;
+      float a = 0.f, b = 0.f, c = 0.f;
+      cudaEventElapsedTime(&a, ev[0], ev[1]);
+      cudaEventElapsedTime(&b, ev[1], ev[2]);
+      cudaEventElapsedTime(&c, ev[2], ev[3]);
       t_spmv += a;
       t_reorth += b;
+      t_check += c;
+      launches += 6;
+      if (hs.done) break;
     }
-  };
-  const int first_check = p->check_every > 8 ? p->check_every : 8;
-  // Residuals of the last two checks give a per-step contraction estimate;
-  // the next check is scheduled where the slowest problem should be near tol
-  // (never later than 4 * check_every, never earlier than check_every).
-  int next_check = first_check;
-  double prev_worst = -1.0;
-  int prev_m = 0;
-  int status = EDG_OK;
-  int j = 0;
-  for (; j < L.m_max; ++j) {
-    if (timing) cudaEventRecord(event_at(3 * j), s);
-    int st = edg::launch_spmv<T, T, double>(NV, n, p->nnz, p->rowptr, p->cols, (const T*)p->vals, (const T*)p->diag,
-                                            X, w, s, n_pad, p->spmv_group);
-    if (st) return st;
-    if (timing) cudaEventRecord(event_at(3 * j + 1), s);
-    launches += 5;
-    // one delayed Gram-Schmidt step: two reads of V[0..j], one CTA per
-    // (row chunk, problem) in each
-    dots_bulk_k<T, NV><<<g_dot, edg::bulk::kThreadsAll, dot_smem, s>>>(V, n_pad, j, w, partial, stride_i, n_seg,
-                                                                         err_word);
-    reduce2_coef_k<NV><<<2 * (j + 1), kThreads, 0, s>>>(partial, (int)n_seg, n_seg, j, hu, hw, alpha, ld_a, beta, ld_b,
-                                                         rc, tickets);
-    update_bulk_k<T, NV><<<g_upd, edg::bulk::kThreadsAll, upd_smem, s>>>(V, n_pad, j, hu, hw, rc, w, normp, stride_i,
-                                                                           wnorm, beta, ld_b, tickets + 1, n_seg,
-                                                                           err_word);
-    scale_store_k<T, NV><<<g_vec, 256, 0, s>>>(w, n, n_pad, wnorm, V + (int64_t)(j + 1) * stride_i, X);
-    if (timing) cudaEventRecord(event_at(3 * j + 2), s);
-    if ((e = cudaGetLastError()) != cudaSuccess) return edg::cuda_status(e, "edg_lanczos: step");
-    const int m = j + 1;
-    const bool check = m >= next_check || m == L.m_max || (int64_t)m == n;
-    if (!check) continue;
-    // recurrence coefficients to the host (a few KB) to detect invariant subspaces
-    e = cudaMemcpyAsync(hb.data(), beta, sizeof(double) * NV * ld_b, cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(ha.data(), alpha, sizeof(double) * NV * ld_a, cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) return edg::cuda_status(e, "edg_lanczos: coefficients");
-    if (timing) accumulate(m);
-    cudaEvent_t c0 = nullptr, c1 = nullptr;
-    if (timing) {
-      c0 = event_at(3 * L.m_max + 0);
-      c1 = event_at(3 * L.m_max + 1);
-      cudaEventRecord(c0, s);
+    for (auto& x : ev) cudaEventDestroy(x);
+  } else {
+    // graph of kStepsPerGraph steps (each with its check), replayed one
+    // replay ahead of the host, which polls the device's progress words
+    constexpr int kStepsPerGraph = 4;
+    cudaStream_t cs = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return edg::cuda_status(e, "edg_lanczos: capture");
+    for (int q = 0; q < kStepsPerGraph && rc_ == EDG_OK; ++q) {
+      rc_ = enqueue_step(cs);
+      if (rc_ == EDG_OK) enqueue_check(cs);
     }
-    launches += 2;
-    std::vector<bool> exact(NV, false);
-    for (int v = 0; v < NV; ++v) {
-      if (m_conv[v]) { m_use[v] = m_conv[v]; continue; }
-      double scale = 0.0;
-      for (int i = 0; i < m; ++i) scale = fmax(scale, fabs(ha[v * ld_a + i]) + fabs(hb[v * ld_b + i]));
-      int mv = m;
-      for (int i = 1; i <= m; ++i)
-        if (fabs(hb[v * ld_b + i]) <= 1e-12 * fmax(scale, 1e-300)) { mv = i; break; }
-      exact[v] = mv < m || (mv == m && fabs(hb[v * ld_b + m]) <= 1e-12 * fmax(scale, 1e-300)) || (int64_t)m == n;
-      m_use[v] = mv;
+    cudaError_t ec = cudaStreamEndCapture(cs, &graph);
+    if (rc_ == EDG_OK && ec != cudaSuccess) rc_ = edg::cuda_status(ec, "edg_lanczos: capture");
+    if (rc_ == EDG_OK && (ec = cudaGraphInstantiate(&exec, graph, 0)) != cudaSuccess)
+      rc_ = edg::cuda_status(ec, "edg_lanczos: graph instantiate");
+    int enq = 0;
+    const int limit = (int)(L.m_max < n ? L.m_max : n);
+    if (rc_ == EDG_OK) {
+      ec = cudaGraphLaunch(exec, s);
+      if (ec != cudaSuccess) rc_ = edg::cuda_status(ec, "edg_lanczos: graph launch");
+      enq += kStepsPerGraph;
     }
-    if ((st = tridiag_all(m_use))) return st;
-    e = cudaMemcpyAsync(hev.data(), tri_eval, sizeof(double) * NV * kMaxK, cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(hs.data(), tri_vec, sizeof(double) * NV * kMaxK * ld_s, cudaMemcpyDeviceToHost, s);
-    if (timing && e == cudaSuccess) e = cudaEventRecord(c1, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) return edg::cuda_status(e, "edg_lanczos: ritz values");
-    if (timing) {
-      float a = 0.f;
-      cudaEventElapsedTime(&a, c0, c1);
-      t_check += a;
-    }
-    bool all = true;
-    for (int v = 0; v < NV; ++v) {
-      if (m_conv[v]) continue;
-      const int mv = m_use[v], kk = k < mv ? k : mv;
-      bool ok = kk == k || exact[v];
-      for (int q = 0; q < kk; ++q) {
-        double theta = hev[v * kMaxK + q];
-        double last = hs[((size_t)v * kMaxK + q) * ld_s + (mv - 1)];
-        double r = exact[v] ? 0.0 : fabs(hb[v * ld_b + mv] * last);
-        res[v * k + q] = r;
-        if (r > p->tol * fmax(1.0, fabs(theta))) ok = false;
+    while (rc_ == EDG_OK) {
+      const bool more = enq < limit;
+      if (more) {
+        ec = cudaGraphLaunch(exec, s);
+        if (ec != cudaSuccess) {
+          rc_ = edg::cuda_status(ec, "edg_lanczos: graph launch");
+          break;
+        }
+        enq += kStepsPerGraph;
       }
-      if (ok) m_conv[v] = mv;
-      else all = false;
+      const int target = more ? enq - kStepsPerGraph : limit;
+      rc_ = wait_progress(target < limit ? target : limit);
+      if (rc_) break;
+      if (progress ? progress[1] != 0 : (read_state(&hs) == EDG_OK && hs.done)) break;
+      if (!more) break;
     }
-    if (all) { ++j; break; }
-    if (m == L.m_max) { status = EDG_ERR_NOT_CONVERGED; ++j; break; }
-    // schedule the next check from the worst relative residual
-    double worst = 0.0;
-    for (int v = 0; v < NV; ++v) {
-      if (m_conv[v]) continue;
-      for (int q = 0; q < k; ++q) {
-        const double theta = hev[v * kMaxK + q];
-        worst = fmax(worst, res[v * k + q] / fmax(1.0, fabs(theta)));
-      }
-    }
-    int step = p->check_every;
-    if (prev_worst > 0.0 && worst > 0.0 && worst < prev_worst && m > prev_m) {
-      const double rate = log(worst / prev_worst) / (double)(m - prev_m);  // < 0
-      const double need = log(p->tol / worst) / rate;                      // steps to reach tol
-      int predicted = (int)floor(need * 0.8);
-      if (predicted > step) step = predicted < 4 * p->check_every ? predicted : 4 * p->check_every;
-    }
-    prev_worst = worst;
-    prev_m = m;
-    next_check = m + step;
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    cudaStreamSynchronize(s);
+    cudaStreamDestroy(cs);
+    if (rc_) return rc_;
+    launches += (int64_t)enq * 6;
   }
-  for (int v = 0; v < NV; ++v) m_use[v] = m_conv[v] ? m_conv[v] : (j < 1 ? 1 : j);
-  int st = tridiag_all(m_use);
-  if (st) return st;
+  if ((rc_ = read_state(&hs))) return rc_;
+  const int j_end = hs.j;
+  std::vector<double> hev((size_t)NV * kMaxK);
   e = cudaMemcpyAsync(hev.data(), tri_eval, sizeof(double) * NV * kMaxK, cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-  if (e != cudaSuccess) return edg::cuda_status(e, "edg_lanczos: final ritz values");
+  if (e != cudaSuccess) return edg::cuda_status(e, "edg_lanczos: ritz values");
   int m_all = 1;
   for (int v = 0; v < NV; ++v) {
-    const int kk = k < m_use[v] ? k : m_use[v];
+    const int mv = hs.m_conv[v] ? hs.m_conv[v] : (hs.m_use[v] ? hs.m_use[v] : 1);
+    const int kk = k < mv ? k : mv;
     for (int q = 0; q < k; ++q) {
       evals[v * k + q] = q < kk ? hev[v * kMaxK + q] : NAN;
-      if (resid_out) resid_out[v * k + q] = q < kk ? res[v * k + q] : NAN;
+      if (resid_out) resid_out[v * k + q] = q < kk ? hs.resid[v][q] : NAN;
     }
-    if (iters_out) iters_out[v] = m_use[v];
-    m_all = m_use[v] > m_all ? m_use[v] : m_all;
+    if (iters_out) iters_out[v] = mv;
+    m_all = mv > m_all ? mv : m_all;
   }
   if (evecs) {
     // S rows beyond each problem's m are zero, so one pass over m_all vectors serves all problems
@@ -795,18 +952,19 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
     return EDG_ERR_TIMEOUT;
   }
   if (timing) {
-    accumulate(j);
     launches += 2 + (evecs ? 4 * k : 0);
     p->stats[0] = t_spmv;
-    p->stats[1] = (double)ev_done;
+    p->stats[1] = (double)j_end;
     p->stats[2] = t_reorth;
     p->stats[3] = (double)launches;
-    p->stats[4] = (double)j;
+    p->stats[4] = (double)j_end;
     p->stats[5] = t_check;
-    for (auto& x : ev) cudaEventDestroy(x);
   }
-  if (status == EDG_ERR_NOT_CONVERGED) edg::set_error("edg_lanczos: not converged in %d steps", L.m_max);
-  return status;
+  if (hs.status == EDG_ERR_NOT_CONVERGED) {
+    edg::set_error("edg_lanczos: not converged in %d steps", L.m_max);
+    return EDG_ERR_NOT_CONVERGED;
+  }
+  return EDG_OK;
 }
 
 template <typename T>

@@ -102,8 +102,9 @@ template <typename SV, typename SX, typename SY, int NV, int G>
 __global__ void __launch_bounds__(256) spmv_k(int64_t n, const int64_t* __restrict__ rowptr,
                                               const int32_t* __restrict__ cols, const SV* __restrict__ vals,
                                               const SV* __restrict__ diag, const SX* __restrict__ x,
-                                              SY* __restrict__ y, int64_t y_plane) {
+                                              SY* __restrict__ y, int64_t y_plane, const int* __restrict__ skip) {
   using A = typename AccOf<SV, SX>::type;
+  if (skip != nullptr && *skip) return;  // a device-driven solver has finished
   const int lane = threadIdx.x & (G - 1);
   const int64_t group = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / G;
   const int64_t n_groups = ((int64_t)gridDim.x * blockDim.x) / G;
@@ -163,18 +164,19 @@ inline int spmv_group(int64_t n, int64_t nnz) {
 // group = threads per row (2, 4, 8, 16, 32) or 0 for the heuristic.
 template <typename SV, typename SX, typename SY, int NV>
 int launch_spmv_nv(int64_t n, int64_t nnz, const int64_t* rowptr, const int32_t* cols, const SV* vals,
-                   const SV* diag, const SX* x, SY* y, cudaStream_t s, int64_t y_plane = 0, int group = 0) {
+                   const SV* diag, const SX* x, SY* y, cudaStream_t s, int64_t y_plane = 0, int group = 0,
+                   const int* skip = nullptr) {
   const int threads = 256;
   int g = group > 0 ? group : spmv_group(n, nnz);
   // one row per thread group: enough resident groups to hide the gather latency
   int64_t blocks = ceil_div(n * g, threads);
   unsigned grid = (unsigned)(blocks < (int64_t)kSmCount * 256 ? blocks : (int64_t)kSmCount * 256);
   switch (g) {
-    case 2: spmv_k<SV, SX, SY, NV, 2><<<grid, threads, 0, s>>>(n, rowptr, cols, vals, diag, x, y, y_plane); break;
-    case 4: spmv_k<SV, SX, SY, NV, 4><<<grid, threads, 0, s>>>(n, rowptr, cols, vals, diag, x, y, y_plane); break;
-    case 8: spmv_k<SV, SX, SY, NV, 8><<<grid, threads, 0, s>>>(n, rowptr, cols, vals, diag, x, y, y_plane); break;
-    case 16: spmv_k<SV, SX, SY, NV, 16><<<grid, threads, 0, s>>>(n, rowptr, cols, vals, diag, x, y, y_plane); break;
-    default: spmv_k<SV, SX, SY, NV, 32><<<grid, threads, 0, s>>>(n, rowptr, cols, vals, diag, x, y, y_plane); break;
+    case 2: spmv_k<SV, SX, SY, NV, 2><<<grid, threads, 0, s>>>(n, rowptr, cols, vals, diag, x, y, y_plane, skip); break;
+    case 4: spmv_k<SV, SX, SY, NV, 4><<<grid, threads, 0, s>>>(n, rowptr, cols, vals, diag, x, y, y_plane, skip); break;
+    case 8: spmv_k<SV, SX, SY, NV, 8><<<grid, threads, 0, s>>>(n, rowptr, cols, vals, diag, x, y, y_plane, skip); break;
+    case 16: spmv_k<SV, SX, SY, NV, 16><<<grid, threads, 0, s>>>(n, rowptr, cols, vals, diag, x, y, y_plane, skip); break;
+    default: spmv_k<SV, SX, SY, NV, 32><<<grid, threads, 0, s>>>(n, rowptr, cols, vals, diag, x, y, y_plane, skip); break;
   }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_status(e, "spmv");
@@ -183,16 +185,17 @@ int launch_spmv_nv(int64_t n, int64_t nnz, const int64_t* rowptr, const int32_t*
 
 template <typename SV, typename SX, typename SY>
 int launch_spmv(int nvec, int64_t n, int64_t nnz, const int64_t* rowptr, const int32_t* cols, const SV* vals,
-                const SV* diag, const SX* x, SY* y, cudaStream_t s, int64_t y_plane = 0, int group = 0) {
+                const SV* diag, const SX* x, SY* y, cudaStream_t s, int64_t y_plane = 0, int group = 0,
+                const int* skip = nullptr) {
   if (group != 0 && group != 2 && group != 4 && group != 8 && group != 16 && group != 32) {
     set_error("spmv: group must be 0, 2, 4, 8, 16 or 32, got %d", group);
     return EDG_ERR_ARG;
   }
   switch (nvec) {
-    case 1: return launch_spmv_nv<SV, SX, SY, 1>(n, nnz, rowptr, cols, vals, diag, x, y, s, y_plane, group);
-    case 2: return launch_spmv_nv<SV, SX, SY, 2>(n, nnz, rowptr, cols, vals, diag, x, y, s, y_plane, group);
-    case 3: return launch_spmv_nv<SV, SX, SY, 3>(n, nnz, rowptr, cols, vals, diag, x, y, s, y_plane, group);
-    case 4: return launch_spmv_nv<SV, SX, SY, 4>(n, nnz, rowptr, cols, vals, diag, x, y, s, y_plane, group);
+    case 1: return launch_spmv_nv<SV, SX, SY, 1>(n, nnz, rowptr, cols, vals, diag, x, y, s, y_plane, group, skip);
+    case 2: return launch_spmv_nv<SV, SX, SY, 2>(n, nnz, rowptr, cols, vals, diag, x, y, s, y_plane, group, skip);
+    case 3: return launch_spmv_nv<SV, SX, SY, 3>(n, nnz, rowptr, cols, vals, diag, x, y, s, y_plane, group, skip);
+    case 4: return launch_spmv_nv<SV, SX, SY, 4>(n, nnz, rowptr, cols, vals, diag, x, y, s, y_plane, group, skip);
     default: set_error("spmv: nvec must be 1..4, got %d", nvec); return EDG_ERR_ARG;
   }
 }

@@ -132,6 +132,7 @@ class LanczosProblem(C.Structure):
         ("v0", P),
         ("spmv_group", I32),
         ("stats", P),
+        ("host_progress", P),
     ]
 
 

@@ -110,17 +110,34 @@ def _problem(dtype, n, nnz, rowptr, cols, vals, diag, nvec, k, max_iter, tol, ch
     return p
 
 
+_PROGRESS = {}
+
+
+def _progress_words(device):
+    """Pinned host words the device-driven solver reports its progress in
+    (one buffer per device; calls on a device are stream-ordered)."""
+    idx = torch.device(device).index or 0
+    if idx not in _PROGRESS:
+        _PROGRESS[idx] = torch.zeros(4, dtype=torch.int32, pin_memory=True)
+    return _PROGRESS[idx]
+
+
 def run_lanczos(dtype, n, nnz, rowptr, cols, vals, diag, nvec=1, k=1, max_iter=300, tol=1e-12, check_every=5,
                 seed=1234, v0=None, want_vectors=True, allow_unconverged=False, workspace=None, stats=None,
-                group=0):
+                group=0, poll_host=True):
     """Low-level call of ``edg_lanczos``; ``diag`` is ``[n][nvec]`` in the dtype.
 
     ``stats``: optional float64 numpy array of 6 entries filled with the
-    phase timings of the run (see edg_lanczos_problem.stats).
+    phase timings of the run (see edg_lanczos_problem.stats); the steps are
+    then launched one by one with events around each phase.  Without it the
+    steps run as replays of a CUDA graph; ``poll_host=False`` makes the host
+    synchronise once per replay instead of polling pinned progress words.
     """
     max_iter = int(min(max_iter, n))
     p = _problem(dtype, n, nnz, rowptr, cols, vals, diag, nvec, k, max_iter, tol, check_every, seed, v0, stats,
                  group)
+    progress = _progress_words(rowptr.device) if poll_host else None
+    p.host_progress = progress.data_ptr() if poll_host else None
     wb = lib.edg_lanczos_workspace_bytes(ctypes.byref(p))
     if wb < 0:
         raise _lib.EdgError(-1, _lib.last_error())

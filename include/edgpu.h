@@ -265,12 +265,18 @@ int edg_convert(int32_t dtype_in, const void* in, int32_t dtype_out, void* out,
 /* Lanczos ground states                                                     */
 /* Replaces scipy.sparse.linalg.eigsh(H, k, which="SA") as called from       */
 /* QMB_hamiltonian.diagonalize (edlgt/modeling/qmb_hamiltonian.py:260-332).  */
-/* Lanczos with full (classical Gram-Schmidt, twice) reorthogonalisation on  */
-/* nvec independent problems that share the off-diagonal matrix, vectors in  */
-/* f64 or f32 (dtype 0/1) and every inner product, recurrence coefficient    */
-/* and the tridiagonal eigensolve in f64 on the device.  Stops when the k   */
-/* lowest Ritz values of every problem have residual                         */
-/* |beta_{j+1} s_j| <= tol * max(1, |theta|), or after max_iter steps.       */
+/* Lanczos with full reorthogonalisation (delayed classical Gram-Schmidt,   */
+/* two passes over the basis per step) on nvec independent problems that    */
+/* share the off-diagonal matrix, vectors in f64 or f32 (dtype 0/1) and     */
+/* every inner product, recurrence coefficient and the tridiagonal          */
+/* eigensolve in f64 on the device.  Stops when the k lowest Ritz values of */
+/* every problem have residual |beta_{j+1} s_j| <= tol * max(1, |theta|),   */
+/* or after max_iter steps.  The step index, the convergence checks and     */
+/* their schedule live on the device: the host records a few steps (and     */
+/* their checks) in a CUDA graph and replays it, one replay ahead, polling  */
+/* the progress words the device writes to host_progress; no stream         */
+/* synchronisation happens inside the step loop.  With stats set, the steps */
+/* are launched one by one with CUDA events around each phase instead.      */
 /* ------------------------------------------------------------------------ */
 
 typedef struct {
@@ -293,6 +299,9 @@ typedef struct {
                           /* [0] matvec ms, [1] matvec launches, [2] reorth */
                           /* ms, [3] kernel launches, [4] Lanczos steps,    */
                           /* [5] check ms (CUDA events on the stream)       */
+  int32_t* host_progress; /* optional PINNED host memory, >= 4 int32: the   */
+                          /* device writes [0] steps done, [1] done flag;   */
+                          /* NULL = the host synchronises once per replay   */
 } edg_lanczos_problem;
 
 /* Bytes of device workspace edg_lanczos needs. */
