@@ -426,6 +426,15 @@ def run_edgpu(args, world, rank, local):
                          "'linear' and 'sparse' formats, both run)",
                "phases_s": {k: st0[k] for k in ("sector_s", "assembly_s", "solve_s")},
                "energy_matches_gpu": bool(abs(st0["energy_density"] * L - e64[1]) < 1e-8 * abs(e64[1]))}
+    # the largest configuration (C5), on one GPU only: it holds most of HBM
+    largest = None
+    if world == 1 and not args.no_largest:
+        del model, mat, vals32, diag32, diag64, diags, flush
+        torch.cuda.empty_cache()
+        clk_l = ClockSampler(local)
+        clk_l.start()
+        largest = largest_config(dev, args.warmup)
+        largest["clocks"] = clk_l.stop()
     if rank != 0:
         return
     launches = int(agg32[3] + agg64[3]) + 1  # + the f32->f64 start-vector conversion
@@ -471,6 +480,7 @@ def run_edgpu(args, world, rank, local):
         "gpu_launches": launches,
         "clocks": clk,
         "cpu_baseline": cpu,
+        "largest_config": largest,
     }
     print(json.dumps(line), flush=True)
     del _lib
@@ -867,32 +877,33 @@ Z3_G = tuple(float(g) for g in np.geomspace(0.7, 1.6, 8))
 Z3_MASS = 0.5
 
 
-def run_z3(args, world, rank, local):
-    """2D Z3 lattice gauge theory with staggered matter on the 4x3 periodic
-    lattice, Gauss law + zero charge + zero momentum (245,518,920
-    representatives of 1,473,154,452 Gauss-law states), matrix-free; 8
-    couplings g in geomspace(0.7, 1.6, 8), t = 1, m = 0.5, batched.  One step
-    is the mixed-precision time-to-solution of the 8 ground states (f32
-    thick-restart Lanczos + f64 refinement); the plain f64 solver is timed
-    beside it."""
+def largest_config(dev, warmup=2):
+    """The largest configuration: 2D Z3 lattice gauge theory with staggered
+    matter on the 4x3 periodic lattice, Gauss law + zero charge + zero
+    momentum (245,518,920 representatives of 1,473,154,452 Gauss-law
+    states), matrix-free; 8 couplings g in geomspace(0.7, 1.6, 8), t = 1,
+    m = 0.5, batched.  Mixed-precision time-to-solution (f32 thick-restart
+    Lanczos + f64 refinement) and the plain f64 solver's, both on this GPU,
+    plus the batched matvec timed alone.  Returns a dict."""
     import torch
 
     from edgpu.models.zn_model import ZnModel
 
-    dev = torch.device("cuda", local)
-    torch.cuda.set_device(dev)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
     model = ZnModel((4, 3), 3, momentum=True, device=dev)
     eng = model.engine
     cp = model.build_Hamiltonian(np.array(Z3_G), Z3_MASS)
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t0
     nvec = 8
     coup = torch.from_numpy(np.ascontiguousarray(cp)).to(dev)
     n = eng.n_rows
-    # matvec timing (warm-up launches first)
     mv = {}
     for dt in (torch.float32, torch.float64):
         x = torch.rand((n, nvec), dtype=dt, device=dev)
         y = torch.empty_like(x)
-        for _ in range(args.warmup):
+        for _ in range(warmup):
             eng.matvec(x, y, coup, nvec)
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record()
@@ -911,69 +922,71 @@ def run_z3(args, world, rank, local):
     images = float(hops.double().mean().item()) + 2 * L.n_sites
     del occ, hops
     torch.cuda.empty_cache()
-    clock = ClockSampler(local)
-    clock.start()
     res_mixed = model.diagonalize_Hamiltonian(1, precision="mixed")
-    clocks = clock.stop()
     e_mixed = res_mixed.evals[:, 0].copy()
-    res_mixed.evecs = None  # 15.7 GB of f64 vectors: free them for the f64 solver's basis
+    res_mixed.evecs = None  # free the f64 vectors for the f64 solver's basis
     res64 = model.diagonalize_Hamiltonian(1, precision="fp64")
     e64 = res64.evals[:, 0].copy()
     res64.evecs = None
-    rel = float(np.max(np.abs(e_mixed - e64) / np.abs(e64)))
-    t_mixed = res_mixed.stats["total_ms"]
-    t64 = res64.stats["total_ms"]
-    # e2e: the public model API from host couplings to host energies
-    del model, eng, coup
-    torch.cuda.empty_cache()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    m2 = ZnModel((4, 3), 3, momentum=True, device=dev)
-    m2.build_Hamiltonian(np.array(Z3_G), Z3_MASS)
-    r2 = m2.diagonalize_Hamiltonian(1, precision="mixed")
-    e_host = np.asarray(r2.evals, dtype=np.float64)
-    r2.evecs = None
-    e2e_ms = 1e3 * (time.perf_counter() - t0)
+    t_mixed, t64 = res_mixed.stats["total_ms"], res64.stats["total_ms"]
     hbm, src = peaks()
-    sx32 = 4 * nvec
-    compulsory = n * (8 + 4 + 2 * sx32)
-    image_bytes = n * images * (4 + sx32)
-    ach = (compulsory + image_bytes) / (mv[torch.float32] * 1e-3) / 1e9
+    # compulsory bytes of one batched matvec (matrix-free): keys + x + y
+    comp32 = n * (8 + 2 * 4 * nvec)
+    comp64 = n * (8 + 2 * 8 * nvec)
+    # with the gathers: per row its own orbit entry; per image an orbit entry
+    # and an x row
+    gath32 = comp32 + n * 4 + n * images * (4 + 4 * nvec)
+    out = {
+        "workload": f"Z3 LGT + staggered matter, 4x3 periodic, Gauss law + zero charge + zero momentum, {n} rows "
+                    f"({L.n_gauss} Gauss-law states), matrix-free; g in {[round(g, 4) for g in Z3_G]}, t=1, "
+                    f"m={Z3_MASS}; 8 ground states",
+        "rows": n, "setup_s": setup_s, "basis_build_ms": eng.build_ms,
+        "mixed_ms": t_mixed, "fp64_ms": t64, "speedup_mixed_vs_fp64": t64 / t_mixed,
+        "ground_states_per_s_mixed": nvec / (t_mixed * 1e-3),
+        "max_rel_dE_mixed_vs_fp64": float(np.max(np.abs(e_mixed - e64) / np.abs(e64))), "target": 1e-9,
+        "energies_mixed": e_mixed.tolist(), "energies_fp64": e64.tolist(),
+        "solver_mixed": {k: res_mixed.stats[k] for k in ("m", "k_keep", "matvecs32", "cycles32", "matvecs64",
+                                                          "cycles64", "phase1_ms", "phase2_ms", "matvec_ms",
+                                                          "reorth_ms")},
+        "solver_fp64": {k: res64.stats[k] for k in ("m", "k_keep", "matvecs64", "cycles64", "matvec_ms",
+                                                     "reorth_ms")},
+        "matvec": {"kernel": "zn_matvec_k<3, T, 8>", "ms_f32_x8": mv[torch.float32], "ms_f64_x8": mv[torch.float64],
+                   "images_per_row": images,
+                   "compulsory_bytes_f32": comp32, "compulsory_GBps_f32": comp32 / (mv[torch.float32] * 1e-3) / 1e9,
+                   "compulsory_frac_f32": comp32 / (mv[torch.float32] * 1e-3) / 1e9 / hbm,
+                   "compulsory_bytes_f64": comp64, "compulsory_frac_f64": comp64 / (mv[torch.float64] * 1e-3) / 1e9 / hbm,
+                   "with_gathers_bytes_f32": gath32,
+                   "with_gathers_frac_f32": gath32 / (mv[torch.float32] * 1e-3) / 1e9 / hbm,
+                   "peak": hbm, "peak_source": src,
+                   "bytes": "compulsory = rows x (8 key + 32 x + 32 y) [f32 x8]; with gathers adds the row's own "
+                            "4-byte orbit entry and, per image, a 4-byte orbit entry and a 32-byte x row"},
+        "cpu_baseline": None,
+        "cpu_baseline_note": "no CPU reference at this size: ed-lgt has no Z3 model with matter and its int32 "
+                             "triplets overflow here; the oracle covers lattices up to 4x2",
+    }
+    del model, eng, coup, res_mixed, res64
+    torch.cuda.empty_cache()
+    return out
+
+
+def run_z3(args, world, rank, local):
+    """The largest configuration on its own line (see largest_config)."""
+    import torch
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    clock = ClockSampler(local)
+    clock.start()
+    blk = largest_config(dev, args.warmup)
+    clocks = clock.stop()
     if rank == 0:
         print(json.dumps({
-            "metric": METRIC, "workload": "z3", "value": nvec * world / (t_mixed * 1e-3), "unit": "ground_states/s",
-            "n_gpus": world, "steps": 1, "warmup": args.warmup, "ms_per_step": t_mixed, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32 Krylov/matvec + f64 dots, recurrence, refinement",
+            "metric": METRIC, "workload": "z3", "value": blk["ground_states_per_s_mixed"] * world,
+            "unit": "ground_states/s", "n_gpus": world, "steps": 1, "warmup": args.warmup,
+            "ms_per_step": blk["mixed_ms"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 Krylov/matvec + f64 dots, recurrence, refinement",
             "data": "synthetic (model Hamiltonian; no reference run exists for Z3 with matter)",
-            "config": {"workload": "Z3 LGT + staggered matter, 4x3 periodic, Gauss law + zero charge + zero momentum, "
-                                   f"{n} rows ({L.n_gauss} Gauss-law states), matrix-free; g in "
-                                   f"{[round(g, 4) for g in Z3_G]}, t=1, m={Z3_MASS}",
-                       "solver": {k: res_mixed.stats[k] for k in ("m", "k_keep", "matvecs32", "cycles32",
-                                                                  "matvecs64", "cycles64")},
-                       "l2": "inputs larger than L2 (keys 2 GB, orbit table 5.9 GB, vectors 7.9 GB)"},
-            "fp64_ms": t64, "fp64_solver": {k: res64.stats[k] for k in ("m", "k_keep", "matvecs64", "cycles64")},
-            "speedup_vs_fp64": t64 / t_mixed,
-            "max_rel_dE_mixed_vs_fp64": rel,
-            "energies_mixed": e_mixed.tolist(), "energies_fp64": e64.tolist(),
-            "residual_mixed": res_mixed.residuals[:, 0].tolist(),
-            "basis_build_ms": m2.engine.build_ms,
-            "phase_ms": {"f32": res_mixed.stats["phase1_ms"], "f64_refine": res_mixed.stats["phase2_ms"],
-                         "matvec": res_mixed.stats["matvec_ms"], "reorth": res_mixed.stats["reorth_ms"]},
-            "matvec_ms": {"f32_x8": mv[torch.float32], "f64_x8": mv[torch.float64]},
-            "images_per_row": images,
-            "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
-                         "traffic": None, "peak_source": src,
-                         "kernel": "zn_matvec_k<3, float, 8>",
-                         "bytes_model": "per row: key 8 + own orbit entry 4 + x and y rows 2*32; per image: orbit "
-                                        "entry 4 + x row 32"},
-            "e2e": {"value": nvec / (e2e_ms * 1e-3), "unit": "ground_states/s", "ms_per_step": e2e_ms,
-                    "h2d_bytes_per_step": int(cp.nbytes), "d2h_bytes_per_step": int(e_host.nbytes),
-                    "includes": "basis build, couplings upload, mixed solve, energies to host"},
-            "cpu_baseline": None,
-            "cpu_baseline_note": "no CPU reference at this size: ed-lgt has no Z3 model with matter and its int32 "
-                                 "triplets overflow here; the oracle covers lattices up to 4x2",
-            "gpu_launches": res_mixed.stats["launches"],
-            "clocks": clocks,
+            "config": {"workload": blk["workload"]}, "largest_config": blk, "clocks": clocks,
         }), flush=True)
 
 
@@ -984,6 +997,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="edgpu", choices=["edgpu", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-largest", action="store_true",
+                    help="skip the largest-configuration block (Z3 4x3, about 6 minutes; run at N=1 only)")
     ap.add_argument("--workload", default="sweep", choices=["sweep", "batch", "quench", "z3", "corr", "entropy", "momentum"],
                     help="sweep: SU(2) L=14 coupling sweep (the headline); batch: QED 3x2 instance batch; "
                          "quench: SU(2) L=16 Krylov dynamics; z3: Z3 4x3 zero-momentum matrix-free batch; "
