@@ -160,7 +160,7 @@ __global__ void __launch_bounds__(kThreads) beta_k(const double* __restrict__ no
 // (may be null).
 template <typename T, int NV>
 __global__ void scale_store_k(const double* __restrict__ w, int64_t n, int64_t n_pad, const double* __restrict__ beta,
-                              T* __restrict__ plane, T* __restrict__ X) {
+                              T* __restrict__ plane, T* __restrict__ X, int xs) {
   double inv[NV];
 #pragma unroll
   for (int v = 0; v < NV; ++v) inv[v] = beta[v] > 0.0 ? 1.0 / beta[v] : 0.0;
@@ -169,7 +169,7 @@ __global__ void scale_store_k(const double* __restrict__ w, int64_t n, int64_t n
     for (int v = 0; v < NV; ++v) {
       const T x = (T)(w[(int64_t)v * n_pad + r] * inv[v]);
       if (plane) plane[(int64_t)v * n_pad + r] = x;
-      if (X && r < n) X[r * NV + v] = x;
+      if (X && r < n) X[r * xs + v] = x;
     }
   }
 }
@@ -178,7 +178,8 @@ __global__ void scale_store_k(const double* __restrict__ w, int64_t n, int64_t n
 // update pass) and the interleaved matvec input X; nothing once done.
 template <typename T, int NV>
 __global__ void scale_next_k(const double* __restrict__ w, int64_t n, int64_t n_pad, const double* __restrict__ wnorm,
-                             T* __restrict__ V, int64_t stride_i, T* __restrict__ X, const DevState* __restrict__ st) {
+                             T* __restrict__ V, int64_t stride_i, T* __restrict__ X, int xs,
+                             const DevState* __restrict__ st) {
   if (st->done) return;
   T* plane = V + (int64_t)st->j * stride_i;
   double inv[NV];
@@ -189,7 +190,7 @@ __global__ void scale_next_k(const double* __restrict__ w, int64_t n, int64_t n_
     for (int v = 0; v < NV; ++v) {
       const T x = (T)(w[(int64_t)v * n_pad + r] * inv[v]);
       plane[(int64_t)v * n_pad + r] = x;
-      if (r < n) X[r * NV + v] = x;
+      if (r < n) X[r * xs + v] = x;
     }
   }
 }
@@ -677,7 +678,7 @@ Layout make_layout(const edg_lanczos_problem* p) {
   L.nblk_upd = edg::kSmCount * 8;
   int64_t off = 0;
   L.V = off; off = align256(off + (int64_t)(L.m_max + 1) * L.n_pad * nv * esz);
-  L.X = off; off = align256(off + n * nv * esz);
+  L.X = off; off = align256(off + n * (nv == 3 ? 4 : nv) * esz);  // matvec input, rows padded to 4 for nv = 3
   L.w = off; off = align256(off + L.n_pad * nv * 8);
   L.h = off; off = align256(off + (int64_t)(2 * (L.m_max + 1) + 3) * nv * 8);  // hu | hw | rc | |w|
   L.partial = off; off = align256(off + (int64_t)L.nblk_dot * (L.m_max + 1) * 2 * nv * 8);
@@ -727,6 +728,7 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
   int* err_word = tickets + 2;                          // EDG_ERR_TIMEOUT when a ring wait ran out
   const unsigned g_vec = edg::grid_for(n_pad, 256);
   const int first_check = p->check_every > 8 ? p->check_every : 8;
+  constexpr int kXs = NV == 3 ? 4 : NV;  // row stride of the matvec input X
   cudaError_t e;
   // device address of the caller's pinned progress words (NULL: host syncs)
   int32_t* progress_dev = nullptr;
@@ -746,7 +748,7 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
   start_k<T, NV><<<edg::grid_for(n_pad * NV, 256), 256, 0, s>>>(n, n_pad, p->seed, (const T*)p->v0, w);
   norm_k<NV><<<L.nblk_upd, kThreads, 0, s>>>(w, n_pad, normp);
   beta_k<NV><<<1, kThreads, 0, s>>>(normp, L.nblk_upd, h);
-  scale_store_k<T, NV><<<g_vec, 256, 0, s>>>(w, n, n_pad, h, V, X);
+  scale_store_k<T, NV><<<g_vec, 256, 0, s>>>(w, n, n_pad, h, V, X, kXs);
   zero_k<NV><<<(NV * ld_b + 255) / 256, 256, 0, s>>>(beta, NV * ld_b);
   zero_k<NV><<<(NV * ld_a + 255) / 256, 256, 0, s>>>(alpha, NV * ld_a);
   state_init_k<<<1, 32, 0, s>>>(st, first_check);
@@ -786,7 +788,7 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
   // done flag from the device state
   auto enqueue_step = [&](cudaStream_t cs) -> int {
     int st_ = edg::launch_spmv<T, T, double>(NV, n, p->nnz, p->rowptr, p->cols, (const T*)p->vals,
-                                             (const T*)p->diag, X, w, cs, n_pad, p->spmv_group, &st->done);
+                                             (const T*)p->diag, X, w, cs, n_pad, p->spmv_group, &st->done, kXs);
     if (st_) return st_;
     dots_bulk_k<T, NV><<<g_dot, edg::bulk::kThreadsAll, dot_smem, cs>>>(V, n_pad, st, w, partial, stride_i, n_seg,
                                                                           err_word);
@@ -795,7 +797,7 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
     update_bulk_k<T, NV><<<g_upd, edg::bulk::kThreadsAll, upd_smem, cs>>>(V, n_pad, st, hu, hw, rc, w, normp, stride_i,
                                                                             wnorm, beta, ld_b, tickets + 1, n_seg,
                                                                             err_word);
-    scale_next_k<T, NV><<<g_vec, 256, 0, cs>>>(w, n, n_pad, wnorm, V, stride_i, X, st);
+    scale_next_k<T, NV><<<g_vec, 256, 0, cs>>>(w, n, n_pad, wnorm, V, stride_i, X, kXs, st);
     return EDG_OK;
   };
   auto enqueue_check = [&](cudaStream_t cs) {
@@ -840,7 +842,7 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
     for (int j = 0; j < L.m_max; ++j) {
       cudaEventRecord(ev[0], s);
       int st_ = edg::launch_spmv<T, T, double>(NV, n, p->nnz, p->rowptr, p->cols, (const T*)p->vals,
-                                               (const T*)p->diag, X, w, s, n_pad, p->spmv_group, &st->done);
+                                               (const T*)p->diag, X, w, s, n_pad, p->spmv_group, &st->done, kXs);
       if (st_) return st_;
       cudaEventRecord(ev[1], s);
       dots_bulk_k<T, NV><<<g_dot, edg::bulk::kThreadsAll, dot_smem, s>>>(V, n_pad, st, w, partial, stride_i, n_seg,
@@ -850,7 +852,7 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
       update_bulk_k<T, NV><<<g_upd, edg::bulk::kThreadsAll, upd_smem, s>>>(V, n_pad, st, hu, hw, rc, w, normp,
                                                                              stride_i, wnorm, beta, ld_b, tickets + 1,
                                                                              n_seg, err_word);
-      scale_next_k<T, NV><<<g_vec, 256, 0, s>>>(w, n, n_pad, wnorm, V, stride_i, X, st);
+      scale_next_k<T, NV><<<g_vec, 256, 0, s>>>(w, n, n_pad, wnorm, V, stride_i, X, kXs, st);
       cudaEventRecord(ev[2], s);
       enqueue_check(s);
       cudaEventRecord(ev[3], s);
@@ -939,7 +941,7 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
                                                                    stride_i, w);
       norm_k<NV><<<L.nblk_upd, kThreads, 0, s>>>(w, n_pad, normp);
       beta_k<NV><<<1, kThreads, 0, s>>>(normp, L.nblk_upd, h);
-      scale_store_k<T, NV><<<g_vec, 256, 0, s>>>(w, n, n_pad, h, (T*)nullptr, (T*)evecs + (int64_t)q * n * NV);
+      scale_store_k<T, NV><<<g_vec, 256, 0, s>>>(w, n, n_pad, h, (T*)nullptr, (T*)evecs + (int64_t)q * n * NV, NV);
     }
     if ((e = cudaGetLastError()) != cudaSuccess) return edg::cuda_status(e, "edg_lanczos: ritz vectors");
   }

@@ -83,6 +83,36 @@ __device__ __forceinline__ void group_reduce(cd& a) {
   }
 }
 
+// One row of x (NV entries at stride XS): a single 16-byte (f32) or two
+// 16-byte (f64) loads when the rows are padded to four entries, else one
+// load per entry.
+template <typename SX, int NV, int XS>
+struct RowX {
+  __device__ static void ld(const SX* x, int64_t c, typename Store<SX>::acc (&out)[NV]) {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) out[v] = Store<SX>::ld(x, c * XS + v);
+  }
+};
+template <int NV>
+struct RowX<float, NV, 4> {
+  __device__ static void ld(const float* x, int64_t c, double (&out)[NV]) {
+    const float4 q = __ldg(reinterpret_cast<const float4*>(x) + c);
+    const float f[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+    for (int v = 0; v < NV; ++v) out[v] = (double)f[v];
+  }
+};
+template <int NV>
+struct RowX<double, NV, 4> {
+  __device__ static void ld(const double* x, int64_t c, double (&out)[NV]) {
+    const double2 a = __ldg(reinterpret_cast<const double2*>(x) + 2 * c);
+    const double2 b = __ldg(reinterpret_cast<const double2*>(x) + 2 * c + 1);
+    const double f[4] = {a.x, a.y, b.x, b.y};
+#pragma unroll
+    for (int v = 0; v < NV; ++v) out[v] = f[v];
+  }
+};
+
 // SV: matrix value/diag storage, SX: x storage, SY: y storage.  The
 // accumulator is complex when either the matrix or the vector is.
 template <typename SV, typename SX>
@@ -98,7 +128,7 @@ struct AccOf<float2, float> {
   using type = cd;
 };
 
-template <typename SV, typename SX, typename SY, int NV, int G>
+template <typename SV, typename SX, typename SY, int NV, int G, int XS>
 __global__ void __launch_bounds__(256) spmv_k(int64_t n, const int64_t* __restrict__ rowptr,
                                               const int32_t* __restrict__ cols, const SV* __restrict__ vals,
                                               const SV* __restrict__ diag, const SX* __restrict__ x,
@@ -133,17 +163,21 @@ __global__ void __launch_bounds__(256) spmv_k(int64_t n, const int64_t* __restri
 #pragma unroll
         for (int k = 0; k < U; ++k)
           if (p0 + (int64_t)k * G < end) {
+            typename Store<SX>::acc xr[NV];
+            RowX<SX, NV, XS>::ld(x, c[k], xr);
 #pragma unroll
-            for (int v = 0; v < NV; ++v) fma_acc(acc[v], a[k], Store<SX>::ld(x, c[k] * NV + v));
+            for (int v = 0; v < NV; ++v) fma_acc(acc[v], a[k], xr[v]);
           }
       }
     }
 #pragma unroll
     for (int v = 0; v < NV; ++v) group_reduce<G>(acc[v]);
     if (r < n && lane == 0) {
+      typename Store<SX>::acc xr[NV];
+      RowX<SX, NV, XS>::ld(x, r, xr);
 #pragma unroll
       for (int v = 0; v < NV; ++v) {
-        fma_acc(acc[v], Store<SV>::ld(diag, r * NV + v), Store<SX>::ld(x, r * NV + v));
+        fma_acc(acc[v], Store<SV>::ld(diag, r * NV + v), xr[v]);
         Store<SY>::st(y, y_plane > 0 ? v * y_plane + r : r * NV + v, acc[v]);
       }
     }
@@ -162,40 +196,55 @@ inline int spmv_group(int64_t n, int64_t nnz) {
 
 // y_plane > 0 writes y planar (y[v * y_plane + r]) instead of interleaved;
 // group = threads per row (2, 4, 8, 16, 32) or 0 for the heuristic.
-template <typename SV, typename SX, typename SY, int NV>
-int launch_spmv_nv(int64_t n, int64_t nnz, const int64_t* rowptr, const int32_t* cols, const SV* vals,
-                   const SV* diag, const SX* x, SY* y, cudaStream_t s, int64_t y_plane = 0, int group = 0,
-                   const int* skip = nullptr) {
+template <typename SV, typename SX, typename SY, int NV, int XS>
+int launch_spmv_xs(int64_t n, int64_t nnz, const int64_t* rowptr, const int32_t* cols, const SV* vals,
+                   const SV* diag, const SX* x, SY* y, cudaStream_t s, int64_t y_plane, int group, const int* skip) {
   const int threads = 256;
   int g = group > 0 ? group : spmv_group(n, nnz);
   // one row per thread group: enough resident groups to hide the gather latency
   int64_t blocks = ceil_div(n * g, threads);
   unsigned grid = (unsigned)(blocks < (int64_t)kSmCount * 256 ? blocks : (int64_t)kSmCount * 256);
   switch (g) {
-    case 2: spmv_k<SV, SX, SY, NV, 2><<<grid, threads, 0, s>>>(n, rowptr, cols, vals, diag, x, y, y_plane, skip); break;
-    case 4: spmv_k<SV, SX, SY, NV, 4><<<grid, threads, 0, s>>>(n, rowptr, cols, vals, diag, x, y, y_plane, skip); break;
-    case 8: spmv_k<SV, SX, SY, NV, 8><<<grid, threads, 0, s>>>(n, rowptr, cols, vals, diag, x, y, y_plane, skip); break;
-    case 16: spmv_k<SV, SX, SY, NV, 16><<<grid, threads, 0, s>>>(n, rowptr, cols, vals, diag, x, y, y_plane, skip); break;
-    default: spmv_k<SV, SX, SY, NV, 32><<<grid, threads, 0, s>>>(n, rowptr, cols, vals, diag, x, y, y_plane, skip); break;
+    case 2: spmv_k<SV, SX, SY, NV, 2, XS><<<grid, threads, 0, s>>>(n, rowptr, cols, vals, diag, x, y, y_plane, skip); break;
+    case 4: spmv_k<SV, SX, SY, NV, 4, XS><<<grid, threads, 0, s>>>(n, rowptr, cols, vals, diag, x, y, y_plane, skip); break;
+    case 8: spmv_k<SV, SX, SY, NV, 8, XS><<<grid, threads, 0, s>>>(n, rowptr, cols, vals, diag, x, y, y_plane, skip); break;
+    case 16: spmv_k<SV, SX, SY, NV, 16, XS><<<grid, threads, 0, s>>>(n, rowptr, cols, vals, diag, x, y, y_plane, skip); break;
+    default: spmv_k<SV, SX, SY, NV, 32, XS><<<grid, threads, 0, s>>>(n, rowptr, cols, vals, diag, x, y, y_plane, skip); break;
   }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_status(e, "spmv");
   return EDG_OK;
 }
 
+template <typename SV, typename SX, typename SY, int NV>
+int launch_spmv_nv(int64_t n, int64_t nnz, const int64_t* rowptr, const int32_t* cols, const SV* vals,
+                   const SV* diag, const SX* x, SY* y, cudaStream_t s, int64_t y_plane = 0, int group = 0,
+                   const int* skip = nullptr, int x_stride = NV) {
+  if constexpr (NV == 3 && !Store<SX>::cplx) {
+    // rows of x padded to four entries: one aligned vector load per gather
+    if (x_stride == 4)
+      return launch_spmv_xs<SV, SX, SY, NV, 4>(n, nnz, rowptr, cols, vals, diag, x, y, s, y_plane, group, skip);
+  }
+  return launch_spmv_xs<SV, SX, SY, NV, NV>(n, nnz, rowptr, cols, vals, diag, x, y, s, y_plane, group, skip);
+}
+
 template <typename SV, typename SX, typename SY>
 int launch_spmv(int nvec, int64_t n, int64_t nnz, const int64_t* rowptr, const int32_t* cols, const SV* vals,
                 const SV* diag, const SX* x, SY* y, cudaStream_t s, int64_t y_plane = 0, int group = 0,
-                const int* skip = nullptr) {
+                const int* skip = nullptr, int x_stride = 0) {
   if (group != 0 && group != 2 && group != 4 && group != 8 && group != 16 && group != 32) {
     set_error("spmv: group must be 0, 2, 4, 8, 16 or 32, got %d", group);
     return EDG_ERR_ARG;
   }
   switch (nvec) {
-    case 1: return launch_spmv_nv<SV, SX, SY, 1>(n, nnz, rowptr, cols, vals, diag, x, y, s, y_plane, group, skip);
-    case 2: return launch_spmv_nv<SV, SX, SY, 2>(n, nnz, rowptr, cols, vals, diag, x, y, s, y_plane, group, skip);
-    case 3: return launch_spmv_nv<SV, SX, SY, 3>(n, nnz, rowptr, cols, vals, diag, x, y, s, y_plane, group, skip);
-    case 4: return launch_spmv_nv<SV, SX, SY, 4>(n, nnz, rowptr, cols, vals, diag, x, y, s, y_plane, group, skip);
+    case 1: return launch_spmv_nv<SV, SX, SY, 1>(n, nnz, rowptr, cols, vals, diag, x, y, s, y_plane, group, skip,
+                                                       x_stride ? x_stride : 1);
+    case 2: return launch_spmv_nv<SV, SX, SY, 2>(n, nnz, rowptr, cols, vals, diag, x, y, s, y_plane, group, skip,
+                                                       x_stride ? x_stride : 2);
+    case 3: return launch_spmv_nv<SV, SX, SY, 3>(n, nnz, rowptr, cols, vals, diag, x, y, s, y_plane, group, skip,
+                                                       x_stride ? x_stride : 3);
+    case 4: return launch_spmv_nv<SV, SX, SY, 4>(n, nnz, rowptr, cols, vals, diag, x, y, s, y_plane, group, skip,
+                                                       x_stride ? x_stride : 4);
     default: set_error("spmv: nvec must be 1..4, got %d", nvec); return EDG_ERR_ARG;
   }
 }
