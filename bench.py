@@ -325,12 +325,18 @@ def run_edgpu(args, world, rank, local):
     # ---------------- mixed batched: warm-up + timed steps --------------------
     # matvec threads-per-row: the autotuner's choice (or --spmv-group), fixed
     # before the timed region
-    g32 = args.spmv_group or tune_spmv_group(mat, 3, 1, vals=vals32)
+    from edgpu.solvers import sell_layout, tune_matvec32
+
+    # f32 matvec layout (SELL or CSR) and threads per row: the autotuner's
+    # choices (or --spmv-group, which forces CSR), fixed before the timed region
+    fmt32, gsel = ("csr", args.spmv_group) if args.spmv_group else tune_matvec32(mat, 3, vals32)
+    sell32 = sell_layout(mat, vals32) if fmt32 == "sell" else False
+    g32 = gsel if fmt32 == "csr" else tune_spmv_group(mat, 3, 1, vals=vals32)
     g64 = args.spmv_group or tune_spmv_group(mat, 3, 0, vals=mat.vals)
 
     def mixed_step(s32, s64):
         return lanczos_mixed(mat, diags=diags, vals32=vals32, diag32=diag32, diag64=diag64, stats32=s32, stats64=s64,
-                             group32=g32, group64=g64)
+                             group32=g32, group64=g64, sell=sell32)
 
     for _ in range(args.warmup):
         mixed_step(None, None)
@@ -366,8 +372,11 @@ def run_edgpu(args, world, rank, local):
     hbm, peak_kind = peaks()
     nv = 3
     n_pad = (n + 3) // 4 * 4
-    # matvec: values + columns + row pointers + x (f32) + y (f64) + diagonal (f32)
-    spmv_bytes = nnz * (4 + 4) + 8 * (n + 1) + n * nv * 4 + n * nv * 8 + n * nv * 4
+    # matvec: values + columns + row index + x (f32) + y (f64) + diagonal (f32);
+    # the row index is rowptr (8 B a row) for CSR, the row permutation (4 B a
+    # row) plus a width and an offset per slice of 32 rows (12 B) for SELL
+    row_index = 8 * (n + 1) if fmt32 == "csr" else 4 * n + 12 * ((n + 31) // 32)
+    spmv_bytes = nnz * (4 + 4) + row_index + n * nv * 4 + n * nv * 8 + n * nv * 4
     spmv_ms = agg32[0] / max(agg32[1], 1)  # agg32/agg64: the one instrumented sweep
     spmv_achieved = spmv_bytes / (spmv_ms * 1e-3) / 1e9
     # reorthogonalisation of step j (delayed Gram-Schmidt), per row of every
@@ -471,7 +480,11 @@ def run_edgpu(args, world, rank, local):
                      "achieved": reorth_achieved, "peak": hbm, "unit": "GB/s", "frac": reorth_achieved / hbm,
                      "peak_source": peak_kind, "algorithmic_bytes_per_solve": reorth_bytes,
                      "ms_per_solve": reorth_ms_step, "ms_per_lanczos_step": reorth_ms, "traffic": None},
-        "roofline_matvec": {"kernel": f"batched f32 CSR+diag matvec (spmv_k<float,float,double,3,{g32}>)",
+        "roofline_matvec": {"kernel": ("batched f32 SELL-32-sigma + diag matvec (sell_spmv_k<float,3,4>), "
+                                       f"slice padding {sell32.padding:.3f} of the stored pairs"
+                                       if fmt32 == "sell" else
+                                       f"batched f32 CSR+diag matvec (spmv_k<float,float,double,3,{g32},4>)"),
+                            "layout_choice": fmt32,
                             "bound": "hbm", "achieved": spmv_achieved, "peak": hbm, "unit": "GB/s",
                             "frac": spmv_achieved / hbm, "peak_source": peak_kind,
                             "algorithmic_bytes_per_launch": spmv_bytes, "avg_launch_ms": spmv_ms, "traffic": None},

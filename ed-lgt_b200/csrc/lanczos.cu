@@ -786,9 +786,17 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
   const unsigned g_red = 2u * (unsigned)(L.m_max + 1 < 2 * edg::kSmCount ? L.m_max + 1 : 2 * edg::kSmCount);
   // one Lanczos step and its check; every kernel reads the step index and the
   // done flag from the device state
+  const bool sell = p->sell_entries != nullptr && p->dtype == 1;
+  auto matvec = [&](cudaStream_t cs) -> int {
+    if (sell)
+      return edg::launch_sell_spmv(NV, kXs, (n + 31) / 32, p->sell_perm, p->sell_width, p->sell_off,
+                                   (const uint2*)p->sell_entries, (const float*)p->diag, (const float*)X, w, n_pad,
+                                   &st->done, cs);
+    return edg::launch_spmv<T, T, double>(NV, n, p->nnz, p->rowptr, p->cols, (const T*)p->vals, (const T*)p->diag, X,
+                                          w, cs, n_pad, p->spmv_group, &st->done, kXs);
+  };
   auto enqueue_step = [&](cudaStream_t cs) -> int {
-    int st_ = edg::launch_spmv<T, T, double>(NV, n, p->nnz, p->rowptr, p->cols, (const T*)p->vals,
-                                             (const T*)p->diag, X, w, cs, n_pad, p->spmv_group, &st->done, kXs);
+    int st_ = matvec(cs);
     if (st_) return st_;
     dots_bulk_k<T, NV><<<g_dot, edg::bulk::kThreadsAll, dot_smem, cs>>>(V, n_pad, st, w, partial, stride_i, n_seg,
                                                                           err_word);
@@ -841,8 +849,7 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
     for (auto& x : ev) cudaEventCreate(&x);
     for (int j = 0; j < L.m_max; ++j) {
       cudaEventRecord(ev[0], s);
-      int st_ = edg::launch_spmv<T, T, double>(NV, n, p->nnz, p->rowptr, p->cols, (const T*)p->vals,
-                                               (const T*)p->diag, X, w, s, n_pad, p->spmv_group, &st->done, kXs);
+      int st_ = matvec(s);
       if (st_) return st_;
       cudaEventRecord(ev[1], s);
       dots_bulk_k<T, NV><<<g_dot, edg::bulk::kThreadsAll, dot_smem, s>>>(V, n_pad, st, w, partial, stride_i, n_seg,
@@ -990,6 +997,8 @@ int check_problem(const edg_lanczos_problem* p) {
   EDG_REQUIRE(p->max_iter >= 1 && p->max_iter <= 2000, "edg_lanczos: max_iter must be 1..2000");
   EDG_REQUIRE(p->check_every >= 1, "edg_lanczos: check_every must be >= 1");
   EDG_REQUIRE(p->rowptr && p->diag, "edg_lanczos: null matrix pointer");
+  EDG_REQUIRE(p->sell_entries == nullptr || (p->sell_perm && p->sell_width && p->sell_off),
+              "edg_lanczos: incomplete SELL layout");
   return EDG_OK;
 }
 

@@ -249,4 +249,10 @@ int launch_spmv(int nvec, int64_t n, int64_t nnz, const int64_t* rowptr, const i
   }
 }
 
+// Sliced ELL (SELL-32-sigma) matvec of the f32 Krylov path (sell.cu):
+// y[v * y_plane + row] = (A + diag) x, x rows at stride x_stride.
+int launch_sell_spmv(int nvec, int x_stride, int64_t n_slices, const int32_t* perm, const int32_t* width,
+                     const int64_t* off, const uint2* entries, const float* diag, const float* x, double* y,
+                     int64_t y_plane, const int* skip, cudaStream_t s);
+
 }  // namespace edg

@@ -22,7 +22,8 @@ import torch
 from . import _lib
 from ._lib import check, lib, ptr, stream_handle
 
-__all__ = ["LanczosResult", "lanczos", "lanczos_mixed", "stack_diagonals", "tune_spmv_group"]
+__all__ = ["LanczosResult", "SellLayout", "lanczos", "lanczos_mixed", "sell_layout", "stack_diagonals",
+           "tune_matvec32", "tune_spmv_group"]
 
 SPMV_GROUPS = (2, 4, 8, 16, 32)
 
@@ -80,6 +81,94 @@ def tune_spmv_group(mat, nvec=1, dtype=0, reps=5, vals=None, diag=None, ctx=None
     return best
 
 
+class SellLayout:
+    """SELL-32-sigma copy of a matrix's off-diagonal part with f32 values
+    (``edg_sell_order`` / ``edg_scan_i64`` / ``edg_sell_fill``), the layout of
+    the f32 Krylov path's matvec: rows sorted by length inside windows of 4096,
+    slices of 32 rows, each slice's entries column-major as 8-byte
+    (column, value) pairs."""
+
+    def __init__(self, mat, vals=None):
+        dev = mat.rowptr.device
+        n = mat.n
+        st = stream_handle()
+        ns = int(lib.edg_sell_slices(n))
+        self.n, self.n_slices = n, ns
+        self.perm = torch.empty(max(ns * 32, 1), dtype=torch.int32, device=dev)
+        self.width = torch.empty(max(ns, 1), dtype=torch.int32, device=dev)
+        counts = torch.empty(max(ns, 1), dtype=torch.int64, device=dev)
+        self.off = torch.empty(ns + 1, dtype=torch.int64, device=dev)
+        check(lib.edg_sell_order(ptr(mat.rowptr), n, ptr(self.perm), ptr(self.width), ptr(counts), st),
+              "edg_sell_order")
+        scratch = torch.empty(max(1, lib.edg_scan_scratch_elems(ns)), dtype=torch.int64, device=dev)
+        check(lib.edg_scan_i64(ptr(counts), ptr(self.off), ns, ptr(scratch), st), "edg_scan_i64")
+        self.pairs = int(self.off[ns].item()) if ns else 0
+        self.entries = torch.empty(max(self.pairs, 1) * 2, dtype=torch.int32, device=dev)
+        v = mat.vals if vals is None else vals
+        dt = 1 if v.dtype == torch.float32 else 0
+        if mat.nnz:
+            check(lib.edg_sell_fill(dt, ptr(mat.rowptr), ptr(mat.cols), ptr(v), n, ptr(self.perm), ptr(self.width),
+                                    ptr(self.off), ptr(self.entries), st), "edg_sell_fill")
+        else:
+            self.entries.zero_()
+        self.nnz = mat.nnz
+
+    @property
+    def padding(self):
+        """Fraction of stored pairs that are slice padding."""
+        return 1.0 - self.nnz / max(self.pairs, 1)
+
+
+def sell_layout(mat, vals32=None):
+    """The matrix's SELL layout (built once, kept on the matrix)."""
+    lay = getattr(mat, "_sell32", None)
+    if lay is None:
+        lay = mat._sell32 = SellLayout(mat, vals32)
+    return lay
+
+
+def tune_matvec32(mat, nvec, vals32=None, reps=5, ctx=None):
+    """Autotuner of the f32 matvec layout: times the SELL kernel against the
+    fastest CSR thread-per-row choice on this matrix (CUDA events after a
+    warm-up launch) and keeps the choice in the tuning context under the
+    matrix shape.  Returns ("sell", 0) or ("csr", threads per row)."""
+    from .context import default_context
+
+    ctx = ctx if ctx is not None else default_context(mat.rowptr.device)
+    key = _spmv_key(mat.n, mat.nnz, 0x5E11, nvec)
+    got = ctx.get(key, 2)
+    if got is not None:
+        return ("sell", 0) if got[0] == 1 else ("csr", got[1])
+    dev = mat.rowptr.device
+    vals32 = mat.vals.to(torch.float32) if vals32 is None else vals32
+    g = tune_spmv_group(mat, nvec, 1, vals=vals32, ctx=ctx)
+    lay = sell_layout(mat, vals32)
+    diag = torch.zeros((mat.n, nvec), dtype=torch.float32, device=dev)
+    x = torch.ones((mat.n, nvec), dtype=torch.float32, device=dev)
+    y32 = torch.empty_like(x)
+    y64 = torch.empty((nvec, mat.n), dtype=torch.float64, device=dev)
+
+    def t_of(launch):
+        launch()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            launch()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    t_csr = t_of(lambda: check(lib.edg_spmv_group(1, mat.n, mat.nnz, ptr(mat.rowptr), ptr(mat.cols) if mat.nnz else None,
+                                                  ptr(vals32) if mat.nnz else None, ptr(diag), nvec, ptr(x), ptr(y32),
+                                                  g, stream_handle()), "edg_spmv_group"))
+    t_sell = t_of(lambda: check(lib.edg_spmv_sell(mat.n, nvec, ptr(lay.perm), ptr(lay.width), ptr(lay.off),
+                                                  ptr(lay.entries), ptr(diag), ptr(x), ptr(y64), mat.n,
+                                                  stream_handle()), "edg_spmv_sell"))
+    choice = ("sell", 0) if t_sell < t_csr else ("csr", g)
+    ctx.put(key, (1 if choice[0] == "sell" else 0, g))
+    return choice
+
+
 class LanczosResult:
     def __init__(self, evals, evecs, iters, resid):
         self.evals = evals      # (nvec, k) float64 numpy
@@ -89,7 +178,7 @@ class LanczosResult:
 
 
 def _problem(dtype, n, nnz, rowptr, cols, vals, diag, nvec, k, max_iter, tol, check_every, seed, v0, stats=None,
-             group=0):
+             group=0, sell=None):
     p = _lib.LanczosProblem()
     p.dtype = dtype
     p.n_rows = n
@@ -107,6 +196,9 @@ def _problem(dtype, n, nnz, rowptr, cols, vals, diag, nvec, k, max_iter, tol, ch
     p.v0 = ptr(v0) if v0 is not None else None
     p.stats = stats.ctypes.data if stats is not None else None
     p.spmv_group = group
+    if sell is not None:
+        p.sell_perm, p.sell_width, p.sell_off = ptr(sell.perm), ptr(sell.width), ptr(sell.off)
+        p.sell_entries = ptr(sell.entries)
     return p
 
 
@@ -124,7 +216,7 @@ def _progress_words(device):
 
 def run_lanczos(dtype, n, nnz, rowptr, cols, vals, diag, nvec=1, k=1, max_iter=300, tol=1e-12, check_every=5,
                 seed=1234, v0=None, want_vectors=True, allow_unconverged=False, workspace=None, stats=None,
-                group=0, poll_host=True):
+                group=0, poll_host=True, sell=None):
     """Low-level call of ``edg_lanczos``; ``diag`` is ``[n][nvec]`` in the dtype.
 
     ``stats``: optional float64 numpy array of 6 entries filled with the
@@ -132,10 +224,12 @@ def run_lanczos(dtype, n, nnz, rowptr, cols, vals, diag, nvec=1, k=1, max_iter=3
     then launched one by one with events around each phase.  Without it the
     steps run as replays of a CUDA graph; ``poll_host=False`` makes the host
     synchronise once per replay instead of polling pinned progress words.
+    ``sell``: a :class:`SellLayout` of the matrix (f32 path only) for the
+    matvec.
     """
     max_iter = int(min(max_iter, n))
     p = _problem(dtype, n, nnz, rowptr, cols, vals, diag, nvec, k, max_iter, tol, check_every, seed, v0, stats,
-                 group)
+                 group, sell if dtype == 1 else None)
     progress = _progress_words(rowptr.device) if poll_host else None
     p.host_progress = progress.data_ptr() if poll_host else None
     wb = lib.edg_lanczos_workspace_bytes(ctypes.byref(p))
@@ -174,7 +268,7 @@ def stack_diagonals(diags, dtype):
 
 def lanczos_mixed(mat, diags=None, k=1, tol32=1e-5, tol=1e-12, max_iter=400, refine_iter=5, check_every=5,
                   seed=1234, stats32=None, stats64=None, vals32=None, diag32=None, diag64=None, tune=True,
-                  group32=0, group64=0):
+                  group32=0, group64=0, sell=None):
     """Mixed-precision (f32 Krylov, f64 recurrence) Lanczos + f64 refinement.
 
     ``diags``: list of f64 device diagonals (one per problem, <= 4) sharing the
@@ -191,10 +285,15 @@ def lanczos_mixed(mat, diags=None, k=1, tol32=1e-5, tol=1e-12, max_iter=400, ref
         diag32 = stack_diagonals(diags, torch.float32)
     if diag64 is None:
         diag64 = stack_diagonals(diags, torch.float64)
+    if sell is None and tune and not group32:
+        fmt, g = tune_matvec32(mat, nvec, vals32)
+        sell = sell_layout(mat, vals32) if fmt == "sell" else False
+        group32 = group32 or g
+    lay = sell_layout(mat, vals32) if sell is True else (sell or None)
     g32 = group32 or (tune_spmv_group(mat, nvec, 1, vals=vals32) if tune else 0)
     g64 = group64 or (tune_spmv_group(mat, nvec, 0, vals=mat.vals) if tune else 0)
     r32 = run_lanczos(1, mat.n, mat.nnz, mat.rowptr, mat.cols, vals32, diag32, nvec=nvec, k=k, max_iter=max_iter,
-                      tol=tol32, check_every=check_every, seed=seed, stats=stats32, group=g32)
+                      tol=tol32, check_every=check_every, seed=seed, stats=stats32, group=g32, sell=lay)
     # f64 refinement: short Lanczos restarted from the f32 Ritz vector (ground state)
     v0 = torch.empty((mat.n, nvec), dtype=torch.float64, device=diag64.device)
     check(lib.edg_convert(1, ptr(r32.evecs), 0, ptr(v0), mat.n * nvec, stream_handle()), "edg_convert")

@@ -257,6 +257,29 @@ int edg_spmv_group(int32_t dtype, int64_t n_rows, int64_t nnz,
                    const void* diag, int32_t nvec, const void* x, void* y,
                    int32_t group, cudaStream_t stream);
 
+/* Sliced ELL (SELL-32-sigma) layout of the off-diagonal matrix for the f32
+ * Krylov path (same product as csr_spmv, qmb_hamiltonian.py:705-730, with a
+ * row layout built for coalesced loads): rows sorted by length (descending,
+ * stable) inside windows of 4096 rows, slices of 32 sorted rows, entries of
+ * a slice stored column-major as 8-byte (int32 column, f32 value) pairs.
+ * Build: edg_sell_order (perm [n_slices*32], -1 = padding; width and
+ * counts [n_slices] = width * 32), exclusive scan of counts into off
+ * [n_slices+1] (edg_scan_i64), then edg_sell_fill (entries [off[n_slices]]
+ * pairs; dtype of vals 0 = f64, 1 = f32). */
+int64_t edg_sell_slices(int64_t n_rows);
+int edg_sell_order(const int64_t* rowptr, int64_t n_rows, int32_t* perm,
+                   int32_t* width, int64_t* counts, cudaStream_t stream);
+int edg_sell_fill(int32_t dtype, const int64_t* rowptr, const int32_t* cols,
+                  const void* vals, int64_t n_rows, const int32_t* perm,
+                  const int32_t* width, const int64_t* off, void* entries,
+                  cudaStream_t stream);
+/* y[v * y_plane + r] (f64, planar; y_plane 0 = n_rows) = (A + diag) x with
+ * x interleaved [n_rows][nvec] (f32), diag [n_rows][nvec] (f32). */
+int edg_spmv_sell(int64_t n_rows, int32_t nvec, const int32_t* perm,
+                  const int32_t* width, const int64_t* off, const void* entries,
+                  const float* diag, const float* x, double* y, int64_t y_plane,
+                  cudaStream_t stream);
+
 /* Casts between f64 <-> f32 (or c128 <-> c64) arrays of n scalars. */
 int edg_convert(int32_t dtype_in, const void* in, int32_t dtype_out, void* out,
                 int64_t n_scalars, cudaStream_t stream);
@@ -302,6 +325,10 @@ typedef struct {
   int32_t* host_progress; /* optional PINNED host memory, >= 4 int32: the   */
                           /* device writes [0] steps done, [1] done flag;   */
                           /* NULL = the host synchronises once per replay   */
+  const int32_t* sell_perm;   /* optional SELL layout of the off-diagonal   */
+  const int32_t* sell_width;  /* matrix (edg_sell_*), used by the f32 path  */
+  const int64_t* sell_off;    /* when sell_entries is not NULL              */
+  const void* sell_entries;
 } edg_lanczos_problem;
 
 /* Bytes of device workspace edg_lanczos needs. */
