@@ -329,9 +329,14 @@ def run_edgpu(args, world, rank, local):
 
     # f32 matvec layout (SELL or CSR) and threads per row: the autotuner's
     # choices (or --spmv-group, which forces CSR), fixed before the timed region
-    fmt32, gsel = ("csr", args.spmv_group) if args.spmv_group else tune_matvec32(mat, 3, vals32)
-    sell32 = sell_layout(mat, vals32) if fmt32 == "sell" else False
-    g32 = gsel if fmt32 == "csr" else tune_spmv_group(mat, 3, 1, vals=vals32)
+    if args.matvec_layout == "auto":
+        fmt32, param = ("csr", args.spmv_group) if args.spmv_group else tune_matvec32(mat, 3, vals32)
+    elif args.matvec_layout == "sell":
+        fmt32, param = "sell", args.sell_window
+    else:
+        fmt32, param = "csr", args.spmv_group or tune_spmv_group(mat, 3, 1, vals=vals32)
+    sell32 = sell_layout(mat, vals32, param) if fmt32 == "sell" else False
+    g32 = param if fmt32 == "csr" else tune_spmv_group(mat, 3, 1, vals=vals32)
     g64 = args.spmv_group or tune_spmv_group(mat, 3, 0, vals=mat.vals)
 
     def mixed_step(s32, s64):
@@ -481,7 +486,8 @@ def run_edgpu(args, world, rank, local):
                      "peak_source": peak_kind, "algorithmic_bytes_per_solve": reorth_bytes,
                      "ms_per_solve": reorth_ms_step, "ms_per_lanczos_step": reorth_ms, "traffic": None},
         "roofline_matvec": {"kernel": ("batched f32 SELL-32-sigma + diag matvec (sell_spmv_k<float,3,4>), "
-                                       f"slice padding {sell32.padding:.3f} of the stored pairs"
+                                       f"sort window {sell32.window}, slice padding {sell32.padding:.3f} of the "
+                                       "stored pairs"
                                        if fmt32 == "sell" else
                                        f"batched f32 CSR+diag matvec (spmv_k<float,float,double,3,{g32},4>)"),
                             "layout_choice": fmt32,
@@ -1018,6 +1024,9 @@ def main():
                          "corr: SU(2) L=16 two-body correlator matrices; entropy: SU(2) L=14 half-chain entanglement; "
                          "momentum: SU(2) L=14 PBC zero-momentum ground state")
     ap.add_argument("--quench-time", type=float, default=20.0)
+    ap.add_argument("--matvec-layout", default="auto", choices=["auto", "sell", "csr"],
+                    help="f32 matvec layout of the headline solve; auto = the autotuner's choice")
+    ap.add_argument("--sell-window", type=int, default=32, help="SELL sort window with --matvec-layout sell")
     ap.add_argument("--spmv-group", type=int, default=0,
                     help="matvec threads per row (2/4/8/16/32); 0 = autotune before the timed region")
     args = ap.parse_args()

@@ -8,26 +8,29 @@
 // entry stream is one 256-byte contiguous warp access (the CSR kernel's loads
 // of columns and values touch one segment per row of the warp), and only the
 // x gathers stay scattered.  Rows shorter than their slice's width are padded
-// with (column 0, value 0) entries; the length sort keeps that padding small.
-// perm[sorted position] gives the original row (-1 for the slice padding of
-// the last window); y and the diagonal are addressed through it.
+// with (column -1, value 0) entries, which the matvec loads but does not
+// gather.  The sort window sigma trades padding (a long window) against the
+// locality of the x gathers (neighbouring rows of the basis order touch
+// neighbouring columns, which the L1 cache serves): sigma = 32 keeps the basis
+// order.  perm[sorted position] gives the original row (-1 for the slice
+// padding of the last window); y and the diagonal are addressed through it.
 #include "spmv.cuh"
 
 namespace {
 
-constexpr int kSellWindow = 4096;  // rows per sorting window (128 slices)
+constexpr int kSellWindowMax = 4096;  // longest sorting window (128 slices)
 constexpr int kLenBuckets = 256;   // lengths >= 255 share the last bucket
 
 // One CTA per window: stable counting sort of its rows by length, descending.
 // The bucket of every row is staged in shared memory and the histogram is
 // parallel; thread 0 then places the rows in row order (deterministic).
-__global__ void __launch_bounds__(256) sell_sort_k(const int64_t* __restrict__ rowptr, int64_t n,
+__global__ void __launch_bounds__(256) sell_sort_k(const int64_t* __restrict__ rowptr, int64_t n, int window,
                                                    int32_t* __restrict__ perm, int32_t* __restrict__ width,
                                                    int64_t* __restrict__ counts) {
   __shared__ int hist[kLenBuckets];
-  __shared__ unsigned char bucket[kSellWindow];
-  const int64_t w0 = (int64_t)blockIdx.x * kSellWindow;
-  const int64_t w1 = w0 + kSellWindow < n ? w0 + kSellWindow : n;
+  __shared__ unsigned char bucket[kSellWindowMax];
+  const int64_t w0 = (int64_t)blockIdx.x * window;
+  const int64_t w1 = w0 + window < n ? w0 + window : n;
   for (int b = threadIdx.x; b < kLenBuckets; b += blockDim.x) hist[b] = 0;
   __syncthreads();
   for (int64_t r = w0 + threadIdx.x; r < w1; r += blockDim.x) {
@@ -49,7 +52,7 @@ __global__ void __launch_bounds__(256) sell_sort_k(const int64_t* __restrict__ r
   __syncthreads();
   // slice padding of the last window, then every slice's width (its first
   // row is its longest)
-  const int64_t w_end = w0 + kSellWindow;
+  const int64_t w_end = w0 + window;
   for (int64_t q = w1 + threadIdx.x; q < w_end && q < (n + 31) / 32 * 32; q += blockDim.x) perm[q] = -1;
   __syncthreads();
   for (int64_t sl = w0 / 32 + threadIdx.x; sl * 32 < w1; sl += blockDim.x) {
@@ -75,7 +78,7 @@ __global__ void sell_fill_k(const int64_t* __restrict__ rowptr, const int32_t* _
     const int64_t beg = r >= 0 ? rowptr[r] : 0, len = r >= 0 ? rowptr[r + 1] - beg : 0;
     uint2* e = entries + off[sl];
     for (int k = 0; k < w; ++k) {
-      uint2 p = make_uint2(0u, 0u);
+      uint2 p = make_uint2(0xFFFFFFFFu, 0u);  // padding: no gather
       if (k < len) {
         p.x = (unsigned)cols[beg + k];
         p.y = __float_as_uint((float)vals[beg + k]);
@@ -108,10 +111,10 @@ __global__ void __launch_bounds__(256) sell_spmv_k(int64_t n_slices, const int32
     for (int k0 = 0; k0 < w; k0 += U) {
       uint2 p[U];
 #pragma unroll
-      for (int u = 0; u < U; ++u) p[u] = k0 + u < w ? __ldg(e + (int64_t)(k0 + u) * 32) : make_uint2(0u, 0u);
+      for (int u = 0; u < U; ++u) p[u] = k0 + u < w ? __ldg(e + (int64_t)(k0 + u) * 32) : make_uint2(0xFFFFFFFFu, 0u);
 #pragma unroll
       for (int u = 0; u < U; ++u) {
-        if (k0 + u < w) {
+        if (p[u].x != 0xFFFFFFFFu) {
           double xr[NV];
           edg::RowX<SX, NV, XS>::ld(x, (int64_t)p[u].x, xr);
           const double a = (double)__uint_as_float(p[u].y);
@@ -161,13 +164,15 @@ int launch_sell_spmv(int nvec, int x_stride, int64_t n_slices, const int32_t* pe
 
 extern "C" int64_t edg_sell_slices(int64_t n_rows) { return n_rows < 0 ? -1 : (n_rows + 31) / 32; }
 
-extern "C" int edg_sell_order(const int64_t* rowptr, int64_t n_rows, int32_t* perm, int32_t* width,
-                              int64_t* counts, cudaStream_t stream) {
+extern "C" int edg_sell_order(const int64_t* rowptr, int64_t n_rows, int32_t window, int32_t* perm,
+                              int32_t* width, int64_t* counts, cudaStream_t stream) {
   EDG_REQUIRE(n_rows >= 0 && n_rows < INT32_MAX, "edg_sell_order: n_rows out of range");
+  EDG_REQUIRE(window >= 32 && window <= kSellWindowMax && window % 32 == 0,
+              "edg_sell_order: window must be a multiple of 32 in [32, %d], got %d", kSellWindowMax, window);
   EDG_REQUIRE(rowptr && perm && width && counts, "edg_sell_order: null pointer");
   if (n_rows == 0) return EDG_OK;
-  const unsigned windows = (unsigned)((n_rows + kSellWindow - 1) / kSellWindow);
-  sell_sort_k<<<windows, 256, 0, stream>>>(rowptr, n_rows, perm, width, counts);
+  const unsigned windows = (unsigned)((n_rows + window - 1) / window);
+  sell_sort_k<<<windows, 256, 0, stream>>>(rowptr, n_rows, window, perm, width, counts);
   EDG_CHECK_LAUNCH("edg_sell_order");
   return EDG_OK;
 }
@@ -192,10 +197,27 @@ extern "C" int edg_sell_fill(int32_t dtype, const int64_t* rowptr, const int32_t
 
 extern "C" int edg_spmv_sell(int64_t n_rows, int32_t nvec, const int32_t* perm, const int32_t* width,
                              const int64_t* off, const void* entries, const float* diag, const float* x,
-                             double* y, int64_t y_plane, cudaStream_t stream) {
+                             int32_t x_stride, double* y, int64_t y_plane, cudaStream_t stream) {
   EDG_REQUIRE(n_rows >= 0 && nvec >= 1 && nvec <= 4, "edg_spmv_sell: bad size");
+  EDG_REQUIRE(x_stride == nvec || (nvec == 3 && x_stride == 4), "edg_spmv_sell: x_stride must be nvec "
+                                                                "(or 4 for nvec = 3)");
   EDG_REQUIRE(perm && width && off && entries && diag && x && y, "edg_spmv_sell: null pointer");
   if (n_rows == 0) return EDG_OK;
-  return edg::launch_sell_spmv(nvec, nvec, (n_rows + 31) / 32, perm, width, off, (const uint2*)entries, diag, x, y,
-                               y_plane > 0 ? y_plane : n_rows, nullptr, stream);
+  return edg::launch_sell_spmv(nvec, x_stride, (n_rows + 31) / 32, perm, width, off, (const uint2*)entries, diag, x,
+                               y, y_plane > 0 ? y_plane : n_rows, nullptr, stream);
+}
+
+// CSR matvec in the f32 Krylov path's configuration (f32 values, diagonal
+// and x with rows at stride x_stride, f64 planar output), for the autotuner's
+// comparison with the SELL layout.
+extern "C" int edg_spmv_f32_planar(int64_t n_rows, int64_t nnz, const int64_t* rowptr, const int32_t* cols,
+                                   const float* vals, const float* diag, int32_t nvec, const float* x,
+                                   int32_t x_stride, double* y, int64_t y_plane, int32_t group, cudaStream_t stream) {
+  EDG_REQUIRE(n_rows >= 0 && nnz >= 0 && nvec >= 1 && nvec <= 4, "edg_spmv_f32_planar: bad size");
+  EDG_REQUIRE(x_stride == nvec || (nvec == 3 && x_stride == 4), "edg_spmv_f32_planar: x_stride must be nvec "
+                                                               "(or 4 for nvec = 3)");
+  EDG_REQUIRE(rowptr && diag && x && y && (nnz == 0 || (cols && vals)), "edg_spmv_f32_planar: null pointer");
+  if (n_rows == 0) return EDG_OK;
+  return edg::launch_spmv<float, float, double>(nvec, n_rows, nnz, rowptr, cols, vals, diag, x, y, stream,
+                                                y_plane > 0 ? y_plane : n_rows, group, nullptr, x_stride);
 }

@@ -283,9 +283,10 @@ _SIGS = {
     "edg_spmv": (I32, [I32, I64, I64, P, P, P, P, I32, P, P, P]),
     "edg_convert": (I32, [I32, P, I32, P, I64, P]),
     "edg_sell_slices": (I64, [I64]),
-    "edg_sell_order": (I32, [P, I64, P, P, P, P]),
+    "edg_sell_order": (I32, [P, I64, I32, P, P, P, P]),
     "edg_sell_fill": (I32, [I32, P, P, P, I64, P, P, P, P, P]),
-    "edg_spmv_sell": (I32, [I64, I32, P, P, P, P, P, P, P, I64, P]),
+    "edg_spmv_sell": (I32, [I64, I32, P, P, P, P, P, P, I32, P, I64, P]),
+    "edg_spmv_f32_planar": (I32, [I64, I64, P, P, P, P, I32, P, I32, P, I64, I32, P]),
     "edg_spmv_group": (I32, [I32, I64, I64, P, P, P, P, I32, P, P, I32, P]),
     "edg_lanczos_workspace_bytes": (I64, [C.POINTER(LanczosProblem)]),
     "edg_lanczos": (I32, [C.POINTER(LanczosProblem), P, I64, P, P, P, P, P]),

@@ -83,22 +83,22 @@ def tune_spmv_group(mat, nvec=1, dtype=0, reps=5, vals=None, diag=None, ctx=None
 
 class SellLayout:
     """SELL-32-sigma copy of a matrix's off-diagonal part with f32 values
-    (``edg_sell_order`` / ``edg_scan_i64`` / ``edg_sell_fill``), the layout of
-    the f32 Krylov path's matvec: rows sorted by length inside windows of 4096,
-    slices of 32 rows, each slice's entries column-major as 8-byte
-    (column, value) pairs."""
+    (``edg_sell_order`` / ``edg_scan_i64`` / ``edg_sell_fill``), a layout of
+    the f32 Krylov path's matvec: rows sorted by length inside windows of
+    ``window`` rows (32 keeps the basis order), slices of 32 rows, each
+    slice's entries column-major as 8-byte (column, value) pairs."""
 
-    def __init__(self, mat, vals=None):
+    def __init__(self, mat, vals=None, window=32):
         dev = mat.rowptr.device
         n = mat.n
         st = stream_handle()
         ns = int(lib.edg_sell_slices(n))
-        self.n, self.n_slices = n, ns
+        self.n, self.n_slices, self.window = n, ns, int(window)
         self.perm = torch.empty(max(ns * 32, 1), dtype=torch.int32, device=dev)
         self.width = torch.empty(max(ns, 1), dtype=torch.int32, device=dev)
         counts = torch.empty(max(ns, 1), dtype=torch.int64, device=dev)
         self.off = torch.empty(ns + 1, dtype=torch.int64, device=dev)
-        check(lib.edg_sell_order(ptr(mat.rowptr), n, ptr(self.perm), ptr(self.width), ptr(counts), st),
+        check(lib.edg_sell_order(ptr(mat.rowptr), n, self.window, ptr(self.perm), ptr(self.width), ptr(counts), st),
               "edg_sell_order")
         scratch = torch.empty(max(1, lib.edg_scan_scratch_elems(ns)), dtype=torch.int64, device=dev)
         check(lib.edg_scan_i64(ptr(counts), ptr(self.off), ns, ptr(scratch), st), "edg_scan_i64")
@@ -110,7 +110,7 @@ class SellLayout:
             check(lib.edg_sell_fill(dt, ptr(mat.rowptr), ptr(mat.cols), ptr(v), n, ptr(self.perm), ptr(self.width),
                                     ptr(self.off), ptr(self.entries), st), "edg_sell_fill")
         else:
-            self.entries.zero_()
+            self.entries.fill_(-1)
         self.nnz = mat.nnz
 
     @property
@@ -119,34 +119,40 @@ class SellLayout:
         return 1.0 - self.nnz / max(self.pairs, 1)
 
 
-def sell_layout(mat, vals32=None):
-    """The matrix's SELL layout (built once, kept on the matrix)."""
-    lay = getattr(mat, "_sell32", None)
-    if lay is None:
-        lay = mat._sell32 = SellLayout(mat, vals32)
-    return lay
+def sell_layout(mat, vals32=None, window=32):
+    """The matrix's SELL layout for a sort window (built once, kept on the
+    matrix)."""
+    cache = getattr(mat, "_sell32", None)
+    if cache is None:
+        cache = mat._sell32 = {}
+    if window not in cache:
+        cache[window] = SellLayout(mat, vals32, window)
+    return cache[window]
+
+
+SELL_WINDOWS = (32, 256, 4096)
 
 
 def tune_matvec32(mat, nvec, vals32=None, reps=5, ctx=None):
-    """Autotuner of the f32 matvec layout: times the SELL kernel against the
-    fastest CSR thread-per-row choice on this matrix (CUDA events after a
-    warm-up launch) and keeps the choice in the tuning context under the
-    matrix shape.  Returns ("sell", 0) or ("csr", threads per row)."""
+    """Autotuner of the f32 Krylov path's matvec: times, in that path's
+    configuration (f32 values and x with padded rows, f64 planar output),
+    the CSR kernel for every threads-per-row choice and the SELL kernel for
+    every sort window (CUDA events after a warm-up launch), and keeps the
+    fastest in the tuning context under the matrix shape.  Returns
+    ("csr", threads per row) or ("sell", window)."""
     from .context import default_context
 
     ctx = ctx if ctx is not None else default_context(mat.rowptr.device)
     key = _spmv_key(mat.n, mat.nnz, 0x5E11, nvec)
     got = ctx.get(key, 2)
     if got is not None:
-        return ("sell", 0) if got[0] == 1 else ("csr", got[1])
+        return ("sell", got[1]) if got[0] == 1 else ("csr", got[1])
     dev = mat.rowptr.device
     vals32 = mat.vals.to(torch.float32) if vals32 is None else vals32
-    g = tune_spmv_group(mat, nvec, 1, vals=vals32, ctx=ctx)
-    lay = sell_layout(mat, vals32)
+    xs = 4 if nvec == 3 else nvec
     diag = torch.zeros((mat.n, nvec), dtype=torch.float32, device=dev)
-    x = torch.ones((mat.n, nvec), dtype=torch.float32, device=dev)
-    y32 = torch.empty_like(x)
-    y64 = torch.empty((nvec, mat.n), dtype=torch.float64, device=dev)
+    x = torch.ones((mat.n, xs), dtype=torch.float32, device=dev)
+    y = torch.empty((nvec, mat.n), dtype=torch.float64, device=dev)
 
     def t_of(launch):
         launch()
@@ -158,15 +164,26 @@ def tune_matvec32(mat, nvec, vals32=None, reps=5, ctx=None):
         torch.cuda.synchronize()
         return a.elapsed_time(b) / reps
 
-    t_csr = t_of(lambda: check(lib.edg_spmv_group(1, mat.n, mat.nnz, ptr(mat.rowptr), ptr(mat.cols) if mat.nnz else None,
-                                                  ptr(vals32) if mat.nnz else None, ptr(diag), nvec, ptr(x), ptr(y32),
-                                                  g, stream_handle()), "edg_spmv_group"))
-    t_sell = t_of(lambda: check(lib.edg_spmv_sell(mat.n, nvec, ptr(lay.perm), ptr(lay.width), ptr(lay.off),
-                                                  ptr(lay.entries), ptr(diag), ptr(x), ptr(y64), mat.n,
-                                                  stream_handle()), "edg_spmv_sell"))
-    choice = ("sell", 0) if t_sell < t_csr else ("csr", g)
-    ctx.put(key, (1 if choice[0] == "sell" else 0, g))
-    return choice
+    best, best_t = None, float("inf")
+    for g in SPMV_GROUPS:
+        t = t_of(lambda: check(lib.edg_spmv_f32_planar(mat.n, mat.nnz, ptr(mat.rowptr),
+                                                       ptr(mat.cols) if mat.nnz else None,
+                                                       ptr(vals32) if mat.nnz else None, ptr(diag), nvec, ptr(x), xs,
+                                                       ptr(y), mat.n, g, stream_handle()), "edg_spmv_f32_planar"))
+        if t < best_t:
+            best, best_t = ("csr", g), t
+    for wdw in SELL_WINDOWS:
+        lay = sell_layout(mat, vals32, wdw)
+        t = t_of(lambda: check(lib.edg_spmv_sell(mat.n, nvec, ptr(lay.perm), ptr(lay.width), ptr(lay.off),
+                                                 ptr(lay.entries), ptr(diag), ptr(x), xs, ptr(y), mat.n,
+                                                 stream_handle()), "edg_spmv_sell"))
+        if t < best_t:
+            best, best_t = ("sell", wdw), t
+    # layouts that lost are not kept on the matrix
+    keep = best[1] if best[0] == "sell" else None
+    mat._sell32 = {w: l for w, l in mat._sell32.items() if w == keep}
+    ctx.put(key, (1 if best[0] == "sell" else 0, best[1]))
+    return best
 
 
 class LanczosResult:
@@ -286,9 +303,11 @@ def lanczos_mixed(mat, diags=None, k=1, tol32=1e-5, tol=1e-12, max_iter=400, ref
     if diag64 is None:
         diag64 = stack_diagonals(diags, torch.float64)
     if sell is None and tune and not group32:
-        fmt, g = tune_matvec32(mat, nvec, vals32)
-        sell = sell_layout(mat, vals32) if fmt == "sell" else False
-        group32 = group32 or g
+        fmt, param = tune_matvec32(mat, nvec, vals32)
+        if fmt == "sell":
+            sell = sell_layout(mat, vals32, param)
+        else:
+            sell, group32 = False, param
     lay = sell_layout(mat, vals32) if sell is True else (sell or None)
     g32 = group32 or (tune_spmv_group(mat, nvec, 1, vals=vals32) if tune else 0)
     g64 = group64 or (tune_spmv_group(mat, nvec, 0, vals=mat.vals) if tune else 0)

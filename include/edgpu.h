@@ -260,25 +260,35 @@ int edg_spmv_group(int32_t dtype, int64_t n_rows, int64_t nnz,
 /* Sliced ELL (SELL-32-sigma) layout of the off-diagonal matrix for the f32
  * Krylov path (same product as csr_spmv, qmb_hamiltonian.py:705-730, with a
  * row layout built for coalesced loads): rows sorted by length (descending,
- * stable) inside windows of 4096 rows, slices of 32 sorted rows, entries of
- * a slice stored column-major as 8-byte (int32 column, f32 value) pairs.
- * Build: edg_sell_order (perm [n_slices*32], -1 = padding; width and
- * counts [n_slices] = width * 32), exclusive scan of counts into off
- * [n_slices+1] (edg_scan_i64), then edg_sell_fill (entries [off[n_slices]]
- * pairs; dtype of vals 0 = f64, 1 = f32). */
+ * stable) inside windows of `window` rows (a multiple of 32, at most 4096;
+ * 32 keeps the basis order), slices of 32 sorted rows, entries of a slice
+ * stored column-major as 8-byte (int32 column, f32 value) pairs, padding
+ * marked by column -1.  Build: edg_sell_order (perm [n_slices*32], -1 =
+ * padding; width and counts [n_slices] = width * 32), exclusive scan of
+ * counts into off [n_slices+1] (edg_scan_i64), then edg_sell_fill (entries
+ * [off[n_slices]] pairs; dtype of vals 0 = f64, 1 = f32). */
 int64_t edg_sell_slices(int64_t n_rows);
-int edg_sell_order(const int64_t* rowptr, int64_t n_rows, int32_t* perm,
-                   int32_t* width, int64_t* counts, cudaStream_t stream);
+int edg_sell_order(const int64_t* rowptr, int64_t n_rows, int32_t window,
+                   int32_t* perm, int32_t* width, int64_t* counts,
+                   cudaStream_t stream);
 int edg_sell_fill(int32_t dtype, const int64_t* rowptr, const int32_t* cols,
                   const void* vals, int64_t n_rows, const int32_t* perm,
                   const int32_t* width, const int64_t* off, void* entries,
                   cudaStream_t stream);
 /* y[v * y_plane + r] (f64, planar; y_plane 0 = n_rows) = (A + diag) x with
- * x interleaved [n_rows][nvec] (f32), diag [n_rows][nvec] (f32). */
+ * x interleaved (f32 rows of x_stride entries: nvec, or 4 for nvec = 3),
+ * diag [n_rows][nvec] (f32). */
 int edg_spmv_sell(int64_t n_rows, int32_t nvec, const int32_t* perm,
                   const int32_t* width, const int64_t* off, const void* entries,
-                  const float* diag, const float* x, double* y, int64_t y_plane,
-                  cudaStream_t stream);
+                  const float* diag, const float* x, int32_t x_stride,
+                  double* y, int64_t y_plane, cudaStream_t stream);
+/* The CSR matvec in the same configuration (f32 values, diagonal and x, f64
+ * planar y): the f32 Krylov path's CSR kernel, for layout comparisons. */
+int edg_spmv_f32_planar(int64_t n_rows, int64_t nnz, const int64_t* rowptr,
+                        const int32_t* cols, const float* vals,
+                        const float* diag, int32_t nvec, const float* x,
+                        int32_t x_stride, double* y, int64_t y_plane,
+                        int32_t group, cudaStream_t stream);
 
 /* Casts between f64 <-> f32 (or c128 <-> c64) arrays of n scalars. */
 int edg_convert(int32_t dtype_in, const void* in, int32_t dtype_out, void* out,

@@ -19,7 +19,8 @@ def _mat(name, dev, g=None, m=None):
 
 @pytest.mark.parametrize("name", ["su2_1d_L10_obc", "su2_1d_L10_pbc", "qed2d_3x2_q0", "qed1d_L8_obc"])
 @pytest.mark.parametrize("nvec", [1, 2, 3, 4])
-def test_sell_matvec_matches_csr(name, nvec):
+@pytest.mark.parametrize("window", [32, 4096])
+def test_sell_matvec_matches_csr(name, nvec, window):
     import torch
 
     from edgpu._lib import check, lib, ptr, stream_handle
@@ -31,16 +32,18 @@ def test_sell_matvec_matches_csr(name, nvec):
         pytest.skip("complex matrix")
     n = mat.n
     v32 = mat.vals.to(torch.float32)
-    lay = SellLayout(mat, v32)
+    lay = SellLayout(mat, v32, window)
     # perm: a permutation of the rows, slice padding marked -1; rows sorted by
-    # length (descending) inside windows of 4096
+    # length (descending, stable) inside the windows
     perm = lay.perm.cpu().numpy()
     assert np.array_equal(np.sort(perm[perm >= 0]), np.arange(n))
     assert np.all(perm[n:] == -1) if len(perm) > n else True
     lens = np.diff(mat.rowptr.cpu().numpy())
-    for w0 in range(0, n, 4096):
-        seg = perm[w0: min(w0 + 4096, n)]
+    for w0 in range(0, n, window):
+        seg = perm[w0: min(w0 + window, n)]
         assert np.all(np.diff(lens[seg]) <= 0)
+        same = np.diff(lens[seg]) == 0
+        assert np.all(np.diff(seg)[same] > 0)  # stable
     assert lay.pairs >= mat.nnz
     g = torch.Generator(device="cpu").manual_seed(7)
     x = torch.rand((n, nvec), generator=g, dtype=torch.float32).to(dev)
@@ -50,7 +53,7 @@ def test_sell_matvec_matches_csr(name, nvec):
     check(lib.edg_spmv(1, n, mat.nnz, ptr(mat.rowptr), ptr(mat.cols), ptr(v32), ptr(diag), nvec, ptr(x), ptr(y_csr),
                        stream_handle()), "edg_spmv")
     check(lib.edg_spmv_sell(n, nvec, ptr(lay.perm), ptr(lay.width), ptr(lay.off), ptr(lay.entries), ptr(diag), ptr(x),
-                            ptr(y_sell), n, stream_handle()), "edg_spmv_sell")
+                            nvec, ptr(y_sell), n, stream_handle()), "edg_spmv_sell")
     # exact product in f64 from the same f32 inputs, for the comparison
     H = mat.to_scipy(include_diag=False).astype(np.float32).astype(np.float64)
     xd = x.cpu().numpy().astype(np.float64)
