@@ -509,12 +509,14 @@ def run_edgpu(args, world, rank, local):
 # other workloads of the same path (not the headline line)
 def run_batch(args, world, rank, local):
     """QED 3x2 OBC: 64 couplings (g log-uniform in [0.1, 5], m uniform in
-    [0, 2], seed 0) in the Q = 0 sector plus the Q = -2, -1, 1, 2 sectors; one
-    persistent batched launch replayed from a CUDA graph per step."""
+    [0, 2], seed 0) in the Q = 0 sector plus the Q = -2, -1, 1, 2 sectors,
+    then the same batch with SU(2) chains of L = 10 and 12 (dims 8,953 and
+    73,789) added.  Each solve is one (instance, row-tile) batched launch per
+    precision phase, replayed from a CUDA graph; mixed precision and f64."""
     import torch
 
-    from edgpu.batch import SmallBatch
-    from edgpu.models import QED_Model
+    from edgpu.batch import TiledBatch
+    from edgpu.models import QED_Model, SU2_Model
 
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
@@ -523,7 +525,7 @@ def run_batch(args, world, rank, local):
     ms = rng.uniform(0.0, 2.0, 64)
     charge_bg = {-2: [1, 0, 0, 0, 0, 1], -1: [1, 0, 0, 0, 0, 0], 1: [-1, 0, 0, 0, 0, 0], 2: [-1, 0, 0, 0, 0, -1]}
 
-    def build_all():
+    def build_c3():
         mats = []
         base = QED_Model(spin=1, pure_theory=False, lvals=[3, 2], has_obc=[True, True], device=dev)
         for g, m in zip(gs, ms):
@@ -536,51 +538,82 @@ def run_batch(args, world, rank, local):
             mats.append(mq.H.mat)
         return mats
 
-    mats = build_all()
-    batch = SmallBatch(mats, k=1)
-    batch.capture()
-    for _ in range(args.warmup):
-        batch.solve()
-    torch.cuda.synchronize()
-    barrier(world)
-    ts = []
-    for _ in range(args.steps):
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record()
-        batch.solve()
-        b.record()
-        torch.cuda.synchronize()
-        ts.append(a.elapsed_time(b))
-    ms_step = max_over_ranks(float(np.mean(ts)), world, dev)
-    n_inst = len(mats)
+    def build_su2():
+        mats = []
+        for L_ in (10, 12):
+            m2 = SU2_Model(spin=0.5, pure_theory=False, lvals=[L_], has_obc=[True], sectors=[L_], device=dev)
+            m2.build_Hamiltonian(1.0, 0.5)
+            mats.append(m2.H.mat)
+        return mats
+
+    c3 = build_c3()
+    mixed_batch = c3 + build_su2()
+    out = {}
+    for label, mats in (("c3", c3), ("c3_plus_su2_L10_L12", mixed_batch)):
+        for prec in ("mixed", "fp64"):
+            tb = TiledBatch(mats, k=1, precision=prec)
+            tb.capture()
+            for _ in range(args.warmup):
+                tb.solve()
+            torch.cuda.synchronize()
+            ts = []
+            for _ in range(args.steps):
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record()
+                tb.solve()
+                b.record()
+                torch.cuda.synchronize()
+                ts.append(a.elapsed_time(b))
+            tb.check_status()
+            ms_step = max_over_ranks(float(np.mean(ts)), world, dev)
+            out[f"{label}/{prec}"] = {"ms_per_solve": ms_step, "instances_per_s": len(mats) * world / (ms_step * 1e-3),
+                                     "tile_rows": tb.tile_rows, "lanes": tb.lanes,
+                                     "energies_first": tb.evals[:3, 0].cpu().numpy().tolist()}
+        e_m = TiledBatch(mats, precision="mixed").solve(use_graph=False).cpu().numpy()[:, 0]
+        e_d = TiledBatch(mats, precision="fp64").solve(use_graph=False).cpu().numpy()[:, 0]
+        out[f"{label}/max_rel_dE_mixed_vs_fp64"] = float(np.max(np.abs(e_m - e_d) / np.abs(e_d)))
+        out[f"{label}/instances"] = len(mats)
+        out[f"{label}/dims"] = sorted({int(m.n) for m in mats})
     # e2e: instances from host couplings to energies on the host
+    torch.cuda.synchronize()
     t0 = time.perf_counter()
-    mats2 = build_all()
-    b2 = SmallBatch(mats2, k=1)
-    b2.launch()
-    e_host = b2.evals.cpu().numpy()
+    mats2 = build_c3()
+    tb2 = TiledBatch(mats2, k=1, precision="mixed")
+    tb2.launch()
+    e_host = tb2.evals.cpu().numpy()
     e2e_ms = 1e3 * (time.perf_counter() - t0)
-    # CPU: the reference's sequential eigsh loop over the same instances
+    # CPU: scipy eigsh (the reference's solver, ARPACK) on each instance's
+    # canonical matrix in a loop
     from scipy.sparse.linalg import eigsh
 
-    Hs = [m.to_scipy() for m in mats]
-    t0 = time.perf_counter()
-    for H in Hs:
-        eigsh(H, k=1, which="SA")
-    cpu_s = time.perf_counter() - t0
+    def cpu_loop(ms_):
+        Hs = [m.to_scipy() for m in ms_]
+        t0_ = time.perf_counter()
+        for H in Hs:
+            if H.shape[0] > 3:
+                eigsh(H, k=1, which="SA")
+        return time.perf_counter() - t0_
+
+    cpu_c3 = cpu_loop(c3)
+    cpu_mixed = cpu_loop(mixed_batch)
     if rank == 0:
+        head = out["c3/mixed"]
         print(json.dumps({
-            "metric": METRIC, "workload": "batch", "value": n_inst * world / (ms_step * 1e-3),
-            "unit": "instances/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "metric": METRIC, "workload": "batch", "value": head["instances_per_s"], "unit": "instances/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": head["ms_per_solve"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 Krylov/matvec + f64 dots, recurrence, eigen-solve; f64 refinement",
             "data": "synthetic (model Hamiltonians)",
             "config": {"workload": "QED 2D 3x2 OBC spin 1 with matter: 64 (g, m) in Q=0 (dim 90) + Q=-2..2 sectors "
-                                   "(dims 26, 52, 67, 26), one persistent launch per step (CUDA graph)",
-                       "instances_per_step": n_inst},
-            "e2e": {"value": n_inst / (e2e_ms * 1e-3), "unit": "instances/s", "ms_per_step": e2e_ms,
+                                   "(dims 26, 52, 67, 26); and the same plus SU(2) L=10, 12 open chains; one "
+                                   "(instance, row-tile) batched launch per precision phase (CUDA graph)",
+                       "instances_per_step": out["c3/instances"]},
+            "batches": out,
+            "e2e": {"value": out["c3/instances"] / (e2e_ms * 1e-3), "unit": "instances/s", "ms_per_step": e2e_ms,
                     "h2d_bytes_per_step": None, "d2h_bytes_per_step": int(e_host.nbytes)},
-            "cpu_baseline": {"value": n_inst / cpu_s, "unit": "instances/s", "cores": 1, "kind": "port",
-                             "sample": "scipy eigsh(k=1, SA) on each instance's canonical matrix in a loop"},
+            "cpu_baseline": {"value": out["c3/instances"] / cpu_c3, "unit": "instances/s", "cores": 1, "kind": "port",
+                             "sample": "scipy eigsh(k=1, SA) on each instance's canonical matrix in a loop",
+                             "c3_plus_su2_instances_per_s": out["c3_plus_su2_L10_L12/instances"] / cpu_mixed},
         }), flush=True)
 
 
