@@ -574,6 +574,23 @@ def run_batch(args, world, rank, local):
         out[f"{label}/max_rel_dE_mixed_vs_fp64"] = float(np.max(np.abs(e_m - e_d) / np.abs(e_d)))
         out[f"{label}/instances"] = len(mats)
         out[f"{label}/dims"] = sorted({int(m.n) for m in mats})
+    # beside it: the one-CTA-per-instance f64 kernel (instances up to 4096
+    # rows, no grid-wide waits), for the small-instance batch
+    from edgpu.batch import SmallBatch
+
+    sb = SmallBatch(c3, k=1)
+    sb.capture()
+    for _ in range(args.warmup):
+        sb.solve()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(args.steps):
+        sb.solve()
+    b.record()
+    torch.cuda.synchronize()
+    sb_ms = a.elapsed_time(b) / args.steps
+    out["c3/one_cta_per_instance_fp64"] = {"ms_per_solve": sb_ms, "instances_per_s": len(c3) / (sb_ms * 1e-3)}
     # e2e: instances from host couplings to energies on the host
     torch.cuda.synchronize()
     t0 = time.perf_counter()
