@@ -793,8 +793,9 @@ def run_corr(args, world, rank, local):
 
 
 def run_entropy(args, world, rank, local):
-    """Half-chain entanglement in the SU(2) 1D L=14 OBC sector (dim 616,227)
-    of a seeded, normalised complex128 state: one step is the bipartition maps
+    """Half-chain entanglement in the SU(2) 1D L=14 periodic chain's N_tot=14
+    sector (dim 1,232,454) of a seeded, normalised complex128 state: one step
+    is the bipartition maps
     (QuantumModel._get_partition, both parts), the state matrix, rho = M M^dagger
     and its spectrum (QMB_state.entanglement_entropy)."""
     import torch
@@ -855,7 +856,8 @@ def run_entropy(args, world, rank, local):
             "unit": "entropies/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "complex128 state and matrix, f64 spectrum", "data": "synthetic (seeded random normalised state)",
-            "config": {"workload": f"SU(2) 1D L=14 OBC N_tot=14 sector, dim {n}; subsystem sites 0-6 "
+            "config": {"workload": f"SU(2) 1D L={L} {'periodic' if PBC else 'open'} chain, N_tot={L} sector, dim {n}; "
+                                   "subsystem sites 0-6 "
                                    f"({part['subsys_dim']} x {part['env_dim']} state matrix)"},
             "phase_ms": {"maps_and_matrix": ms - float(np.mean(spec_ms)), "rho_and_spectrum": float(np.mean(spec_ms))},
             "oracle_check": {"maps_bit_exact": maps_ok, "abs_dS": abs(s - s_ref), "entropy": s},
