@@ -57,6 +57,12 @@ PBC = True
 SWEEP = (0.5, 1.0, 2.0)
 MASS = 0.5
 METRIC = "Lanczos GS time-to-solution & matvec GB/s: mixed/batched vs plain FP64 GPU at 1e-9 rel."
+# DRAM traffic of the headline kernels from one ncu capture each (the
+# profiles/su2_L14pbc_* summaries): both reorthogonalisation passes at step 30
+# moved 495.07 + 526.08 MB against 488.05 + 532.40 MB algorithmic; one CSR
+# matvec launch (2 lanes a row) moved 179.21 + 21.61 MB
+REORTH_TRAFFIC_RATIO = (495.07 + 526.08) / (488.05 + 532.40)
+MATVEC_TRAFFIC_BYTES = (179.21 + 21.61) * 1e6
 UNIT = "ground_states/s"
 WORKLOAD = (f"SU(2) 1D Yang-Mills + staggered matter, j_max=1/2, {'periodic' if PBC else 'open'} chain L={L}, "
             f"N_tot={L} sector; ground states for g^2 in {list(SWEEP)}, m={MASS}")
@@ -484,7 +490,11 @@ def run_edgpu(args, world, rank, local):
                      "bound": "hbm",
                      "achieved": reorth_achieved, "peak": hbm, "unit": "GB/s", "frac": reorth_achieved / hbm,
                      "peak_source": peak_kind, "algorithmic_bytes_per_solve": reorth_bytes,
-                     "ms_per_solve": reorth_ms_step, "ms_per_lanczos_step": reorth_ms, "traffic": None},
+                     "ms_per_solve": reorth_ms_step, "ms_per_lanczos_step": reorth_ms,
+                     "traffic": REORTH_TRAFFIC_RATIO * reorth_bytes,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of both passes at step 30 "
+                                       f"of this workload = {REORTH_TRAFFIC_RATIO:.4f} x their algorithmic bytes "
+                                       "(profiles/su2_L14pbc_reorth_bulk_ncu.md), applied per solve"},
         "roofline_matvec": {"kernel": ("batched f32 SELL-32-sigma + diag matvec (sell_spmv_k<float,3,4>), "
                                        f"sort window {sell32.window}, slice padding {sell32.padding:.3f} of the "
                                        "stored pairs"
@@ -493,7 +503,12 @@ def run_edgpu(args, world, rank, local):
                             "layout_choice": fmt32,
                             "bound": "hbm", "achieved": spmv_achieved, "peak": hbm, "unit": "GB/s",
                             "frac": spmv_achieved / hbm, "peak_source": peak_kind,
-                            "algorithmic_bytes_per_launch": spmv_bytes, "avg_launch_ms": spmv_ms, "traffic": None},
+                            "algorithmic_bytes_per_launch": spmv_bytes, "avg_launch_ms": spmv_ms,
+                            "traffic": (MATVEC_TRAFFIC_BYTES if fmt32 == "csr" and g32 == 2 and n == 1232454
+                                        else None),
+                            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of "
+                                              "spmv_k<float, float, double, 3, 2, 4> on this matrix "
+                                              "(profiles/su2_L14pbc_matvec_ncu.md)"},
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                 "ms_per_step": float(np.mean(e2e_ms)), "steps": len(e2e_ms)},
         "gpu_launches": launches,
