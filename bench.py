@@ -57,8 +57,8 @@ PBC = True
 SWEEP = (0.5, 1.0, 2.0)
 MASS = 0.5
 METRIC = "Lanczos GS time-to-solution & matvec GB/s: mixed/batched vs plain FP64 GPU at 1e-9 rel."
-# DRAM traffic of the headline kernels from one ncu capture each (the
-# profiles/su2_L14pbc_* summaries): both reorthogonalisation passes at step 30
+# DRAM traffic of the headline kernels from one ncu capture each on this
+# workload (summaries kept under profiles/): both reorthogonalisation passes at step 30
 # moved 495.07 + 526.08 MB against 488.05 + 532.40 MB algorithmic; one CSR
 # matvec launch (2 lanes a row) moved 179.21 + 21.61 MB
 REORTH_TRAFFIC_RATIO = (495.07 + 526.08) / (488.05 + 532.40)
@@ -493,8 +493,8 @@ def run_edgpu(args, world, rank, local):
                      "ms_per_solve": reorth_ms_step, "ms_per_lanczos_step": reorth_ms,
                      "traffic": REORTH_TRAFFIC_RATIO * reorth_bytes,
                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of both passes at step 30 "
-                                       f"of this workload = {REORTH_TRAFFIC_RATIO:.4f} x their algorithmic bytes "
-                                       "(profiles/su2_L14pbc_reorth_bulk_ncu.md), applied per solve"},
+                                       f"of this workload = {REORTH_TRAFFIC_RATIO:.4f} x their algorithmic bytes, "
+                                       "applied per solve"},
         "roofline_matvec": {"kernel": ("batched f32 SELL-32-sigma + diag matvec (sell_spmv_k<float,3,4>), "
                                        f"sort window {sell32.window}, slice padding {sell32.padding:.3f} of the "
                                        "stored pairs"
@@ -507,8 +507,7 @@ def run_edgpu(args, world, rank, local):
                             "traffic": (MATVEC_TRAFFIC_BYTES if fmt32 == "csr" and g32 == 2 and n == 1232454
                                         else None),
                             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of "
-                                              "spmv_k<float, float, double, 3, 2, 4> on this matrix "
-                                              "(profiles/su2_L14pbc_matvec_ncu.md)"},
+                                              "spmv_k<float, float, double, 3, 2, 4> on this matrix"},
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                 "ms_per_step": float(np.mean(e2e_ms)), "steps": len(e2e_ms)},
         "gpu_launches": launches,
