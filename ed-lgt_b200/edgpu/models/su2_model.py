@@ -1,10 +1,11 @@
-"""SU(2) Yang-Mills (+ staggered matter) with hard-core gluons, j_max = 1/2.
+"""SU(2) Yang-Mills (+ staggered matter): the hard-core-gluon model
+(j_max = 1/2) and the generic model (any j_max, or ``use_generic_model``).
 
 Mirrors edlgt/models/SU2_model.py: constructor and sector (:31-171: total
 fermion number ``sectors``, link Casimir constraints T2_p - T2_m = 0, Z2 flux
 parities for pure PBC theories, optional static charges ``bg_list``),
-couplings ``SU2_Hamiltonian_couplings`` (:555-624) and
-``build_base_Hamiltonian`` (:200-355).
+couplings ``SU2_Hamiltonian_couplings`` (:555-624), ``build_base_Hamiltonian``
+(:200-355) and ``build_gen_Hamiltonian`` (:357-472).
 """
 
 from __future__ import annotations
@@ -15,7 +16,7 @@ import numpy as np
 
 from ..lattice import origin_surfaces, staggered_mask
 from ..modeling import LocalTerm, PlaquetteTerm, QMB_hamiltonian, TwoBodyTerm
-from ..operators import su2_dressed_site_operators, su2_gauge_invariant_states
+from ..operators import su2_dressed_site_operators, su2_gauge_invariant_states, su2_gen_dressed_site_operators
 from .quantum_model import QuantumModel
 
 logger = logging.getLogger(__name__)
@@ -26,15 +27,16 @@ __all__ = ["SU2_Model"]
 class SU2_Model(QuantumModel):
     def __init__(self, spin, pure_theory, bg_list=None, sectors=None, use_generic_model=False, **kwargs):
         super().__init__(**kwargs)
-        if use_generic_model or spin >= 1:
-            raise NotImplementedError("only the hard-core-gluon (j_max = 1/2) SU(2) model runs on the device engine")
         self.spin = spin
+        self.use_generic_model = bool(use_generic_model)
+        self.generic = self.use_generic_model or spin >= 1
         self.pure_theory = pure_theory
         self.background = max(bg_list) if bg_list is not None else 0
         self.bg_list = bg_list if self.background != 0 else None
         self.gauge_basis, self.gauge_states = su2_gauge_invariant_states(spin, pure_theory, lattice_dim=self.dim,
                                                                          background=self.background)
-        ops = su2_dressed_site_operators(spin, pure_theory, lattice_dim=self.dim, background=self.background)
+        factory = su2_gen_dressed_site_operators if self.generic else su2_dressed_site_operators
+        ops = factory(spin, pure_theory, lattice_dim=self.dim, background=self.background)
         self.project_operators(ops, bg_sector_list=self.bg_list)
         if pure_theory:
             global_ops, global_sectors = None, None
@@ -157,9 +159,59 @@ class SU2_Model(QuantumModel):
             self.Hlocal.add_term(term.get_Hamiltonian(sign * half, mask=left))
 
     def build_Hamiltonian(self, g, m=None, theta=0.0, lambda_noise=0.0, dtype_mode="auto"):
-        self.build_base_Hamiltonian(g, m, theta, lambda_noise, dtype_mode)
+        if self.generic:
+            self.build_gen_Hamiltonian(g, m, dtype_mode)
+        else:
+            self.build_base_Hamiltonian(g, m, theta, lambda_noise, dtype_mode)
+
+    # the 16 species patterns of a plaquette's four corners in the generic
+    # model (edlgt/models/SU2_model.py:428-445), corners in the order
+    # (p0, p1), (p1, m0), (m1, p0), (m0, m1)
+    _GEN_PLAQUETTE_SET = (
+        "AB AB AB AB", "AA AB BB AB", "AB AB AA BB", "AA AB BA BB", "AB BB AB AA", "AA BB BB AA", "AB BB AA BA",
+        "AA BB BA BA", "BB AA AB AB", "BA AA BB AB", "BB AA AA BB", "BA AA BA BB", "BB BA AB AA", "BA BA BB AA",
+        "BB BA AA BA", "BA BA BA BA",
+    )
+
+    def gen_hamiltonian_blocks(self, g, m=None):
+        """Term blocks of the generic model: electric Casimir, staggered mass on
+        N_tot, the two hopping species [Q1_p^dag, Q2_m] and [Q2_p^dag, Q1_m]
+        with their conjugates, and the plaquettes of the 16 corner-species
+        patterns (edlgt/models/SU2_model.py:357-472)."""
+        self.SU2_Hamiltonian_couplings(g, m)
+        c = self.coeffs
+        dp = self.def_params
+        blocks = [LocalTerm(self.ops["E_square"], "E_square", **dp).get_Hamiltonian(strength=c["E"])]
+        if not self.pure_theory:
+            for lab in ("even", "odd"):
+                term = LocalTerm(self.ops["N_tot"], "N_tot", **dp)
+                blocks.append(term.get_Hamiltonian(c[f"m_{lab}"], staggered_mask(self.lvals, lab)))
+            for d in self.directions:
+                for lab in ("even", "odd"):
+                    for names in ([f"Q1_p{d}_dag", f"Q2_m{d}"], [f"Q2_p{d}_dag", f"Q1_m{d}"]):
+                        term = TwoBodyTerm(d, [self.ops[o] for o in names], names, **dp)
+                        blocks.append(term.get_Hamiltonian(strength=c[f"t{d}_{lab}"], add_dagger=True,
+                                                           mask=staggered_mask(self.lvals, lab)))
+        if self.dim > 1:
+            planes = ["xy"] if self.dim == 2 else ["xy", "xz", "yz"]
+            for pdir in planes:
+                for pat in self._GEN_PLAQUETTE_SET:
+                    s0, s1, s2, s3 = pat.split()
+                    names = [f"C{s0}_p{pdir[0]},p{pdir[1]}", f"C{s1}_p{pdir[1]},m{pdir[0]}",
+                             f"C{s2}_m{pdir[1]},p{pdir[0]}", f"C{s3}_m{pdir[0]},m{pdir[1]}"]
+                    term = PlaquetteTerm([pdir[0], pdir[1]], [self.ops[o] for o in names], names, **dp)
+                    blocks.append(term.get_Hamiltonian(strength=c["B"], add_dagger=True))
+        return blocks
+
+    def build_gen_Hamiltonian(self, g, m=None, dtype_mode="auto"):
+        self.default_params()
+        for b in self.gen_hamiltonian_blocks(g, m):
+            self.H.add_term(b)
+        self.H.build(self.ham_format, force_complex=(self._resolve_dtype_mode(dtype_mode) == "complex"))
 
     def hamiltonian_blocks(self, g, m=None, theta=0.0, lambda_noise=0.0):
+        if self.generic:
+            return self.gen_hamiltonian_blocks(g, m)
         self.SU2_Hamiltonian_couplings(g, m, theta)
         c = self.coeffs
         dp = self.def_params

@@ -33,6 +33,7 @@ __all__ = [
     "su2_singlets",
     "su2_gauge_invariant_states",
     "su2_dressed_site_operators",
+    "su2_gen_dressed_site_operators",
 ]
 
 getcontext().prec = 50
@@ -365,3 +366,164 @@ def _su2_ops_cached(spin, pure_theory, lattice_dim, background=0):
             ops["Vpx"] = csr_matrix(ops["Vpx_dag"].conj().T)
     return ops
 
+
+
+# ---------------------------------------------------------------------------
+# Generic truncation j_max (any half-integer), the reference's generalized
+# rishon construction (edlgt/operators/SU2_rishons.py:105-234,
+# edlgt/operators/SU2_operators.py:302-622).
+# ---------------------------------------------------------------------------
+
+
+def _rishon_ops_gen(s2):
+    """Rishon operators of one half-link truncated at doubled spin ``s2``.
+
+    The space is the direct sum of the irreps j = 0, 1/2, ..., s2/2 (block by
+    block, m descending inside a block).  ``Zr`` and ``Zg`` lower the irrep by
+    one half: the state k of irrep j + 1/2 goes to the state k (red) or
+    k - 1 (green) of irrep j, with the amplitude
+    sqrt((j + m + 1) / sqrt((2j + 1)(2j + 2))) (red) or
+    sqrt((j - m + 1) / sqrt((2j + 1)(2j + 2))) (green), m the magnetic number of
+    the target state; this is the normalisation of the reference's generic
+    construction (its ``chi_function``).  Two rishon species: B = (Zr, Zg) and
+    A = (Zg^dag, -Zr^dag).  ``P`` is (-1)^(2j) on each block.
+    """
+    starts = [j2 * (j2 + 1) // 2 for j2 in range(s2 + 2)]
+    size = starts[s2 + 1]
+    ops = {}
+    pdiag = []
+    for j2 in range(s2 + 1):
+        pdiag += [(-1.0) ** j2] * (j2 + 1)
+    ops["P"] = diags(pdiag, 0, shape=(size, size), format="csr")
+    ops["Iz"] = identity(size, format="csr")
+    for color in "rg":
+        rows, cols, vals = [], [], []
+        for j2 in range(s2):  # target irrep j2, source irrep j2 + 1
+            j = j2 / 2
+            norm = np.sqrt((2 * j + 1) * (2 * j + 2))
+            for k, m2 in enumerate(_m_values(j2)):
+                m = m2 / 2
+                num = (j + m + 1) if color == "r" else (j - m + 1)
+                rows.append(starts[j2] + k)
+                cols.append(starts[j2 + 1] + k + (0 if color == "r" else 1))
+                vals.append(np.sqrt(num / norm))
+        z = csr_matrix((vals, (rows, cols)), shape=(size, size))
+        ops[f"Z{color}"] = z
+        ops[f"Z{color}_dag"] = csr_matrix(z.T)
+        ops[f"ZB_{color}"] = z
+        ops[f"ZB_{color}_dag"] = ops[f"Z{color}_dag"]
+    ops["ZA_r"] = ops["ZB_g_dag"]
+    ops["ZA_g"] = csr_matrix(-ops["ZB_r_dag"])
+    ops["ZA_r_dag"] = csr_matrix(ops["ZA_r"].T)
+    ops["ZA_g_dag"] = csr_matrix(ops["ZA_g"].T)
+    for sp in "AB":
+        for color in "rg":
+            ops[f"Z{sp}_{color}_P"] = csr_matrix(ops[f"Z{sp}_{color}"] @ ops["P"])
+            ops[f"P_Z{sp}_{color}_dag"] = csr_matrix(ops["P"] @ ops[f"Z{sp}_{color}_dag"])
+    return ops
+
+
+# Corner operators of the generic model: slot -> factor (with {a} / {b} the
+# first / second rishon species of C{a}{b}, {c} the colour), slots ordered
+# [m_x, m_y, (m_z,) p_x, p_y, (p_z)]; as listed in
+# edlgt/operators/SU2_operators.py:381-397 (2D) and 455-503 (3D).
+_GEN_CORNERS_2D = {
+    "px,py": {2: "Z{a}_{c}_P", 3: "Z{b}_{c}_dag"},
+    "py,mx": {0: "P_Z{b}_{c}_dag", 1: "P", 2: "P", 3: "Z{a}_{c}"},
+    "mx,my": {0: "Z{a}_{c}_P", 1: "Z{b}_{c}_dag"},
+    "my,px": {1: "Z{a}_{c}_P", 2: "Z{b}_{c}_dag"},
+}
+_GEN_CORNERS_3D = {
+    "px,py": {3: "Z{a}_{c}_P", 4: "Z{b}_{c}_dag"},
+    "py,mx": {0: "P_Z{b}_{c}_dag", 1: "P", 2: "P", 3: "P", 4: "Z{a}_{c}"},
+    "mx,my": {0: "Z{a}_{c}_P", 1: "Z{b}_{c}_dag"},
+    "my,px": {1: "Z{a}_{c}_P", 2: "P", 3: "Z{b}_{c}_dag"},
+    "px,pz": {3: "Z{a}_{c}_P", 4: "P", 5: "Z{b}_{c}_dag"},
+    "pz,mx": {0: "P_Z{b}_{c}_dag", 1: "P", 2: "P", 3: "P", 4: "P", 5: "Z{a}_{c}"},
+    "mx,mz": {0: "Z{a}_{c}_P", 1: "P", 2: "Z{b}_{c}_dag"},
+    "mz,px": {2: "Z{a}_{c}_P", 3: "Z{b}_{c}_dag"},
+    "py,pz": {4: "Z{a}_{c}_P", 5: "Z{b}_{c}_dag"},
+    "pz,my": {1: "P_Z{b}_{c}_dag", 2: "P", 3: "P", 4: "P", 5: "Z{a}_{c}"},
+    "my,mz": {1: "Z{a}_{c}_P", 2: "Z{b}_{c}_dag"},
+    "mz,py": {2: "Z{a}_{c}_P", 3: "P", 4: "Z{b}_{c}_dag"},
+}
+
+
+def su2_gen_dressed_site_operators(spin, pure_theory, lattice_dim, background=0) -> dict:
+    """Dressed-site operators of the generic SU(2) model (full local space).
+
+    Electric Casimirs and parities per half-link, corner operators
+    C{a}{b}_{corner} of both rishon species (2D and 3D), the two hopping
+    species Q1 = psi_r^dag Zg^dag - psi_g^dag Zr^dag and
+    Q2 = psi_r^dag Zr + psi_g^dag Zg (parity strings over the half-links in
+    front of the target one) with their adjoints, matter numbers, E_square and
+    the background Casimir."""
+    return dict(_su2_gen_ops_cached(float(spin), pure_theory, lattice_dim, float(background)))
+
+
+@lru_cache(maxsize=32)
+def _su2_gen_ops_cached(spin, pure_theory, lattice_dim, background=0):
+    s2 = int(round(2 * spin))
+    if abs(s2 - 2 * spin) > 1e-12 or s2 < 1:
+        raise ValueError(f"spin must be a positive half-integer, got {spin}")
+    D = lattice_dim
+    dirs = "xyz"[:D]
+    base = _rishon_ops_gen(s2) | su2_generators(spin)
+    if background:
+        base["T2_bg"] = su2_generators(background)["T2"]
+    if not pure_theory:
+        base |= fermion_ops(two_species=True)
+        base |= su2_generators(0.5, matter=True)
+    ops = {}
+
+    def chain(place):
+        names = ["Iz"] * (2 * D)
+        for k, v in place.items():
+            names[k] = v
+        return names
+
+    for name in ("T2", "P"):
+        for d, ax in enumerate(dirs):
+            ops[f"{name}_m{ax}"] = kron_chain(base, chain({d: name}))
+            ops[f"{name}_p{ax}"] = kron_chain(base, chain({D + d: name}))
+    corners = _GEN_CORNERS_2D if D == 2 else (_GEN_CORNERS_3D if D == 3 else {})
+    for a in "AB":
+        for b in "AB":
+            for corner, place in corners.items():
+                acc = None
+                for c in "rg":
+                    t = kron_chain(base, chain({k: v.format(a=a, b=b, c=c) for k, v in place.items()}))
+                    acc = t if acc is None else acc + t
+                ops[f"C{a}{b}_{corner}"] = csr_matrix(acc)
+    if not pure_theory:
+        for name in list(ops):
+            ops[name] = csr_matrix(kron(base["ID_psi"], ops[name]))
+        hop = {}
+        for side in "mp":
+            for d, ax in enumerate(dirs):
+                slot = d if side == "m" else D + d
+
+                def term(c, z):
+                    return kron_chain(base, [f"psi_{c}_dag_P"] + ["P"] * slot + [z] + ["Iz"] * (2 * D - slot - 1))
+
+                hop[f"Q1_{side}{ax}_dag"] = csr_matrix(term("r", "Zg_dag") - term("g", "Zr_dag"))
+                hop[f"Q2_{side}{ax}_dag"] = csr_matrix(term("r", "Zr") + term("g", "Zg"))
+        ops |= hop
+        # every operator's adjoint under the name without "_dag"
+        adj = {name.replace("_dag", ""): csr_matrix(op.conj().T) for name, op in ops.items()}
+        ops |= adj
+        for label in ("r", "g", "tot", "single", "pair", "zero"):
+            ops[f"N_{label}"] = kron_chain(base, [f"N_{label}"] + ["Iz"] * (2 * D))
+    e2 = None
+    for side in "pm":
+        for ax in dirs:
+            t = 0.5 * ops[f"T2_{side}{ax}"]
+            e2 = t if e2 is None else e2 + t
+    ops["E_square"] = csr_matrix(e2)
+    if background:
+        bg_len = sum(j2 + 1 for j2 in range(0, int(round(2 * background)) + 1))
+        for name in list(ops):
+            ops[name] = csr_matrix(kron(identity(bg_len), ops[name]))
+        ids = ["Iz"] * (2 * D) if pure_theory else ["ID_psi"] + ["Iz"] * (2 * D)
+        ops["bg"] = kron_chain(base, ["T2_bg"] + ids)
+    return ops

@@ -140,3 +140,25 @@ def string_case_inputs(golden, name):
                 link_op_diags=golden[f"{name}/link_diags"], link_sectors=golden[f"{name}/link_sectors"],
                 pair_list=pairs, string_op_diags=golden[f"{name}/string_diags"],
                 string_sectors=golden[f"{name}/string_sectors"])
+
+
+# generic SU(2) model cases (j_max >= 1, or use_generic_model), same
+# parameters as tests/golden/make_golden.py's SU2_GEN_CASES
+SU2_GEN_CASES = {
+    "su2gen_1d_L4_obc_j1": (dict(spin=1, pure_theory=False, lvals=[4], has_obc=[True], sectors=[4]), 1.0, 1.0),
+    "su2gen_1d_L6_obc_j1": (dict(spin=1, pure_theory=False, lvals=[6], has_obc=[True], sectors=[6]), 0.8, 0.5),
+    "su2gen_1d_L4_pbc_j1": (dict(spin=1, pure_theory=False, lvals=[4], has_obc=[False], sectors=[4]), 1.3, 0.7),
+    "su2gen_1d_L6_obc_j12": (dict(spin=0.5, pure_theory=False, lvals=[6], has_obc=[True], sectors=[6],
+                                  use_generic_model=True), 1.0, 0.5),
+    "su2gen_1d_L4_obc_j32": (dict(spin=1.5, pure_theory=False, lvals=[4], has_obc=[True], sectors=[4]), 1.0, 1.0),
+    "su2gen_2d_2x2_pure_pbc_j1": (dict(spin=1, pure_theory=True, lvals=[2, 2], has_obc=[False, False]), 1.2, None),
+    "su2gen_2d_2x2_obc_j1": (dict(spin=1, pure_theory=False, lvals=[2, 2], has_obc=[True, True], sectors=[4]),
+                             1.0, 1.0),
+}
+
+
+def build_generic(name, device="cpu"):
+    from edgpu.models import SU2_Model
+
+    kw, g, m = SU2_GEN_CASES[name]
+    return SU2_Model(**kw, device=device), g, m

@@ -23,6 +23,13 @@ def golden_small():
 
 
 @pytest.fixture(scope="session")
+def golden_generic():
+    import numpy as np
+
+    return np.load(os.path.join(GOLDEN, "generic_su2_cases.npz"))
+
+
+@pytest.fixture(scope="session")
 def golden_string():
     import numpy as np
 

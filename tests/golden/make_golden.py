@@ -6,7 +6,7 @@ and numba/scipy/sympy:
     python tests/golden/make_golden.py [group ...]
 
 Groups: small, pins, dynamics, big, twobody, entropy, momentum, full,
-nbody, overlap, state, local, integrated, string.  Output: .npz files next to
+nbody, overlap, state, local, integrated, string, generic.  Output: .npz files next to
 this script.  Nothing here is imported by the library or by the GPU tests;
 the tests only read the .npz files.
 
@@ -645,9 +645,45 @@ def gen_string():
     np.savez_compressed(os.path.join(HERE, "string_cases.npz"), **out)
 
 
+SU2_GEN_CASES = {
+    "su2gen_1d_L4_obc_j1": (dict(spin=1, pure_theory=False, lvals=[4], has_obc=[True], sectors=[4]), 1.0, 1.0),
+    "su2gen_1d_L6_obc_j1": (dict(spin=1, pure_theory=False, lvals=[6], has_obc=[True], sectors=[6]), 0.8, 0.5),
+    "su2gen_1d_L4_pbc_j1": (dict(spin=1, pure_theory=False, lvals=[4], has_obc=[False], sectors=[4]), 1.3, 0.7),
+    "su2gen_1d_L6_obc_j12": (dict(spin=0.5, pure_theory=False, lvals=[6], has_obc=[True], sectors=[6],
+                                  use_generic_model=True), 1.0, 0.5),
+    "su2gen_1d_L4_obc_j32": (dict(spin=1.5, pure_theory=False, lvals=[4], has_obc=[True], sectors=[4]), 1.0, 1.0),
+    "su2gen_2d_2x2_pure_pbc_j1": (dict(spin=1, pure_theory=True, lvals=[2, 2], has_obc=[False, False]), 1.2, None),
+    "su2gen_2d_2x2_obc_j1": (dict(spin=1, pure_theory=False, lvals=[2, 2], has_obc=[True, True], sectors=[4]),
+                             1.0, 1.0),
+}
+
+
+def gen_generic_su2():
+    """The generic SU(2) model (j_max >= 1, or use_generic_model): the
+    reference's SU2_gen_dressed_site_operators and build_gen_Hamiltonian
+    (edlgt/operators/SU2_operators.py:302-622, edlgt/models/SU2_model.py:
+    357-472): sector keys, canonical matrices and the lowest energies."""
+    out = {}
+    for name, (kw, g, mass) in SU2_GEN_CASES.items():
+        t0 = time.time()
+        model = su2_model(kw)
+        out |= sector_record(model, f"{name}/", True)
+        model.build_Hamiltonian(g, mass)
+        out |= matrix_record(canonical(model), f"{name}/H_", True)
+        out[f"{name}/g"] = np.float64(g)
+        out[f"{name}/m"] = np.float64(np.nan if mass is None else mass)
+        k = 2 if len(model.sector_configs) > 3 else 1
+        model.diagonalize_Hamiltonian(k, "sparse")
+        out[f"{name}/energies"] = np.asarray(model.H.Nenergies)
+        print(name, len(model.sector_configs), list(model.loc_dims), f"{time.time() - t0:.1f}s", flush=True)
+    np.savez_compressed(os.path.join(HERE, "generic_su2_cases.npz"), **out)
+
+
 if __name__ == "__main__":
     groups = sys.argv[1:] or ["small", "pins", "dynamics", "big", "twobody", "entropy", "momentum", "full", "nbody",
-                             "overlap", "state", "local", "integrated", "string"]
+                             "overlap", "state", "local", "integrated", "string", "generic"]
+    if "generic" in groups:
+        gen_generic_su2()
     if "string" in groups:
         gen_string()
     if "integrated" in groups:
