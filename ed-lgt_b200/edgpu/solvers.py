@@ -283,7 +283,7 @@ def stack_diagonals(diags, dtype):
     return torch.stack([d.to(dtype) for d in diags], dim=1).contiguous()
 
 
-def lanczos_mixed(mat, diags=None, k=1, tol32=1e-5, tol=1e-12, max_iter=400, refine_iter=5, check_every=5,
+def lanczos_mixed(mat, diags=None, k=1, tol32=1e-4, tol=1e-12, max_iter=400, refine_iter=5, check_every=5,
                   seed=1234, stats32=None, stats64=None, vals32=None, diag32=None, diag64=None, tune=True,
                   group32=0, group64=0, sell=None):
     """Mixed-precision (f32 Krylov, f64 recurrence) Lanczos + f64 refinement.
