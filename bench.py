@@ -485,8 +485,9 @@ def run_edgpu(args, world, rank, local):
                                "f64_steps": agg64[4],
                                "source": "one instrumented sweep (CUDA events around every phase of every step)"},
         "setup_phases": phases_setup,
-        "roofline": {"kernel": "f32 delayed Gram-Schmidt reorthogonalisation (dots_rows_k<float,3> + "
-                               "update_rows_k<float,3> + scale_store_k, two reads of the basis per Lanczos step)",
+        "roofline": {"kernel": "f32 delayed Gram-Schmidt reorthogonalisation (dots_bulk_k<float,3> + "
+                               "update_bulk_k<float,3>: the Krylov basis streamed through a shared-memory ring of "
+                               "bulk copies, two reads of the basis per Lanczos step)",
                      "bound": "hbm",
                      "achieved": reorth_achieved, "peak": hbm, "unit": "GB/s", "frac": reorth_achieved / hbm,
                      "peak_source": peak_kind, "algorithmic_bytes_per_solve": reorth_bytes,

@@ -9,7 +9,9 @@
 // terms use only the operator diagonal and drop |op_cc| < 1e-10 exactly like
 // localbody_data_par (sym_qmb_operations.py:565-602).  Each row's entries are
 // then sorted by column and duplicates are summed, which yields the canonical
-// (summed) matrix of edlgt/modeling/qmb_hamiltonian.py:196-199.
+// (summed) matrix of edlgt/modeling/qmb_hamiltonian.py:196-199.  Kernels are
+// templated on the key type (one word, or two words past 63 bits of key
+// space: keys.cuh).
 #include "lookup.cuh"
 
 namespace {
@@ -44,13 +46,37 @@ __device__ __forceinline__ void decode_digits(const edg_assembly& a, uint64_t ke
     key /= d;
   }
 }
+__device__ __forceinline__ void decode_digits(const edg_assembly& a, edg::u128 key, uint8_t* dig) {
+  const int n_hi = a.sector.n_hi;
+  uint64_t w = (uint64_t)key;
+  for (int s = a.n_sites - 1; s >= n_hi; --s) {
+    uint64_t d = (uint64_t)a.loc_dims[s];
+    dig[s] = (uint8_t)(w % d);
+    w /= d;
+  }
+  w = (uint64_t)(key >> 64);
+  for (int s = n_hi - 1; s >= 0; --s) {
+    uint64_t d = (uint64_t)a.loc_dims[s];
+    dig[s] = (uint8_t)(w % d);
+    w /= d;
+  }
+}
 
+template <typename K>
+__device__ __forceinline__ int64_t find_row(const edg_lookup_table& t, K q) {
+  if constexpr (sizeof(K) == 8)
+    return edg::find_key(t, q);
+  else
+    return edg::find_key_t(t, q);
+}
+
+template <typename K>
 __global__ void __launch_bounds__(kThreads) count_k(edg_assembly a, int64_t* __restrict__ row_bound) {
   uint8_t dig[EDG_MAX_SITES];
   const int dm = a.dmax;
   for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < a.sector.n;
        r += (int64_t)gridDim.x * blockDim.x) {
-    decode_digits(a, a.sector.keys[r], dig);
+    decode_digits(a, edg::ld_key<K>(a.sector.keys, r), dig);
     int64_t total = 0;
     for (int k = 0; k < a.n_terms; ++k) {
       int nops = a.term_nops[k];
@@ -66,7 +92,7 @@ __global__ void __launch_bounds__(kThreads) count_k(edg_assembly a, int64_t* __r
   }
 }
 
-template <typename V>
+template <typename V, typename K>
 __global__ void __launch_bounds__(kThreads) fill_k(edg_assembly a, const int64_t* __restrict__ offsets,
                                                    int32_t* __restrict__ tcols, double* __restrict__ tvals,
                                                    int64_t* __restrict__ row_nnz, double* __restrict__ diag,
@@ -75,7 +101,7 @@ __global__ void __launch_bounds__(kThreads) fill_k(edg_assembly a, const int64_t
   const int dm = a.dmax;
   for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < a.sector.n;
        r += (int64_t)gridDim.x * blockDim.x) {
-    const uint64_t key = a.sector.keys[r];
+    const K key = edg::ld_key<K>(a.sector.keys, r);
     decode_digits(a, key, dig);
     // ---- diagonal terms ----
     V d = V::zero();
@@ -106,15 +132,15 @@ __global__ void __launch_bounds__(kThreads) fill_k(edg_assembly a, const int64_t
       if (empty) continue;
       const V coef = V::load(a.term_coef, k);
       while (true) {
-        uint64_t kk = key;
+        K kk = key;
         V amp = coef;
         for (int j = 0; j < nops; ++j) {
           int64_t e = ((int64_t)tab[j] * dm + bra[j]) * dm + idx[j];
           int ket = a.t_ket[e];
           amp = amp * V::load(a.t_amp, e);
-          kk += (uint64_t)((int64_t)(ket - bra[j]) * (int64_t)a.strides[site[j]]);
+          kk += edg::key_step<K>((int64_t)(ket - bra[j]) * (int64_t)a.strides[site[j]], site[j], a.sector.n_hi);
         }
-        int64_t col = edg::find_key(a.sector, kk);
+        int64_t col = find_row(a.sector, kk);
         if (col < 0) {
           atomicExch(err, EDG_ERR_MISSING_KET);
         } else if (col == r) {
@@ -190,6 +216,11 @@ int check_assembly(const edg_assembly* a, const char* who) {
   EDG_REQUIRE(a->dmax > 0 && a->dmax <= 255, "%s: dmax out of range", who);
   EDG_REQUIRE(a->sector.n >= 0 && a->sector.n < (int64_t(1) << 31), "%s: sector too large for int32 columns", who);
   EDG_REQUIRE(a->n_terms >= 0 && a->n_dterms >= 0, "%s: negative term count", who);
+  EDG_REQUIRE(a->sector.key_words >= 0 && a->sector.key_words <= 2, "%s: key_words must be 1 or 2", who);
+  EDG_REQUIRE(a->sector.key_words != 2 ||
+                  (a->sector.n_hi > 0 && a->sector.n_hi < a->n_sites &&
+                   (reinterpret_cast<uintptr_t>(a->sector.keys) & 15) == 0),
+              "%s: two-word keys need 0 < n_hi < n_sites and 16-byte aligned keys", who);
   return EDG_OK;
 }
 
@@ -199,7 +230,11 @@ extern "C" int edg_assemble_count(const edg_assembly* a, int64_t* row_bound, cud
   int st = check_assembly(a, "edg_assemble_count");
   if (st) return st;
   if (a->sector.n == 0) return EDG_OK;
-  count_k<<<edg::grid_for(a->sector.n, kThreads), kThreads, 0, stream>>>(*a, row_bound);
+  const unsigned grid = edg::grid_for(a->sector.n, kThreads);
+  if (a->sector.key_words == 2)
+    count_k<edg::u128><<<grid, kThreads, 0, stream>>>(*a, row_bound);
+  else
+    count_k<uint64_t><<<grid, kThreads, 0, stream>>>(*a, row_bound);
   EDG_CHECK_LAUNCH("edg_assemble_count");
   return EDG_OK;
 }
@@ -211,10 +246,19 @@ extern "C" int edg_assemble_fill(const edg_assembly* a, const int64_t* offsets, 
   if (st) return st;
   if (a->sector.n == 0) return EDG_OK;
   unsigned grid = edg::grid_for(a->sector.n, kThreads);
-  if (a->complex_values)
-    fill_k<Cplx><<<grid, kThreads, 0, stream>>>(*a, offsets, tmp_cols, tmp_vals, row_nnz, diag, diag_present, error_flag);
+  const bool wide = a->sector.key_words == 2;
+  if (a->complex_values && wide)
+    fill_k<Cplx, edg::u128><<<grid, kThreads, 0, stream>>>(*a, offsets, tmp_cols, tmp_vals, row_nnz, diag, diag_present,
+                                                            error_flag);
+  else if (a->complex_values)
+    fill_k<Cplx, uint64_t><<<grid, kThreads, 0, stream>>>(*a, offsets, tmp_cols, tmp_vals, row_nnz, diag, diag_present,
+                                                          error_flag);
+  else if (wide)
+    fill_k<Real, edg::u128><<<grid, kThreads, 0, stream>>>(*a, offsets, tmp_cols, tmp_vals, row_nnz, diag, diag_present,
+                                                            error_flag);
   else
-    fill_k<Real><<<grid, kThreads, 0, stream>>>(*a, offsets, tmp_cols, tmp_vals, row_nnz, diag, diag_present, error_flag);
+    fill_k<Real, uint64_t><<<grid, kThreads, 0, stream>>>(*a, offsets, tmp_cols, tmp_vals, row_nnz, diag, diag_present,
+                                                          error_flag);
   EDG_CHECK_LAUNCH("edg_assemble_fill");
   return EDG_OK;
 }

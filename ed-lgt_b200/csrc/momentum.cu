@@ -267,6 +267,7 @@ extern "C" int edg_momentum_translations(const edg_lookup_table* sector, const u
   EDG_REQUIRE(n_sites >= 1 && n_sites <= EDG_MAX_SITES && n_shifts >= 1 && n_shifts <= kMaxShifts,
               "edg_momentum_translations: bad sizes");
   EDG_REQUIRE(sector->n < (int64_t)INT32_MAX, "edg_momentum_translations: sector above 2^31 rows");
+  EDG_REQUIRE(sector->key_words <= 1, "edg_momentum_translations: one-word keys only (key space below 2^63)");
   EDG_REQUIRE((local_map == nullptr && row_sign == nullptr) || (map_dim >= 1 && map_dim <= 256),
               "edg_momentum_translations: map_dim must be 1..256");
   EDG_REQUIRE((row_sign == nullptr) == (label_sign == nullptr), "edg_momentum_translations: label_sign and row_sign go together");

@@ -1,4 +1,4 @@
-// Symmetry-sector enumeration on packed uint64 keys.
+// Symmetry-sector enumeration on packed keys of one or two 64-bit words.
 //
 // One level = one site.  Candidate i of level `depth` is (parent p = i / d,
 // state c = i % d) with d = loc_dims[depth]; it survives when
@@ -10,8 +10,11 @@
 // Survivors are written in candidate order, which keeps parents in order and
 // states ascending: the final level is sorted by key, i.e. lexicographically
 // (the order produced by edlgt/symmetries/symmetry_sector.py:785-967).
-// Digits of earlier sites are decoded from the parent key.
+// Digits of earlier sites are decoded from the parent key.  Kernels are
+// templated on the key type (keys.cuh): uint64_t, or a 128-bit pair of words
+// when the key space exceeds 63 bits.
 #include "internal.cuh"
+#include "keys.cuh"
 
 namespace {
 
@@ -20,12 +23,14 @@ constexpr int kItems = 8;
 constexpr int kTile = kThreads * kItems;
 constexpr int kMaxGlob = 4;
 
-__device__ __forceinline__ int digit_of(const edg_sector_tables& t, uint64_t key, int site) {
-  return (int)((key / t.strides[site]) % (uint64_t)t.loc_dims[site]);
+template <typename K>
+__device__ __forceinline__ int digit_of(const edg_sector_tables& t, K key, int site) {
+  return edg::key_digit(key, site, t.n_hi, t.strides[site], (uint64_t)t.loc_dims[site]);
 }
 
 // Evaluates candidate (parent_key, parent sums, state c) at `depth`.
-__device__ __forceinline__ bool candidate_ok(const edg_sector_tables& t, int depth, uint64_t pkey,
+template <typename K>
+__device__ __forceinline__ bool candidate_ok(const edg_sector_tables& t, int depth, K pkey,
                                              const int32_t* __restrict__ psums, int c, int32_t* nsums) {
   const int n = t.n_sites, dm = t.dmax;
   if (!t.site_allowed[depth * dm + c]) return false;
@@ -82,22 +87,24 @@ struct Level {
   int64_t n_cand;
 };
 
-__device__ __forceinline__ bool eval_candidate(const edg_sector_tables& t, const Level& L, int64_t i,
-                                               uint64_t* key_out, int32_t* sums_out) {
+template <typename K>
+__device__ __forceinline__ bool eval_candidate(const edg_sector_tables& t, const Level& L, int64_t i, K* key_out,
+                                               int32_t* sums_out) {
   if (i >= L.n_cand) return false;
   int64_t p = i / L.d;
   int c = (int)(i - p * L.d);
-  uint64_t pkey = L.depth == 0 ? 0ull : L.prev_keys[p];
+  K pkey = L.depth == 0 ? K(0) : edg::ld_key<K>(L.prev_keys, p);
   const int32_t* ps = (L.depth == 0 || L.n_glob == 0) ? nullptr : L.prev_sums + p * L.n_glob;
   bool ok = candidate_ok(t, L.depth, pkey, ps, c, sums_out);
-  *key_out = pkey + (uint64_t)c * t.strides[L.depth];
+  *key_out = pkey + edg::key_step<K>((int64_t)c * (int64_t)t.strides[L.depth], L.depth, t.n_hi);
   return ok;
 }
 
+template <typename K>
 __global__ void __launch_bounds__(kThreads) level_count(edg_sector_tables t, Level L, int64_t* __restrict__ block_counts) {
   int64_t base = (int64_t)blockIdx.x * kTile;
   int local = 0;
-  uint64_t key;
+  K key;
   int32_t sums[kMaxGlob];
 #pragma unroll 1
   for (int it = 0; it < kItems; ++it) {
@@ -117,6 +124,7 @@ __global__ void __launch_bounds__(kThreads) level_count(edg_sector_tables t, Lev
   }
 }
 
+template <typename K>
 __global__ void __launch_bounds__(kThreads) level_fill(edg_sector_tables t, Level L, const int64_t* __restrict__ block_offsets,
                                                        uint64_t* __restrict__ next_keys, int32_t* __restrict__ next_sums) {
   __shared__ int warp_cnt[kThreads / 32];
@@ -128,7 +136,7 @@ __global__ void __launch_bounds__(kThreads) level_fill(edg_sector_tables t, Leve
 #pragma unroll 1
   for (int it = 0; it < kItems; ++it) {
     int64_t i = base + (int64_t)it * kThreads + threadIdx.x;
-    uint64_t key = 0;
+    K key = 0;
     int32_t sums[kMaxGlob];
     bool ok = eval_candidate(t, L, i, &key, sums);
     unsigned ballot = __ballot_sync(0xffffffffu, ok);
@@ -138,7 +146,7 @@ __global__ void __launch_bounds__(kThreads) level_fill(edg_sector_tables t, Leve
     for (int w = 0; w < warp; ++w) pos += warp_cnt[w];
     pos += __popc(ballot & ((1u << lane) - 1u));
     if (ok) {
-      next_keys[pos] = key;
+      edg::st_key(next_keys, pos, key);
       for (int g = 0; g < L.n_glob; ++g) next_sums[pos * L.n_glob + g] = sums[g];
     }
     __syncthreads();
@@ -158,6 +166,8 @@ int check_tables(const edg_sector_tables* t, int32_t depth, int64_t n_prev, cons
   EDG_REQUIRE(t->n_glob >= 0 && t->n_glob <= kMaxGlob, "%s: at most %d global symmetries", who, kMaxGlob);
   EDG_REQUIRE(n_prev >= 0, "%s: negative parent count", who);
   EDG_REQUIRE(depth == 0 ? n_prev == 1 : true, "%s: level 0 expands one empty parent", who);
+  EDG_REQUIRE(t->key_words == 0 || t->key_words == 1 || t->key_words == 2, "%s: key_words must be 1 or 2", who);
+  EDG_REQUIRE(t->key_words != 2 || (t->n_hi > 0 && t->n_hi < t->n_sites), "%s: n_hi out of range", who);
   return EDG_OK;
 }
 
@@ -174,9 +184,14 @@ extern "C" int edg_sector_level_count(const edg_sector_tables* t, int32_t depth,
   if (st) return st;
   int d = t->loc_dims[depth];
   EDG_REQUIRE(d > 0 && d <= t->dmax, "edg_sector_level_count: bad local dimension");
+  EDG_REQUIRE(t->key_words != 2 || depth == 0 || (reinterpret_cast<uintptr_t>(prev_keys) & 15) == 0,
+              "edg_sector_level_count: two-word keys must be 16-byte aligned");
   Level L{depth, d, t->n_glob, prev_keys, prev_sums, n_prev * (int64_t)d};
   int64_t nb = edg_sector_level_blocks(L.n_cand);
-  level_count<<<(unsigned)nb, kThreads, 0, stream>>>(*t, L, block_offsets);
+  if (t->key_words == 2)
+    level_count<edg::u128><<<(unsigned)nb, kThreads, 0, stream>>>(*t, L, block_offsets);
+  else
+    level_count<uint64_t><<<(unsigned)nb, kThreads, 0, stream>>>(*t, L, block_offsets);
   EDG_CHECK_LAUNCH("edg_sector_level_count");
   return edg_scan_i64(block_offsets, block_offsets, nb, scratch, stream);
 }
@@ -188,9 +203,15 @@ extern "C" int edg_sector_level_fill(const edg_sector_tables* t, int32_t depth, 
   if (st) return st;
   int d = t->loc_dims[depth];
   EDG_REQUIRE(d > 0 && d <= t->dmax, "edg_sector_level_fill: bad local dimension");
+  EDG_REQUIRE(t->key_words != 2 || ((depth == 0 || (reinterpret_cast<uintptr_t>(prev_keys) & 15) == 0) &&
+                                     (reinterpret_cast<uintptr_t>(next_keys) & 15) == 0),
+              "edg_sector_level_fill: two-word keys must be 16-byte aligned");
   Level L{depth, d, t->n_glob, prev_keys, prev_sums, n_prev * (int64_t)d};
   int64_t nb = edg_sector_level_blocks(L.n_cand);
-  level_fill<<<(unsigned)nb, kThreads, 0, stream>>>(*t, L, block_offsets, next_keys, next_sums);
+  if (t->key_words == 2)
+    level_fill<edg::u128><<<(unsigned)nb, kThreads, 0, stream>>>(*t, L, block_offsets, next_keys, next_sums);
+  else
+    level_fill<uint64_t><<<(unsigned)nb, kThreads, 0, stream>>>(*t, L, block_offsets, next_keys, next_sums);
   EDG_CHECK_LAUNCH("edg_sector_level_fill");
   return EDG_OK;
 }
@@ -221,7 +242,57 @@ __global__ void configs_to_keys_k(const uint16_t* __restrict__ configs, int64_t 
   }
 }
 
+// Two-word keys: digits of sites [n_hi, n) from the low word, of [0, n_hi)
+// from the high word.
+__global__ void keys_to_configs_wide_k(const uint64_t* __restrict__ keys, int64_t n, int n_sites, int n_hi,
+                                       const int32_t* __restrict__ loc_dims, uint16_t* __restrict__ configs) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    uint64_t lo = keys[2 * i], hi = keys[2 * i + 1];
+    for (int s = n_sites - 1; s >= n_hi; --s) {
+      uint64_t d = (uint64_t)loc_dims[s];
+      configs[i * n_sites + s] = (uint16_t)(lo % d);
+      lo /= d;
+    }
+    for (int s = n_hi - 1; s >= 0; --s) {
+      uint64_t d = (uint64_t)loc_dims[s];
+      configs[i * n_sites + s] = (uint16_t)(hi % d);
+      hi /= d;
+    }
+  }
+}
+
+__global__ void configs_to_keys_wide_k(const uint16_t* __restrict__ configs, int64_t n, int n_sites, int n_hi,
+                                       const uint64_t* __restrict__ strides, uint64_t* __restrict__ keys) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    uint64_t hi = 0, lo = 0;
+    for (int s = 0; s < n_hi; ++s) hi += (uint64_t)configs[i * n_sites + s] * strides[s];
+    for (int s = n_hi; s < n_sites; ++s) lo += (uint64_t)configs[i * n_sites + s] * strides[s];
+    keys[2 * i] = lo;
+    keys[2 * i + 1] = hi;
+  }
+}
+
 }  // namespace
+
+extern "C" int edg_keys_to_configs_wide(const uint64_t* keys, int64_t n, int32_t n_sites, int32_t n_hi,
+                                        const int32_t* loc_dims, uint16_t* configs, cudaStream_t stream) {
+  EDG_REQUIRE(n >= 0 && n_sites > 1 && n_sites <= EDG_MAX_SITES && n_hi > 0 && n_hi < n_sites,
+              "edg_keys_to_configs_wide: bad sizes");
+  if (n == 0) return EDG_OK;
+  keys_to_configs_wide_k<<<edg::grid_for(n, 256), 256, 0, stream>>>(keys, n, n_sites, n_hi, loc_dims, configs);
+  EDG_CHECK_LAUNCH("edg_keys_to_configs_wide");
+  return EDG_OK;
+}
+
+extern "C" int edg_configs_to_keys_wide(const uint16_t* configs, int64_t n, int32_t n_sites, int32_t n_hi,
+                                        const uint64_t* strides, uint64_t* keys, cudaStream_t stream) {
+  EDG_REQUIRE(n >= 0 && n_sites > 1 && n_sites <= EDG_MAX_SITES && n_hi > 0 && n_hi < n_sites,
+              "edg_configs_to_keys_wide: bad sizes");
+  if (n == 0) return EDG_OK;
+  configs_to_keys_wide_k<<<edg::grid_for(n, 256), 256, 0, stream>>>(configs, n, n_sites, n_hi, strides, keys);
+  EDG_CHECK_LAUNCH("edg_configs_to_keys_wide");
+  return EDG_OK;
+}
 
 extern "C" int edg_keys_to_configs(const uint64_t* keys, int64_t n, int32_t n_sites, const int32_t* loc_dims,
                                    uint16_t* configs, cudaStream_t stream) {

@@ -334,6 +334,7 @@ extern "C" int edg_twobody_expval(const edg_lookup_table* sector, const uint64_t
   EDG_REQUIRE(n_sites >= 2 && n_sites <= EDG_MAX_SITES && dmax >= 1 && dmax <= 256 && psi_stride >= 1,
               "edg_twobody_expval: bad sizes");
   EDG_REQUIRE(psi_dtype >= 0 && psi_dtype <= 3, "edg_twobody_expval: psi_dtype must be 0..3");
+  EDG_REQUIRE(sector->key_words <= 1, "edg_twobody_expval: one-word keys only (key space below 2^63)");
   EDG_REQUIRE(n_pairs >= 0 && n_pairs <= n_sites * (n_sites - 1) / 2 && (n_pairs == 0 || (pair_i && pair_j)),
               "edg_twobody_expval: bad pair list");
   EDG_REQUIRE(((uintptr_t)t_amp & 15) == 0, "edg_twobody_expval: t_amp must be 16-byte aligned");

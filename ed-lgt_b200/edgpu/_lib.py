@@ -74,6 +74,8 @@ class SectorTables(C.Structure):
         ("nb_id", P),
         ("nb_site_start", P),
         ("nb_sites", P),
+        ("key_words", I32),
+        ("n_hi", I32),
     ]
 
 
@@ -84,6 +86,9 @@ class LookupTable(C.Structure):
         ("bucket_start", P),
         ("shift", I32),
         ("n_buckets", I64),
+        ("key_words", I32),
+        ("n_hi", I32),
+        ("lo_space", U64),
     ]
 
 
@@ -276,6 +281,9 @@ _SIGS = {
     "edg_keys_to_configs": (I32, [P, I64, I32, P, P, P]),
     "edg_configs_to_keys": (I32, [P, I64, I32, P, P, P]),
     "edg_lookup_build": (I32, [P, I64, I32, I64, P, P]),
+    "edg_lookup_build_wide": (I32, [P, I64, I32, U64, I32, I64, P, P]),
+    "edg_keys_to_configs_wide": (I32, [P, I64, I32, I32, P, P, P]),
+    "edg_configs_to_keys_wide": (I32, [P, I64, I32, I32, P, P, P]),
     "edg_lookup": (I32, [C.POINTER(LookupTable), P, I64, P, P]),
     "edg_assemble_count": (I32, [C.POINTER(Assembly), P, P]),
     "edg_assemble_fill": (I32, [C.POINTER(Assembly), P, P, P, P, P, P, P, P]),
@@ -293,6 +301,7 @@ _SIGS = {
     "edg_tridiag_lowest": (I32, [P, P, I32, I32, P, P, P, P]),
     "edg_tridiag_lowest_noalloc": (I32, [P, P, I32, I32, P, P, P]),
     "edg_local_expval": (I32, [P, I64, C.POINTER(SiteDims), I32, P, I32, I64, P, I32, P, P]),
+    "edg_local_expval_wide": (I32, [P, I64, I32, C.POINTER(SiteDims), I32, P, I32, I64, P, I32, P, P]),
     "edg_small_batch_work_elems": (I64, [I64, I32, I32]),
     "edg_lanczos_small_batched": (I32, [C.POINTER(SmallBatch), P, P]),
     "edg_ctx_create": (P, []),

@@ -39,6 +39,7 @@ def partition_map(sector, sites):
     used ascending): index[r] is row r's position among the distinct part
     configurations (a device int64 tensor), unique_configs their uint16 table
     in ascending lexicographic order (host)."""
+    sector.require_narrow("partition map")
     sites = sorted(int(s) for s in sites)
     dev = sector.device
     n = len(sector)

@@ -52,8 +52,13 @@ def site_expval_device(sector, op, psi, out=None):
     dims = _lib.SiteDims()
     for s in range(n_sites):
         dims.d[s] = int(sector.loc_dims[s])
-    check(lib.edg_local_expval(ptr(sector.keys), len(sector), ctypes.byref(dims), n_sites, ptr(p), codes[p.dtype], 1,
-                               ptr(dd), dd.shape[1], ptr(out), stream_handle()), "edg_local_expval")
+    if sector.wide:
+        check(lib.edg_local_expval_wide(ptr(sector.keys), len(sector), sector.n_hi, ctypes.byref(dims), n_sites, ptr(p),
+                                        codes[p.dtype], 1, ptr(dd), dd.shape[1], ptr(out), stream_handle()),
+              "edg_local_expval_wide")
+    else:
+        check(lib.edg_local_expval(ptr(sector.keys), len(sector), ctypes.byref(dims), n_sites, ptr(p), codes[p.dtype],
+                                   1, ptr(dd), dd.shape[1], ptr(out), stream_handle()), "edg_local_expval")
     return out
 
 
@@ -82,6 +87,7 @@ def twobody_corr_device(sector, op_a, op_b, psi, pairs=None):
     with lattice_twobody_exp_val (edlgt/modeling/twobody_term.py:160-264).
     op_a, op_b: (n_sites, dmax, dmax) projected site operators; psi: device
     vector in the sector basis."""
+    sector.require_narrow("two-body correlators")
     n_sites = sector.n_sites
     dmax = int(op_a.shape[-1])
     key = ("tb", id(op_a), id(op_b), sector.device, tuple(int(d) for d in sector.loc_dims))

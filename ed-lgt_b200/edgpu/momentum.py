@@ -71,6 +71,7 @@ class MomentumBasis:
         """``local_map`` / ``label_sign``: the translation-charge variant (1D,
         unit cell 1): the local map applied with every unit shift and the
         per-state signs whose product twists the odd shifts."""
+        sector.require_narrow("momentum basis")
         dev = sector.device
         self.sector = sector
         self.device = dev

@@ -36,18 +36,49 @@ __all__ = [
     "get_link_sector_configs",
     "global_abelian_sector",
     "compute_strides",
+    "key_layout",
     "config_to_index_binarysearch",
 ]
 
 SYM_TOL = 1e-13
 
 
-def compute_strides(loc_dims) -> np.ndarray:
-    """Mixed-radix strides with the last site fastest (``tools/magic.py:41-80``)."""
+KEY_WORD_LIMIT = 2**63
+
+
+def key_layout(loc_dims):
+    """Key layout of a lattice: ``(key_words, n_hi, lo_space)``.
+
+    One word (``(1, 0, prod d)``) when the product of the local dimensions is
+    below 2^63.  Otherwise two words: the low word takes the longest run of
+    trailing sites whose dimensions multiply to less than 2^63 (``lo_space``),
+    the high word the ``n_hi`` leading sites, whose product must also stay
+    below 2^63 (126 bits of key space in all).  The key is then the 128-bit
+    number ``hi * 2**64 + lo``, ordered like the configurations."""
+    dims = [int(d) for d in np.asarray(loc_dims, dtype=np.int64)]
+    total = math.prod(dims)
+    if total < KEY_WORD_LIMIT:
+        return 1, 0, total
+    lo_space, n_hi = 1, len(dims)
+    while n_hi > 0 and lo_space * dims[n_hi - 1] < KEY_WORD_LIMIT:
+        n_hi -= 1
+        lo_space *= dims[n_hi]
+    if math.prod(dims[:n_hi]) >= KEY_WORD_LIMIT:
+        raise OverflowError("the product of local dimensions exceeds a two-word (126-bit) key")
+    return 2, n_hi, lo_space
+
+
+def compute_strides(loc_dims, n_hi: int = 0) -> np.ndarray:
+    """Mixed-radix strides with the last site fastest (``tools/magic.py:41-80``).
+
+    With ``n_hi > 0`` (two-word keys) the strides of sites ``[0, n_hi)`` are
+    relative to the high word and restart at 1 on site ``n_hi - 1``."""
     loc_dims = np.asarray(loc_dims, dtype=np.int64)
     strides = np.empty(len(loc_dims), dtype=np.uint64)
     run = 1
     for k in range(len(loc_dims) - 1, -1, -1):
+        if k == n_hi - 1:
+            run = 1
         strides[k] = run
         run *= int(loc_dims[k])
     return strides
@@ -115,11 +146,10 @@ class SectorSpec:
         n = len(self.loc_dims)
         if not 0 < n <= _lib.MAX_SITES:
             raise ValueError(f"1..{_lib.MAX_SITES} sites supported, got {n}")
-        if math.prod(int(d) for d in self.loc_dims) >= 2**63:
-            raise OverflowError("the product of local dimensions does not fit a 63-bit key")
+        self.key_words, self.n_hi, self.lo_space = key_layout(self.loc_dims)
         self.n_sites = n
         self.dmax = int(self.loc_dims.max())
-        self.strides = compute_strides(self.loc_dims)
+        self.strides = compute_strides(self.loc_dims, self.n_hi)
         dm = self.dmax
 
         def pad(a, lead):
@@ -303,12 +333,16 @@ class _DeviceTables:
         t.nb_id = ptr(k["ni"])
         t.nb_site_start = ptr(k["nss"])
         t.nb_sites = ptr(k["nsi"])
+        t.key_words = spec.key_words
+        t.n_hi = spec.n_hi
         self.struct = t
 
 
 class Sector:
-    """A symmetry sector: sorted uint64 keys on the device (int64 storage).
+    """A symmetry sector: sorted keys on the device (int64 storage).
 
+    One-word keys are a ``(N,)`` tensor; two-word keys (key space above 2^63,
+    :func:`key_layout`) a ``(N, 2)`` tensor of (low, high) words.
     ``configs`` decodes the keys to the reference's ``(N, n_sites)`` uint16
     table on demand; ``index_of`` looks configurations up on the device.
     """
@@ -317,7 +351,10 @@ class Sector:
         self.keys = keys
         self.loc_dims = np.asarray(loc_dims, dtype=np.int64)
         self.n_sites = len(self.loc_dims)
-        self.strides = compute_strides(self.loc_dims)
+        self.key_words, self.n_hi, self.lo_space = key_layout(self.loc_dims)
+        if (keys.dim() == 2) != (self.key_words == 2):
+            raise ValueError("key tensor shape does not match the key layout of loc_dims")
+        self.strides = compute_strides(self.loc_dims, self.n_hi)
         self.device = keys.device if device is None else device
         self._configs = None
         self._lookup = None
@@ -329,9 +366,20 @@ class Sector:
     def dim(self) -> int:
         return len(self)
 
+    @property
+    def wide(self) -> bool:
+        """True for two-word keys."""
+        return self.key_words == 2
+
+    def require_narrow(self, what: str):
+        """Refuses callers that handle one-word keys only."""
+        if self.wide:
+            raise NotImplementedError(f"{what}: sectors whose key space exceeds 63 bits are not supported")
+
     # ------------------------------------------------------------------ lookup
     def lookup_table(self):
-        """Bucket table over the top key bits (built once, kept on the device)."""
+        """Bucket table over the top bits of the dense key (built once, kept
+        on the device)."""
         if self._lookup is None:
             n = len(self)
             key_space = int(np.prod(self.loc_dims.astype(object)))
@@ -340,31 +388,45 @@ class Sector:
             shift = key_bits - bucket_bits
             n_buckets = ((key_space - 1) >> shift) + 1
             starts = torch.empty(n_buckets + 1, dtype=torch.int64, device=self.device)
-            check(lib.edg_lookup_build(ptr(self.keys), n, shift, n_buckets, ptr(starts), stream_handle()),
-                  "edg_lookup_build")
+            if self.wide:
+                check(lib.edg_lookup_build_wide(ptr(self.keys), n, 2, self.lo_space, shift, n_buckets, ptr(starts),
+                                                stream_handle()), "edg_lookup_build_wide")
+            else:
+                check(lib.edg_lookup_build(ptr(self.keys), n, shift, n_buckets, ptr(starts), stream_handle()),
+                      "edg_lookup_build")
             t = _lib.LookupTable()
             t.keys = ptr(self.keys)
             t.n = n
             t.bucket_start = ptr(starts)
             t.shift = shift
             t.n_buckets = n_buckets
+            t.key_words = self.key_words
+            t.n_hi = self.n_hi
+            t.lo_space = self.lo_space if self.wide else 0
             self._lookup = (t, starts)
         return self._lookup[0]
 
     def encode(self, configs) -> torch.Tensor:
-        """(M, n_sites) configurations -> int64 keys on the device."""
+        """(M, n_sites) configurations -> int64 keys on the device ((M,) or
+        (M, 2) for two-word keys)."""
         c = torch.as_tensor(np.ascontiguousarray(np.asarray(configs, dtype=np.uint16)).reshape(-1, self.n_sites))
         c = c.to(self.device)
         strides = torch.from_numpy(self.strides.astype(np.int64)).to(self.device)
-        keys = torch.empty(c.shape[0], dtype=torch.int64, device=self.device)
-        check(lib.edg_configs_to_keys(ptr(c), c.shape[0], self.n_sites, ptr(strides), ptr(keys), stream_handle()),
-              "edg_configs_to_keys")
+        m = c.shape[0]
+        if self.wide:
+            keys = torch.empty((m, 2), dtype=torch.int64, device=self.device)
+            check(lib.edg_configs_to_keys_wide(ptr(c), m, self.n_sites, self.n_hi, ptr(strides), ptr(keys),
+                                               stream_handle()), "edg_configs_to_keys_wide")
+        else:
+            keys = torch.empty(m, dtype=torch.int64, device=self.device)
+            check(lib.edg_configs_to_keys(ptr(c), m, self.n_sites, ptr(strides), ptr(keys), stream_handle()),
+                  "edg_configs_to_keys")
         return keys
 
     def index_of(self, configs) -> np.ndarray:
         """Row index of each configuration, -1 when not in the sector."""
         q = self.encode(configs)
-        out = torch.empty_like(q)
+        out = torch.empty(q.shape[0], dtype=torch.int64, device=self.device)
         check(lib.edg_lookup(self.lookup_table(), ptr(q), q.shape[0], ptr(out), stream_handle()), "edg_lookup")
         return out.cpu().numpy()
 
@@ -375,12 +437,17 @@ class Sector:
             n = len(self)
             out = torch.empty((max(n, 1), self.n_sites), dtype=torch.int16, device=self.device)
             ld = torch.from_numpy(self.loc_dims.astype(np.int32)).to(self.device)
-            check(lib.edg_keys_to_configs(ptr(self.keys), n, self.n_sites, ptr(ld), ptr(out), stream_handle()),
-                  "edg_keys_to_configs")
+            if self.wide:
+                check(lib.edg_keys_to_configs_wide(ptr(self.keys), n, self.n_sites, self.n_hi, ptr(ld), ptr(out),
+                                                   stream_handle()), "edg_keys_to_configs_wide")
+            else:
+                check(lib.edg_keys_to_configs(ptr(self.keys), n, self.n_sites, ptr(ld), ptr(out), stream_handle()),
+                      "edg_keys_to_configs")
             self._configs = out[:n].cpu().numpy().view(np.uint16)
         return self._configs
 
     def host_keys(self) -> np.ndarray:
+        """uint64 keys on the host: (N,), or (N, 2) (low, high) words."""
         return self.keys.cpu().numpy().view(np.uint64)
 
 
@@ -390,7 +457,8 @@ def enumerate_sector(spec: SectorSpec, device=None) -> Sector:
     tables = _DeviceTables(spec, device)
     st = stream_handle()
     ng = spec.glob_val.shape[0]
-    prev_keys = torch.zeros(1, dtype=torch.int64, device=device)
+    kshape = (lambda m: (m, 2)) if spec.key_words == 2 else (lambda m: (m,))
+    prev_keys = torch.zeros(kshape(1), dtype=torch.int64, device=device)
     prev_sums = torch.zeros(max(ng, 1), dtype=torch.int32, device=device)
     n_prev = 1
     level_sizes = []
@@ -402,7 +470,7 @@ def enumerate_sector(spec: SectorSpec, device=None) -> Sector:
         check(lib.edg_sector_level_count(C_ref(tables.struct), depth, ptr(prev_keys), ptr(prev_sums), n_prev,
                                          ptr(offsets), ptr(scratch), st), "edg_sector_level_count")
         total = int(offsets[nb].item())
-        next_keys = torch.empty(max(total, 1), dtype=torch.int64, device=device)
+        next_keys = torch.empty(kshape(max(total, 1)), dtype=torch.int64, device=device)
         next_sums = torch.empty(max(total * ng, 1), dtype=torch.int32, device=device)
         if total > 0:
             check(lib.edg_sector_level_fill(C_ref(tables.struct), depth, ptr(prev_keys), ptr(prev_sums), n_prev,

@@ -84,6 +84,21 @@ int edg_scan_i64(const int64_t* in, int64_t* out, int64_t n, int64_t* scratch,
                  cudaStream_t stream);
 
 /* ------------------------------------------------------------------------ */
+/* Sector keys                                                               */
+/* A configuration (c_0 .. c_{n-1}) is the mixed-radix number                */
+/* sum_s c_s * stride_s with the last site fastest (edlgt/tools/magic.py:     */
+/* 41-140).  When the product of the local dimensions is below 2^63 a key is */
+/* one uint64 word (key_words = 1).  Otherwise (key_words = 2) the sites are */
+/* split at n_hi: the high word holds sites [0, n_hi), the low word sites    */
+/* [n_hi, n_sites), each a mixed-radix number below 2^63 whose strides are    */
+/* relative to its own word (stride of site n_hi-1 and of site n_sites-1 is  */
+/* 1).  A two-word key takes 16 bytes, low word first, 16-byte aligned: the   */
+/* unsigned 128-bit integer hi * 2^64 + lo, whose order is the               */
+/* lexicographic order of the configurations.  Key arrays passed as          */
+/* "uint64_t*" hold key_words words per key.  Up to 126 bits of key space.   */
+/* ------------------------------------------------------------------------ */
+
+/* ------------------------------------------------------------------------ */
 /* Sector enumeration                                                        */
 /* Replaces iterative_sitebased_sym_sector_configs,                          */
 /* iterative_sitebased_sym_sector_configs1, iterative_link_sector_configs,    */
@@ -123,6 +138,9 @@ typedef struct {
   const int32_t* nb_id;           /* [n_act] constraint id                   */
   const int32_t* nb_site_start;   /* [n_nb+1] site list offsets              */
   const int32_t* nb_sites;        /* flattened site lists                    */
+  /* key layout (see "Sector keys" above): 1 word, or 2 words split at n_hi  */
+  int32_t key_words;              /* 1 or 2                                  */
+  int32_t n_hi;                   /* sites [0, n_hi) in the high word (W=2)  */
 } edg_sector_tables;
 
 /* Number of per-block counters (int64) the level kernels need for n
@@ -157,6 +175,15 @@ int edg_keys_to_configs(const uint64_t* keys, int64_t n, int32_t n_sites,
 int edg_configs_to_keys(const uint16_t* configs, int64_t n, int32_t n_sites,
                         const uint64_t* strides, uint64_t* keys,
                         cudaStream_t stream);
+/* The same for two-word keys split at n_hi (keys: 2n words; strides within
+ * each word, device array of n_sites). */
+int edg_keys_to_configs_wide(const uint64_t* keys, int64_t n, int32_t n_sites,
+                             int32_t n_hi, const int32_t* loc_dims,
+                             uint16_t* configs, cudaStream_t stream);
+int edg_configs_to_keys_wide(const uint16_t* configs, int64_t n,
+                             int32_t n_sites, int32_t n_hi,
+                             const uint64_t* strides, uint64_t* keys,
+                             cudaStream_t stream);
 
 /* ------------------------------------------------------------------------ */
 /* config -> index lookup                                                    */
@@ -169,14 +196,26 @@ typedef struct {
   const uint64_t* keys;         /* [n] sorted ascending, unique              */
   int64_t n;
   const int64_t* bucket_start;  /* [n_buckets+1]                             */
-  int32_t shift;                /* bucket = key >> shift                     */
+  int32_t shift;                /* bucket = dense key >> shift               */
   int64_t n_buckets;
+  /* key layout; zero-initialised tables read as one-word keys              */
+  int32_t key_words;            /* 0 or 1: one word; 2: two words            */
+  int32_t n_hi;                 /* sites [0, n_hi) in the high word          */
+  uint64_t lo_space;            /* product of the low word's dimensions: the */
+                                /* dense key is hi * lo_space + lo (W = 2)   */
 } edg_lookup_table;
 
 /* Fills bucket_start (n_buckets+1 entries) for keys < n_buckets << shift. */
 int edg_lookup_build(const uint64_t* keys, int64_t n, int32_t shift,
                      int64_t n_buckets, int64_t* bucket_start,
                      cudaStream_t stream);
+/* Bucket table for keys of key_words words (1 or 2): bucket_start[b] is
+ * the first row whose dense key (hi * lo_space + lo for two words) is
+ * >= b << shift, and bucket_start[n_buckets] = n.  shift < 64 for one-word
+ * keys, < 127 for two; every dense key must be < n_buckets << shift. */
+int edg_lookup_build_wide(const uint64_t* keys, int64_t n, int32_t key_words,
+                          uint64_t lo_space, int32_t shift, int64_t n_buckets,
+                          int64_t* bucket_start, cudaStream_t stream);
 int edg_lookup(const edg_lookup_table* table, const uint64_t* queries,
                int64_t m, int64_t* index_out, cudaStream_t stream);
 
@@ -527,6 +566,12 @@ int edg_local_expval(const uint64_t* keys, int64_t n, const edg_site_dims* dims,
                      int32_t n_sites, const void* psi, int32_t psi_dtype,
                      int64_t psi_stride, const double* diag, int32_t dmax,
                      double* out, cudaStream_t stream);
+/* The same over two-word keys split at n_hi (keys: 2n words). */
+int edg_local_expval_wide(const uint64_t* keys, int64_t n, int32_t n_hi,
+                          const edg_site_dims* dims, int32_t n_sites,
+                          const void* psi, int32_t psi_dtype,
+                          int64_t psi_stride, const double* diag,
+                          int32_t dmax, double* out, cudaStream_t stream);
 
 /* Two-body correlators, TwoBodyTerm.get_expval / lattice_twobody_exp_val
  * (edlgt/modeling/twobody_term.py:160-264): corr[i * n_sites + j] =

@@ -68,6 +68,22 @@ def keys_of(configs, loc_dims):
     return (c * strides_of(loc_dims)[None, :]).sum(axis=1, dtype=np.uint64)
 
 
+def _narrow(loc_dims):
+    return int(np.prod(np.asarray(loc_dims, dtype=object))) < 2**63
+
+
+def searchable(configs, loc_dims):
+    """Row keys whose order is the lexicographic order of the configurations:
+    uint64 mixed-radix keys when the key space is below 2^63, else the
+    configurations as big-endian byte strings (the comparison
+    config_to_index_binarysearch makes element by element,
+    edlgt/symmetries/generate_configs.py:145-173)."""
+    c = np.ascontiguousarray(np.atleast_2d(configs), dtype=np.uint16)
+    if _narrow(loc_dims):
+        return keys_of(c, loc_dims)
+    return np.ascontiguousarray(c.astype(">u2")).view(f"V{2 * c.shape[1]}").reshape(-1)
+
+
 def sector_configs(loc_dims, glob_diags=None, glob_sectors=None, glob_type="U", link_diags=None, link_sectors=None,
                    pair_list=None, string_diags=None, string_sectors=None, nbody_diags=None, nbody_sectors=None,
                    nbody_sites=None, nbody_type="U"):
@@ -146,8 +162,8 @@ def sector_configs(loc_dims, glob_diags=None, glob_sectors=None, glob_type="U", 
 
 def config_to_index(queries, sector_cfg, loc_dims):
     """Row of each query configuration in the sorted table, -1 if absent."""
-    keys = keys_of(sector_cfg, loc_dims)
-    q = keys_of(np.atleast_2d(queries), loc_dims)
+    keys = searchable(sector_cfg, loc_dims)
+    q = searchable(np.atleast_2d(queries), loc_dims)
     pos = np.searchsorted(keys, q)
     pos_c = np.minimum(pos, len(keys) - 1)
     hit = (pos < len(keys)) & (keys[pos_c] == q)
@@ -167,8 +183,9 @@ def nbody_triplets(op_list, op_sites, cfg, loc_dims):
     """(row, col, val) of prod_j op_j[site_j] in the sector (rows in order)."""
     op_sites = [int(s) for s in op_sites]
     trans = [_transitions(np.asarray(op_list[j][op_sites[j]], dtype=np.complex128)) for j in range(len(op_sites))]
-    keys = keys_of(cfg, loc_dims)
-    strides = strides_of(loc_dims).astype(np.int64)
+    narrow = _narrow(loc_dims)
+    keys = searchable(cfg, loc_dims)
+    strides = strides_of(loc_dims).astype(np.int64) if narrow else None
     bra_states = cfg[:, op_sites].astype(np.int64)
     rows_out, cols_out, vals_out = [], [], []
     # group rows by their local bra states on the acted sites
@@ -184,16 +201,21 @@ def nbody_triplets(op_list, op_sites, cfg, loc_dims):
         if not combos or any(len(c) != len(b) for c in combos):
             continue
         for t, combo in enumerate(combos):
-            delta = 0
             amp = 1.0 + 0.0j
-            for j, (k, a) in enumerate(combo):
-                delta += (k - int(b[j])) * int(strides[op_sites[j]])
+            for _, a in combo:
                 amp *= a
-            ket_keys = (keys.astype(np.int64) + delta).astype(np.uint64)
+            if narrow:
+                delta = sum((k - int(b[j])) * int(strides[op_sites[j]]) for j, (k, _) in enumerate(combo))
+                ket_keys = (keys[rows].astype(np.int64) + delta).astype(np.uint64)
+            else:
+                kc = cfg[rows].copy()
+                for j, (k, _) in enumerate(combo):
+                    kc[:, op_sites[j]] = k
+                ket_keys = searchable(kc, loc_dims)
             pos = np.searchsorted(keys, ket_keys)
             pos_c = np.minimum(pos, len(keys) - 1)
             col = np.where((pos < len(keys)) & (keys[pos_c] == ket_keys), pos_c, -1)
-            per_row.append((rows, t, col[rows], amp))
+            per_row.append((rows, t, col, amp))
     if not per_row:
         return np.zeros(0, np.int64), np.zeros(0, np.int64), np.zeros(0, np.complex128)
     for rows, t, col, amp in per_row:

@@ -162,3 +162,18 @@ def build_generic(name, device="cpu"):
 
     kw, g, m = SU2_GEN_CASES[name]
     return SU2_Model(**kw, device=device), g, m
+
+
+# lattices whose key space exceeds 63 bits (two-word keys); fixtures from
+# tests/golden/make_golden.py wide
+WIDE_CASES = {
+    "qed2d_4x4_pure_pbc_s1": (dict(spin=1, pure_theory=True, lvals=[4, 4], has_obc=[False, False]), 1.1),
+    "qed2d_4x4_pure_obc_s2": (dict(spin=2, pure_theory=True, lvals=[4, 4], has_obc=[True, True]), 0.9),
+}
+
+
+def build_wide(name, device="cpu"):
+    from edgpu.models import QED_Model
+
+    kw, g = WIDE_CASES[name]
+    return QED_Model(**kw, device=device), g

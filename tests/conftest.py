@@ -121,3 +121,10 @@ def golden_integrated():
     import numpy as np
 
     return np.load(os.path.join(GOLDEN, "integrated_cases.npz"))
+
+
+@pytest.fixture(scope="session")
+def golden_wide():
+    import numpy as np
+
+    return np.load(os.path.join(GOLDEN, "wide_cases.npz"))

@@ -6,7 +6,7 @@ and numba/scipy/sympy:
     python tests/golden/make_golden.py [group ...]
 
 Groups: small, pins, dynamics, big, twobody, entropy, momentum, full,
-nbody, overlap, state, local, integrated, string, generic.  Output: .npz files next to
+nbody, overlap, state, local, integrated, string, generic, wide.  Output: .npz files next to
 this script.  Nothing here is imported by the library or by the GPU tests;
 the tests only read the .npz files.
 
@@ -679,9 +679,46 @@ def gen_generic_su2():
     np.savez_compressed(os.path.join(HERE, "generic_su2_cases.npz"), **out)
 
 
+WIDE_CASES = {
+    # name: (kwargs, g); pure gauge lattices whose key space exceeds 63 bits
+    "qed2d_4x4_pure_pbc_s1": (dict(spin=1, pure_theory=True, lvals=[4, 4], has_obc=[False, False]), 1.1),
+    "qed2d_4x4_pure_obc_s2": (dict(spin=2, pure_theory=True, lvals=[4, 4], has_obc=[True, True]), 0.9),
+}
+
+
+def gen_wide():
+    """Sectors whose key space exceeds 63 bits (product of the local
+    dimensions >= 2^63): the reference's uint16 sector tables (dimension,
+    sha256 of the table bytes, every 997th row), the canonical matrix digest
+    and the two lowest energies."""
+    out = {}
+    for name, (kw, g) in WIDE_CASES.items():
+        t0 = time.time()
+        model = qed_model(kw)
+        cfg = np.ascontiguousarray(model.sector_configs, dtype=np.uint16)
+        out[f"{name}/dim"] = np.int64(cfg.shape[0])
+        out[f"{name}/configs_sha"] = np.array(sha(cfg))
+        out[f"{name}/sample_rows"] = np.arange(0, cfg.shape[0], 997, dtype=np.int64)
+        out[f"{name}/sample_configs"] = cfg[::997].copy()
+        out[f"{name}/loc_dims"] = np.asarray(model.loc_dims, dtype=np.int64)
+        out[f"{name}/g"] = np.float64(g)
+        t1 = time.time()
+        model.build_Hamiltonian(g)
+        out |= matrix_record(canonical(model), f"{name}/H_", False)
+        t2 = time.time()
+        model.diagonalize_Hamiltonian(2, "sparse")
+        out[f"{name}/energies"] = np.asarray(model.H.Nenergies)
+        out[f"{name}/seconds"] = np.array([t1 - t0, t2 - t1, time.time() - t2])
+        print(name, cfg.shape[0], f"bits {np.log2(np.prod(np.asarray(model.loc_dims, dtype=float))):.1f}",
+              f"{time.time() - t0:.1f}s", model.H.Nenergies, flush=True)
+    np.savez_compressed(os.path.join(HERE, "wide_cases.npz"), **out)
+
+
 if __name__ == "__main__":
     groups = sys.argv[1:] or ["small", "pins", "dynamics", "big", "twobody", "entropy", "momentum", "full", "nbody",
-                             "overlap", "state", "local", "integrated", "string", "generic"]
+                             "overlap", "state", "local", "integrated", "string", "generic", "wide"]
+    if "wide" in groups:
+        gen_wide()
     if "generic" in groups:
         gen_generic_su2()
     if "string" in groups:

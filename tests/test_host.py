@@ -58,8 +58,12 @@ def test_z2_generator_bits():
 
 
 def test_key_overflow_rejected():
+    """Two-word keys cover up to 126 bits of key space; beyond it the spec
+    is refused."""
+    spec = SectorSpec([1000] * 8)
+    assert (spec.key_words, spec.n_hi, spec.lo_space) == (2, 2, 1000**6)
     with pytest.raises(OverflowError):
-        SectorSpec([1000] * 8)
+        SectorSpec([1000] * 13)
 
 
 def test_term_instances_follow_reference_loops():

@@ -289,3 +289,68 @@ def test_generic_su2_matches_reference(name, golden_generic):
     e_ref = golden_generic[f"{name}/energies"]
     w, _ = O.lowest_eigs(H, len(e_ref))
     assert np.allclose(w / model.n_sites, e_ref, atol=1e-10, rtol=0)
+
+
+def _digest(H):
+    import hashlib
+
+    rows = np.repeat(np.arange(H.shape[0], dtype=np.int64), np.diff(H.indptr))
+    cols = H.indices.astype(np.int64)
+    w = 1.0 / (1.0 + ((rows * 7919 + cols * 104729) % 1009))
+    return H.nnz, hashlib.sha256(np.stack([rows, cols]).tobytes()).hexdigest(), complex(np.sum(H.data * w))
+
+
+def test_two_word_key_layout():
+    """Key spaces above 63 bits split into a high word (leading sites) and a
+    low word (the longest trailing run below 2^63); the 128-bit number
+    hi * 2^64 + lo orders configurations lexicographically."""
+    from edgpu.symmetries import compute_strides, key_layout
+
+    assert key_layout([19] * 14) == (1, 0, 19**14)
+    words, n_hi, lo_space = key_layout([19] * 16)
+    assert (words, n_hi, lo_space) == (2, 2, 19**14)
+    dims = [5, 19, 19, 5, 19, 85, 85, 19, 19, 85, 85, 19, 5, 19, 19, 5]
+    words, n_hi, lo_space = key_layout(dims)
+    assert words == 2 and lo_space < 2**63 and lo_space * dims[n_hi - 1] >= 2**63
+    assert np.prod(np.asarray(dims[:n_hi], dtype=object)) < 2**63
+    st = compute_strides(dims, n_hi)
+    assert st[n_hi - 1] == 1 and st[-1] == 1
+    rng = np.random.default_rng(0)
+    cfg = np.stack([rng.integers(0, d, 4000) for d in dims], axis=1)
+    cfg = cfg[np.lexsort(cfg.T[::-1])]
+    big = [(int(sum(int(c[s]) * int(st[s]) for s in range(n_hi))) << 64)
+           + int(sum(int(c[s]) * int(st[s]) for s in range(n_hi, len(dims)))) for c in cfg]
+    assert all(a <= b for a, b in zip(big, big[1:]))
+    with pytest.raises(OverflowError):
+        key_layout([255] * 17)
+
+
+@pytest.mark.parametrize("name", sorted(__import__("cases").WIDE_CASES))
+def test_wide_sector_matches_reference(name, golden_wide):
+    """Pure-gauge 4x4 QED lattices with a key space above 63 bits: the
+    oracle's sector table equals the reference's (sha256 of the uint16
+    table, sampled rows), the lookup finds every sampled row, and (periodic
+    lattice) the canonical matrix digest and two lowest energies match."""
+    import hashlib
+
+    from cases import build_wide
+
+    model, g = build_wide(name)
+    assert np.array_equal(model.loc_dims, golden_wide[f"{name}/loc_dims"])
+    assert model.sector_spec.key_words == 2
+    cfg = O.sector_configs(**model.sector_inputs)
+    assert cfg.shape[0] == int(golden_wide[f"{name}/dim"])
+    assert hashlib.sha256(np.ascontiguousarray(cfg).tobytes()).hexdigest() == str(golden_wide[f"{name}/configs_sha"])
+    rows = golden_wide[f"{name}/sample_rows"]
+    assert np.array_equal(cfg[rows], golden_wide[f"{name}/sample_configs"])
+    assert np.array_equal(O.config_to_index(cfg[rows], cfg, model.loc_dims), rows)
+    if name.endswith("pbc_s1"):
+        H = O.assemble(model.hamiltonian_blocks(g), cfg, model.loc_dims)
+        nnz, pat, ws = _digest(H)
+        assert nnz == int(golden_wide[f"{name}/H_nnz"])
+        assert pat == str(golden_wide[f"{name}/H_pattern_sha"])
+        ref = complex(golden_wide[f"{name}/H_wsum"])
+        assert abs(ws - ref) <= 1e-10 * abs(ref)
+        e_ref = golden_wide[f"{name}/energies"]
+        w, _ = O.lowest_eigs(H, len(e_ref))
+        assert np.allclose(w / model.n_sites, e_ref, atol=1e-10, rtol=0)
