@@ -196,6 +196,10 @@ class QMB_hamiltonian:
         self.mat = assemble_blocks(self.sector, self.blocks, phase_weights=self.phase_weights,
                                    force_complex=force_complex, extra_diag=ed if ed != 0 else None)
         self.Ham_type = "gpu"
+        # spectra of an earlier matrix no longer apply
+        self._evecs = None
+        self._evals_total = None
+        self._thermal = None
         logger.info(f"SPARSITY: {(self.mat.nnz + self.shape[0]) / self.shape[0] ** 2:.3e}")
 
     def to_scipy(self):
@@ -301,18 +305,7 @@ class QMB_hamiltonian:
         convert_hamiltonian("dense"), qmb_hamiltonian.py:227-258, 300-302):
         the matrix is densified on the device (``edg_csr_to_dense``) and
         diagonalised by the library Hermitian solver."""
-        from .._lib import check, lib, ptr, stream_handle
-
-        n = self.shape[0]
-        if n > self.DENSE_MAX:
-            raise ValueError(f"dense diagonalisation limited to {self.DENSE_MAX} states, the sector has {n}")
-        mat = self.mat
-        dt = torch.complex128 if mat.is_complex else torch.float64
-        dense = torch.empty((n, n), dtype=dt, device=self.sector.device)
-        flag = torch.empty(1, dtype=torch.int32, device=self.sector.device)
-        check(lib.edg_csr_to_dense(2 if mat.is_complex else 0, n, ptr(mat.rowptr), ptr(mat.cols) if mat.nnz else None,
-                                   ptr(mat.vals) if mat.nnz else None, ptr(mat.diag), ptr(dense), ptr(flag),
-                                   stream_handle()), "edg_csr_to_dense")
+        dense = self._densify()
         w, v = torch.linalg.eigh(dense)
         del dense
         ph = self._row_phase()
@@ -331,8 +324,83 @@ class QMB_hamiltonian:
         self.GSpsi = self.Npsi[0]
         self.Ham_type = "dense"
 
+    def _densify(self, original_basis=False):
+        """The sector matrix as a dense device array (``edg_csr_to_dense``), in
+        the assembled (possibly real) form, or with the real form's phases put
+        back: H = D H' D^dagger, the reference's basis."""
+        from .._lib import check, lib, ptr, stream_handle
+
+        n = self.shape[0]
+        if n > self.DENSE_MAX:
+            raise ValueError(f"dense matrices limited to {self.DENSE_MAX} states, the sector has {n}")
+        if self.mat is None:
+            self.build()
+        mat = self.mat
+        dt = torch.complex128 if mat.is_complex else torch.float64
+        dense = torch.empty((n, n), dtype=dt, device=self.sector.device)
+        flag = torch.empty(1, dtype=torch.int32, device=self.sector.device)
+        check(lib.edg_csr_to_dense(2 if mat.is_complex else 0, n, ptr(mat.rowptr), ptr(mat.cols) if mat.nnz else None,
+                                   ptr(mat.vals) if mat.nnz else None, ptr(mat.diag), ptr(dense), ptr(flag),
+                                   stream_handle()), "edg_csr_to_dense")
+        if original_basis:
+            ph = self._row_phase()
+            if ph is not None:
+                dense = ph[:, None] * dense.to(torch.complex128) * ph.conj()[None, :]
+        return dense
+
     def _full(self):
         return getattr(self, "_evecs", None) is not None and self.n_eigs == self.shape[0]
+
+    def _thermal_system(self, vectors=False, square=False):
+        """Eigen-system behind the traces of exp(-beta H) that the reference
+        takes of the sparse matrix exponential when fewer than all eigenpairs
+        were computed (qmb_hamiltonian.py:446-452, 486-489, 505-508, 545-551;
+        quantum_model.py:904-938): Tr f(H) exp(-beta H) is a sum over the
+        eigenvalues.  Returns (total eigenvalues (host), eigenvectors in the
+        reference basis (device) or None, per-eigenstate weights
+        v^dagger (H o H) v of the elementwise-squared matrix or None).
+
+        Uses the stored spectrum when every eigenvalue is there (the dense
+        format); otherwise the densified matrix is diagonalised once on the
+        device by the library Hermitian solver and kept until the matrix
+        changes."""
+        n = self.shape[0]
+        c = getattr(self, "_thermal", None)
+        if c is None or c["mat"] is not self.mat:
+            c = {"mat": self.mat, "w": None, "v": None, "sq": None}
+            self._thermal = c
+        ev = getattr(self, "_evals_total", None)
+        if c["w"] is None and getattr(self, "_evecs", None) is not None and ev is not None and len(ev) == n:
+            c["w"], c["v"] = np.asarray(ev), self._evecs
+        need_v = vectors or square
+        if c["w"] is None or (need_v and c["v"] is None):
+            dense = self._densify(original_basis=True)
+            if need_v:
+                w, v = torch.linalg.eigh(dense)
+                c["v"] = v
+            else:
+                w = torch.linalg.eigvalsh(dense)
+            c["w"] = w.cpu().numpy()
+            del dense
+        if square and c["sq"] is None:
+            h = self._densify(original_basis=True)
+            v = c["v"]
+            if h.is_complex() or v.is_complex():
+                h, v = h.to(torch.complex128), v.to(torch.complex128)
+            g = (h * h) @ v
+            c["sq"] = torch.sum(v.conj() * g, dim=0).real.cpu().numpy()
+            del h, g
+        return c["w"], c["v"], c["sq"]
+
+    def _h2_weights(self):
+        """Per-eigenstate weights of the Tr(H^2 exp(-beta H)) term: lambda^2
+        for the sparse formats (the reference's csc matrix power), and
+        v^dagger (H o H) v for the dense format (its dense array is squared
+        elementwise, qmb_hamiltonian.py:505-508)."""
+        if self.Ham_type == "dense":
+            return self._thermal_system(square=True)[2]
+        w = self._thermal_system()[0]
+        return w * w
 
     def energy_of(self, state):
         """<state| H |state> (total energy) for a vector in the original basis."""
@@ -347,11 +415,15 @@ class QMB_hamiltonian:
         return torch.complex(self.mat.matvec(x.real.contiguous()), self.mat.matvec(x.imag.contiguous()))
 
     def partition_function(self, beta):
-        """QMB_hamiltonian.partition_function (qmb_hamiltonian.py:428-452), on
-        the stored energy densities of the full spectrum."""
-        if not self._full():
-            raise NotImplementedError("the partition function needs the full spectrum (diagonalize 'full')")
-        Z = float(np.sum(np.exp(-beta * self.Nenergies)))
+        """QMB_hamiltonian.partition_function (qmb_hamiltonian.py:428-452):
+        with the full spectrum, the sum over the stored energy densities;
+        otherwise Tr exp(-beta H) of the sector matrix (the reference's sparse
+        expm branch), summed over its eigenvalues."""
+        if self._full():
+            Z = float(np.sum(np.exp(-beta * self.Nenergies)))
+        else:
+            w = self._thermal_system()[0]
+            Z = float(np.sum(np.exp(-beta * w)))
         if Z <= 0:
             raise ValueError(f"Z must be positive, not {Z}.")
         return Z
@@ -360,30 +432,43 @@ class QMB_hamiltonian:
         return -1 / beta * np.log(self.partition_function(beta))
 
     def thermal_average(self, beta):
+        """Energy density average (full spectrum) or Tr(H exp(-beta H)) / Z
+        (qmb_hamiltonian.py:471-489)."""
         Z = self.partition_function(beta)
-        return float(self.Nenergies.dot(np.exp(-beta * self.Nenergies)) / Z)
+        if self._full():
+            return float(self.Nenergies.dot(np.exp(-beta * self.Nenergies)) / Z)
+        w = self._thermal_system()[0]
+        return float(w.dot(np.exp(-beta * w)) / Z)
 
     def F_prime(self, beta):
+        """-<H^2> - <H>^2 of qmb_hamiltonian.py:491-508, with the same two
+        branches as partition_function."""
         Z = self.partition_function(beta)
-        exph2 = np.square(self.Nenergies).dot(np.exp(-beta * self.Nenergies)) / Z
+        if self._full():
+            exph2 = np.square(self.Nenergies).dot(np.exp(-beta * self.Nenergies)) / Z
+        else:
+            w = self._thermal_system()[0]
+            exph2 = self._h2_weights().dot(np.exp(-beta * w)) / Z
         return float(-exph2 - self.thermal_average(beta) ** 2)
 
     def get_beta(self, state, threshold=1e-10, max_iter=1000):
-        """Newton solve of QMB_hamiltonian.get_beta (qmb_hamiltonian.py:510-564),
-        full-spectrum branch: thermal average of the energy densities against
-        the state's total energy <state|H|state>."""
-        if not self._full():
-            raise NotImplementedError("get_beta needs the full spectrum (diagonalize 'full')")
+        """Newton solve of QMB_hamiltonian.get_beta (qmb_hamiltonian.py:510-564)
+        against the state's total energy <state|H|state>: with the full
+        spectrum, on the energy densities (as the reference); otherwise on
+        the traces of exp(-beta H) of the sector matrix."""
         e_state = self.energy_of(state)
+        if self._full():
+            E, H2 = self.Nenergies, np.square(self.Nenergies)
+        else:
+            E, H2 = self._thermal_system()[0], self._h2_weights()
         beta, accuracy, it = 1e-7, 1.0, 0
-        E = self.Nenergies
         while accuracy > threshold and it < max_iter:
             it += 1
             wgt = np.exp(-beta * E)
             Z = np.sum(wgt)
             Em = E.dot(wgt) / Z
             F = Em - e_state
-            Fp = -np.square(E).dot(wgt) / Z - Em ** 2
+            Fp = -H2.dot(wgt) / Z - Em ** 2
             prev = beta
             beta = beta - F / Fp
             accuracy = abs(beta - prev)

@@ -495,24 +495,35 @@ class QuantumModel:
         return fid
 
     def compute_expH(self, beta):
-        """exp(-beta H) (dense, host) from the full spectrum."""
-        v, e = self._full_spectrum()
+        """exp(-beta H) (dense, host; quantum_model.py:904-906), from the
+        eigen-system of the sector matrix (the stored full spectrum, or one
+        dense eigen-solve on the device)."""
+        v, e = self._thermal_spectrum()
         w = torch.exp(-beta * torch.from_numpy(e).to(v.device))
         return ((v * w[None, :]) @ v.conj().T).cpu().numpy()
 
     def get_thermal_beta(self, state, threshold):
         return self.H.get_beta(state, threshold)
 
+    def _thermal_spectrum(self):
+        """(eigenvectors in the reference basis, total eigenvalues) for
+        traces of exp(-beta H), whether or not all eigenpairs were asked for."""
+        if self.H._full():
+            return self.H._evecs, self.H._evals_total
+        w, v, _ = self.H._thermal_system(vectors=True)
+        return v, w
+
     def _full_spectrum(self):
         if not self.H._full():
             raise ValueError(f"Need all H eigvals {self.H.shape[0]}, not only {getattr(self, 'n_eigs', None)}")
         return self.H._evecs, self.H._evals_total
 
-    def _eig_site_obs(self, name):
+    def _eig_site_obs(self, name, v=None):
         """(n_eigs, n_sites) array of <E_i| op_s |E_i> for a diagonal local
         operator, for all eigenstates at once: |V|^2 (rows x states)
         contracted with the per-row site values."""
-        v, _ = self._full_spectrum()
+        if v is None:
+            v, _ = self._full_spectrum()
         op = self.ops[name]
         diag = torch.from_numpy(np.real(np.array([np.diagonal(op[s]) for s in range(op.shape[0])]))
                                 .astype(np.float64)).to(v.device)
@@ -532,10 +543,12 @@ class QuantumModel:
 
     def canonical_avg(self, local_obs, beta):
         """Tr(O exp(-beta H)) / (Z n_sites), O = sum_s op_s
-        (edlgt/models/quantum_model.py:911-938), from the full spectrum."""
-        _, e = self._full_spectrum()
+        (edlgt/models/quantum_model.py:911-938), from the eigen-system of the
+        sector matrix (the stored full spectrum, or one dense eigen-solve on
+        the device)."""
+        v, e = self._thermal_spectrum()
         w = np.exp(-beta * (e - e.min()))
-        obs = self._eig_site_obs(local_obs).sum(axis=1)
+        obs = self._eig_site_obs(local_obs, v).sum(axis=1)
         return float(np.dot(w, obs) / (np.sum(w) * self.n_sites))
 
     def microcanonical_avg(self, local_obs_list, state, special_norms=None, staggered_avgs=None):

@@ -128,3 +128,10 @@ def golden_wide():
     import numpy as np
 
     return np.load(os.path.join(GOLDEN, "wide_cases.npz"))
+
+
+@pytest.fixture(scope="session")
+def golden_thermal():
+    import numpy as np
+
+    return np.load(os.path.join(GOLDEN, "thermal_cases.npz"))

@@ -6,7 +6,7 @@ and numba/scipy/sympy:
     python tests/golden/make_golden.py [group ...]
 
 Groups: small, pins, dynamics, big, twobody, entropy, momentum, full,
-nbody, overlap, state, local, integrated, string, generic, wide.  Output: .npz files next to
+nbody, overlap, state, local, integrated, string, generic, wide, thermal.  Output: .npz files next to
 this script.  Nothing here is imported by the library or by the GPU tests;
 the tests only read the .npz files.
 
@@ -679,6 +679,49 @@ def gen_generic_su2():
     np.savez_compressed(os.path.join(HERE, "generic_su2_cases.npz"), **out)
 
 
+def gen_thermal():
+    """Thermal functions without the full spectrum: the reference's expm
+    branches (edlgt/modeling/qmb_hamiltonian.py:446-452, 486-489, 505-508,
+    545-551; edlgt/models/quantum_model.py:904-938) after a two-eigenvalue
+    diagonalisation of SU(2) L=6 PBC (g=1, m=5, dim 282), in the "sparse"
+    format (Tr(H^2 e^-bH) by matrix power) and the "dense" format (the
+    elementwise square of the dense array)."""
+    from edlgt.modeling import LocalTerm
+
+    out = {}
+    kw = SU2_CASES["su2_1d_L6_pbc"][0]
+    for fmt in ("sparse", "dense"):
+        model = su2_model(kw)
+        model.build_Hamiltonian(1.0, 5.0)
+        model.diagonalize_Hamiltonian(2, fmt)
+        p = f"{fmt}/"
+        for beta in (0.3, 0.7):
+            q = f"{p}b{beta}/"
+            out[q + "Z"] = np.float64(model.H.partition_function(beta))
+            out[q + "F"] = np.float64(model.H.free_energy(beta))
+            out[q + "E_thermal"] = np.float64(model.H.thermal_average(beta))
+            out[q + "F_prime"] = np.float64(model.H.F_prime(beta))
+            # canonical_avg's formula with the reference's own pieces (its
+            # csc_matrix call on the LocalTerm triplets is rejected by scipy)
+            rows, cols, vals = LocalTerm(model.ops["T2_px"], "T2_px", **model.def_params).get_Hamiltonian(1)
+            n = len(model.sector_configs)
+            op = coo_matrix((vals, (rows, cols)), shape=(n, n)).tocsc()
+            expm_matrix = model.compute_expH(beta)
+            Z = np.real(expm_matrix.trace())
+            out[q + "canonical_T2_px"] = np.float64(np.real(op.dot(expm_matrix).trace()) / (Z * model.n_sites))
+        out[p + "energies"] = np.asarray(model.H.Nenergies)
+        if fmt == "sparse":
+            # in the dense format the reference's Newton iteration (with the
+            # elementwise square) runs away and exhausts the host memory, so
+            # the thermal beta is pinned in the sparse format only
+            config = model.overlap_QMB_state("V")
+            state = model.get_qmb_state_from_configs([config])
+            out[p + "config"] = np.asarray(config, dtype=np.int64)
+            out[p + "beta_state"] = np.float64(model.get_thermal_beta(state, 1e-10))
+        print("thermal", fmt, out[p + "b0.7/Z"], out[p + "b0.7/F_prime"], flush=True)
+    np.savez_compressed(os.path.join(HERE, "thermal_cases.npz"), **out)
+
+
 WIDE_CASES = {
     # name: (kwargs, g); pure gauge lattices whose key space exceeds 63 bits
     "qed2d_4x4_pure_pbc_s1": (dict(spin=1, pure_theory=True, lvals=[4, 4], has_obc=[False, False]), 1.1),
@@ -716,7 +759,9 @@ def gen_wide():
 
 if __name__ == "__main__":
     groups = sys.argv[1:] or ["small", "pins", "dynamics", "big", "twobody", "entropy", "momentum", "full", "nbody",
-                             "overlap", "state", "local", "integrated", "string", "generic", "wide"]
+                             "overlap", "state", "local", "integrated", "string", "generic", "wide", "thermal"]
+    if "thermal" in groups:
+        gen_thermal()
     if "wide" in groups:
         gen_wide()
     if "generic" in groups:

@@ -73,10 +73,11 @@ def test_exact_time_evolution(full_model, golden_full):
 def test_dense_limit_and_partial_spectrum(dev):
     """An integer n_eigs with the dense format keeps every energy and the
     first n_eigs states (the reference's dense branch); thermal functions
-    then refuse to run on a partial spectrum."""
+    then take the reference's expm branch: Tr exp(-beta H) over the total
+    energies, not the energy densities."""
     model, g, mass = build("qed1d_L8_obc", device=dev)
     model.build_Hamiltonian(g, mass)
     model.diagonalize_Hamiltonian(3, "dense")
     assert len(model.H.Nenergies) == model.H.shape[0] and len(model.H.Npsi) == 3
-    with pytest.raises(NotImplementedError):
-        model.H.partition_function(1.0)
+    e_tot = np.asarray(model.H.Nenergies) * model.n_sites
+    assert np.isclose(model.H.partition_function(1.0), np.sum(np.exp(-e_tot)), rtol=1e-12, atol=0)

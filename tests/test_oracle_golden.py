@@ -354,3 +354,26 @@ def test_wide_sector_matches_reference(name, golden_wide):
         e_ref = golden_wide[f"{name}/energies"]
         w, _ = O.lowest_eigs(H, len(e_ref))
         assert np.allclose(w / model.n_sites, e_ref, atol=1e-10, rtol=0)
+
+
+def test_thermal_expm_branches_match_reference(golden_thermal):
+    """The traces the reference takes of expm(-beta H) after a partial
+    diagonalisation, restated on the oracle's matrix of SU(2) L=6 PBC:
+    Tr(H^2 e^-bH) by matrix power in the sparse format and by the elementwise
+    square in the dense format (qmb_hamiltonian.py:446-452, 486-489,
+    505-508)."""
+    from scipy.linalg import expm
+
+    model, _, _ = build("su2_1d_L6_pbc")
+    cfg = O.sector_configs(**model.sector_inputs)
+    H = O.assemble(model.hamiltonian_blocks(1.0, 5.0), cfg, model.loc_dims).toarray()
+    for beta in (0.3, 0.7):
+        M = expm(-beta * H)
+        Z = np.real(np.trace(M))
+        E = np.real(np.trace(H @ M)) / Z
+        for fmt, H2 in (("sparse", H @ H), ("dense", H * H)):
+            q = f"{fmt}/b{beta}/"
+            assert np.isclose(Z, golden_thermal[q + "Z"], rtol=1e-10, atol=0)
+            assert np.isclose(E, golden_thermal[q + "E_thermal"], rtol=1e-10, atol=0)
+            fp = -np.real(np.trace(H2 @ M)) / Z - E**2
+            assert np.isclose(fp, golden_thermal[q + "F_prime"], rtol=1e-9, atol=0)
