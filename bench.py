@@ -411,9 +411,11 @@ def run_edgpu(args, world, rank, local):
         t0 = time.perf_counter()
         m2 = SU2_Model(**model_kwargs(), device=dev)
         dg = []
+        tables_bytes = 0
         for g in SWEEP:
             m2.build_Hamiltonian(g, MASS)
             dg.append(m2.H.mat.diag.clone())
+            tables_bytes += sum(t.numel() * t.element_size() for t in m2.H.mat._keep)
         r64e, _ = lanczos_mixed(m2.H.mat, diags=dg)
         gs_host = torch.empty(r64e.evecs[0].shape, dtype=r64e.evecs[0].dtype, pin_memory=True)
         gs_host.copy_(r64e.evecs[0])  # ground states to pinned host memory
@@ -428,7 +430,7 @@ def run_edgpu(args, world, rank, local):
         spec_bytes = sum(np.asarray(getattr(spec, a)).nbytes for a in (
             "site_allowed", "glob_val", "glob_target", "glob_rem_min", "glob_rem_max", "link_val", "link_target",
             "pair_start", "pair_s0", "pair_s1", "pair_dir"))
-        h2d = spec_bytes + len(SWEEP) * sum(t.numel() * t.element_size() for t in m2.H.mat._keep)
+        h2d = spec_bytes + tables_bytes
         del m2
     e2e = 3 * world / (max_over_ranks(float(np.mean(e2e_ms)), world, dev) * 1e-3)
 

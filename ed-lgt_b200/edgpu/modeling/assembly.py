@@ -19,6 +19,8 @@ eigenvectors map back by ``psi = D psi'``.
 
 from __future__ import annotations
 
+import hashlib
+
 import numpy as np
 import torch
 
@@ -120,22 +122,29 @@ def _phase_vec(weights_row):
     return np.power(1j, np.asarray(weights_row, dtype=np.int64) % 4)
 
 
-def assemble_blocks(sector, blocks, phase_weights=None, force_complex=False, extra_diag=None):
-    """Assemble the canonical matrix of ``sum(blocks)`` in ``sector``.
-
-    ``extra_diag``: optional constant added to every diagonal element (identity
-    terms).  Returns a :class:`DeviceMatrix`.
-    """
-    n_sites = sector.n_sites
-    loc_dims = sector.loc_dims
-    dmax = None
+def _offdiag_signature(blocks, phase_weights, force_complex, dmax):
+    """Content hash of everything the off-diagonal part of the matrix depends
+    on: the off-diagonal blocks' operators, instances, strengths and h.c.
+    flags, the real form's phase weights and the form request."""
+    h = hashlib.sha256(repr((bool(force_complex), int(dmax))).encode())
+    if phase_weights is not None:
+        h.update(np.ascontiguousarray(np.asarray(phase_weights, dtype=np.int64)).tobytes())
     for b in blocks:
-        dmax = b.ops[0].shape[-1] if dmax is None else dmax
-    if dmax is None:
-        dmax = int(loc_dims.max())
-    dev = sector.device
+        if b.diagonal:
+            continue
+        h.update(repr((b.strength, b.add_dagger, len(b.ops))).encode())
+        h.update(np.ascontiguousarray(b.sites).tobytes())
+        for o in b.ops:
+            o = np.ascontiguousarray(o)
+            h.update(repr((str(o.dtype), o.shape)).encode())
+            h.update(o.tobytes())
+    return h.hexdigest()
 
-    # ---- off-diagonal instances: tables and records (complex, untransformed) ----
+
+def _offdiag_tables(blocks, phase_weights, force_complex, dmax):
+    """Local transition tables and instance records of the off-diagonal
+    blocks, and whether they admit the real form (every gauge-transformed
+    table has one common phase and every instance's total phase is real)."""
     raw_tables = []  # list of (d x d) complex matrices
     table_site = []
     table_index = {}
@@ -160,23 +169,9 @@ def assemble_blocks(sector, blocks, phase_weights=None, force_complex=False, ext
                     raise ValueError("a term instance acts twice on the same site")
                 coef = np.conj(b.strength) if dag else b.strength
                 terms.append((tuple(int(s) for s in inst), tuple(tabs), complex(coef)))
-    # diagonal terms
-    dterms = []  # (site, diag vector, coef)
-    for b in blocks:
-        if not b.diagonal:
-            continue
-        for inst in b.sites:
-            s = int(inst[0])
-            dterms.append((s, np.diagonal(np.asarray(b.ops[0][s], dtype=np.complex128)).copy(), complex(b.strength)))
-
-    # ---- real form (gauge transform + per-table phase extraction) ----
-    use_real = False
-    tables_real = None
-    coefs_real = None
+    real_ok, tables_real, coefs_real = False, None, None
     if not force_complex:
-        tabs_t = []
-        ok = True
-        phases = []
+        tabs_t, phases, ok = [], [], True
         for t, m in enumerate(raw_tables):
             if phase_weights is not None:
                 phi = _phase_vec(phase_weights[table_site[t]])
@@ -198,22 +193,18 @@ def assemble_blocks(sector, blocks, phase_weights=None, force_complex=False, ext
                     break
                 cr.append(z.real)
         if ok:
-            for _, dvec, coef in dterms:
-                if np.any(np.abs(dvec.imag) > 1e-12) or abs(coef.imag) > 1e-12:
-                    ok = False
-                    break
-        if ok:
-            use_real = True
-            tables_real = tabs_t
-            coefs_real = cr
-    is_complex = not use_real
+            real_ok, tables_real, coefs_real = True, tabs_t, cr
+    return raw_tables, terms, real_ok, tables_real, coefs_real
+
+
+def _table_arrays(raw_tables, terms, dmax, is_complex, tables_real, coefs_real):
     nt = max(len(raw_tables), 1)
     t_count = np.zeros((nt, dmax), dtype=np.int32)
     t_ket = np.zeros((nt, dmax, dmax), dtype=np.uint8)
     t_amp = np.zeros((nt, dmax, dmax, 2 if is_complex else 1), dtype=np.float64)
     for t, m0 in enumerate(raw_tables):
         mags = np.abs(m0)
-        m = tables_real[t] if use_real else m0
+        m = m0 if is_complex else tables_real[t]
         for bra in range(dmax):
             kets = np.nonzero(mags[bra] > OP_TOL)[0]
             t_count[t, bra] = len(kets)
@@ -238,44 +229,134 @@ def assemble_blocks(sector, blocks, phase_weights=None, force_complex=False, ext
             term_coef[k] = (coef.real, coef.imag)
         else:
             term_coef[k, 0] = coefs_real[k]
-    n_d = len(dterms)
-    dterm_site = np.zeros(max(n_d, 1), dtype=np.int32)
-    dterm_diag = np.zeros((max(n_d, 1), dmax, 2 if is_complex else 1), dtype=np.float64)
-    dterm_coef = np.zeros((max(n_d, 1), 2 if is_complex else 1), dtype=np.float64)
-    for k, (s, dvec, coef) in enumerate(dterms):
-        dterm_site[k] = s
-        if is_complex:
-            dterm_diag[k, : len(dvec), 0] = dvec.real
-            dterm_diag[k, : len(dvec), 1] = dvec.imag
-            dterm_coef[k] = (coef.real, coef.imag)
-        else:
-            dterm_diag[k, : len(dvec), 0] = dvec.real
-            dterm_coef[k, 0] = coef.real
+    return [t_count, t_ket, t_amp, term_nops, term_site, term_table, term_coef]
+
+
+def assemble_blocks(sector, blocks, phase_weights=None, force_complex=False, extra_diag=None):
+    """Assemble the canonical matrix of ``sum(blocks)`` in ``sector``.
+
+    ``extra_diag``: optional constant added to every diagonal element (identity
+    terms).  Returns a :class:`DeviceMatrix`.
+
+    The off-diagonal part (CSR plus the diagonal contributions of instances
+    that map a state to itself) depends only on the off-diagonal blocks, the
+    phase weights and the form; the sector keeps the last one built, and a
+    build whose off-diagonal blocks hash to the same content (a coupling
+    sweep that changes diagonal terms only) reuses it and computes only the
+    diagonal.
+    """
+    import ctypes
+
+    loc_dims = sector.loc_dims
+    dmax = None
+    for b in blocks:
+        dmax = b.ops[0].shape[-1] if dmax is None else dmax
+    if dmax is None:
+        dmax = int(loc_dims.max())
+    dev = sector.device
+    st = stream_handle()
+    n = len(sector)
+
+    # diagonal terms: (site, diag vector, coef)
+    dterms = []
+    for b in blocks:
+        if not b.diagonal:
+            continue
+        for inst in b.sites:
+            s = int(inst[0])
+            dterms.append((s, np.diagonal(np.asarray(b.ops[0][s], dtype=np.complex128)).copy(), complex(b.strength)))
+    dterms_real = all(not np.any(np.abs(dvec.imag) > 1e-12) and abs(coef.imag) <= 1e-12 for _, dvec, coef in dterms)
 
     def up(a):
         return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
 
-    keep = [up(t_count), up(t_ket), up(t_amp), up(term_nops), up(term_site), up(term_table), up(term_coef),
-            up(dterm_site), up(dterm_diag), up(dterm_coef)]
+    # ---- off-diagonal part: reused or built ----
+    sig = _offdiag_signature(blocks, phase_weights, force_complex, dmax)
+    off = getattr(sector, "_offdiag_cache", None)
+    reused = off is not None and off["sig"] == sig and off["use_real"] == (off["real_ok"] and dterms_real)
+    keep = []
+    if not reused:
+        raw_tables, terms, real_ok, tables_real, coefs_real = _offdiag_tables(blocks, phase_weights, force_complex,
+                                                                              dmax)
+        use_real = real_ok and dterms_real
+        arrays = _table_arrays(raw_tables, terms, dmax, not use_real, tables_real, coefs_real)
+        keep = [up(a) for a in arrays]
+        off = _assemble_offdiag(sector, dev, st, n, 1 if use_real else 2, dmax, not use_real, len(terms), keep)
+        off.update(sig=sig, real_ok=real_ok, use_real=use_real)
+        sector._offdiag_cache = off
+    is_complex = not off["use_real"]
+    w = 2 if is_complex else 1
+
+    # ---- diagonal terms: one pass without off-diagonal instances ----
+    diag = off["diag"].clone()
+    present = off["present"].clone()
+    n_d = len(dterms)
+    if n_d > 0 and n > 0:
+        dterm_site = np.zeros(n_d, dtype=np.int32)
+        dterm_diag = np.zeros((n_d, dmax, w), dtype=np.float64)
+        dterm_coef = np.zeros((n_d, w), dtype=np.float64)
+        for k, (s, dvec, coef) in enumerate(dterms):
+            dterm_site[k] = s
+            dterm_diag[k, : len(dvec), 0] = dvec.real
+            dterm_coef[k, 0] = coef.real
+            if is_complex:
+                dterm_diag[k, : len(dvec), 1] = dvec.imag
+                dterm_coef[k, 1] = coef.imag
+        dk = [up(dterm_site), up(dterm_diag), up(dterm_coef)]
+        keep += dk
+        a = _assembly_struct(sector, dmax, is_complex)
+        a.n_terms = 0
+        a.n_dterms = n_d
+        a.dterm_site, a.dterm_diag, a.dterm_coef = ptr(dk[0]), ptr(dk[1]), ptr(dk[2])
+        zeros = torch.zeros(n + 1, dtype=torch.int64, device=dev)
+        one_i = torch.empty(1, dtype=torch.int32, device=dev)
+        one_d = torch.empty(w, dtype=torch.float64, device=dev)
+        row_nnz = torch.empty(n, dtype=torch.int64, device=dev)
+        d_diag = torch.empty(n * w, dtype=torch.float64, device=dev)
+        d_present = torch.empty(n, dtype=torch.uint8, device=dev)
+        err = torch.zeros(1, dtype=torch.int32, device=dev)
+        check(lib.edg_assemble_fill(ctypes.byref(a), ptr(zeros), ptr(one_i), ptr(one_d), ptr(row_nnz), ptr(d_diag),
+                                    ptr(d_present), ptr(err), st), "edg_assemble_fill")
+        diag += d_diag
+        present |= d_present
+    if extra_diag is not None and extra_diag != 0:
+        if is_complex:
+            diag.view(-1, 2)[:, 0] += float(np.real(extra_diag))
+            diag.view(-1, 2)[:, 1] += float(np.imag(extra_diag))
+        else:
+            diag += float(np.real(extra_diag))
+        present.fill_(1)
+    mat = DeviceMatrix(n, off["rowptr"], off["cols"], off["vals"], diag, present, is_complex,
+                       phase_weights if (not is_complex and phase_weights is not None) else None)
+    mat._keep = keep  # device tables uploaded by this build
+    mat.raw_entries = off["raw_entries"]  # generated entries before the per-row merge
+    mat.offdiag_reused = reused  # off-diagonal part shared with an earlier build
+    return mat
+
+
+def _assembly_struct(sector, dmax, is_complex):
     a = _lib.Assembly()
-    a.n_sites = n_sites
+    a.n_sites = sector.n_sites
     a.dmax = dmax
-    for s in range(n_sites):
-        a.loc_dims[s] = int(loc_dims[s])
+    for s in range(sector.n_sites):
+        a.loc_dims[s] = int(sector.loc_dims[s])
         a.strides[s] = int(sector.strides[s])
     a.sector = sector.lookup_table()
     a.complex_values = 1 if is_complex else 0
-    a.t_count, a.t_ket, a.t_amp = ptr(keep[0]), ptr(keep[1]), ptr(keep[2])
-    a.n_terms = n_terms
-    a.term_nops, a.term_site, a.term_table, a.term_coef = ptr(keep[3]), ptr(keep[4]), ptr(keep[5]), ptr(keep[6])
-    a.n_dterms = n_d
-    a.dterm_site, a.dterm_diag, a.dterm_coef = ptr(keep[7]), ptr(keep[8]), ptr(keep[9])
+    return a
 
+
+def _assemble_offdiag(sector, dev, st, n, w, dmax, is_complex, n_terms, tabs):
+    """Off-diagonal instances only: count, scan, fill (with per-row merge)
+    and compaction; returns the CSR, the diagonal contributions of
+    instances whose ket is the bra, and their presence flags."""
     import ctypes
 
-    st = stream_handle()
-    n = len(sector)
-    w = 2 if is_complex else 1
+    a = _assembly_struct(sector, dmax, is_complex)
+    a.t_count, a.t_ket, a.t_amp = ptr(tabs[0]), ptr(tabs[1]), ptr(tabs[2])
+    a.n_terms = n_terms
+    a.term_nops, a.term_site, a.term_table, a.term_coef = ptr(tabs[3]), ptr(tabs[4]), ptr(tabs[5]), ptr(tabs[6])
+    a.n_dterms = 0
     bound = torch.empty(max(n, 1), dtype=torch.int64, device=dev)
     check(lib.edg_assemble_count(ctypes.byref(a), ptr(bound), st), "edg_assemble_count")
     offsets = torch.empty(n + 1, dtype=torch.int64, device=dev)
@@ -301,16 +382,5 @@ def assemble_blocks(sector, blocks, phase_weights=None, force_complex=False, ext
     check(lib.edg_assemble_compact(n, 1 if is_complex else 0, ptr(offsets), ptr(tmp_cols), ptr(tmp_vals),
                                    ptr(rowptr), ptr(cols), ptr(vals), st), "edg_assemble_compact")
     del tmp_cols, tmp_vals
-    diag = diag[: n * w]
-    if extra_diag is not None and extra_diag != 0:
-        if is_complex:
-            diag.view(-1, 2)[:, 0] += float(np.real(extra_diag))
-            diag.view(-1, 2)[:, 1] += float(np.imag(extra_diag))
-        else:
-            diag += float(np.real(extra_diag))
-        present.fill_(1)
-    mat = DeviceMatrix(n, rowptr, cols[:nnz], vals[: nnz * w], diag, present[:n], is_complex,
-                       phase_weights if (use_real and phase_weights is not None) else None)
-    mat._keep = keep
-    mat.raw_entries = total  # generated entries before the per-row merge
-    return mat
+    return {"rowptr": rowptr, "cols": cols[:nnz], "vals": vals[: nnz * w], "diag": diag[: n * w],
+            "present": present[:n], "raw_entries": total, "keep": tabs}
