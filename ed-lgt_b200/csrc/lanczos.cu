@@ -14,7 +14,9 @@
 //   r = sqrt(alpha_u - s.s), c = (omega - s.z) / r
 //   alpha_j = (omega - 2 z.s + s.T s) / r^2, beta_j = (z_{j-1} - (T s)_{j-1}) / r
 //   one read of V[0..j): V[j] = q_j = (u_j - V s) / r ; w -= V z + q_j c
-//   V[j+1] = w / |w| (the next candidate), beta_{j+1} = |w| / r (refined at j+1)
+//   V[j+1] = w / r (the next candidate, written by the update pass; the
+//   step's formulas do not depend on a candidate's scale), beta_{j+1} = |w| / r
+//   (refined at j+1)
 // T is the j x j tridiagonal block of the previous steps.
 // Every check_every steps the k lowest Ritz pairs of the tridiagonal matrix are
 // computed on the device (multisection + inverse iteration) and the residual
@@ -49,7 +51,7 @@ struct DevState {
   int m_conv[4];   // per problem: dimension at convergence, 0 while running
   int m_use[4];    // per problem: dimension of its last tridiagonal solve
   int ticket;      // last-CTA counter of the check kernel
-  int pad;
+  int win;         // reorthogonalisation window (0: all of V[0..j))
   double prev_worst;
   double worst[4];       // worst relative residual of an unconverged problem
   double resid[4][kMaxK];
@@ -174,25 +176,10 @@ __global__ void scale_store_k(const double* __restrict__ w, int64_t n, int64_t n
   }
 }
 
-// The next candidate: V[j] = w / |w| (j = the state's step, advanced by the
-// update pass) and the interleaved matvec input X; nothing once done.
-template <typename T, int NV>
-__global__ void scale_next_k(const double* __restrict__ w, int64_t n, int64_t n_pad, const double* __restrict__ wnorm,
-                             T* __restrict__ V, int64_t stride_i, T* __restrict__ X, int xs,
-                             const DevState* __restrict__ st) {
-  if (st->done) return;
-  T* plane = V + (int64_t)st->j * stride_i;
-  double inv[NV];
-#pragma unroll
-  for (int v = 0; v < NV; ++v) inv[v] = wnorm[v] > 0.0 ? 1.0 / wnorm[v] : 0.0;
-  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n_pad; r += (int64_t)gridDim.x * blockDim.x) {
-#pragma unroll
-    for (int v = 0; v < NV; ++v) {
-      const T x = (T)(w[(int64_t)v * n_pad + r] * inv[v]);
-      plane[(int64_t)v * n_pad + r] = x;
-      if (r < n) X[r * xs + v] = x;
-    }
-  }
+// First Krylov vector of the reorthogonalisation window at step j.
+__device__ __forceinline__ int window_start(const DevState* st, int j) {
+  const int w = st->win;
+  return (w > 0 && j > w) ? j - w : 0;
 }
 
 // Sums of 16 per-lane values over a warp, scattered: afterwards lanes L and
@@ -254,8 +241,9 @@ __global__ void __launch_bounds__(kThreads) reduce2_coef_k(const double* __restr
   __shared__ int last;
   if (st->done) return;
   const int j = st->j;
+  const int lo = window_start(st, j);
   const int r = blockIdx.x % 2;
-  for (int i = blockIdx.x / 2; i <= j; i += gridDim.x / 2) {
+  for (int i = lo + blockIdx.x / 2; i <= j; i += gridDim.x / 2) {
     double a[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) a[v] = 0.0;
@@ -276,11 +264,11 @@ __global__ void __launch_bounds__(kThreads) reduce2_coef_k(const double* __restr
     const double* al = alpha + (int64_t)v * lda;
     double* be = beta + (int64_t)v * ldb;
     double ss = 0.0, sz = 0.0, sts = 0.0;
-    for (int k = lane; k < j; k += 32) {
+    for (int k = lo + lane; k < j; k += 32) {
       const double sk = __ldcg(hu + k * NV + v), zk = __ldcg(hw + k * NV + v);
-      // (T s)_k over the leading j x j tridiagonal block
+      // (T s)_k over the leading j x j tridiagonal block (s = 0 below lo)
       double ts = al[k] * sk;
-      if (k > 0) ts = fma(be[k], __ldcg(hu + (k - 1) * NV + v), ts);
+      if (k > lo) ts = fma(be[k], __ldcg(hu + (k - 1) * NV + v), ts);
       if (k + 1 < j) ts = fma(be[k + 1], __ldcg(hu + (k + 1) * NV + v), ts);
       ss = fma(sk, sk, ss);
       sz = fma(sk, zk, sz);
@@ -294,9 +282,9 @@ __global__ void __launch_bounds__(kThreads) reduce2_coef_k(const double* __restr
     }
     if (lane == 0) {
       double ts_last = 0.0;
-      if (j > 0) {
+      if (j > lo) {
         ts_last = al[j - 1] * __ldcg(hu + (j - 1) * NV + v);
-        if (j > 1) ts_last = fma(be[j - 1], __ldcg(hu + (j - 2) * NV + v), ts_last);
+        if (j - 2 >= lo) ts_last = fma(be[j - 1], __ldcg(hu + (j - 2) * NV + v), ts_last);
       }
       const double r2 = __ldcg(hu + j * NV + v) - ss;
       const double rr = r2 > 0.0 ? sqrt(r2) : 0.0;
@@ -305,7 +293,7 @@ __global__ void __launch_bounds__(kThreads) reduce2_coef_k(const double* __restr
       rc[v] = ri;
       rc[NV + v] = (omega - sz) * ri;
       alpha[(int64_t)v * lda + j] = (omega - 2.0 * sz + sts) * ri * ri;
-      if (j > 0) be[j] = (__ldcg(hw + (j - 1) * NV + v) - ts_last) * ri;
+      if (j > lo) be[j] = (__ldcg(hw + (j - 1) * NV + v) - ts_last) * ri;
     }
   }
   if (threadIdx.x == 0) *counter = 0;
@@ -333,10 +321,11 @@ __global__ void __launch_bounds__(edg::bulk::kThreadsAll) dots_bulk_k(const T* _
   init_barriers(sm);
   const Run run = run_of((int64_t)NV * n_seg);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int n_vec = j + 1;
+  const int lo = window_start(st, j);
+  const int n_vec = j + 1 - lo;
   if (warp == kConsumers / 32) {
     if (lane == 0) {
-      produce(sm, V, n_pad, stride_i, n_seg, n_vec, run);
+      produce(sm, V + (int64_t)lo * stride_i, n_pad, stride_i, n_seg, n_vec, run);
       if (sm.err) atomicExch(err_out, EDG_ERR_TIMEOUT);
     }
     return;
@@ -381,7 +370,7 @@ __global__ void __launch_bounds__(edg::bulk::kThreadsAll) dots_bulk_k(const T* _
         double a = 0.0;
         for (int wi = 0; wi < kConsumers / 32; ++wi) a += sm.red[wi][tid];
         const int t = tid >> 1, r = tid & 1;
-        partial[(((int64_t)(i0 + t) * 2 + r) * NV + v) * n_seg + g] = a;
+        partial[(((int64_t)(lo + i0 + t) * 2 + r) * NV + v) * n_seg + g] = a;
       }
       edg::bulk::consumers_sync();
     }
@@ -389,14 +378,18 @@ __global__ void __launch_bounds__(edg::bulk::kThreadsAll) dots_bulk_k(const T* _
 }
 
 // Update pass: for every row of the CTA's segments, V[j] <- (u - sum_{i<j}
-// V[i] s_i) / r, w <- w - sum_{i<j} V[i] z_i - V[j] c; per-CTA partials of
+// V[i] s_i) / r, w <- w - sum_{i<j} V[i] z_i - V[j] c; the next candidate
+// V[j+1] = w / r goes straight to the Krylov slot and the matvec input X (its
+// norm, beta_{j+1}, is what the next step's dots see: every formula of the
+// step is invariant under the candidate's scale); per-CTA partials of
 // |w_v|^2, and the last CTA (ticket) forms |w_v| and beta_{j+1}.
 template <typename T, int NV>
 __global__ void __launch_bounds__(edg::bulk::kThreadsAll) update_bulk_k(
     T* __restrict__ V, int64_t n_pad, DevState* __restrict__ st, const double* __restrict__ hu,
-    const double* __restrict__ hw, const double* __restrict__ rc, double* __restrict__ w,
+    const double* __restrict__ hw, const double* __restrict__ rc, const double* __restrict__ w,
     double* __restrict__ norm_partial, int64_t stride_i, double* __restrict__ wnorm, double* __restrict__ beta,
-    int ldb, int* __restrict__ counter, int64_t n_seg, int* __restrict__ err_out) {
+    int ldb, int* __restrict__ counter, int64_t n_seg, int* __restrict__ err_out, T* __restrict__ X, int xs,
+    int64_t n) {
   using namespace edg::bulk;
   if (st->done) return;
   const int j = st->j;
@@ -405,9 +398,10 @@ __global__ void __launch_bounds__(edg::bulk::kThreadsAll) update_bulk_k(
   init_barriers(sm);
   const Run run = run_of((int64_t)NV * n_seg);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int lo = window_start(st, j);
   if (warp == kConsumers / 32) {
     if (lane == 0) {
-      produce(sm, (const T*)V, n_pad, stride_i, n_seg, j, run);
+      produce(sm, (const T*)V + (int64_t)lo * stride_i, n_pad, stride_i, n_seg, j - lo, run);
       if (sm.err) atomicExch(err_out, EDG_ERR_TIMEOUT);
     }
     return;
@@ -424,21 +418,21 @@ __global__ void __launch_bounds__(edg::bulk::kThreadsAll) update_bulk_k(
     const int64_t q = g * kSegQuads + tid;
     const bool has = q < nq;
     T* U = V + (int64_t)j * stride_i + (int64_t)v * n_pad + 4 * q;
-    double* wp = w + (int64_t)v * n_pad + 4 * q;
+    const double* wp = w + (int64_t)v * n_pad + 4 * q;
     double u4[4] = {0, 0, 0, 0}, w4[4] = {0, 0, 0, 0};
     if (has) {
       ld4(U, u4);
       ld4(wp, w4);
     }
-    for (int i0 = 0; i0 < j; i0 += kVecs, ++k) {
-      const int nt = min(kVecs, j - i0);
+    for (int i0 = 0; i0 < j - lo; i0 += kVecs, ++k) {
+      const int nt = min(kVecs, j - lo - i0);
       // the tile's coefficients (the same addresses in every lane: L1
       // broadcasts), loaded before the stage wait so they overlap it
       double si[kVecs], zi[kVecs];
 #pragma unroll
       for (int t = 0; t < kVecs; ++t) {
-        si[t] = t < nt ? __ldg(hu + (i0 + t) * NV + v) : 0.0;
-        zi[t] = t < nt ? __ldg(hw + (i0 + t) * NV + v) : 0.0;
+        si[t] = t < nt ? __ldg(hu + (lo + i0 + t) * NV + v) : 0.0;
+        zi[t] = t < nt ? __ldg(hw + (lo + i0 + t) * NV + v) : 0.0;
       }
       const bool ok = acquire(sm, k);
       if (ok && has) {
@@ -466,9 +460,13 @@ __global__ void __launch_bounds__(edg::bulk::kThreadsAll) update_bulk_k(
         q4[e] = (double)(T)(u4[e] * ri);
         w4[e] = fma(-q4[e], c, w4[e]);
         sq = fma(w4[e], w4[e], sq);
+        w4[e] *= ri;
       }
       st4(U, q4);
-      st4(wp, w4);
+      st4(U + stride_i, w4);
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
+        if (4 * q + e < n) X[(4 * q + e) * xs + v] = (T)w4[e];
 #pragma unroll
       for (int vv = 0; vv < NV; ++vv)
         if (vv == v) nrm[vv] += sq;
@@ -618,10 +616,11 @@ __global__ void __launch_bounds__(kThreads) check_k(DevState* __restrict__ st, c
   }
 }
 
-__global__ void state_init_k(DevState* st, int first_check) {
+__global__ void state_init_k(DevState* st, int first_check, int win) {
   if (threadIdx.x != 0) return;
   DevState s{};
   s.next_check = first_check;
+  s.win = win;
   s.prev_worst = -1.0;
   *st = s;
 }
@@ -751,7 +750,7 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
   scale_store_k<T, NV><<<g_vec, 256, 0, s>>>(w, n, n_pad, h, V, X, kXs);
   zero_k<NV><<<(NV * ld_b + 255) / 256, 256, 0, s>>>(beta, NV * ld_b);
   zero_k<NV><<<(NV * ld_a + 255) / 256, 256, 0, s>>>(alpha, NV * ld_a);
-  state_init_k<<<1, 32, 0, s>>>(st, first_check);
+  state_init_k<<<1, 32, 0, s>>>(st, first_check, p->reorth_window);
   if ((e = cudaMemsetAsync(tickets, 0, 4 * sizeof(int), s)) != cudaSuccess)
     return edg::cuda_status(e, "edg_lanczos: tickets");
   if ((e = cudaGetLastError()) != cudaSuccess) return edg::cuda_status(e, "edg_lanczos: start");
@@ -804,8 +803,7 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
                                                    tickets);
     update_bulk_k<T, NV><<<g_upd, edg::bulk::kThreadsAll, upd_smem, cs>>>(V, n_pad, st, hu, hw, rc, w, normp, stride_i,
                                                                             wnorm, beta, ld_b, tickets + 1, n_seg,
-                                                                            err_word);
-    scale_next_k<T, NV><<<g_vec, 256, 0, cs>>>(w, n, n_pad, wnorm, V, stride_i, X, kXs, st);
+                                                                            err_word, X, kXs, n);
     return EDG_OK;
   };
   auto enqueue_check = [&](cudaStream_t cs) {
@@ -858,8 +856,7 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
                                                     rc, tickets);
       update_bulk_k<T, NV><<<g_upd, edg::bulk::kThreadsAll, upd_smem, s>>>(V, n_pad, st, hu, hw, rc, w, normp,
                                                                              stride_i, wnorm, beta, ld_b, tickets + 1,
-                                                                             n_seg, err_word);
-      scale_next_k<T, NV><<<g_vec, 256, 0, s>>>(w, n, n_pad, wnorm, V, stride_i, X, kXs, st);
+                                                                             n_seg, err_word, X, kXs, n);
       cudaEventRecord(ev[2], s);
       enqueue_check(s);
       cudaEventRecord(ev[3], s);
@@ -872,7 +869,7 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
       t_spmv += a;
       t_reorth += b;
       t_check += c;
-      launches += 6;
+      launches += 5;
       if (hs.done) break;
     }
     for (auto& x : ev) cudaEventDestroy(x);
@@ -922,7 +919,7 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
     cudaStreamSynchronize(s);
     cudaStreamDestroy(cs);
     if (rc_) return rc_;
-    launches += (int64_t)enq * 6;
+    launches += (int64_t)enq * 5;
   }
   if ((rc_ = read_state(&hs))) return rc_;
   const int j_end = hs.j;
@@ -997,6 +994,7 @@ int check_problem(const edg_lanczos_problem* p) {
   EDG_REQUIRE(p->max_iter >= 1 && p->max_iter <= 2000, "edg_lanczos: max_iter must be 1..2000");
   EDG_REQUIRE(p->check_every >= 1, "edg_lanczos: check_every must be >= 1");
   EDG_REQUIRE(p->rowptr && p->diag, "edg_lanczos: null matrix pointer");
+  EDG_REQUIRE(p->reorth_window >= 0, "edg_lanczos: reorth_window must be >= 0");
   EDG_REQUIRE(p->sell_entries == nullptr || (p->sell_perm && p->sell_width && p->sell_off),
               "edg_lanczos: incomplete SELL layout");
   return EDG_OK;

@@ -142,6 +142,7 @@ class LanczosProblem(C.Structure):
         ("sell_width", P),
         ("sell_off", P),
         ("sell_entries", P),
+        ("reorth_window", I32),
     ]
 
 

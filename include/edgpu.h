@@ -378,6 +378,11 @@ typedef struct {
   const int32_t* sell_width;  /* matrix (edg_sell_*), used by the f32 path  */
   const int64_t* sell_off;    /* when sell_entries is not NULL              */
   const void* sell_entries;
+  int32_t reorth_window;  /* 0: full reorthogonalisation; W > 0: each step */
+                          /* orthogonalises against the last W Krylov      */
+                          /* vectors only (local reorthogonalisation: the  */
+                          /* lowest Ritz pair converges as with the full   */
+                          /* one, later copies of it are not suppressed)   */
 } edg_lanczos_problem;
 
 /* Bytes of device workspace edg_lanczos needs. */
