@@ -336,19 +336,26 @@ def run_edgpu(args, world, rank, local):
 
     # f32 matvec layout (SELL or CSR) and threads per row: the autotuner's
     # choices (or --spmv-group, which forces CSR), fixed before the timed region
+    from edgpu.solvers import packed_layout
+
     if args.matvec_layout == "auto":
         fmt32, param = ("csr", args.spmv_group) if args.spmv_group else tune_matvec32(mat, 3, vals32)
     elif args.matvec_layout == "sell":
         fmt32, param = "sell", args.sell_window
+    elif args.matvec_layout == "packed":
+        fmt32, param = "packed", 2
     else:
         fmt32, param = "csr", args.spmv_group or tune_spmv_group(mat, 3, 1, vals=vals32)
     sell32 = sell_layout(mat, vals32, param) if fmt32 == "sell" else False
-    g32 = param if fmt32 == "csr" else tune_spmv_group(mat, 3, 1, vals=vals32)
+    pk32 = packed_layout(mat) if fmt32 == "packed" else None
+    if fmt32 == "packed" and pk32 is None:
+        raise SystemExit("--matvec-layout packed: the matrix does not pack")
+    g32 = param if fmt32 in ("csr", "packed") else tune_spmv_group(mat, 3, 1, vals=vals32)
     g64 = args.spmv_group or tune_spmv_group(mat, 3, 0, vals=mat.vals)
 
     def mixed_step(s32, s64):
         return lanczos_mixed(mat, diags=diags, vals32=vals32, diag32=diag32, diag64=diag64, stats32=s32, stats64=s64,
-                             group32=g32, group64=g64, sell=sell32, window32=WINDOW32)
+                             group32=g32, group64=g64, sell=sell32, window32=WINDOW32, packed=pk32)
 
     for _ in range(args.warmup):
         mixed_step(None, None)
@@ -384,11 +391,18 @@ def run_edgpu(args, world, rank, local):
     hbm, peak_kind = peaks()
     nv = 3
     n_pad = (n + 3) // 4 * 4
-    # matvec: values + columns + row index + x (f32) + y (f64) + diagonal (f32);
-    # the row index is rowptr (8 B a row) for CSR, the row permutation (4 B a
-    # row) plus a width and an offset per slice of 32 rows (12 B) for SELL
-    row_index = 8 * (n + 1) if fmt32 == "csr" else 4 * n + 12 * ((n + 31) // 32)
-    spmv_bytes = nnz * (4 + 4) + row_index + n * nv * 4 + n * nv * 8 + n * nv * 4
+    # matvec: entries + row index + x (f32) + y (f64) + diagonal (f32); an
+    # entry is a value and a column (8 B) for CSR and SELL; the
+    # dictionary-packed tiles read one 4-byte word per slot (entries and the
+    # tiles' padding) plus one int32 offset per tile of 16 rows (their value
+    # table, a few bytes, once per CTA); the row index is rowptr (8 B a row)
+    # for CSR, the row permutation (4 B a row) plus a width and an offset per
+    # slice of 32 rows (12 B) for SELL
+    if fmt32 == "packed":
+        stream = pk32.stream_bytes
+    else:
+        stream = nnz * 8 + (8 * (n + 1) if fmt32 == "csr" else 4 * n + 12 * ((n + 31) // 32))
+    spmv_bytes = stream + n * nv * 4 + n * nv * 8 + n * nv * 4
     spmv_ms = agg32[0] / max(agg32[1], 1)  # agg32/agg64: the one instrumented sweep
     spmv_achieved = spmv_bytes / (spmv_ms * 1e-3) / 1e9
     # reorthogonalisation of step j (delayed Gram-Schmidt over the window
@@ -475,6 +489,8 @@ def run_edgpu(args, world, rank, local):
         "steps": args.steps,
         "warmup": args.warmup,
         "ms_per_step": ms,
+        "step_ms_spread": {"min": float(np.min(step_ms)), "median": float(np.median(step_ms)),
+                           "max": float(np.max(step_ms))},
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
@@ -509,6 +525,10 @@ def run_edgpu(args, world, rank, local):
                                        f"sort window {sell32.window}, slice padding {sell32.padding:.3f} of the "
                                        "stored pairs"
                                        if fmt32 == "sell" else
+                                       "batched f32 dictionary-packed tiled matvec (packed_spmv_k<float,3,4>): "
+                                       f"{pk32.count} distinct values, {pk32.colbits}-bit columns, tiles of 16 rows, "
+                                       f"padding {pk32.padding:.3f} of the words"
+                                       if fmt32 == "packed" else
                                        f"batched f32 CSR+diag matvec (spmv_k<float,float,double,3,{g32},4>)"),
                             "layout_choice": fmt32,
                             "bound": "hbm", "achieved": spmv_achieved, "peak": hbm, "unit": "GB/s",
@@ -1100,7 +1120,7 @@ def main():
                          "corr: SU(2) L=16 two-body correlator matrices; entropy: SU(2) L=14 half-chain entanglement; "
                          "momentum: SU(2) L=14 PBC zero-momentum ground state")
     ap.add_argument("--quench-time", type=float, default=20.0)
-    ap.add_argument("--matvec-layout", default="auto", choices=["auto", "sell", "csr"],
+    ap.add_argument("--matvec-layout", default="auto", choices=["auto", "sell", "csr", "packed"],
                     help="f32 matvec layout of the headline solve; auto = the autotuner's choice")
     ap.add_argument("--sell-window", type=int, default=32, help="SELL sort window with --matvec-layout sell")
     ap.add_argument("--spmv-group", type=int, default=0,

@@ -225,40 +225,14 @@ __device__ __forceinline__ double warp_reduce_scatter16(const double* v16) {
   return a[0] + __shfl_xor_sync(0xffffffffu, a[0], 1);
 }
 
-// hu[i][v] (r = 0), hw[i][v] (r = 1) = sum over the segment partials (fixed
-// order), for i <= j strided over the CTA pairs of a fixed grid.  The last
-// CTA to finish (ticket counter, reset by it) then computes, one warp per
-// problem, r and c of the delayed step and the new tridiagonal entries
-// alpha_j, beta_j from hu, hw and the previous alpha, beta.
+// Coefficients of the delayed step from the totals hu, hw of V[lo..j] . u and
+// V[lo..j] . w: one warp per problem computes r and c and the new
+// tridiagonal entries alpha_j, beta_j from hu, hw and the previous alpha,
+// beta (run by the last CTA of the pass that formed the totals).
 template <int NV>
-__global__ void __launch_bounds__(kThreads) reduce2_coef_k(const double* __restrict__ partial, int nblocks,
-                                                           int64_t ld_p, const DevState* __restrict__ st,
-                                                           double* __restrict__ hu, double* __restrict__ hw,
-                                                           double* __restrict__ alpha, int lda,
-                                                           double* __restrict__ beta, int ldb,
-                                                           double* __restrict__ rc, int* __restrict__ counter) {
-  __shared__ double red[(kThreads / 32) * NV];
-  __shared__ int last;
-  if (st->done) return;
-  const int j = st->j;
-  const int lo = window_start(st, j);
-  const int r = blockIdx.x % 2;
-  for (int i = lo + blockIdx.x / 2; i <= j; i += gridDim.x / 2) {
-    double a[NV];
-#pragma unroll
-    for (int v = 0; v < NV; ++v) a[v] = 0.0;
-    for (int b = threadIdx.x; b < nblocks; b += kThreads)
-#pragma unroll
-      for (int v = 0; v < NV; ++v) a[v] += partial[(((int64_t)i * 2 + r) * NV + v) * ld_p + b];
-    block_sum<NV>(a, red);
-    if (threadIdx.x < NV) (r == 0 ? hu : hw)[i * NV + threadIdx.x] = a[threadIdx.x];
-  }
-  if (threadIdx.x < NV) __threadfence();  // the writers publish before the ticket
-  __syncthreads();
-  if (threadIdx.x == 0) last = atomicAdd(counter, 1) == (int)gridDim.x - 1;
-  __syncthreads();
-  if (!last) return;
-  __threadfence();
+__device__ __forceinline__ void coef_epilogue(int lo, int j, const double* __restrict__ hu,
+                                              const double* __restrict__ hw, double* __restrict__ alpha, int lda,
+                                              double* __restrict__ beta, int ldb, double* __restrict__ rc) {
   const int lane = threadIdx.x & 31, v = threadIdx.x >> 5;
   if (v < NV) {
     const double* al = alpha + (int64_t)v * lda;
@@ -296,6 +270,43 @@ __global__ void __launch_bounds__(kThreads) reduce2_coef_k(const double* __restr
       if (j > lo) be[j] = (__ldcg(hw + (j - 1) * NV + v) - ts_last) * ri;
     }
   }
+}
+
+// hu[i][v] (r = 0), hw[i][v] (r = 1) = sum over the segment partials (fixed
+// order), for i <= j strided over the CTA pairs of a fixed grid.  The last
+// CTA to finish (ticket counter, reset by it) then computes, one warp per
+// problem, r and c of the delayed step and the new tridiagonal entries
+// alpha_j, beta_j from hu, hw and the previous alpha, beta.
+template <int NV>
+__global__ void __launch_bounds__(kThreads) reduce2_coef_k(const double* __restrict__ partial, int nblocks,
+                                                           int64_t ld_p, const DevState* __restrict__ st,
+                                                           double* __restrict__ hu, double* __restrict__ hw,
+                                                           double* __restrict__ alpha, int lda,
+                                                           double* __restrict__ beta, int ldb,
+                                                           double* __restrict__ rc, int* __restrict__ counter) {
+  __shared__ double red[(kThreads / 32) * NV];
+  __shared__ int last;
+  if (st->done) return;
+  const int j = st->j;
+  const int lo = window_start(st, j);
+  const int r = blockIdx.x % 2;
+  for (int i = lo + blockIdx.x / 2; i <= j; i += gridDim.x / 2) {
+    double a[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) a[v] = 0.0;
+    for (int b = threadIdx.x; b < nblocks; b += kThreads)
+#pragma unroll
+      for (int v = 0; v < NV; ++v) a[v] += partial[(((int64_t)i * 2 + r) * NV + v) * ld_p + b];
+    block_sum<NV>(a, red);
+    if (threadIdx.x < NV) (r == 0 ? hu : hw)[i * NV + threadIdx.x] = a[threadIdx.x];
+  }
+  if (threadIdx.x < NV) __threadfence();  // the writers publish before the ticket
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(counter, 1) == (int)gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  coef_epilogue<NV>(lo, j, hu, hw, alpha, lda, beta, ldb, rc);
   if (threadIdx.x == 0) *counter = 0;
 }
 
@@ -492,15 +503,335 @@ __global__ void __launch_bounds__(edg::bulk::kThreadsAll) update_bulk_k(
   edg::bulk::consumers_sync();
   if (!sm.last) return;
   __threadfence();
-  if (tid < NV) {
+  if (warp < NV) {  // warp v: lanes stride over the CTAs, fixed-order butterfly
     double a = 0.0;
-    for (int b = 0; b < (int)gridDim.x; ++b) a += __ldcg(norm_partial + (int64_t)b * NV + tid);
-    const double nv = sqrt(a);
-    wnorm[tid] = nv;
-    beta[(int64_t)tid * ldb + j + 1] = nv * rc[tid];
+    for (int b = lane; b < (int)gridDim.x; b += 32) a += __ldcg(norm_partial + (int64_t)b * NV + warp);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    if (lane == 0) {
+      const double nv = sqrt(a);
+      wnorm[warp] = nv;
+      beta[(int64_t)warp * ldb + j + 1] = nv * rc[warp];
+    }
   }
   if (tid == 0) {
     *counter = 0;
+    st->j = j + 1;  // every CTA read j before arriving at the ticket
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Reorthogonalisation of one step for a short basis window (at most kSmallMax
+// vectors V[lo..j]: the local window of the f32 phase, or the steps of a
+// short refinement) as ONE cooperative launch: the dots phase, a grid-wide
+// barrier, the step's coefficients formed by every CTA from the dots
+// partials (the same sums in the same order everywhere), and the update
+// phase over the rows in reverse order (the rows read last by the dots
+// phase, still in L2, come first).  Every load of a row quad is in flight at
+// once.  Same arithmetic as the ring passes row by row; only the order of
+// the cross-CTA sums differs.
+// ---------------------------------------------------------------------------
+constexpr int kSmallMax = 8;        // vectors of V[lo..j] the small pass takes
+constexpr int kSmallThreads = 256;  // threads of a small-pass CTA
+constexpr int kSmallGridMax = edg::kSmCount * 4;  // CTAs of a small pass at most (the resident ones)
+
+// four consecutive Krylov entries as loaded (converted to double when used)
+template <typename T>
+struct Raw4;
+template <>
+struct Raw4<float> {
+  float4 a;
+  __device__ void ld(const float* p) { a = *reinterpret_cast<const float4*>(p); }
+  __device__ double operator[](int e) const { return (double)(e == 0 ? a.x : e == 1 ? a.y : e == 2 ? a.z : a.w); }
+};
+template <>
+struct Raw4<double> {
+  double2 a, b;
+  __device__ void ld(const double* p) {
+    a = *reinterpret_cast<const double2*>(p);
+    b = *reinterpret_cast<const double2*>(p + 2);
+  }
+  __device__ double operator[](int e) const { return e == 0 ? a.x : e == 1 ? a.y : e == 2 ? b.x : b.y; }
+};
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Grid-wide barrier of the small pass (every CTA is resident: cooperative
+// launch).  bar[0] counts arrivals, bar[1] is the generation.  A wait longer
+// than 1 s writes EDG_ERR_TIMEOUT to *err; once *err is set no CTA waits any
+// more and every thread gets false.
+__device__ bool small_barrier(unsigned* bar, int* err) {
+  __shared__ int ok_s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned g = ld_acquire_u32(bar + 1);
+    __threadfence();
+    const unsigned arrived = atomicAdd(bar, 1u);
+    if (arrived == gridDim.x - 1) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      const uint64_t t0 = edg::bulk::now_ns();
+      for (unsigned spins = 1; ld_acquire_u32(bar + 1) == g; ++spins) {
+        if ((spins & 255u) == 0) {
+          if (*(volatile int*)err) break;
+          if (edg::bulk::now_ns() - t0 > 1000000000ull) {
+            atomicExch(err, EDG_ERR_TIMEOUT);
+            break;
+          }
+        }
+      }
+    }
+    __threadfence();
+    ok_s = *(volatile int*)err == 0;
+  }
+  __syncthreads();
+  return ok_s != 0;
+}
+
+// Coefficients of the delayed step for one problem (one warp) from its
+// totals tot[2t] = V[lo+t] . u, tot[2t+1] = V[lo+t] . w (t <= j - lo) and the
+// previous alpha, beta (entries below j only): 1/r, c, alpha_j, beta_j (the
+// same formulas as coef_epilogue); lane 0 returns them.
+__device__ __forceinline__ void coef_small(int lo, int j, const double* tot, const double* __restrict__ al,
+                                           const double* __restrict__ be, double* out /*[4]*/) {
+  const int lane = threadIdx.x & 31;
+  double ss = 0.0, sz = 0.0, sts = 0.0;
+  for (int k = lo + lane; k < j; k += 32) {
+    const int t = k - lo;
+    const double sk = tot[2 * t], zk = tot[2 * t + 1];
+    double ts = al[k] * sk;
+    if (k > lo) ts = fma(be[k], tot[2 * (t - 1)], ts);
+    if (k + 1 < j) ts = fma(be[k + 1], tot[2 * (t + 1)], ts);
+    ss = fma(sk, sk, ss);
+    sz = fma(sk, zk, sz);
+    sts = fma(sk, ts, sts);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    ss += __shfl_xor_sync(0xffffffffu, ss, o);
+    sz += __shfl_xor_sync(0xffffffffu, sz, o);
+    sts += __shfl_xor_sync(0xffffffffu, sts, o);
+  }
+  if (lane == 0) {
+    const int tj = j - lo;
+    double ts_last = 0.0;
+    if (j > lo) {
+      ts_last = al[j - 1] * tot[2 * (tj - 1)];
+      if (j - 2 >= lo) ts_last = fma(be[j - 1], tot[2 * (tj - 2)], ts_last);
+    }
+    const double r2 = tot[2 * tj] - ss;
+    const double rr = r2 > 0.0 ? sqrt(r2) : 0.0;
+    const double ri = rr > 0.0 ? 1.0 / rr : 0.0;
+    const double omega = tot[2 * tj + 1];
+    out[0] = ri;
+    out[1] = (omega - sz) * ri;
+    out[2] = (omega - 2.0 * sz + sts) * ri * ri;
+    out[3] = j > lo ? (tot[2 * (tj - 1) + 1] - ts_last) * ri : 0.0;
+  }
+}
+
+// The small pass.  Dots phase: CTA block b of problem v (gridDim.x = NV * G, v
+// = blockIdx.x / G) sums V[lo+t] . u and V[lo+t] . w over its row quads into
+// partial[cta][2t + r].  After the barrier every CTA forms the totals of all
+// problems and their coefficients (CTA 0 writes them out: hu, hw, alpha_j,
+// beta_j, rc).  Update phase: every thread takes row quads of all NV
+// problems: V[j] <- (u - sum V[i] s_i) / r, w <- w - sum V[i] z_i - V[j] c,
+// the next candidate V[j+1] = w / r to its Krylov slot and whole interleaved
+// rows of the matvec input X; per-CTA partials of |w_v|^2, and the last CTA
+// (ticket) forms |w_v| and beta_{j+1} and advances the step.  A barrier that
+// runs out ends the solve (done flag; the error word says why).
+template <typename T, int NV, int KV>
+__global__ void __launch_bounds__(kSmallThreads) reorth_small_k(
+    T* __restrict__ V, int64_t n_pad, DevState* __restrict__ st, const double* __restrict__ w,
+    double* __restrict__ partial, int64_t stride_i, double* __restrict__ hu, double* __restrict__ hw,
+    double* __restrict__ alpha, int lda, double* __restrict__ beta, int ldb, double* __restrict__ rc,
+    double* __restrict__ norm_partial, double* __restrict__ wnorm, int* __restrict__ ticket,
+    unsigned* __restrict__ bar, int* __restrict__ err, T* __restrict__ X, int xs, int64_t n) {
+  __shared__ double red[kSmallThreads / 32][2 * kSmallMax];
+  __shared__ double tot[NV][2 * kSmallMax];
+  __shared__ double coef[NV][4];
+  __shared__ double nred[kSmallThreads / 32][NV];
+  __shared__ int last;
+  if (st->done) return;
+  const int j = st->j;
+  const int lo = window_start(st, j);
+  const int n_vec = j + 1 - lo;  // <= KV (the host picks this pass only then)
+  const int n_w = n_vec - 1;     // window vectors besides the candidate
+  const int G = (int)gridDim.x / NV;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int64_t nq = n_pad / 4;
+  // ---- dots phase --------------------------------------------------------
+  {
+    const int v = (int)blockIdx.x / G, b = (int)blockIdx.x - v * G;
+    const T* Vv = V + (int64_t)lo * stride_i + (int64_t)v * n_pad;
+    const T* U = V + (int64_t)j * stride_i + (int64_t)v * n_pad;
+    const double* wv = w + (int64_t)v * n_pad;
+    double acc[2 * kSmallMax];
+#pragma unroll
+    for (int t = 0; t < 2 * kSmallMax; ++t) acc[t] = 0.0;
+    for (int64_t q = (int64_t)b * kSmallThreads + tid; q < nq; q += (int64_t)G * kSmallThreads) {
+      Raw4<T> x[KV], u;
+      Raw4<double> ww;
+      u.ld(U + 4 * q);
+      ww.ld(wv + 4 * q);
+#pragma unroll
+      for (int t = 0; t < KV; ++t)
+        if (t < n_vec) x[t].ld(Vv + (int64_t)t * stride_i + 4 * q);
+#pragma unroll
+      for (int t = 0; t < KV; ++t)
+        if (t < n_vec) {
+          acc[2 * t] = fma(x[t][0], u[0], fma(x[t][1], u[1], fma(x[t][2], u[2], fma(x[t][3], u[3], acc[2 * t]))));
+          acc[2 * t + 1] =
+              fma(x[t][0], ww[0], fma(x[t][1], ww[1], fma(x[t][2], ww[2], fma(x[t][3], ww[3], acc[2 * t + 1]))));
+        }
+    }
+    const int idx = ((lane >> 4) & 1) * 8 + ((lane >> 3) & 1) * 4 + ((lane >> 2) & 1) * 2 + ((lane >> 1) & 1);
+    const double sum = warp_reduce_scatter16(acc);
+    if ((lane & 1) == 0) red[warp][idx] = sum;
+    __syncthreads();
+    if (tid < 2 * n_vec) {
+      double a = 0.0;
+      for (int wi = 0; wi < kSmallThreads / 32; ++wi) a += red[wi][tid];
+      partial[(int64_t)blockIdx.x * (2 * kSmallMax) + tid] = a;
+    }
+  }
+  if (!small_barrier(bar, err)) {
+    if (tid == 0) atomicExch(&st->done, 1);
+    return;
+  }
+  // ---- totals and coefficients (every CTA, the same order everywhere) -----
+  for (int e = warp; e < NV * 2 * n_vec; e += kSmallThreads / 32) {
+    const int vv = e / (2 * n_vec), rem = e - vv * 2 * n_vec;
+    double a = 0.0;
+    for (int bb = lane; bb < G; bb += 32) a += __ldcg(partial + (int64_t)(vv * G + bb) * (2 * kSmallMax) + rem);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    if (lane == 0) tot[vv][rem] = a;
+  }
+  __syncthreads();
+  if (warp < NV) {
+    double out[4];
+    coef_small(lo, j, tot[warp], alpha + (int64_t)warp * lda, beta + (int64_t)warp * ldb, out);
+    if (lane == 0) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) coef[warp][q] = out[q];
+      if (blockIdx.x == 0) {
+        rc[warp] = out[0];
+        rc[NV + warp] = out[1];
+        alpha[(int64_t)warp * lda + j] = out[2];
+        if (j > lo) beta[(int64_t)warp * ldb + j] = out[3];
+        for (int t = 0; t < n_vec; ++t) {
+          hu[(lo + t) * NV + warp] = tot[warp][2 * t];
+          hw[(lo + t) * NV + warp] = tot[warp][2 * t + 1];
+        }
+      }
+    }
+  }
+  __syncthreads();
+  // ---- update phase: quads of all problems, the grid's quads in reverse ---
+  double nrm[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) nrm[v] = 0.0;
+  {
+    const int64_t S = (int64_t)gridDim.x * kSmallThreads;
+    const int64_t first = (int64_t)blockIdx.x * kSmallThreads + tid;
+    const int64_t q_last = first < nq ? first + ((nq - 1 - first) / S) * S : -1;
+    for (int64_t q = q_last; q >= 0; q -= S) {
+      double xo[NV][4];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        T* U = V + (int64_t)j * stride_i + (int64_t)v * n_pad + 4 * q;
+        Raw4<T> x[KV - 1], u;
+        Raw4<double> ww;
+        u.ld(U);
+        ww.ld(w + (int64_t)v * n_pad + 4 * q);
+#pragma unroll
+        for (int t = 0; t < KV - 1; ++t)
+          if (t < n_w) x[t].ld(V + (int64_t)(lo + t) * stride_i + (int64_t)v * n_pad + 4 * q);
+        double u4[4], w4[4], q4[4], sq = 0.0;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          u4[e] = u[e];
+          w4[e] = ww[e];
+        }
+#pragma unroll
+        for (int t = 0; t < KV - 1; ++t)
+          if (t < n_w) {
+            const double s_t = tot[v][2 * t], z_t = tot[v][2 * t + 1];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              u4[e] = fma(-x[t][e], s_t, u4[e]);
+              w4[e] = fma(-x[t][e], z_t, w4[e]);
+            }
+          }
+        const double ri = coef[v][0], c = coef[v][1];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          q4[e] = (double)(T)(u4[e] * ri);
+          w4[e] = fma(-q4[e], c, w4[e]);
+          sq = fma(w4[e], w4[e], sq);
+          w4[e] *= ri;
+          xo[v][e] = w4[e];
+        }
+        st4(U, q4);
+        st4(U + stride_i, w4);
+        nrm[v] += sq;
+      }
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int64_t r = 4 * q + e;
+        if (r >= n) break;
+        if (xs == 4) {
+          double row[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+          for (int v = 0; v < NV && v < 4; ++v) row[v] = xo[v][e];
+          st4(X + r * 4, row);
+        } else {
+#pragma unroll
+          for (int v = 0; v < NV; ++v) X[r * xs + v] = (T)xo[v][e];
+        }
+      }
+    }
+  }
+  // ---- |w_v|^2: CTA partials, the last CTA finishes the step ------------
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    double a = nrm[v];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+    if (lane == 0) nred[warp][v] = a;
+  }
+  __syncthreads();
+  if (tid < NV) {
+    double a = 0.0;
+    for (int wi = 0; wi < kSmallThreads / 32; ++wi) a += nred[wi][tid];
+    norm_partial[(int64_t)blockIdx.x * NV + tid] = a;
+    __threadfence();
+  }
+  __syncthreads();
+  if (tid == 0) last = atomicAdd(ticket, 1) == (int)gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  if (warp < NV) {  // warp v: lanes stride over the CTAs, fixed-order butterfly
+    double a = 0.0;
+    for (int bb = lane; bb < (int)gridDim.x; bb += 32) a += __ldcg(norm_partial + (int64_t)bb * NV + warp);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    if (lane == 0) {
+      const double nv = sqrt(a);
+      wnorm[warp] = nv;
+      beta[(int64_t)warp * ldb + j + 1] = nv * coef[warp][0];
+    }
+  }
+  if (tid == 0) {
+    *ticket = 0;
     st->j = j + 1;  // every CTA read j before arriving at the ticket
   }
 }
@@ -654,7 +985,7 @@ __global__ void ritz_k(const T* __restrict__ V, int64_t n_pad, int m, const doub
 // Workspace layout
 // ---------------------------------------------------------------------------
 struct Layout {
-  int64_t V, X, w, h, partial, normp, alpha, beta, tri_eval, tri_vec, tri_work, sync, state, total;
+  int64_t V, X, w, h, partial, small, normp, alpha, beta, tri_eval, tri_vec, tri_work, sync, state, total;
   int nblk_dot, nblk_upd, m_max, ld_h;
   int64_t n_pad;
 };
@@ -681,13 +1012,14 @@ Layout make_layout(const edg_lanczos_problem* p) {
   L.w = off; off = align256(off + L.n_pad * nv * 8);
   L.h = off; off = align256(off + (int64_t)(2 * (L.m_max + 1) + 3) * nv * 8);  // hu | hw | rc | |w|
   L.partial = off; off = align256(off + (int64_t)L.nblk_dot * (L.m_max + 1) * 2 * nv * 8);
+  L.small = off; off = align256(off + (int64_t)kSmallGridMax * 2 * kSmallMax * 8);  // dots partials of the small passes
   L.normp = off; off = align256(off + (int64_t)L.nblk_upd * nv * 8);
   L.alpha = off; off = align256(off + (int64_t)nv * (L.m_max + 1) * 8);   // [nv][m_max+1]
   L.beta = off; off = align256(off + (int64_t)nv * (L.m_max + 2) * 8);    // [nv][m_max+2]
   L.tri_eval = off; off = align256(off + (int64_t)nv * kMaxK * 8);
   L.tri_vec = off; off = align256(off + (int64_t)nv * kMaxK * (L.m_max + 1) * 8);
   L.tri_work = off; off = align256(off + (int64_t)nv * 6 * (L.m_max + 1) * 8);
-  L.sync = off; off = align256(off + 4 * (int64_t)sizeof(int));  // last-CTA tickets | error word
+  L.sync = off; off = align256(off + 8 * (int64_t)sizeof(int));  // last-CTA tickets | error word | grid barrier
   L.state = off; off = align256(off + (int64_t)sizeof(DevState));
   L.total = off;
   return L;
@@ -724,7 +1056,8 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
   double* rc = hw + (int64_t)(L.m_max + 1) * NV;     // [2][NV]: 1/r, c of the current step
   double* wnorm = rc + 2 * NV;                        // [NV]: |w| of the next candidate
   int* tickets = (int*)(ws + L.sync);                  // [2] last-CTA counters (left at 0)
-  int* err_word = tickets + 2;                          // EDG_ERR_TIMEOUT when a ring wait ran out
+  int* err_word = tickets + 2;                          // EDG_ERR_TIMEOUT when a ring or barrier wait ran out
+  unsigned* small_bar = (unsigned*)(tickets + 4);       // [2] grid barrier of the small pass (count, generation)
   const unsigned g_vec = edg::grid_for(n_pad, 256);
   const int first_check = p->check_every > 8 ? p->check_every : 8;
   constexpr int kXs = NV == 3 ? 4 : NV;  // row stride of the matvec input X
@@ -751,7 +1084,7 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
   zero_k<NV><<<(NV * ld_b + 255) / 256, 256, 0, s>>>(beta, NV * ld_b);
   zero_k<NV><<<(NV * ld_a + 255) / 256, 256, 0, s>>>(alpha, NV * ld_a);
   state_init_k<<<1, 32, 0, s>>>(st, first_check, p->reorth_window);
-  if ((e = cudaMemsetAsync(tickets, 0, 4 * sizeof(int), s)) != cudaSuccess)
+  if ((e = cudaMemsetAsync(tickets, 0, 8 * sizeof(int), s)) != cudaSuccess)
     return edg::cuda_status(e, "edg_lanczos: tickets");
   if ((e = cudaGetLastError()) != cudaSuccess) return edg::cuda_status(e, "edg_lanczos: start");
   // the reorthogonalisation passes: persistent grids of the bulk-copy kernels
@@ -785,8 +1118,44 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
   const unsigned g_red = 2u * (unsigned)(L.m_max + 1 < 2 * edg::kSmCount ? L.m_max + 1 : 2 * edg::kSmCount);
   // one Lanczos step and its check; every kernel reads the step index and the
   // done flag from the device state
+  // short windows (the local window of the f32 phase, or a refinement of at
+  // most kSmallMax steps) take the streaming small passes
+  const bool small_passes = (p->reorth_window > 0 && p->reorth_window < kSmallMax) || L.m_max <= kSmallMax;
+  // most vectors of V[lo..j] a step reads: window + 1, or the Krylov limit
+  const int small_kv = p->reorth_window > 0 && p->reorth_window < kSmallMax
+                           ? (p->reorth_window + 1 < L.m_max ? p->reorth_window + 1 : L.m_max)
+                           : L.m_max;
+  double* small_partial = (double*)(ws + L.small);
+  const int64_t nq = n_pad / 4;
+  auto clamp_grid = [](int64_t want, int64_t cap) { return (unsigned)(want < 1 ? 1 : (want < cap ? want : cap)); };
+  // the small pass: one cooperative launch whose grid is the CTAs resident at
+  // once, split evenly over the problems
+  const int small_kv_t = small_kv <= 5 ? 5 : kSmallMax;
+  int occ_small = 0;
+  if (small_passes) {
+    int coop = 0;
+    cudaError_t eo = cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+    if (eo == cudaSuccess)
+      eo = small_kv_t == 5 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_small, reorth_small_k<T, NV, 5>,
+                                                                           kSmallThreads, 0)
+                           : cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                                 &occ_small, reorth_small_k<T, NV, kSmallMax>, kSmallThreads, 0);
+    if (eo != cudaSuccess) return edg::cuda_status(eo, "edg_lanczos: small-pass occupancy");
+    if (!coop || occ_small < 1) {
+      edg::set_error("edg_lanczos: the small reorthogonalisation pass needs a cooperative launch");
+      return EDG_ERR_ARG;
+    }
+  }
+  const int64_t small_resident = (int64_t)n_sm * (occ_small < 1 ? 1 : occ_small);
+  const unsigned g_small =
+      clamp_grid((nq + kSmallThreads - 1) / kSmallThreads,
+                 (small_resident < kSmallGridMax ? small_resident : kSmallGridMax) / NV) * NV;
   const bool sell = p->sell_entries != nullptr && p->dtype == 1;
   auto matvec = [&](cudaStream_t cs) -> int {
+    if (p->pk_words != nullptr)
+      return edg::launch_packed_spmv<T>(NV, kXs, n, p->pk_tile_off, p->pk_words, (const T*)p->pk_table,
+                                        p->pk_count, p->pk_colbits, (const T*)p->diag, X, w, n_pad, &st->done,
+                                        err_word, cs);
     if (sell)
       return edg::launch_sell_spmv(NV, kXs, (n + 31) / 32, p->sell_perm, p->sell_width, p->sell_off,
                                    (const uint2*)p->sell_entries, (const float*)p->diag, (const float*)X, w, n_pad,
@@ -794,9 +1163,17 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
     return edg::launch_spmv<T, T, double>(NV, n, p->nnz, p->rowptr, p->cols, (const T*)p->vals, (const T*)p->diag, X,
                                           w, cs, n_pad, p->spmv_group, &st->done, kXs);
   };
-  auto enqueue_step = [&](cudaStream_t cs) -> int {
-    int st_ = matvec(cs);
-    if (st_) return st_;
+  // the reorthogonalisation of one step: dots, coefficients, update
+  auto enqueue_reorth = [&](cudaStream_t cs) -> cudaError_t {
+    if (small_passes) {
+      int* tk = tickets + 1;
+      void* args[] = {&V, (void*)&n_pad, &st, &w, &small_partial, (void*)&stride_i, &hu, &hw, &alpha, (void*)&ld_a,
+                      &beta, (void*)&ld_b, &rc, &normp, &wnorm, &tk, &small_bar, &err_word, &X, (void*)&kXs,
+                      (void*)&n};
+      const void* fn = small_kv_t == 5 ? (const void*)reorth_small_k<T, NV, 5>
+                                       : (const void*)reorth_small_k<T, NV, kSmallMax>;
+      return cudaLaunchCooperativeKernel(fn, dim3(g_small), dim3(kSmallThreads), args, 0, cs);
+    }
     dots_bulk_k<T, NV><<<g_dot, edg::bulk::kThreadsAll, dot_smem, cs>>>(V, n_pad, st, w, partial, stride_i, n_seg,
                                                                           err_word);
     reduce2_coef_k<NV><<<g_red, kThreads, 0, cs>>>(partial, (int)n_seg, n_seg, st, hu, hw, alpha, ld_a, beta, ld_b, rc,
@@ -804,7 +1181,14 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
     update_bulk_k<T, NV><<<g_upd, edg::bulk::kThreadsAll, upd_smem, cs>>>(V, n_pad, st, hu, hw, rc, w, normp, stride_i,
                                                                             wnorm, beta, ld_b, tickets + 1, n_seg,
                                                                             err_word, X, kXs, n);
-    return EDG_OK;
+    return cudaGetLastError();
+  };
+  const int launches_per_step = small_passes ? 3 : 5;  // matvec, reorthogonalisation, check
+  auto enqueue_step = [&](cudaStream_t cs) -> int {
+    int st_ = matvec(cs);
+    if (st_) return st_;
+    const cudaError_t er = enqueue_reorth(cs);
+    return er == cudaSuccess ? EDG_OK : edg::cuda_status(er, "edg_lanczos: reorthogonalisation");
   };
   auto enqueue_check = [&](cudaStream_t cs) {
     check_k<NV><<<NV, kThreads, 0, cs>>>(st, alpha, ld_a, beta, ld_b, L.m_max, n, k, p->tol, p->check_every,
@@ -850,13 +1234,7 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
       int st_ = matvec(s);
       if (st_) return st_;
       cudaEventRecord(ev[1], s);
-      dots_bulk_k<T, NV><<<g_dot, edg::bulk::kThreadsAll, dot_smem, s>>>(V, n_pad, st, w, partial, stride_i, n_seg,
-                                                                           err_word);
-      reduce2_coef_k<NV><<<g_red, kThreads, 0, s>>>(partial, (int)n_seg, n_seg, st, hu, hw, alpha, ld_a, beta, ld_b,
-                                                    rc, tickets);
-      update_bulk_k<T, NV><<<g_upd, edg::bulk::kThreadsAll, upd_smem, s>>>(V, n_pad, st, hu, hw, rc, w, normp,
-                                                                             stride_i, wnorm, beta, ld_b, tickets + 1,
-                                                                             n_seg, err_word, X, kXs, n);
+      if ((e = enqueue_reorth(s)) != cudaSuccess) return edg::cuda_status(e, "edg_lanczos: reorthogonalisation");
       cudaEventRecord(ev[2], s);
       enqueue_check(s);
       cudaEventRecord(ev[3], s);
@@ -869,7 +1247,7 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
       t_spmv += a;
       t_reorth += b;
       t_check += c;
-      launches += 5;
+      launches += launches_per_step;
       if (hs.done) break;
     }
     for (auto& x : ev) cudaEventDestroy(x);
@@ -919,7 +1297,7 @@ int run_lanczos(const edg_lanczos_problem* p, char* ws, double* evals, void* eve
     cudaStreamSynchronize(s);
     cudaStreamDestroy(cs);
     if (rc_) return rc_;
-    launches += (int64_t)enq * 5;
+    launches += (int64_t)enq * launches_per_step;
   }
   if ((rc_ = read_state(&hs))) return rc_;
   const int j_end = hs.j;
@@ -997,6 +1375,10 @@ int check_problem(const edg_lanczos_problem* p) {
   EDG_REQUIRE(p->reorth_window >= 0, "edg_lanczos: reorth_window must be >= 0");
   EDG_REQUIRE(p->sell_entries == nullptr || (p->sell_perm && p->sell_width && p->sell_off),
               "edg_lanczos: incomplete SELL layout");
+  EDG_REQUIRE(p->pk_words == nullptr ||
+                  (p->pk_tile_off && p->pk_table && p->pk_count >= 1 && p->pk_count <= EDG_PACK_MAX_VALUES &&
+                   p->pk_colbits >= 1 && p->pk_colbits <= 31 && p->n_rows < ((int64_t)1 << p->pk_colbits)),
+              "edg_lanczos: incomplete or inconsistent packed layout");
   return EDG_OK;
 }
 

@@ -143,6 +143,11 @@ class LanczosProblem(C.Structure):
         ("sell_off", P),
         ("sell_entries", P),
         ("reorth_window", I32),
+        ("pk_tile_off", P),
+        ("pk_words", P),
+        ("pk_table", P),
+        ("pk_count", I32),
+        ("pk_colbits", I32),
     ]
 
 
@@ -296,6 +301,11 @@ _SIGS = {
     "edg_sell_fill": (I32, [I32, P, P, P, I64, P, P, P, P, P]),
     "edg_spmv_sell": (I32, [I64, I32, P, P, P, P, P, P, I32, P, I64, P]),
     "edg_spmv_f32_planar": (I32, [I64, I64, P, P, P, P, I32, P, I32, P, I64, I32, P]),
+    "edg_pack_collect": (I32, [I32, P, I64, P, I32, P, P]),
+    "edg_pack_tiles": (I64, [I64]),
+    "edg_pack_tile_counts": (I32, [I64, P, P, P]),
+    "edg_pack_encode": (I32, [I32, I64, I64, P, P, P, P, I32, I32, P, P, P, P, P]),
+    "edg_spmv_packed": (I32, [I32, I64, I32, P, P, P, I32, I32, P, P, I32, P, I64, P, P]),
     "edg_spmv_group": (I32, [I32, I64, I64, P, P, P, P, I32, P, P, I32, P]),
     "edg_lanczos_workspace_bytes": (I64, [C.POINTER(LanczosProblem)]),
     "edg_lanczos": (I32, [C.POINTER(LanczosProblem), P, I64, P, P, P, P, P]),

@@ -22,8 +22,8 @@ import torch
 from . import _lib
 from ._lib import check, lib, ptr, stream_handle
 
-__all__ = ["LanczosResult", "SellLayout", "lanczos", "lanczos_mixed", "sell_layout", "stack_diagonals",
-           "tune_matvec32", "tune_spmv_group"]
+__all__ = ["LanczosResult", "PackedLayout", "SellLayout", "lanczos", "lanczos_mixed", "packed_layout", "sell_layout",
+           "stack_diagonals", "tune_matvec32", "tune_spmv_group"]
 
 SPMV_GROUPS = (2, 4, 8, 16, 32)
 
@@ -132,22 +132,122 @@ def sell_layout(mat, vals32=None, window=32):
 
 SELL_WINDOWS = (32, 256, 4096)
 
+PACK_MAX_VALUES = 4096  # EDG_PACK_MAX_VALUES
+_PACK_LOG2_SLOTS = 14  # hash set of the distinct values (4x the table limit)
+
+
+class PackedLayout:
+    """Dictionary-packed tiled copy of a matrix's off-diagonal part
+    (``edg_pack_collect`` / ``edg_pack_tile_counts`` / ``edg_pack_encode``):
+    one 32-bit word per entry, ``column | (value index << colbits)``, the
+    distinct values in an ascending table -- ``table64`` (the f64 values) and
+    ``table32`` (the same values rounded to f32, so that entry i's f32 value
+    is ``vals.to(float32)[i]``) -- and the rows in tiles of 16, each tile as
+    wide as its longest row and stored k-major (``tile_off`` [n_tiles+1];
+    padding words all ones).  The lattice models' Hamiltonians have a handful
+    of distinct off-diagonal values, so the entry stream is 4 bytes an entry
+    plus the tiles' padding.  ``PackedLayout.build`` returns None for a
+    matrix with too many distinct values or too many words."""
+
+    TILE_ROWS = 16
+
+    def __init__(self, n, nnz, tile_off, words, total, table64, colbits):
+        self.n, self.nnz, self.total = n, nnz, int(total)
+        self.tile_off, self.words = tile_off, words
+        self.table64 = table64
+        self.table32 = table64.to(torch.float32)
+        self.count = int(table64.numel())
+        self.colbits = int(colbits)
+
+    def table(self, dtype):
+        return self.table32 if dtype == 1 else self.table64
+
+    @classmethod
+    def build(cls, mat):
+        if mat.is_complex or mat.n == 0 or mat.nnz == 0:
+            return None
+        dev = mat.rowptr.device
+        st = stream_handle()
+        colbits = max(1, int(mat.n).bit_length())  # n < 2^colbits: the all-ones column marks padding
+        if colbits > 31:
+            return None
+        vals = mat.vals.to(torch.float64).contiguous()
+        slots = torch.full((1 << _PACK_LOG2_SLOTS,), -1, dtype=torch.int64, device=dev)
+        flags = torch.zeros(2, dtype=torch.int32, device=dev)
+        check(lib.edg_pack_collect(0, ptr(vals), mat.nnz, ptr(slots), _PACK_LOG2_SLOTS, ptr(flags), st),
+              "edg_pack_collect")
+        host = slots.cpu().numpy()
+        if int(flags[0].item()):
+            return None
+        bits = np.unique(host[host != -1])
+        # ascending values; -0.0 before +0.0 (they compare equal, the bits differ)
+        uniq = bits.view(np.float64)[np.lexsort((bits, bits.view(np.float64)))]
+        count = int(uniq.size)
+        if count > PACK_MAX_VALUES or (count - 1) >> (32 - colbits):
+            return None
+        n_tiles = int(lib.edg_pack_tiles(mat.n))
+        counts = torch.empty(n_tiles, dtype=torch.int64, device=dev)
+        offsets = torch.empty(n_tiles + 1, dtype=torch.int64, device=dev)
+        check(lib.edg_pack_tile_counts(mat.n, ptr(mat.rowptr), ptr(counts), st), "edg_pack_tile_counts")
+        scratch = torch.empty(max(1, lib.edg_scan_scratch_elems(n_tiles)), dtype=torch.int64, device=dev)
+        check(lib.edg_scan_i64(ptr(counts), ptr(offsets), n_tiles, ptr(scratch), st), "edg_scan_i64")
+        total = int(offsets[n_tiles].item())
+        if total >= 2**31 - 8:
+            return None
+        table64 = torch.from_numpy(np.ascontiguousarray(uniq)).to(dev)
+        tile_off = torch.empty(n_tiles + 1, dtype=torch.int32, device=dev)
+        words = torch.empty(total + 4, dtype=torch.int32, device=dev)
+        check(lib.edg_pack_encode(0, mat.n, total, ptr(mat.rowptr), ptr(mat.cols), ptr(vals), ptr(table64), count,
+                                  colbits, ptr(offsets), ptr(tile_off), ptr(words), ptr(flags[1:]), st),
+              "edg_pack_encode")
+        if int(flags[1].item()):
+            raise _lib.EdgError(-1, "edg_pack_encode: a value is missing from the table")
+        return cls(mat.n, mat.nnz, tile_off, words, total, table64, colbits)
+
+    @property
+    def stream_bytes(self):
+        """Bytes of the entry stream (padding included) and the tile offsets."""
+        return 4 * self.total + 4 * self.tile_off.numel()
+
+    @property
+    def padding(self):
+        """Fraction of the stream's words that are tile padding."""
+        return 1.0 - self.nnz / max(self.total, 1)
+
+    def launch(self, dtype, nvec, diag, x, x_stride, y, y_plane=0, err=None):
+        """y (f64, planar [nvec][y_plane]) = (A + diag) x (``edg_spmv_packed``)."""
+        check(lib.edg_spmv_packed(dtype, self.n, nvec, ptr(self.tile_off), ptr(self.words), ptr(self.table(dtype)),
+                                  self.count, self.colbits, ptr(diag), ptr(x), x_stride, ptr(y), y_plane or self.n,
+                                  ptr(err) if err is not None else None, stream_handle()), "edg_spmv_packed")
+
+
+def packed_layout(mat):
+    """The matrix's dictionary-packed layout (built once, kept on the matrix),
+    or None when the matrix does not pack."""
+    if not hasattr(mat, "_packed"):
+        mat._packed = PackedLayout.build(mat)
+    return mat._packed
+
 
 def tune_matvec32(mat, nvec, vals32=None, reps=5, ctx=None):
     """Autotuner of the f32 Krylov path's matvec: times, in that path's
     configuration (f32 values and x with padded rows, f64 planar output),
-    the CSR kernel for every threads-per-row choice and the SELL kernel for
-    every sort window (CUDA events after a warm-up launch), and keeps the
-    fastest in the tuning context under the matrix shape.  Returns
-    ("csr", threads per row) or ("sell", window)."""
+    the CSR kernel for every threads-per-row choice, the SELL kernel for
+    every sort window and the dictionary-packed kernel when the matrix packs
+    (CUDA events after a warm-up launch), and keeps the fastest in the
+    tuning context under the matrix shape.  Returns ("csr", threads per
+    row), ("sell", window) or ("packed", 2)."""
     from .context import default_context
 
     ctx = ctx if ctx is not None else default_context(mat.rowptr.device)
     key = _spmv_key(mat.n, mat.nnz, 0x5E11, nvec)
     got = ctx.get(key, 2)
-    if got is not None:
-        return ("sell", got[1]) if got[0] == 1 else ("csr", got[1])
+    names = {0: "csr", 1: "sell", 2: "packed"}
+    if got is not None and (got[0] != 2 or packed_layout(mat) is not None):
+        return (names[got[0]], got[1])
     dev = mat.rowptr.device
+    # the packed layout's f32 table holds the f64 values rounded to f32
+    vals32_is_rounded = vals32 is None or bool(torch.equal(vals32, mat.vals.to(torch.float32)))
     vals32 = mat.vals.to(torch.float32) if vals32 is None else vals32
     xs = 4 if nvec == 3 else nvec
     diag = torch.zeros((mat.n, nvec), dtype=torch.float32, device=dev)
@@ -179,10 +279,15 @@ def tune_matvec32(mat, nvec, vals32=None, reps=5, ctx=None):
                                                  stream_handle()), "edg_spmv_sell"))
         if t < best_t:
             best, best_t = ("sell", wdw), t
+    pk = packed_layout(mat) if vals32_is_rounded else None
+    if pk is not None:
+        t = t_of(lambda: pk.launch(1, nvec, diag, x, xs, y, mat.n))
+        if t < best_t:
+            best, best_t = ("packed", 2), t
     # layouts that lost are not kept on the matrix
     keep = best[1] if best[0] == "sell" else None
-    mat._sell32 = {w: l for w, l in mat._sell32.items() if w == keep}
-    ctx.put(key, (1 if best[0] == "sell" else 0, best[1]))
+    mat._sell32 = {w: l for w, l in getattr(mat, "_sell32", {}).items() if w == keep}
+    ctx.put(key, ({"csr": 0, "sell": 1, "packed": 2}[best[0]], best[1]))
     return best
 
 
@@ -195,7 +300,7 @@ class LanczosResult:
 
 
 def _problem(dtype, n, nnz, rowptr, cols, vals, diag, nvec, k, max_iter, tol, check_every, seed, v0, stats=None,
-             group=0, sell=None, window=0):
+             group=0, sell=None, window=0, packed=None):
     p = _lib.LanczosProblem()
     p.dtype = dtype
     p.n_rows = n
@@ -217,6 +322,9 @@ def _problem(dtype, n, nnz, rowptr, cols, vals, diag, nvec, k, max_iter, tol, ch
         p.sell_perm, p.sell_width, p.sell_off = ptr(sell.perm), ptr(sell.width), ptr(sell.off)
         p.sell_entries = ptr(sell.entries)
     p.reorth_window = int(window)
+    if packed is not None:
+        p.pk_tile_off, p.pk_words = ptr(packed.tile_off), ptr(packed.words)
+        p.pk_table, p.pk_count, p.pk_colbits = ptr(packed.table(dtype)), packed.count, packed.colbits
     return p
 
 
@@ -234,7 +342,7 @@ def _progress_words(device):
 
 def run_lanczos(dtype, n, nnz, rowptr, cols, vals, diag, nvec=1, k=1, max_iter=300, tol=1e-12, check_every=5,
                 seed=1234, v0=None, want_vectors=True, allow_unconverged=False, workspace=None, stats=None,
-                group=0, poll_host=True, sell=None, window=0):
+                group=0, poll_host=True, sell=None, window=0, packed=None):
     """Low-level call of ``edg_lanczos``; ``diag`` is ``[n][nvec]`` in the dtype.
 
     ``stats``: optional float64 numpy array of 6 entries filled with the
@@ -245,10 +353,12 @@ def run_lanczos(dtype, n, nnz, rowptr, cols, vals, diag, nvec=1, k=1, max_iter=3
     ``sell``: a :class:`SellLayout` of the matrix (f32 path only) for the
     matvec.  ``window``: 0 for full reorthogonalisation, W > 0 to
     orthogonalise each step against the last W Krylov vectors only.
+    ``packed``: a :class:`PackedLayout` of the matrix for the matvec (its
+    table in the call's dtype; either dtype).
     """
     max_iter = int(min(max_iter, n))
     p = _problem(dtype, n, nnz, rowptr, cols, vals, diag, nvec, k, max_iter, tol, check_every, seed, v0, stats,
-                 group, sell if dtype == 1 else None, window)
+                 group, sell if dtype == 1 else None, window, packed)
     progress = _progress_words(rowptr.device) if poll_host else None
     p.host_progress = progress.data_ptr() if poll_host else None
     wb = lib.edg_lanczos_workspace_bytes(ctypes.byref(p))
@@ -287,7 +397,7 @@ def stack_diagonals(diags, dtype):
 
 def lanczos_mixed(mat, diags=None, k=1, tol32=1e-4, tol=1e-12, max_iter=400, refine_iter=5, check_every=5,
                   seed=1234, stats32=None, stats64=None, vals32=None, diag32=None, diag64=None, tune=True,
-                  group32=0, group64=0, sell=None, window32=4):
+                  group32=0, group64=0, sell=None, window32=4, packed=None):
     """Mixed-precision (f32 Krylov, f64 recurrence) Lanczos + f64 refinement.
 
     ``diags``: list of f64 device diagonals (one per problem, <= 4) sharing the
@@ -315,22 +425,25 @@ def lanczos_mixed(mat, diags=None, k=1, tol32=1e-4, tol=1e-12, max_iter=400, ref
         diag32 = stack_diagonals(diags, torch.float32)
     if diag64 is None:
         diag64 = stack_diagonals(diags, torch.float64)
-    if sell is None and tune and not group32:
+    if sell is None and packed is None and tune and not group32:
         fmt, param = tune_matvec32(mat, nvec, vals32)
         if fmt == "sell":
             sell = sell_layout(mat, vals32, param)
+        elif fmt == "packed":
+            sell, packed = False, packed_layout(mat)
         else:
             sell, group32 = False, param
     lay = sell_layout(mat, vals32) if sell is True else (sell or None)
-    g32 = group32 or (tune_spmv_group(mat, nvec, 1, vals=vals32) if tune else 0)
-    g64 = group64 or (tune_spmv_group(mat, nvec, 0, vals=mat.vals) if tune else 0)
+    pk = packed_layout(mat) if packed is True else (packed or None)
+    g32 = group32 or (tune_spmv_group(mat, nvec, 1, vals=vals32) if tune and pk is None else 0)
+    g64 = group64 or (tune_spmv_group(mat, nvec, 0, vals=mat.vals) if tune and pk is None else 0)
     r32 = run_lanczos(1, mat.n, mat.nnz, mat.rowptr, mat.cols, vals32, diag32, nvec=nvec, k=k, max_iter=max_iter,
                       tol=tol32, check_every=check_every, seed=seed, stats=stats32, group=g32, sell=lay,
-                      window=window32)
+                      window=window32, packed=pk)
     # f64 refinement: short Lanczos restarted from the f32 Ritz vector (ground state)
     v0 = torch.empty((mat.n, nvec), dtype=torch.float64, device=diag64.device)
     check(lib.edg_convert(1, ptr(r32.evecs), 0, ptr(v0), mat.n * nvec, stream_handle()), "edg_convert")
     r64 = run_lanczos(0, mat.n, mat.nnz, mat.rowptr, mat.cols, mat.vals, diag64, nvec=nvec, k=1,
                       max_iter=refine_iter, tol=tol, check_every=refine_iter, seed=seed, v0=v0,
-                      allow_unconverged=True, stats=stats64, group=g64)
+                      allow_unconverged=True, stats=stats64, group=g64, packed=pk)
     return r64, r32

@@ -321,6 +321,51 @@ int edg_spmv_sell(int64_t n_rows, int32_t nvec, const int32_t* perm,
                   const int32_t* width, const int64_t* off, const void* entries,
                   const float* diag, const float* x, int32_t x_stride,
                   double* y, int64_t y_plane, cudaStream_t stream);
+/* Dictionary-packed tiled layout of the off-diagonal matrix (same product
+ * as csr_spmv, qmb_hamiltonian.py:705-730, with 4 bytes an entry): the model
+ * Hamiltonians have few distinct off-diagonal values, so an entry is the
+ * word col | (value index << colbits), n_rows < 2^colbits, the values in an
+ * ascending table of at most 2^(32 - colbits) and at most
+ * EDG_PACK_MAX_VALUES entries.  Rows are grouped in tiles of 16; tile t is
+ * w_t = its longest row wide, and its 16 w_t words [tile_off[t],
+ * tile_off[t+1]) hold entry k of its row s at tile_off[t] + 16 k + s
+ * (k-major, CSR order inside a row), shorter rows padded with the all-ones
+ * word (its column, 2^colbits - 1, is never a real one).
+ * Build: edg_pack_collect inserts the values' bit patterns (dtype 0 f64, 1
+ * f32) into a caller-owned set of 2^log2_slots slots (8-byte slots for f64,
+ * 4-byte for f32) pre-filled with 0xFF bytes, setting overflow[0] when the
+ * set fills (more distinct values than it holds) or a value is a NaN; the
+ * caller reads the set and sorts the distinct values into the table.
+ * edg_pack_tile_counts writes counts [n_tiles] = 16 w_t (n_tiles =
+ * edg_pack_tiles(n_rows)); their exclusive scan offsets [n_tiles+1]
+ * (edg_scan_i64) gives total = offsets[n_tiles] < 2^31 - 4 words, and
+ * edg_pack_encode writes tile_off [n_tiles+1] (int32) and words [total+4],
+ * setting missing[0] if a value is not in the table.  The matvec (y f64
+ * planar, x rows at x_stride, diag [n_rows][nvec], table, diag and x in the
+ * dtype) stages each tile with one bulk copy: f64 gives the same sums, in
+ * the same order, as the CSR kernel with two threads a row; f32 sums each
+ * half row's products in f32 and the rest in f64.  err (device int, may be
+ * NULL) receives EDG_ERR_TIMEOUT if a stage wait ran out (1 s; y is then
+ * incomplete). */
+#define EDG_PACK_MAX_VALUES 4096
+int64_t edg_pack_tiles(int64_t n_rows);
+int edg_pack_tile_counts(int64_t n_rows, const int64_t* rowptr,
+                         int64_t* counts, cudaStream_t stream);
+int edg_pack_collect(int32_t dtype, const void* vals, int64_t nnz, void* set,
+                     int32_t log2_slots, int32_t* overflow,
+                     cudaStream_t stream);
+int edg_pack_encode(int32_t dtype, int64_t n_rows, int64_t total,
+                    const int64_t* rowptr, const int32_t* cols,
+                    const void* vals, const void* table, int32_t count,
+                    int32_t colbits, const int64_t* offsets,
+                    int32_t* tile_off, uint32_t* words, int32_t* missing,
+                    cudaStream_t stream);
+int edg_spmv_packed(int32_t dtype, int64_t n_rows, int32_t nvec,
+                    const int32_t* tile_off, const uint32_t* words,
+                    const void* table, int32_t count, int32_t colbits,
+                    const void* diag, const void* x, int32_t x_stride,
+                    double* y, int64_t y_plane, int32_t* err,
+                    cudaStream_t stream);
 /* The CSR matvec in the same configuration (f32 values, diagonal and x, f64
  * planar y): the f32 Krylov path's CSR kernel, for layout comparisons. */
 int edg_spmv_f32_planar(int64_t n_rows, int64_t nnz, const int64_t* rowptr,
@@ -383,6 +428,11 @@ typedef struct {
                           /* vectors only (local reorthogonalisation: the  */
                           /* lowest Ritz pair converges as with the full   */
                           /* one, later copies of it are not suppressed)   */
+  const int32_t* pk_tile_off;  /* optional dictionary-packed layout of the  */
+  const uint32_t* pk_words;    /* off-diagonal matrix (edg_pack_*) with its */
+  const void* pk_table;        /* table in the problem dtype; used instead  */
+  int32_t pk_count;            /* of the CSR (and SELL) arrays when         */
+  int32_t pk_colbits;          /* pk_words is not NULL                      */
 } edg_lanczos_problem;
 
 /* Bytes of device workspace edg_lanczos needs. */
