@@ -59,10 +59,13 @@ MASS = 0.5
 WINDOW32 = 4  # local reorthogonalisation window of the f32 phase (the f64 refinement is full)
 METRIC = "Lanczos GS time-to-solution & matvec GB/s: mixed/batched vs plain FP64 GPU at 1e-9 rel."
 # DRAM traffic of the headline kernels from one ncu capture each on this
-# workload (summaries kept under profiles/): both reorthogonalisation passes at step 30
-# moved 495.07 + 526.08 MB against 488.05 + 532.40 MB algorithmic; one CSR
-# matvec launch (2 lanes a row) moved 179.21 + 21.61 MB
-REORTH_TRAFFIC_RATIO = (495.07 + 526.08) / (488.05 + 532.40)
+# workload (summaries kept under profiles/): the one-launch reorthogonalisation
+# of a full window (5 vectors) moved 146.00 + 15.95 MB against 251.42 MB
+# algorithmic (its update phase re-reads the dots phase's rows from L2); one
+# dictionary-packed matvec launch moved 112.87 + 14.91 MB; one CSR matvec
+# launch (2 lanes a row) moved 179.21 + 21.61 MB
+REORTH_TRAFFIC_RATIO = (146.00 + 15.95) / 251.42
+PACKED_MATVEC_TRAFFIC_BYTES = (112.87 + 14.91) * 1e6
 MATVEC_TRAFFIC_BYTES = (179.21 + 21.61) * 1e6
 UNIT = "ground_states/s"
 WORKLOAD = (f"SU(2) 1D Yang-Mills + staggered matter, j_max=1/2, {'periodic' if PBC else 'open'} chain L={L}, "
@@ -510,17 +513,17 @@ def run_edgpu(args, world, rank, local):
                                "f64_steps": agg64[4],
                                "source": "one instrumented sweep (CUDA events around every phase of every step)"},
         "setup_phases": phases_setup,
-        "roofline": {"kernel": "f32 delayed Gram-Schmidt reorthogonalisation (dots_bulk_k<float,3> + "
-                               "update_bulk_k<float,3>: the Krylov basis streamed through a shared-memory ring of "
-                               "bulk copies, two reads of the basis per Lanczos step)",
+        "roofline": {"kernel": f"f32 delayed Gram-Schmidt reorthogonalisation over a window of {WINDOW32} vectors "
+                               "(reorth_small_k<float,3,5>: one cooperative launch per Lanczos step -- dots, grid "
+                               "barrier, coefficients in every CTA, update in reverse row order)",
                      "bound": "hbm",
                      "achieved": reorth_achieved, "peak": hbm, "unit": "GB/s", "frac": reorth_achieved / hbm,
                      "peak_source": peak_kind, "algorithmic_bytes_per_solve": reorth_bytes,
                      "ms_per_solve": reorth_ms_step, "ms_per_lanczos_step": reorth_ms,
                      "traffic": REORTH_TRAFFIC_RATIO * reorth_bytes,
-                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of both passes at step 30 "
-                                       f"of this workload = {REORTH_TRAFFIC_RATIO:.4f} x their algorithmic bytes, "
-                                       "applied per solve"},
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch with a "
+                                       f"full window on this workload = {REORTH_TRAFFIC_RATIO:.4f} x its algorithmic "
+                                       "bytes (L2 reuse between its phases), applied per solve"},
         "roofline_matvec": {"kernel": ("batched f32 SELL-32-sigma + diag matvec (sell_spmv_k<float,3,4>), "
                                        f"sort window {sell32.window}, slice padding {sell32.padding:.3f} of the "
                                        "stored pairs"
@@ -534,10 +537,12 @@ def run_edgpu(args, world, rank, local):
                             "bound": "hbm", "achieved": spmv_achieved, "peak": hbm, "unit": "GB/s",
                             "frac": spmv_achieved / hbm, "peak_source": peak_kind,
                             "algorithmic_bytes_per_launch": spmv_bytes, "avg_launch_ms": spmv_ms,
-                            "traffic": (MATVEC_TRAFFIC_BYTES if fmt32 == "csr" and g32 == 2 and n == 1232454
+                            "traffic": (PACKED_MATVEC_TRAFFIC_BYTES if fmt32 == "packed" and n == 1232454 else
+                                        MATVEC_TRAFFIC_BYTES if fmt32 == "csr" and g32 == 2 and n == 1232454
                                         else None),
                             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of "
-                                              "spmv_k<float, float, double, 3, 2, 4> on this matrix"},
+                                              + ("packed_spmv_k<float, 3, 4>" if fmt32 == "packed" else
+                                                 "spmv_k<float, float, double, 3, 2, 4>") + " on this matrix"},
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                 "ms_per_step": float(np.mean(e2e_ms)), "steps": len(e2e_ms)},
         "gpu_launches": launches,

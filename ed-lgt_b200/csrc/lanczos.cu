@@ -743,7 +743,7 @@ __global__ void __launch_bounds__(kSmallThreads) reorth_small_k(
     const int64_t first = (int64_t)blockIdx.x * kSmallThreads + tid;
     const int64_t q_last = first < nq ? first + ((nq - 1 - first) / S) * S : -1;
     for (int64_t q = q_last; q >= 0; q -= S) {
-      double xo[NV][4];
+      T xo[NV][4];  // the next candidate's rows of X, as stored
 #pragma unroll
       for (int v = 0; v < NV; ++v) {
         T* U = V + (int64_t)j * stride_i + (int64_t)v * n_pad + 4 * q;
@@ -777,7 +777,7 @@ __global__ void __launch_bounds__(kSmallThreads) reorth_small_k(
           w4[e] = fma(-q4[e], c, w4[e]);
           sq = fma(w4[e], w4[e], sq);
           w4[e] *= ri;
-          xo[v][e] = w4[e];
+          xo[v][e] = (T)w4[e];
         }
         st4(U, q4);
         st4(U + stride_i, w4);
@@ -790,11 +790,11 @@ __global__ void __launch_bounds__(kSmallThreads) reorth_small_k(
         if (xs == 4) {
           double row[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-          for (int v = 0; v < NV && v < 4; ++v) row[v] = xo[v][e];
+          for (int v = 0; v < NV && v < 4; ++v) row[v] = (double)xo[v][e];
           st4(X + r * 4, row);
         } else {
 #pragma unroll
-          for (int v = 0; v < NV; ++v) X[r * xs + v] = (T)xo[v][e];
+          for (int v = 0; v < NV; ++v) X[r * xs + v] = xo[v][e];
         }
       }
     }
