@@ -60,13 +60,21 @@ struct Pat<double> {
 };
 
 // Distinct bit patterns of vals into an open-addressing set of 2^log2_slots
-// slots (pre-filled with 0xFF bytes).  A plain read first, so the atomics
-// only happen for values not yet present.  overflow[0] is set when a probe
-// sequence runs past max_probe slots or a value is a NaN.
+// slots (pre-filled with 0xFF bytes).  Each CTA first records the values in
+// a small shared-memory set and only the first of its threads to meet a
+// value probes the global set (a matrix has a handful of values, so without
+// this millions of probes would hit the same few global words); a plain read
+// comes before any atomic.  overflow[0] is set when a global probe sequence
+// runs past max_probe slots or a value is a NaN.
 template <typename T>
 __global__ void pack_collect_k(const T* __restrict__ vals, int64_t nnz, typename Pat<T>::U* __restrict__ set,
                                int log2_slots, int max_probe, int* __restrict__ overflow) {
   using U = typename Pat<T>::U;
+  constexpr int kLocalBits = 8;  // CTA-local set of 256 slots
+  constexpr int kLocalProbe = 16;
+  __shared__ U local[1 << kLocalBits];
+  for (int i = threadIdx.x; i < (1 << kLocalBits); i += blockDim.x) local[i] = Pat<T>::kEmpty;
+  __syncthreads();
   const uint32_t mask = (1u << log2_slots) - 1u;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nnz; i += (int64_t)gridDim.x * blockDim.x) {
     const T v = __ldg(vals + i);
@@ -75,6 +83,23 @@ __global__ void pack_collect_k(const T* __restrict__ vals, int64_t nnz, typename
       atomicExch(overflow, 1);
       continue;
     }
+    // CTA-local set: a value found there has been (or is being) inserted
+    // into the global set by the thread that recorded it
+    bool seen = false;
+    uint32_t ls = Pat<T>::hash(b) >> (32 - kLocalBits);
+    for (int probe = 0; probe < kLocalProbe; ++probe, ls = (ls + 1) & ((1u << kLocalBits) - 1)) {
+      U cur = *(volatile U*)(local + ls);
+      if (cur == b) {
+        seen = true;
+        break;
+      }
+      if (cur == Pat<T>::kEmpty) {
+        cur = atomicCAS(local + ls, Pat<T>::kEmpty, b);
+        if (cur == b) seen = true;
+        if (cur == Pat<T>::kEmpty || cur == b) break;
+      }
+    }
+    if (seen) continue;
     uint32_t s = Pat<T>::hash(b) >> (32 - log2_slots);
     bool placed = false;
     for (int probe = 0; probe < max_probe; ++probe, s = (s + 1) & mask) {

@@ -170,18 +170,26 @@ def _offdiag_tables(blocks, phase_weights, force_complex, dmax):
                 coef = np.conj(b.strength) if dag else b.strength
                 terms.append((tuple(int(s) for s in inst), tuple(tabs), complex(coef)))
     real_ok, tables_real, coefs_real = False, None, None
-    if not force_complex:
-        tabs_t, phases, ok = [], [], True
-        for t, m in enumerate(raw_tables):
-            if phase_weights is not None:
-                phi = _phase_vec(phase_weights[table_site[t]])
-                m = np.conj(phi)[:, None] * m * phi[None, :]
-            ph = _uniform_phase(m)
-            if ph is None:
-                ok = False
-                break
-            tabs_t.append((m / ph).real)
-            phases.append(ph)
+    if not force_complex and raw_tables:
+        # every table at once: gauge-transform, then its common phase (the
+        # phase of its largest entry above OP_TOL, the first in row-major
+        # order), as _uniform_phase does table by table
+        M = np.stack(raw_tables)
+        if phase_weights is not None:
+            phi = _phase_vec(np.asarray(phase_weights)[np.asarray(table_site)])  # (nt, d)
+            M = np.conj(phi)[:, :, None] * M * phi[:, None, :]
+        mag = np.abs(M)
+        keep = mag > OP_TOL
+        flat = np.where(keep, mag, -1.0).reshape(len(raw_tables), -1)
+        big = np.take_along_axis(M.reshape(len(raw_tables), -1), flat.argmax(axis=1)[:, None], axis=1)[:, 0]
+        ph = np.where(keep.reshape(len(raw_tables), -1).any(axis=1), big / np.where(big == 0, 1.0, np.abs(big)),
+                      1.0 + 0.0j)
+        rot = M / ph[:, None, None]
+        bad = keep & (np.abs(rot.imag) > 1e-12 * np.maximum(1.0, np.abs(rot)))
+        ok = not bad.any()
+        if ok:
+            tabs_t = list(rot.real)
+            phases = list(ph)
         if ok:
             cr = []
             for sites, tabs, coef in terms:
@@ -198,37 +206,47 @@ def _offdiag_tables(blocks, phase_weights, force_complex, dmax):
 
 
 def _table_arrays(raw_tables, terms, dmax, is_complex, tables_real, coefs_real):
+    """Device table arrays: per table and bra the kets whose |amplitude| >
+    OP_TOL in ascending order (t_count, t_ket, t_amp, zero beyond the
+    count), and the instance records (term_nops, term_site, term_table,
+    term_coef).  Vectorised over all tables at once."""
     nt = max(len(raw_tables), 1)
     t_count = np.zeros((nt, dmax), dtype=np.int32)
     t_ket = np.zeros((nt, dmax, dmax), dtype=np.uint8)
     t_amp = np.zeros((nt, dmax, dmax, 2 if is_complex else 1), dtype=np.float64)
-    for t, m0 in enumerate(raw_tables):
-        mags = np.abs(m0)
-        m = m0 if is_complex else tables_real[t]
-        for bra in range(dmax):
-            kets = np.nonzero(mags[bra] > OP_TOL)[0]
-            t_count[t, bra] = len(kets)
-            t_ket[t, bra, : len(kets)] = kets
-            if is_complex:
-                t_amp[t, bra, : len(kets), 0] = m[bra, kets].real
-                t_amp[t, bra, : len(kets), 1] = m[bra, kets].imag
-            else:
-                t_amp[t, bra, : len(kets), 0] = m[bra, kets]
+    if raw_tables:
+        mags = np.abs(np.stack([np.asarray(m, dtype=np.complex128) for m in raw_tables]))[:, :dmax, :dmax]
+        vals = np.stack(raw_tables if is_complex else [np.asarray(m) for m in tables_real])[:, :dmax, :dmax]
+        keep = mags > OP_TOL
+        k = mags.shape[-1]
+        order = np.argsort(~keep, axis=-1, kind="stable")  # kept kets first, ascending
+        cnt = keep.sum(axis=-1)
+        valid = np.arange(k)[None, None, :] < cnt[..., None]
+        t_count[:, : mags.shape[1]] = cnt
+        t_ket[:, : mags.shape[1], :k] = np.where(valid, order, 0)
+        picked = np.take_along_axis(vals, order, axis=-1)
+        if is_complex:
+            t_amp[:, : mags.shape[1], :k, 0] = np.where(valid, picked.real, 0.0)
+            t_amp[:, : mags.shape[1], :k, 1] = np.where(valid, picked.imag, 0.0)
+        else:
+            t_amp[:, : mags.shape[1], :k, 0] = np.where(valid, np.real(picked), 0.0)
     n_terms = len(terms)
     term_nops = np.zeros(max(n_terms, 1), dtype=np.int32)
     term_site = np.zeros((max(n_terms, 1), _lib.MAX_OPS), dtype=np.int32)
     term_table = np.zeros((max(n_terms, 1), _lib.MAX_OPS), dtype=np.int32)
     term_coef = np.zeros((max(n_terms, 1), 2 if is_complex else 1), dtype=np.float64)
-    for k, (sites, tabs, coef) in enumerate(terms):
+    for k_, (sites, tabs, coef) in enumerate(terms):
         if len(sites) > _lib.MAX_OPS:
             raise ValueError(f"at most {_lib.MAX_OPS} operator factors per term instance")
-        term_nops[k] = len(sites)
-        term_site[k, : len(sites)] = sites
-        term_table[k, : len(tabs)] = tabs
+        term_nops[k_] = len(sites)
+        term_site[k_, : len(sites)] = sites
+        term_table[k_, : len(tabs)] = tabs
+    if n_terms:
         if is_complex:
-            term_coef[k] = (coef.real, coef.imag)
+            c = np.array([t[2] for t in terms], dtype=np.complex128)
+            term_coef[:n_terms, 0], term_coef[:n_terms, 1] = c.real, c.imag
         else:
-            term_coef[k, 0] = coefs_real[k]
+            term_coef[:n_terms, 0] = coefs_real
     return [t_count, t_ket, t_amp, term_nops, term_site, term_table, term_coef]
 
 
