@@ -212,3 +212,33 @@ def test_mixed_lanczos_on_packed_matches_reference(golden_small):
     assert abs(r_pk.evals[0, 0] / model.n_sites - ref) <= 1e-9 * abs(ref)
     assert abs(r_pk.evals[0, 0] - r_csr.evals[0, 0]) <= 1e-9 * abs(r_csr.evals[0, 0])
     assert r32.iters[0] > 5
+
+
+@pytest.mark.parametrize("window32,refine_iter", [(4, 5), (6, 8), (7, 6), (0, 5)])
+@pytest.mark.parametrize("packed", [True, False])
+def test_short_window_reorthogonalisation_matches_reference(golden_small, window32, refine_iter, packed):
+    """The one-launch reorthogonalisation of short windows, both of its
+    instantiations (up to 5 and up to 8 vectors: windows 4, 6 and 7 of the
+    f32 phase; refinements of 5, 6 and 8 f64 steps), against the reference's
+    ground-state energy (1e-9 relative) on the SU(2) L=10 periodic chain with
+    three couplings; window 0 runs the f32 phase through the ring passes."""
+    import torch
+
+    from edgpu.solvers import lanczos_mixed, stack_diagonals
+
+    model = _model("su2_1d_L10_pbc", "cuda")
+    mat = model.H.mat
+    r64, r32 = lanczos_mixed(mat, window32=window32, refine_iter=refine_iter, sell=False, packed=packed or None,
+                             group32=0 if packed else 2)
+    ref = golden_small["su2_1d_L10_pbc/energies"][0]
+    assert abs(r64.evals[0, 0] / model.n_sites - ref) <= 1e-9 * abs(ref)
+    # a batch of three diagonals (couplings) sharing the off-diagonal part
+    d = mat.diag
+    diags = [d, d + 0.25 * torch.ones_like(d), d - 0.5 * torch.ones_like(d)]
+    rb, _ = lanczos_mixed(mat, diags=diags, window32=window32, refine_iter=refine_iter, sell=False,
+                          packed=packed or None, group32=0 if packed else 2)
+    e = rb.evals[:, 0]
+    assert abs(e[0] - r64.evals[0, 0]) <= 1e-9 * abs(e[0])
+    # a constant shift of the diagonal shifts the ground-state energy by it
+    assert abs((e[1] - e[0]) - 0.25) <= 1e-9 * abs(e[0])
+    assert abs((e[2] - e[0]) + 0.5) <= 1e-9 * abs(e[0])
