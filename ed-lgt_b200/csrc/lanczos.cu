@@ -675,21 +675,37 @@ __global__ void __launch_bounds__(kSmallThreads) reorth_small_k(
     double acc[2 * kSmallMax];
 #pragma unroll
     for (int t = 0; t < 2 * kSmallMax; ++t) acc[t] = 0.0;
-    for (int64_t q = (int64_t)b * kSmallThreads + tid; q < nq; q += (int64_t)G * kSmallThreads) {
-      Raw4<T> x[KV], u;
-      Raw4<double> ww;
-      u.ld(U + 4 * q);
-      ww.ld(wv + 4 * q);
+    // two row quads per iteration (q and q + S) with all their loads in
+    // flight (the update phase sets the kernel's registers; this phase fits
+    // twice its loads in them); quads summed in the order q, q + S, ...
+    const int64_t S = (int64_t)G * kSmallThreads;
+    for (int64_t q = (int64_t)b * kSmallThreads + tid; q < nq; q += 2 * S) {
+      Raw4<T> x[2][KV], u[2];
+      Raw4<double> ww[2];
 #pragma unroll
-      for (int t = 0; t < KV; ++t)
-        if (t < n_vec) x[t].ld(Vv + (int64_t)t * stride_i + 4 * q);
+      for (int h = 0; h < 2; ++h) {
+        const int64_t qq = q + h * S;
+        if (h == 0 || qq < nq) {
+          u[h].ld(U + 4 * qq);
+          ww[h].ld(wv + 4 * qq);
 #pragma unroll
-      for (int t = 0; t < KV; ++t)
-        if (t < n_vec) {
-          acc[2 * t] = fma(x[t][0], u[0], fma(x[t][1], u[1], fma(x[t][2], u[2], fma(x[t][3], u[3], acc[2 * t]))));
-          acc[2 * t + 1] =
-              fma(x[t][0], ww[0], fma(x[t][1], ww[1], fma(x[t][2], ww[2], fma(x[t][3], ww[3], acc[2 * t + 1]))));
+          for (int t = 0; t < KV; ++t)
+            if (t < n_vec) x[h][t].ld(Vv + (int64_t)t * stride_i + 4 * qq);
         }
+      }
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        if (h == 1 && q + S >= nq) break;
+#pragma unroll
+        for (int t = 0; t < KV; ++t)
+          if (t < n_vec) {
+            const Raw4<T>& xt = x[h][t];
+            acc[2 * t] =
+                fma(xt[0], u[h][0], fma(xt[1], u[h][1], fma(xt[2], u[h][2], fma(xt[3], u[h][3], acc[2 * t]))));
+            acc[2 * t + 1] = fma(xt[0], ww[h][0],
+                                 fma(xt[1], ww[h][1], fma(xt[2], ww[h][2], fma(xt[3], ww[h][3], acc[2 * t + 1]))));
+          }
+      }
     }
     const int idx = ((lane >> 4) & 1) * 8 + ((lane >> 3) & 1) * 4 + ((lane >> 2) & 1) * 2 + ((lane >> 1) & 1);
     const double sum = warp_reduce_scatter16(acc);
