@@ -18,6 +18,7 @@ __all__ = ["lib", "check", "EdgError", "MAX_SITES", "MAX_OPS", "SectorTables", "
 
 MAX_SITES = 64
 MAX_OPS = 4
+PACK_MAX_VALUES = 4096  # EDG_PACK_MAX_VALUES
 ZN_MAX_SITES = 14
 ZN_MAX_GROUP = 32
 

@@ -132,7 +132,7 @@ def sell_layout(mat, vals32=None, window=32):
 
 SELL_WINDOWS = (32, 256, 4096)
 
-PACK_MAX_VALUES = 4096  # EDG_PACK_MAX_VALUES
+PACK_MAX_VALUES = _lib.PACK_MAX_VALUES
 _PACK_LOG2_SLOTS = 14  # hash set of the distinct values (4x the table limit)
 
 

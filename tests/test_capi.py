@@ -141,3 +141,60 @@ def test_tiled_batch_plan():
                                          ctypes.byref(n_items), ctypes.byref(wb)) == -1
     assert _lib.lib.edg_tiled_batch_plan(5, dims.ctypes.data, 1, 120, 9, 256, 8, None, None, None,
                                          ctypes.byref(n_items), ctypes.byref(wb)) == -1
+
+
+def test_packed_layout_argument_checks():
+    """The dictionary-packed layout's entry points refuse bad shapes on the
+    host, before any device work (status EDG_ERR_ARG and a message)."""
+    from edgpu import _lib
+
+    L = _lib.lib
+    assert L.edg_pack_tiles(0) == 0 and L.edg_pack_tiles(16) == 1 and L.edg_pack_tiles(17) == 2
+    assert L.edg_pack_tiles(-1) == -1
+    assert L.edg_pack_tile_counts(-1, None, None, None) == -1
+    assert "negative" in _lib.last_error()
+    # the value set: dtype, slot count, null pointers
+    assert L.edg_pack_collect(2, None, 10, 1, 10, 1, None) == -1
+    assert L.edg_pack_collect(1, None, 10, 1, 30, 1, None) == -1 and "log2_slots" in _lib.last_error()
+    assert L.edg_pack_collect(1, None, 10, None, 10, None, None) == -1
+    # encode: the column bits must leave room for the all-ones padding column
+    assert L.edg_pack_encode(0, 16, 100, 1, 1, 1, 1, 4, 4, 1, 1, 1, 1, None) == -1
+    assert "padding column" in _lib.last_error()
+    # encode: more values than the index bits hold (5 column bits leave 27)
+    # or than the table limit
+    assert L.edg_pack_encode(0, 16, 100, 1, 1, 1, 1, _lib.PACK_MAX_VALUES + 1, 5, 1, 1, 1, 1, None) == -1
+    assert L.edg_pack_encode(0, 16, 100, 1, 1, 1, 1, 9, 30, 1, 1, 1, 1, None) == -1
+    assert "index bits" in _lib.last_error()
+    assert L.edg_pack_encode(0, 16, 2**31, 1, 1, 1, 1, 4, 5, 1, 1, 1, 1, None) == -1
+    # matvec: dtype, nvec, x stride, colbits, table size, null pointers
+    args = dict(tile_off=1, words=1, table=1, count=4, colbits=5, diag=1, x=1, xs=3, y=1)
+
+    def mv(dtype=1, n=16, nvec=3, **kw):
+        a = {**args, **kw}
+        return L.edg_spmv_packed(dtype, n, nvec, a["tile_off"], a["words"], a["table"], a["count"], a["colbits"],
+                                 a["diag"], a["x"], a["xs"], a["y"], 0, None, None)
+
+    assert mv(dtype=2) == -1
+    assert mv(nvec=5) == -1
+    assert mv(xs=5) == -1 and "x_stride" in _lib.last_error()
+    assert mv(n=32) == -1 and "colbits" in _lib.last_error()
+    assert mv(count=0) == -1
+    assert mv(words=None) == -1 and "null" in _lib.last_error()
+    assert mv(n=0) == 0  # an empty matrix is a no-op
+
+
+def test_lanczos_problem_rejects_an_incomplete_packed_layout():
+    """edg_lanczos_problem: a packed layout without its tile offsets or with
+    column bits that leave no padding column is refused."""
+    from edgpu import _lib
+
+    p = _lib.LanczosProblem()
+    p.dtype, p.n_rows, p.nnz, p.nvec, p.k, p.max_iter, p.tol, p.check_every = 1, 1000, 0, 3, 1, 50, 1e-8, 5
+    p.rowptr = p.diag = 1
+    assert _lib.lib.edg_lanczos_workspace_bytes(ctypes.byref(p)) > 0
+    p.pk_words, p.pk_table, p.pk_count, p.pk_colbits = 1, 1, 4, 11
+    assert _lib.lib.edg_lanczos_workspace_bytes(ctypes.byref(p)) == -1  # no tile offsets
+    p.pk_tile_off = 1
+    assert _lib.lib.edg_lanczos_workspace_bytes(ctypes.byref(p)) > 0
+    p.pk_colbits = 9  # 2^9 rows: fewer than the 1000 rows
+    assert _lib.lib.edg_lanczos_workspace_bytes(ctypes.byref(p)) == -1
