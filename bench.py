@@ -733,8 +733,11 @@ def run_quench(args, world, rank, local):
     n_t = int(round(T / dt))
     ops = {"T2_px": model.ops["T2_px"], "N_pair": model.ops["N_pair"]}
 
-    def evolve(prec, steps):
-        ev = KrylovEvolver(model.H.mat, m=30, precision=prec, reorth_passes=0)
+    layout = {}
+
+    def evolve(prec, steps, matvec="auto"):
+        ev = KrylovEvolver(model.H.mat, m=30, precision=prec, reorth_passes=0, matvec=matvec)
+        layout[(prec, matvec)] = "packed" if ev.packed is not None else "csr"
         psi = psi0.to(ev.vdtype).clone()
         out = {k: torch.zeros((steps + 1, 16), dtype=torch.float64, device=dev) for k in ops}
         for k in ops:
@@ -755,6 +758,10 @@ def run_quench(args, world, rank, local):
     n_chk = min(n_t, args.steps * 10)
     t128, obs128 = evolve("c128", n_chk)
     dev_max = max(float(np.max(np.abs(obs64[k][: n_chk + 1] - obs128[k]))) for k in ops)
+    # the same complex64 evolution on the CSR matvec, for comparison
+    evolve("c64", 2, "csr")
+    t64c, obs64c = evolve("c64", n_chk, "csr")
+    dev_csr = max(float(np.max(np.abs(obs64[k][: n_chk + 1] - obs64c[k]))) for k in ops)
     if rank == 0:
         print(json.dumps({
             "metric": METRIC, "workload": "quench", "value": n_t / (t64 * 1e-3), "unit": "time_steps/s",
@@ -766,6 +773,9 @@ def run_quench(args, world, rank, local):
                        "c128_check_steps": n_chk},
             "c128_ms_per_step": t128 / max(n_chk, 1),
             "max_observable_deviation_c64_vs_c128": dev_max,
+            "matvec_layout": layout[("c64", "auto")],
+            "c64_csr_ms_per_step": t64c / max(n_chk, 1),
+            "max_observable_deviation_c64_layout_vs_csr": dev_csr,
         }), flush=True)
 
 

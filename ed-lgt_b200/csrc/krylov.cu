@@ -13,6 +13,8 @@
 // QMB_hamiltonian.time_evolution (edlgt/modeling/qmb_hamiltonian.py:334-426).
 #include "spmv.cuh"
 
+#include <type_traits>
+
 #include <cmath>
 
 namespace {
@@ -319,8 +321,19 @@ int run_step(const edg_krylov_problem* p, T* psi, double dt, char* ws, double* e
   scale_k<T, T><<<gv, 256, 0, s>>>(psi, n, misc, V);
   for (int j = 0; j < m; ++j) {
     const T* vj = V + (int64_t)j * n;
-    int st = edg::launch_spmv<SV, T, double2>(1, n, p->nnz, p->rowptr, p->cols, (const SV*)p->vals,
+    int st;
+    if constexpr (std::is_same<SV, double>::value || std::is_same<SV, float>::value) {
+      if (p->pk_words != nullptr)  // real packed matrix: (re, im) as two interleaved right-hand sides
+        st = edg::launch_packed_spmv<SV>(2, 2, n, p->pk_tile_off, p->pk_words, (const SV*)p->pk_table, p->pk_count,
+                                         p->pk_colbits, (const SV*)p->diag, (const SV*)vj, (double*)w, 0, nullptr,
+                                         p->status, s, 1);
+      else
+        st = edg::launch_spmv<SV, T, double2>(1, n, p->nnz, p->rowptr, p->cols, (const SV*)p->vals,
                                               (const SV*)p->diag, vj, w, s, 0, p->spmv_group);
+    } else {
+      st = edg::launch_spmv<SV, T, double2>(1, n, p->nnz, p->rowptr, p->cols, (const SV*)p->vals, (const SV*)p->diag,
+                                            vj, w, s, 0, p->spmv_group);
+    }
     if (st) return st;
     // reorth_passes = 0: local recurrence (against v_{j-1}, v_j only);
     // 1 or 2: classical Gram-Schmidt over the whole basis, once or twice
@@ -355,6 +368,11 @@ int check_k(const edg_krylov_problem* p) {
   EDG_REQUIRE(p->m >= 1 && p->m <= kMaxM, "edg_krylov: m must be 1..%d", kMaxM);
   EDG_REQUIRE(p->reorth_passes >= 0 && p->reorth_passes <= 2, "edg_krylov: reorth_passes must be 0..2");
   EDG_REQUIRE(p->n_rows > 0 && p->rowptr && p->diag, "edg_krylov: empty matrix");
+  EDG_REQUIRE(p->pk_words == nullptr ||
+                  ((p->mat_dtype == 0 || p->mat_dtype == 1) && p->pk_tile_off && p->pk_table && p->pk_count >= 1 &&
+                   p->pk_count <= EDG_PACK_MAX_VALUES && p->pk_colbits >= 1 && p->pk_colbits <= 31 &&
+                   p->n_rows < ((int64_t)1 << p->pk_colbits)),
+              "edg_krylov: a packed layout needs a real matrix (mat_dtype 0 or 1) and a complete layout");
   return EDG_OK;
 }
 

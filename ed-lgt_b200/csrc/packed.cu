@@ -255,6 +255,22 @@ struct XRow<float, NV, 4> {
     for (int v = 0; v < NV; ++v) o[v] = f[v];
   }
 };
+template <>
+struct XRow<float, 2, 2> {  // a complex64 entry as two real parts
+  __device__ static void ld(const float* x, int64_t c, float (&o)[2]) {
+    const float2 q = __ldg(reinterpret_cast<const float2*>(x) + c);
+    o[0] = q.x;
+    o[1] = q.y;
+  }
+};
+template <>
+struct XRow<double, 2, 2> {  // a complex128 entry as two real parts
+  __device__ static void ld(const double* x, int64_t c, double (&o)[2]) {
+    const double2 q = __ldg(reinterpret_cast<const double2*>(x) + c);
+    o[0] = q.x;
+    o[1] = q.y;
+  }
+};
 template <int NV>
 struct XRow<double, NV, 4> {
   __device__ static void ld(const double* x, int64_t c, double (&o)[NV]) {
@@ -295,8 +311,10 @@ __device__ __forceinline__ void gather_tile(const uint32_t* src, int width, int 
   }
 }
 
-// y[v * y_plane + r] (f64) = sum over the row's entries of table[idx] x[col][v]
-// + diag[r][v] x[r][v]; T = f32 or f64 table, diagonal and x.  With f32 (the
+// y[v * y_plane + r] (f64; y[r * NV + v] when y_plane is 0) = sum over the
+// row's entries of table[idx] x[col][v] + diag[r][v] x[r][v] (diag[r] for
+// every v when diag_shared: a complex vector as NV = 2 real parts of one
+// real matrix); T = f32 or f64 table, diagonal and x.  With f32 (the
 // f32 Krylov phase) every lane sums its products in f32 and the two lane sums
 // and the diagonal term are added in f64 (a few f32 roundings per row, no
 // conversion per entry); with f64 the products and sums are f64, in the CSR
@@ -306,8 +324,8 @@ template <typename T, int NV, int XS>
 __global__ void __launch_bounds__(kWarps * 32, 4)
     packed_spmv_k(int64_t n, const int32_t* __restrict__ tile_off, const uint32_t* __restrict__ words,
                   const T* __restrict__ table, int count, int colbits, const T* __restrict__ diag,
-                  const T* __restrict__ x, double* __restrict__ y, int64_t y_plane, const int* __restrict__ skip,
-                  int* __restrict__ err) {
+                  const T* __restrict__ x, double* __restrict__ y, int64_t y_plane, int diag_shared,
+                  const int* __restrict__ skip, int* __restrict__ err) {
   using A = T;  // lane accumulator: f32 lanes for the f32 phase, f64 otherwise
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ int s_err;
@@ -371,7 +389,10 @@ __global__ void __launch_bounds__(kWarps * 32, 4)
       T xr[NV];
       XRow<T, NV, XS>::ld(x, r, xr);
 #pragma unroll
-      for (int v = 0; v < NV; ++v) y[v * y_plane + r] = fma((double)__ldg(diag + r * NV + v), (double)xr[v], tot[v]);
+      for (int v = 0; v < NV; ++v) {
+        const double d = (double)__ldg(diag_shared ? diag + r : diag + r * NV + v);
+        y[y_plane > 0 ? v * y_plane + r : r * NV + v] = fma(d, (double)xr[v], tot[v]);
+      }
     }
     __syncwarp();  // this stage is refilled by the next iteration
     cur = nxt;
@@ -425,7 +446,7 @@ namespace edg {
 template <typename T>
 int launch_packed_spmv(int nvec, int x_stride, int64_t n, const int32_t* tile_off, const uint32_t* words,
                        const T* table, int count, int colbits, const T* diag, const T* x, double* y, int64_t y_plane,
-                       const int* skip, int* err, cudaStream_t s) {
+                       const int* skip, int* err, cudaStream_t s, int diag_shared) {
   const int64_t n_tiles = (n + kTileRows - 1) / kTileRows;
   const int64_t need = (n_tiles + kWarps - 1) / kWarps;
   const unsigned grid = (unsigned)(need < (int64_t)kSmCount * 4 ? need : (int64_t)kSmCount * 4);
@@ -436,7 +457,7 @@ int launch_packed_spmv(int nvec, int x_stride, int64_t n, const int32_t* tile_of
     e = cudaFuncSetAttribute(packed_spmv_k<T, NV, XS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);    \
     if (e == cudaSuccess)                                                                                           \
       packed_spmv_k<T, NV, XS><<<grid, kWarps * 32, smem, s>>>(n, tile_off, words, table, count, colbits, diag, x, \
-                                                               y, y_plane, skip, err);                              \
+                                                               y, y_plane, diag_shared, skip, err);                 \
   } while (0)
   switch (nvec) {
     case 1: EDG_PACKED(1, 1); break;
@@ -457,10 +478,11 @@ int launch_packed_spmv(int nvec, int x_stride, int64_t n, const int32_t* tile_of
 }
 
 template int launch_packed_spmv<float>(int, int, int64_t, const int32_t*, const uint32_t*, const float*, int, int,
-                                       const float*, const float*, double*, int64_t, const int*, int*, cudaStream_t);
+                                       const float*, const float*, double*, int64_t, const int*, int*, cudaStream_t,
+                                       int);
 template int launch_packed_spmv<double>(int, int, int64_t, const int32_t*, const uint32_t*, const double*, int, int,
                                         const double*, const double*, double*, int64_t, const int*, int*,
-                                        cudaStream_t);
+                                        cudaStream_t, int);
 
 }  // namespace edg
 

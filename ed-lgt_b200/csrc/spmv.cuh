@@ -255,12 +255,14 @@ int launch_sell_spmv(int nvec, int x_stride, int64_t n_slices, const int32_t* pe
                      const int64_t* off, const uint2* entries, const float* diag, const float* x, double* y,
                      int64_t y_plane, const int* skip, cudaStream_t s);
 
-// Dictionary-packed CSR matvec (packed.cu): y[v * y_plane + row] (f64) =
-// (A + diag) x, entries col | (value index << colbits), T = f32 or f64;
-// a stage wait that runs out writes EDG_ERR_TIMEOUT to *err (if not null).
+// Dictionary-packed tiled matvec (packed.cu): y[v * y_plane + row] (f64;
+// interleaved y[row * nvec + v] when y_plane is 0) = (A + diag) x, entries
+// col | (value index << colbits), T = f32 or f64; diag_shared: one diagonal
+// value per row for all nvec (a complex vector of a real matrix); a stage
+// wait that runs out writes EDG_ERR_TIMEOUT to *err (if not null).
 template <typename T>
 int launch_packed_spmv(int nvec, int x_stride, int64_t n, const int32_t* tile_off, const uint32_t* words,
                        const T* table, int count, int colbits, const T* diag, const T* x, double* y, int64_t y_plane,
-                       const int* skip, int* err, cudaStream_t s);
+                       const int* skip, int* err, cudaStream_t s, int diag_shared = 0);
 
 }  // namespace edg

@@ -165,6 +165,12 @@ class KrylovProblem(C.Structure):
         ("m", I32),
         ("reorth_passes", I32),
         ("spmv_group", I32),
+        ("pk_tile_off", P),
+        ("pk_words", P),
+        ("pk_table", P),
+        ("pk_count", I32),
+        ("pk_colbits", I32),
+        ("status", P),
     ]
 
 

@@ -24,9 +24,14 @@ __all__ = ["KrylovEvolver", "krylov_evolve"]
 
 
 class KrylovEvolver:
-    """Holds the device copies and the workspace of one Hamiltonian."""
+    """Holds the device copies and the workspace of one Hamiltonian.
 
-    def __init__(self, mat, m=30, precision="c128", reorth_passes=1, spmv_group=None):
+    ``matvec``: "auto" uses the dictionary-packed tiled layout of a real
+    matrix when it packs (a complex vector is two real right-hand sides of
+    it; f32 lane sums for complex64, f64 for complex128), else CSR;
+    "csr" forces CSR."""
+
+    def __init__(self, mat, m=30, precision="c128", reorth_passes=1, spmv_group=None, matvec="auto"):
         if precision not in ("c128", "c64"):
             raise ValueError("precision must be 'c128' or 'c64'")
         self.mat = mat
@@ -55,14 +60,26 @@ class KrylovEvolver:
         p.diag = ptr(diag)
         p.m = self.m
         p.reorth_passes = reorth_passes
+        self.packed = None
+        if matvec == "auto" and not mat.is_complex:
+            from .solvers import packed_layout
+
+            self.packed = packed_layout(mat)
         if spmv_group is None:
             # a complex vector is two real right-hand sides for a real matrix:
-            # tune on that shape (real forms only)
+            # tune the CSR kernel on that shape (real forms only)
             from .solvers import tune_spmv_group
 
-            spmv_group = 0 if mat.is_complex else tune_spmv_group(
+            spmv_group = 0 if (mat.is_complex or self.packed is not None) else tune_spmv_group(
                 mat, 2, 0 if precision == "c128" else 1, vals=mat.vals if precision == "c128" else vals)
         p.spmv_group = int(spmv_group)
+        if self.packed is not None:
+            pk = self.packed
+            p.pk_tile_off, p.pk_words = ptr(pk.tile_off), ptr(pk.words)
+            p.pk_table = ptr(pk.table(0 if precision == "c128" else 1))
+            p.pk_count, p.pk_colbits = pk.count, pk.colbits
+        self.status = torch.zeros(1, dtype=torch.int32, device=dev)
+        p.status = ptr(self.status)
         self.p = p
         wb = lib.edg_krylov_workspace_bytes(ctypes.byref(p))
         if wb < 0:
@@ -70,6 +87,12 @@ class KrylovEvolver:
         self.ws = torch.empty(wb, dtype=torch.uint8, device=dev)
         self.wb = wb
         self.vdtype = torch.complex128 if precision == "c128" else torch.complex64
+
+    def check_status(self):
+        """Raise if a stage wait of the packed matvec ran out (one host read)."""
+        st = int(self.status.item())
+        if st != 0:
+            raise _lib.EdgError(st, "edg_krylov_step: a stage wait of the packed matvec ran out")
 
     def step(self, psi: torch.Tensor, dt: float, want_error=False):
         err = np.zeros(1) if want_error else None
@@ -79,12 +102,12 @@ class KrylovEvolver:
 
 
 def krylov_evolve(mat, psi0, time_line, m=30, precision="c128", keep_states=True, observables=None,
-                  reorth_passes=1):
+                  reorth_passes=1, matvec="auto"):
     """psi(t_k) on a uniform grid (list of device vectors) or, when
     ``observables`` maps names to ``(sector, site_op)`` pairs, the per-site
     expectation values ``{name: (n_t, n_sites) array}``."""
     t = np.asarray(time_line, dtype=float)
-    ev = KrylovEvolver(mat, m=m, precision=precision, reorth_passes=reorth_passes)
+    ev = KrylovEvolver(mat, m=m, precision=precision, reorth_passes=reorth_passes, matvec=matvec)
     psi = psi0.to(ev.vdtype).clone().contiguous()
     states = []
     results = {}
@@ -102,6 +125,7 @@ def krylov_evolve(mat, psi0, time_line, m=30, precision="c128", keep_states=True
         if observables:
             for name, (sector, op) in observables.items():
                 site_expval_device(sector, op, psi, out=results[name][k])
+    ev.check_status()
     if observables:
         return {name: r.cpu().numpy() for name, r in results.items()}
     return states

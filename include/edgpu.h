@@ -595,6 +595,14 @@ typedef struct {
   int32_t m;              /* Krylov dimension, <= 64                        */
   int32_t reorth_passes;  /* 0 local recurrence, 1 or 2 full Gram-Schmidt   */
   int32_t spmv_group;     /* threads per matvec row, 0 = heuristic         */
+  const int32_t* pk_tile_off; /* optional dictionary-packed layout of the   */
+  const uint32_t* pk_words;   /* real off-diagonal matrix (edg_pack_*, mat_ */
+  const void* pk_table;       /* dtype 0 or 1, table in that dtype): the    */
+  int32_t pk_count;           /* matvec treats each complex vector as two   */
+  int32_t pk_colbits;         /* real right-hand sides; used when pk_words  */
+                              /* is not NULL                                */
+  int32_t* status;        /* optional device word: EDG_ERR_TIMEOUT when a   */
+                          /* stage wait of the packed matvec ran out        */
 } edg_krylov_problem;
 
 int64_t edg_krylov_workspace_bytes(const edg_krylov_problem* p);
