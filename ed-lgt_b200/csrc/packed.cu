@@ -1,28 +1,31 @@
-// Dictionary-packed CSR: the off-diagonal matrix with one 32-bit word per
-// entry.
+// Dictionary-packed tiles: the off-diagonal matrix with one 32-bit word per
+// entry slot.
 //
 // The sector Hamiltonians of the lattice gauge models have very few distinct
-// off-diagonal values (products of a handful of local matrix elements: six
-// on the SU(2) j = 1/2 chain), so each entry is stored as
-//     word = column | (value index << colbits),  colbits = bits of n_rows - 1,
-// with the distinct values in a small table.  The entry stream is then 4
-// bytes an entry instead of 8 (f32 value + int32 column) or 12 (f64), and the
-// row offsets are int32.  The product is the same as the CSR one
-// (csr_spmv, edlgt/modeling/qmb_hamiltonian.py:705-730).
+// off-diagonal values (products of a handful of local matrix elements: eight
+// on the periodic SU(2) j = 1/2 chain in its real form), so each entry is
+//     word = column | (value index << colbits),  colbits = bits of n_rows,
+// with the distinct values in a small table.  Rows are grouped in tiles of
+// 16, each tile as wide as its longest row and stored k-major (layout below);
+// the stream is 4 bytes a slot instead of 8 (f32 value + int32 column) or 12
+// (f64) an entry.  The product is the same as the CSR one (csr_spmv,
+// edlgt/modeling/qmb_hamiltonian.py:705-730).
 //
 // Build (on the device, once per matrix):
-//   edg_pack_collect  inserts the bit patterns of the values into a hash set;
-//                     the host reads the set, sorts the distinct values and
-//                     uploads them as the table;
-//   edg_pack_encode   writes the int32 row offsets and the packed words
-//                     (binary search of each value in the sorted table).
+//   edg_pack_collect      inserts the bit patterns of the values into a hash
+//                         set; the host reads the set, sorts the distinct
+//                         values and uploads them as the table;
+//   edg_pack_tile_counts  the tiles' word counts (a scan gives their offsets);
+//   edg_pack_encode       writes the tile offsets and the packed words (binary
+//                         search of each value in the sorted table).
 //
 // Matvec (packed_spmv_k): one warp takes tiles of 16 consecutive rows.  A
-// tile's entries are a contiguous range of the stream, which lane 0 copies
-// into one of the warp's two shared-memory stages with a bulk asynchronous
-// copy (completion on the stage's mbarrier) one tile ahead, while the row
-// offsets are loaded two tiles ahead; two lanes per row then walk their row
-// from shared memory (lane j takes entries j, j + 2, j + 4, ...), gathering x
+// tile is a contiguous, 64-byte-aligned range of the stream, which lane 0
+// copies into one of the warp's two shared-memory stages with a bulk
+// asynchronous copy (completion on the stage's mbarrier) one tile ahead,
+// while the tile offsets are loaded two tiles ahead; two lanes per row then
+// walk their row from shared memory (lane j takes entries j, j + 2, j + 4,
+// ...; the two lanes of all 16 rows read 32 consecutive words), gathering x
 // rows.  The stream is read with whole-range copies that bypass the load
 // pipeline (the CSR kernel's loads touch one segment per row of the warp on
 // every load), which leaves the L1 data pipe to the gathers.  f32 matrices

@@ -1,6 +1,7 @@
-"""The dictionary-packed CSR layout (packed.cu) of the off-diagonal matrix:
-one 32-bit word per entry (column | value index << colbits) and the distinct
-values in a table.  Its matvec computes the CSR product of the reference
+"""The dictionary-packed tiled layout (packed.cu) of the off-diagonal matrix:
+one 32-bit word per entry slot (column | value index << colbits), the
+distinct values in a table, tiles of 16 rows stored k-major and padded to
+their longest row.  Its matvec computes the CSR product of the reference
 (csr_spmv, edlgt/modeling/qmb_hamiltonian.py:705-730).  In f64 it forms the
 same sums in the same order as the CSR kernel with two threads a row, so the
 outputs are compared bit for bit (and to a host f64 product at 1e-12
