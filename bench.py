@@ -68,6 +68,7 @@ REORTH_TRAFFIC_RATIO = (146.00 + 15.95) / 251.42
 PACKED_MATVEC_TRAFFIC_BYTES = (112.87 + 14.91) * 1e6
 MATVEC_TRAFFIC_BYTES = (179.21 + 21.61) * 1e6
 UNIT = "ground_states/s"
+REF_MAX_PIPELINES = 6  # timed pipelines of the reference arm (about 12 s each on 16 host cores)
 WORKLOAD = (f"SU(2) 1D Yang-Mills + staggered matter, j_max=1/2, {'periodic' if PBC else 'open'} chain L={L}, "
             f"N_tot={L} sector; ground states for g^2 in {list(SWEEP)}, m={MASS}")
 
@@ -198,17 +199,22 @@ def run_reference(args):
     process group is created, so other ranks exit at once)."""
     if int(os.environ.get("RANK", "0")) != 0:
         return
-    res = stock_reference(args.steps, args.warmup)
+    # a reference pipeline takes about 12 s on 16 host cores: at most
+    # REF_MAX_PIPELINES of them are timed (the rate is their mean), so the arm
+    # ends within a few minutes whatever --steps asks
+    timed = max(1, min(args.steps, REF_MAX_PIPELINES))
+    res = stock_reference(timed, args.warmup)
     steps = res["steps"]
     ms = 1e3 * float(np.mean([st["total_s"] for st in steps]))
     value = 1e3 / ms
     phases = {k: 1e3 * float(np.mean([st[k] for st in steps])) for k in ("sector_s", "assembly_s", "solve_s")}
     sample = (f"one coupling per step (cycling g^2 over {list(SWEEP)}): SU2_Model(...) sector, build_Hamiltonian, "
-              f"diagonalize_Hamiltonian(1, '{res['format']}') = ARPACK eigsh")
+              f"diagonalize_Hamiltonian(1, '{res['format']}') = ARPACK eigsh; {timed} of the {args.steps} "
+              "requested steps timed (each a full ground-state pipeline)")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "complex128", "data": "synthetic (model Hamiltonian; no dataset)",
+        "warmup": args.warmup, "steps_timed": timed, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "complex128", "data": "synthetic (model Hamiltonian; no dataset)",
         "config": {"workload": WORKLOAD, "sector_dim": steps[0]["dim"] if steps else None, "instances_per_step": 1,
                    "sample": sample},
         "phases_ms_per_step": {"sector": phases["sector_s"], "assembly": phases["assembly_s"],
