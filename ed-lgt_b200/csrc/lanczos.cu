@@ -1,8 +1,13 @@
-// Lanczos ground states with full reorthogonalisation, for nvec independent
-// real-symmetric problems sharing the off-diagonal matrix (batched in one
-// matvec).  Krylov vectors are stored in T (double or float), interleaved
-// [row][vec]; the working vector w, every inner product, the recurrence
-// coefficients and the tridiagonal eigen-solve are double precision.
+// Lanczos ground states with full or windowed reorthogonalisation, for nvec
+// independent real-symmetric problems sharing the off-diagonal matrix
+// (batched in one matvec).  Krylov vectors are stored in T (double or float),
+// planar [vector][problem][row] with rows padded to four; the matvec input X
+// is an interleaved [row][problem] copy of the candidate; the working vector
+// w, every inner product, the recurrence coefficients and the tridiagonal
+// eigen-solve are double precision.  The reorthogonalisation of a step reads
+// V[lo..j] (lo = 0, or j - window): through the bulk-copy ring passes, or,
+// when at most kSmallMax vectors are read, in one cooperative launch
+// (reorth_small_k).
 //
 // Step j, delayed classical Gram-Schmidt with reorthogonalisation (DCGS2,
 // Swirydowicz, Langou, Ananthan, Yang, Thomas, Numer. Linear Algebra Appl.

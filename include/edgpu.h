@@ -394,6 +394,10 @@ int edg_convert(int32_t dtype_in, const void* in, int32_t dtype_out, void* out,
 /* the progress words the device writes to host_progress; no stream         */
 /* synchronisation happens inside the step loop.  With stats set, the steps */
 /* are launched one by one with CUDA events around each phase instead.      */
+/* A step that reorthogonalises against at most 8 vectors (reorth_window of  */
+/* 1..7, or max_iter <= 8) does it in one cooperative launch (dots, a grid    */
+/* barrier with a 1 s limit, update); the device must support cooperative   */
+/* launches.                                                                 */
 /* ------------------------------------------------------------------------ */
 
 typedef struct {
